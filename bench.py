@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-density Woodcock tracker on B200.
+
+One step = one frame of the configured scene: every pixel x spp primary path through
+the tracker (Renderer::Render, renderer.cpp:944-973).  Metric: Gpath-samples/s
+(pixels x spp per second), whole job.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1|c3] [--impl mdwt|reference]
+
+Default workload (c2): syncDDA (-m 2), 3 channels of 256^3 uint8 sparse value noise,
+16^3-voxel macrocells, 1024x1024, 64 spp.  Inputs (volumes, majorants) are resident in
+HBM before timing; L2 (126 MB > the 48 MB volume) is flushed by a 512 MiB write between
+timed steps, outside the timed events.  `value` is device time (CUDA events on the
+render stream); `e2e` goes through the C ABI with host buffers: camera update (host to
+device), frame, framebuffer copy to pinned host memory.  Under torchrun every rank
+renders its own frames (different frame seeds) with no collective: per-GPU work is
+fixed, `scaling` is weak, and time is the max over ranks.
+
+--impl reference times the reference's path restated on the CPU (the OpenMP oracle,
+the reference itself cannot be built: no OptiX/OWL) on the same scene, on all host
+cores, each step a band of image rows; rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c3ndda"])
+    ap.add_argument("--impl", default="mdwt", choices=["mdwt", "reference"])
+    ap.add_argument("--flush-mib", type=int, default=512)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_scene(name):
+    from mdwtracker_b200 import synthetic as syn
+    if name == "c1":
+        return syn.scene_c1()
+    if name == "c2":
+        return syn.scene_c2()
+    if name == "c3":
+        return syn.scene_c3(mode=2)
+    if name == "c3ndda":
+        return syn.scene_c3(mode=0)
+    raise ValueError(name)
+
+
+def workload_name(sc):
+    w, h = sc.resolution
+    return f"{sc.name}_mc{sc.macrocells[0]}_{w}x{h}_{sc.spp}spp"
+
+
+def scene_config(sc, l2note, parallelism):
+    v = sc.volumes[0]
+    return {
+        "workload": workload_name(sc),
+        "mode": sc.mode,
+        "channels": len(sc.volumes),
+        "volume": f"{v.shape[2]}x{v.shape[1]}x{v.shape[0]} {v.dtype}",
+        "macrocells": list(sc.macrocells),
+        "resolution": list(sc.resolution),
+        "spp": sc.spp,
+        "camera": "default (eye (0.5,0.5,3.0) -> centre, fovy 45)",
+        "l2": l2note,
+        "parallelism": parallelism,
+    }
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload):
+    """DRAM bytes per tracker launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"track_kernel_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = os.path.join("/tmp", f"mdwt_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_id), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(sc, budget_s, full=False):
+    """Oracle on the host cores over a band of rows of the same frame."""
+    from oracle import oracle as orc
+    threads = orc.set_threads(os.cpu_count() or 1)
+    o = sc.setup(orc.OracleRenderer())
+    w, h = sc.resolution
+    # calibrate on 1 row, then size the band for the budget
+    t0 = time.perf_counter()
+    o.renderRows(h // 2, h // 2 + 1)
+    dt1 = max(time.perf_counter() - t0, 1e-4)
+    rows = int(max(1, min(h, budget_s / dt1)))
+    r0 = max(0, h // 2 - rows // 2)
+    t0 = time.perf_counter()
+    o.renderRows(r0, r0 + rows)
+    el = time.perf_counter() - t0
+    ps = rows * w * sc.spp
+    return {"value": ps / el / 1e9, "unit": "Gpath-samples/s", "cores": threads, "kind": "port",
+            "sample": f"rows {r0}..{r0 + rows - 1} of the {w}x{h} frame at {sc.spp} spp "
+                      f"({ps} path-samples, {el:.1f} s)"}, o
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sc = make_scene(args.config)
+    from oracle import oracle as orc
+    threads = orc.set_threads(os.cpu_count() or 1)
+    o = sc.setup(orc.OracleRenderer())
+    w, h = sc.resolution
+    t0 = time.perf_counter()
+    o.renderRows(h // 2, h // 2 + 1)
+    dt1 = max(time.perf_counter() - t0, 1e-4)
+    rows = int(max(1, min(h, 6.0 / dt1)))
+    r0 = max(0, h // 2 - rows // 2)
+    for _ in range(args.warmup):
+        o.renderRows(r0, r0 + min(rows, 2))
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.renderRows(r0, r0 + rows)
+        times.append(time.perf_counter() - t0)
+    ps = rows * w * sc.spp
+    value = ps / statistics.mean(times) / 1e9
+    line = {
+        "impl": "reference",
+        "metric": "Gpath-samples/s", "value": value, "unit": "Gpath-samples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": scene_config(sc, "host caches", "host threads"),
+        "cpu_baseline": {"value": value, "unit": "Gpath-samples/s", "cores": threads, "kind": "port",
+                         "sample": f"each step: rows {r0}..{r0 + rows - 1} of the {w}x{h} frame at {sc.spp} spp "
+                                   f"({ps} path-samples)"},
+        "e2e": {"value": value, "unit": "Gpath-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (OptiX 7 + OWL, GL viewer) cannot be built here; its tracking path "
+                "is restated in C++/OpenMP (oracle/mdwt_oracle.cpp) and timed on the host cores",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from mdwtracker_b200 import Renderer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    sc = make_scene(args.config)
+    r = sc.setup(Renderer(local))
+    w, h = sc.resolution
+    stream = torch.cuda.Stream(dev)
+    sptr = stream.cuda_stream
+    flush = torch.empty(args.flush_mib << 20, dtype=torch.uint8, device=dev)
+    # distinct frame seeds per rank: rank r starts r*(warmup+steps) frames later
+    for _ in range(rank * (args.warmup + args.steps)):
+        r.Render(sptr)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            r.Render(sptr)
+    torch.cuda.synchronize(dev)
+    r.resetCounters()
+    launches0 = r.renderInfo()[0]
+    clocks = ClockSampler(torch.cuda.get_device_properties(dev).uuid and f"GPU-{torch.cuda.get_device_properties(dev).uuid}")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(stream)
+            r.Render(sptr)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    launches = r.renderInfo()[0] - launches0
+    cnt = r.counters()
+    ms = statistics.mean(step_ms)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    paths = w * h * sc.spp
+    value = world * paths / (ms / 1e3) / 1e9
+
+    # algorithmic bytes of the tracker (per launch): 8*bpv per density sample,
+    # 4*C_read per macrocell visit, 36 per pixel (accum read+write, RGBA8 write)
+    bpv = sc.volumes[0].dtype.itemsize if all(v.dtype == sc.volumes[0].dtype for v in sc.volumes) else 4
+    bpv = 1 if bpv == 1 else 4
+    creads = len(sc.volumes) if sc.mode == 2 else 1
+    steps = args.steps
+    alg_bytes = (8.0 * bpv * float(cnt[0]) + 4.0 * creads * float(cnt[2]) + 36.0 * w * h * steps) / steps
+    achieved = alg_bytes / (statistics.mean(step_ms) / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+
+    # ---- end to end through the C ABI with host buffers
+    pinned = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
+    cam = ((0.5, 0.5, 3.0), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0), 45.0)
+    e2e_ms = []
+    barrier()
+    for k in range(steps):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r.setCamera(*cam)
+        r.Render(sptr)
+        r._call("get_framebuffer", C.cast(C.c_void_p(pinned.data_ptr()), C.POINTER(C.c_uint32)))
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    barrier()
+    e2e = statistics.mean(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+    h2d = r.renderInfo()[1] + 48  # kernel parameter block + camera vectors
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _ = cpu_baseline(sc, args.cpu_seconds)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "error": str(ex)}
+
+    l2note = f"flushed between timed steps ({args.flush_mib} MiB write, outside the timed events)"
+    line = {
+        "metric": "Gpath-samples/s",
+        "value": value,
+        "unit": "Gpath-samples/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generators in mdwtracker_b200/synthetic.py)",
+        "config": scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": profiled_traffic(workload_name(sc)),
+                     "peak_source": peak_kind, "kernel": "track_kernel",
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": w * h * 4, "ms_per_step": e2e},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "counters": {"density_samples": int(cnt[0]), "rejections": int(cnt[1]), "cells": int(cnt[2]),
+                     "path_samples": int(cnt[3]), "samples_per_path": float(cnt[0]) / max(1, int(cnt[3]))},
+        "step_ms": step_ms,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    r.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,199 @@
+/*
+ * mdwt.h -- C ABI of the B200-native multi-density Woodcock tracker (libmdwt.so).
+ *
+ * The ABI replaces the `dtracker::Renderer` class of alpers-git/MDWTracker
+ * (renderer.h:52-222, renderer.cpp, renderer.cu) for the raw-volume render path,
+ * headless.  Each entry point names the reference member it stands in for.
+ *
+ * Conventions
+ *   - Every call returns an mdwt_status (MDWT_OK == 0).  No call throws, exits or
+ *     prints; mdwt_last_error() returns a text for the last failing call.
+ *   - A context owns one CUDA device and every device buffer of one scene.  A
+ *     context is driven by one host thread at a time (like the reference).
+ *   - Host pointers passed in are only read during the call (the library copies).
+ *   - Setters take effect immediately.  In the reference some members (spp,
+ *     accumulation, dt, materials) reach the device only in Renderer::Update()
+ *     (renderer.cpp:975-1008); here each setter is that member write plus Update().
+ */
+#ifndef MDWT_H
+#define MDWT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mdwt_ctx mdwt_ctx;
+typedef int mdwt_status;
+
+enum {
+  MDWT_OK = 0,
+  MDWT_ERR_BAD_ARG = 1,            /* argument out of range, null pointer, bad channel id */
+  MDWT_ERR_CUDA = 2,               /* a CUDA call failed (text in mdwt_last_error) */
+  MDWT_ERR_IO = 3,                 /* file missing or truncated */
+  MDWT_ERR_TOO_MANY_CHANNELS = 4,  /* more than MDWT_MAX_CHANNELS channels */
+  MDWT_ERR_UNSUPPORTED = 5,        /* mode or data format not supported */
+  MDWT_ERR_STATE = 6,              /* call order violated (e.g. render before init) */
+  MDWT_ERR_OOM = 7,                /* device or host allocation failed */
+  MDWT_ERR_TIMEOUT = 8,            /* a device-side bounded wait gave up */
+  MDWT_ERR_FORMAT = 9,             /* raw file name carries no dims / unknown type */
+  MDWT_ERR_NUMERIC = 10            /* a sample hit the per-sample step cap (NaN/inf input) */
+};
+
+#define MDWT_MAX_CHANNELS 12       /* deviceCode.h:13 */
+
+/* Voxel formats, numbered like raw::DataFormat (rawFile.h:21-35). */
+enum {
+  MDWT_FMT_UNSPECIFIED = 0,
+  MDWT_FMT_INT8 = 1,
+  MDWT_FMT_INT16 = 2,
+  MDWT_FMT_INT32 = 3,
+  MDWT_FMT_UINT8 = 4,
+  MDWT_FMT_UINT16 = 5,
+  MDWT_FMT_UINT32 = 6,
+  MDWT_FMT_FLOAT32 = 7,
+  MDWT_FMT_DOUBLE64 = 8
+};
+
+/* Tracking methods, numbered like dtracker::Mode (renderer.h:24-36). */
+enum {
+  MDWT_MODE_NDDA = 0,        /* BASELINE: one DDA per channel   (deviceCode.cu:858-970) */
+  MDWT_MODE_MULTI = 1,       /* MULTI: min-of-channels free flight (deviceCode.cu:619-745) */
+  MDWT_MODE_SYNCDDA = 2,     /* MULTI_ALT: one DDA, per-channel samplers (deviceCode.cu:747-856) */
+  MDWT_MODE_CUMULATIVE = 3   /* CUMMULATIVE: summed majorant (deviceCode.cu:513-617) */
+};
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Renderer() + the context part of Init (renderer.cpp:334): one context on `device`.
+ * device == MDWT_HOST_ONLY makes a context that touches no GPU: it parses and holds
+ * channels and answers the host-side queries (channel info, dt, macrocell dims,
+ * camera basis) but refuses mdwt_init.  Fails with MDWT_ERR_CUDA when no device. */
+#define MDWT_HOST_ONLY (-1)
+mdwt_status mdwt_create(mdwt_ctx **out, int device);
+/* Renderer::Terminate (renderer.cpp:1010-1014). Frees every device buffer. */
+mdwt_status mdwt_destroy(mdwt_ctx *ctx);
+/* Text of the last failing call on ctx ("" if none).  Valid until the next call. */
+const char *mdwt_last_error(const mdwt_ctx *ctx);
+const char *mdwt_status_string(mdwt_status s);
+/* ABI version, (major << 16) | minor. */
+int mdwt_version(void);
+
+/* ---- data (raw::RawR + Renderer::PushMesh) ----------------------------- */
+
+/* raw::RawR::RawR (rawFile.cpp:31-128) + PushMesh (renderer.cpp:1031-1044):
+ * parse `<name>_<X>x<Y>x<Z>_<type>.raw`, read, convert to float exactly as the
+ * reference (uint8 -> v*255, int8 -> v*255-128, ...), bounds [0,1]^3, value range
+ * seeded with [0,1] and extended by the data.  Fails with MDWT_ERR_TOO_MANY_CHANNELS
+ * at the 13th channel (the reference's `<=` test admits a 13th, renderer.cpp:1033). */
+mdwt_status mdwt_push_channel_raw(mdwt_ctx *ctx, const char *path);
+/* The same from memory: `data` holds dims[0]*dims[1]*dims[2] voxels of `format`, x fastest. */
+mdwt_status mdwt_push_channel(mdwt_ctx *ctx, const void *data, int format, const int64_t dims[3]);
+/* raw::RawR::reshapeBounds (rawFile.cpp:217-237, viewer `-cb`): scale the xyz bounds
+ * of channel ch by scale[3], or by the grid dims when scale is NULL.  Before mdwt_init. */
+mdwt_status mdwt_reshape_bounds(mdwt_ctx *ctx, int ch, const float *scale3);
+/* Channel count, dims and box4f bounds (lo.xyzw, hi.xyzw) of channel ch (RawR::getBounds4f). */
+mdwt_status mdwt_num_channels(const mdwt_ctx *ctx, int *n);
+mdwt_status mdwt_get_channel_info(const mdwt_ctx *ctx, int ch, int64_t dims[3], float bounds8[8]);
+
+/* ---- scene set-up (Renderer::Init) -------------------------------------- */
+
+/* Renderer::macrocellDims (renderer.h:164) / viewer `-mc` (viewer.cpp:204-224):
+ * macrocell COUNT per side.  A zero component takes the default
+ * CalculateMCGridDims(4) (renderer.cpp:641-647, 1342-1355).  Before mdwt_init. */
+mdwt_status mdwt_set_macrocells(mdwt_ctx *ctx, const uint32_t dims[3]);
+/* Renderer::Init(mode, autoSetCamera) (renderer.cpp:324-942), raw branch: uploads the
+ * channels, builds the per-(cell,channel) value ranges (renderer.cu:1116-1179), sets
+ * the default camera when auto_camera != 0, dt from Resetdt, fb 1024x1024 unless resized.
+ * Modes 0..3 are supported; others return MDWT_ERR_UNSUPPORTED. */
+mdwt_status mdwt_init(mdwt_ctx *ctx, int mode, int auto_camera);
+mdwt_status mdwt_get_macrocell_dims(const mdwt_ctx *ctx, uint32_t dims[3]);
+
+/* ---- transfer functions -------------------------------------------------- */
+
+/* Renderer::SetXFColormap (renderer.cpp:1094-1165): n RGBA texels (float, 4*n values);
+ * alpha is raised to the third power, accumulation reset, majorants rebuilt. */
+mdwt_status mdwt_set_tf(mdwt_ctx *ctx, int ch, const float *rgba, int n);
+/* Renderer::SetXFOpacityScale (renderer.cpp:1167-1179). */
+mdwt_status mdwt_set_opacity_scale(mdwt_ctx *ctx, int ch, float scale);
+/* Renderer::SetXFRange (renderer.cpp:1182-1193): the xfDomain of channel ch. */
+mdwt_status mdwt_set_tf_range(mdwt_ctx *ctx, int ch, float lo, float hi);
+/* Renderer::RecalculateDensityRanges (renderer.cu:206-274). Called by the three above. */
+mdwt_status mdwt_recalculate_majorants(mdwt_ctx *ctx);
+
+/* ---- render parameters ---------------------------------------------------- */
+
+/* Renderer::Setdt (renderer.cpp:1460-1466): dt = max(dt, 1e-4). */
+mdwt_status mdwt_set_dt(mdwt_ctx *ctx, float dt);
+/* Renderer::Resetdt, raw branch (renderer.cpp:1444-1454). */
+mdwt_status mdwt_reset_dt(mdwt_ctx *ctx);
+mdwt_status mdwt_get_dt(const mdwt_ctx *ctx, float *dt);
+/* camera::Camera::setOrientation (camera.h:83-110) + Renderer::UpdateCamera
+ * (renderer.cpp:1058-1092); viewer `-c` (viewer.cpp:195-203). */
+mdwt_status mdwt_set_camera(mdwt_ctx *ctx, const float from[3], const float at[3],
+                            const float up[3], float fovy_deg);
+/* The pinhole basis the kernels use: origin, lower-left corner, horizontal, vertical. */
+mdwt_status mdwt_get_camera_basis(const mdwt_ctx *ctx, float out12[12]);
+/* Renderer::Resize (renderer.cpp:1046-1056). */
+mdwt_status mdwt_resize(mdwt_ctx *ctx, int width, int height);
+/* Renderer::spp / enableAccumulation / bgColor (renderer.h:111,124,129). */
+mdwt_status mdwt_set_spp(mdwt_ctx *ctx, int spp);
+mdwt_status mdwt_set_accumulation(mdwt_ctx *ctx, int enable);
+mdwt_status mdwt_set_background(mdwt_ctx *ctx, const float rgb[3]);
+/* viewer `-l` (viewer.cpp:274-284): shadows, gradient shading, light dir, intensity, ambient. */
+mdwt_status mdwt_set_light(mdwt_ctx *ctx, int shadows, int gradient, const float dir[3],
+                           float intensity, float ambient);
+/* Renderer::SetMaterial* (renderer.cpp:1195-1315). */
+mdwt_status mdwt_set_material(mdwt_ctx *ctx, int ch, float diffuse, float specular,
+                              float shininess, float gradient_step, const float spec_rgb[3]);
+/* Renderer::mirrorFramebuffer (renderer.h:177, renderer.cpp:962-972). */
+mdwt_status mdwt_set_mirror(mdwt_ctx *ctx, int enable);
+
+/* ---- frames ------------------------------------------------------------------ */
+
+/* Renderer::Render (renderer.cpp:944-973): one frame, asynchronous on `cuda_stream`
+ * (a cudaStream_t, NULL = the context's own stream).  The frame uses the current
+ * frame/accumulation ids; afterwards they advance exactly like the reference
+ * (owlParamsSet1i(.., accumID++) after the launch). */
+mdwt_status mdwt_render(mdwt_ctx *ctx, void *cuda_stream);
+/* Wait for every frame issued on the context's streams; reports device-side errors. */
+mdwt_status mdwt_sync(mdwt_ctx *ctx);
+/* Renderer::ResetAccumulation (renderer.cpp:1488-1495). */
+mdwt_status mdwt_reset_accumulation(mdwt_ctx *ctx);
+/* frameID, accumID (host counters) and the values the next frame uses. */
+mdwt_status mdwt_get_frame_ids(const mdwt_ctx *ctx, int out4[4]);
+/* RGBA8 framebuffer (LaunchParams::fbPtr), W*H words, row-major from the bottom row. */
+mdwt_status mdwt_get_framebuffer(mdwt_ctx *ctx, uint32_t *host_out);
+/* Accumulation buffer (LaunchParams::accumBuffer), 4*W*H floats. */
+mdwt_status mdwt_get_accum(mdwt_ctx *ctx, float *host_out);
+/* Device pointers of the accumulation (float4) and RGBA8 buffers, for zero-copy readers. */
+mdwt_status mdwt_get_device_buffers(mdwt_ctx *ctx, void **accum, void **fb);
+/* Sum over all frames since the last reset of the per-ray counters of the reference
+ * (prd.samples, prd.rejections, deviceCode.cu:829,847) plus macrocell visits and
+ * path-samples: out[0]=density samples, [1]=rejections, [2]=cells visited, [3]=path-samples. */
+mdwt_status mdwt_get_counters(mdwt_ctx *ctx, uint64_t out4[4]);
+mdwt_status mdwt_reset_counters(mdwt_ctx *ctx);
+/* Per-pixel statistics of the last frame: 4 uint32 per pixel = samples, rejections,
+ * hits (over spp), xor-fold of the hit channel ids.  Off by default (costs a buffer). */
+mdwt_status mdwt_enable_pixel_stats(mdwt_ctx *ctx, int enable);
+mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
+
+/* Launch bookkeeping: out[0] = kernels launched by this context so far, out[1] = bytes
+ * of per-frame parameters a render sends host->device, out[2] = grid and out[3] = block
+ * size of the last tracker launch. */
+mdwt_status mdwt_get_render_info(const mdwt_ctx *ctx, int64_t out4[4]);
+
+/* ---- majorant grid ------------------------------------------------------------ */
+
+/* gridMaximaBuffer (renderer.cpp:706-711): M*C floats (cell-major, channel-minor) for
+ * modes 0..2, M floats for mode 3 (the summed majorant, renderer.cu:111-157). */
+mdwt_status mdwt_get_majorants(mdwt_ctx *ctx, float *host_out);
+/* macrocellsBuffer (renderer.cu:1116-1179): per (cell, channel) value range, 2*M*C floats. */
+mdwt_status mdwt_get_ranges(mdwt_ctx *ctx, float *host_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDWT_H */

@@ -1,0 +1,988 @@
+// mdwt_host.cpp -- host side of libmdwt.so: the C ABI of include/mdwt.h.
+//
+// Stands in for dtracker::Renderer (renderer.h:52-222, renderer.cpp:313-1497) and
+// raw::RawR (rawFile.cpp:31-128) on the raw-volume path.  Owns the device buffers of
+// one scene and launches the sm_100a kernels of mdwt_kernels.cu.  There is no CPU
+// rendering path: every frame and every majorant rebuild runs on the GPU, and a
+// context on a machine without a usable CUDA device fails at mdwt_create.
+//
+// Host arithmetic (camera basis, dt, macrocell projection intervals) is compiled
+// with -ffp-contract=off and fuses only through explicit std::fma, so it matches
+// the oracle's restatement of the same reference code bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mdwt.h"
+#include "mdwt_internal.h"
+
+using namespace mdwt;
+
+namespace {
+
+struct V3 { float x, y, z; };
+inline V3 v3(float x, float y, float z) { return {x, y, z}; }
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 muls(float s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline V3 neg(V3 a) { return {-a.x, -a.y, -a.z}; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline V3 normalize(V3 v) { float s = 1.0f / std::sqrt(dot(v, v)); return muls(s, v); }
+inline F3 f3(V3 v) { return {v.x, v.y, v.z}; }
+
+inline int f2i(float x) {
+  if (!(x == x)) return 0;
+  if (x >= 2147483648.0f) return 2147483647;
+  if (x <= -2147483648.0f) return (-2147483647 - 1);
+  return (int)x;
+}
+
+int fmt_bytes(int f) {
+  switch (f) {
+    case MDWT_FMT_INT8: case MDWT_FMT_UINT8: return 1;
+    case MDWT_FMT_INT16: case MDWT_FMT_UINT16: return 2;
+    case MDWT_FMT_INT32: case MDWT_FMT_UINT32: case MDWT_FMT_FLOAT32: return 4;
+    case MDWT_FMT_DOUBLE64: return 8;
+  }
+  return 0;
+}
+
+struct Channel {
+  int64_t dims[3];
+  int store = kStoreF32;
+  std::vector<uint8_t> u8;    // kStoreU8: the raw bytes (value = b * 255)
+  std::vector<float> f32;     // kStoreF32: the converted floats
+  float lo[4], hi[4];
+  void *dVol = nullptr;
+};
+
+struct TFState {
+  std::vector<float> rgba;    // alpha cubed
+  int n = 0;
+  float vd[2] = {0.f, 1.f};
+  float xd[2] = {0.f, 1.f};
+  float os = 1.0f;
+  float *dAlpha = nullptr;
+  float *dRgba = nullptr;
+  int cap = 0;
+};
+
+struct Material {
+  float diffuse = 0.8f, specular = 0.3f, shininess = 8.0f, gradStep = 0.01f;
+  V3 spec = {1.f, 1.f, 1.f};
+};
+
+struct Camera {  // camera::Camera (camera.h:46-142), the fields UpdateCamera reads
+  V3 vx = {1, 0, 0}, vy = {0, 1, 0}, vz = {0, 0, 1};
+  V3 position = {0, -1, 0};
+  V3 upVector = {0, 1, 0};
+  float fovy = 60.f;
+  void forceUpFrame() {
+    if (std::fabs(dot(vz, upVector)) < 1e-6f) return;
+    vx = normalize(cross(upVector, vz));
+    vy = normalize(cross(vz, vx));
+  }
+  void setOrientation(V3 origin, V3 interest, V3 up, float fovyDeg) {
+    fovy = fovyDeg;
+    position = origin;
+    upVector = up;
+    const bool same = interest.x == origin.x && interest.y == origin.y && interest.z == origin.z;
+    vz = same ? v3(0, 0, 1) : neg(normalize(sub(interest, origin)));
+    vx = cross(up, vz);
+    if (dot(vx, vx) < 1e-8f) vx = v3(0, 1, 0);
+    else vx = normalize(vx);
+    vy = normalize(cross(vz, vx));
+    forceUpFrame();
+  }
+};
+
+}  // namespace
+
+struct mdwt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int numSMs = 0;
+  std::vector<Channel> ch;
+  uint32_t mcReq[3] = {0, 0, 0};
+  uint32_t mc[3] = {0, 0, 0};
+  int mode = 0;
+  bool inited = false;
+  int store = kStoreF32;
+  float dt = 0.05f;
+  int W = 1024, H = 1024;
+  int spp = 1;
+  bool accum = true;
+  V3 bg = {0, 0, 0};
+  bool shadows = false, gradient = false;
+  V3 lightDir = {0.0001f, -1.f, 0.0001f};
+  float lightIntensity = 1.0f, ambient = 0.1f;
+  std::vector<Material> mats;
+  std::vector<TFState> tf;
+  bool mirror = false;
+  Camera cam;
+  V3 cOrg{}, cLlc{}, cHor{}, cVer{};
+  int frameID = 0, accumID = 0, frameParam = 0, accumParam = 0;
+  float *dAccum = nullptr;
+  uint32_t *dFb = nullptr;
+  uint32_t *dStats = nullptr;
+  bool statsOn = false;
+  unsigned long long *dCounters = nullptr;
+  unsigned int *dWork = nullptr;
+  float *dRanges = nullptr;
+  float *dMaj = nullptr;
+  size_t M = 0;
+  float rootLo[3] = {0, 0, 0}, rootHi[3] = {1, 1, 1};
+  float gLo[4] = {0, 0, 0, 0}, gHi[4] = {1, 1, 1, 1};
+  std::string err;
+  int launches = 0;
+  int lastGrid = 0, lastBlock = 0;
+};
+
+namespace {
+
+mdwt_status fail(mdwt_ctx *c, mdwt_status s, const std::string &msg) {
+  if (c) c->err = msg;
+  return s;
+}
+mdwt_status cuda_fail(mdwt_ctx *c, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (e == cudaErrorMemoryAllocation) return fail(c, MDWT_ERR_OOM, m);
+  return fail(c, MDWT_ERR_CUDA, m);
+}
+#define CK(call, what)                                 \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+  } while (0)
+#define CKI(rc, what)                                  \
+  do {                                                 \
+    int r_ = (rc);                                     \
+    if (r_ != 0) return cuda_fail(c, (cudaError_t)r_, what); \
+  } while (0)
+
+void reset_accum_ids(mdwt_ctx *c) { c->accumID = 0; c->accumParam = 0; }
+
+// Renderer::UpdateCamera (renderer.cpp:1058-1092)
+void update_camera(mdwt_ctx *c) {
+  const V3 lookFrom = c->cam.position;
+  const V3 lookAt = sub(c->cam.position, c->cam.vz);
+  const V3 lookUp = c->cam.vy;
+  const float cosFovy = std::cos(c->cam.fovy * (float)(M_PI / 180.f));
+  const float vfov = std::acos(cosFovy) / (float)(M_PI / 180.f);
+  const float aspect = c->W / float(c->H);
+  const float theta = vfov * ((float)M_PI) / 180.0f;
+  const float half_height = std::tan(theta / 2.0f);
+  const float half_width = aspect * half_height;
+  const float focusDist = 10.f;
+  const V3 w = normalize(sub(lookFrom, lookAt));
+  const V3 u = normalize(cross(lookUp, w));
+  const V3 v = cross(w, u);
+  c->cOrg = lookFrom;
+  V3 llc = sub(lookFrom, muls(half_width * focusDist, u));
+  llc = sub(llc, muls(half_height * focusDist, v));
+  llc = sub(llc, muls(focusDist, w));
+  c->cLlc = llc;
+  c->cHor = muls(2.0f * half_width * focusDist, u);
+  c->cVer = muls(2.0f * half_height * focusDist, v);
+  reset_accum_ids(c);
+}
+
+// Renderer::Resetdt, raw branch (renderer.cpp:1444-1454): the loop overwrites its
+// running value, so the last channel decides.
+void reset_dt(mdwt_ctx *c) {
+  float minVoxelSideLength = std::numeric_limits<float>::max();
+  for (size_t i = 0; i < c->ch.size(); ++i) {
+    const Channel &h = c->ch[i];
+    const float sx = (h.hi[0] - h.lo[0]) / (float)h.dims[0];
+    const float sy = (h.hi[1] - h.lo[1]) / (float)h.dims[1];
+    const float sz = (h.hi[2] - h.lo[2]) / (float)h.dims[2];
+    minVoxelSideLength = std::min(sx, std::min(sy, sz));
+  }
+  c->dt = std::max(minVoxelSideLength * 0.5f, 1e-4f);
+  reset_accum_ids(c);
+}
+
+// project (renderer.cu:387-392)
+inline int project(float f, float lo, float hi, int dim) {
+  int v = f2i((float)dim * (f - lo) / (hi - lo));
+  v = v < dim - 1 ? v : dim - 1;
+  return v > 0 ? v : 0;
+}
+
+// Voxel intervals of one axis for the separable range build.  A voxel p enters
+// macrocell k on this axis when its 27-neighbour box (rasterElements,
+// renderer.cu:856-884) projects onto [clo(p), chi(p)] containing k; the cell's value
+// range is then the min/max over the neighbourhoods of those voxels, i.e. over the
+// voxel interval [pmin-1, pmax+1] clipped to the grid.
+bool axis_intervals(int64_t D, int md, float wlo, float whi, std::vector<int> &out) {
+  const float len = (whi - wlo) / (float)D;
+  std::vector<int> clo((size_t)D), chi((size_t)D);
+  std::vector<char> valid((size_t)D);
+  auto corner = [&](int64_t p) { return std::fma((float)p, len, wlo); };
+  for (int64_t p = 0; p < D; p++) {
+    const float vlo = corner(p);
+    float blo = vlo, bhi = vlo + len;
+    for (int64_t n = p - 1; n <= p + 1; n += 2) {
+      if (n < 0 || n >= D) continue;
+      const float nl = corner(n);
+      blo = std::fmin(blo, nl);
+      bhi = std::fmax(bhi, nl);
+    }
+    valid[(size_t)p] = blo < bhi;
+    clo[(size_t)p] = project(blo, wlo, whi, md);
+    chi[(size_t)p] = std::min(project(bhi, wlo, whi, md), md - 1);
+  }
+  out.assign(2 * (size_t)md, 0);
+  for (int k = 0; k < md; k++) {
+    int64_t pmin = -1, pmax = -1, cnt = 0;
+    for (int64_t p = 0; p < D; p++) {
+      if (!valid[(size_t)p] || clo[(size_t)p] > k || chi[(size_t)p] < k) continue;
+      if (pmin < 0) pmin = p;
+      pmax = p;
+      cnt++;
+    }
+    if (cnt == 0) { out[2 * k] = 1; out[2 * k + 1] = 0; continue; }
+    if (cnt != pmax - pmin + 1) return false;  // non-monotone projection: degenerate bounds
+    out[2 * k] = (int)std::max<int64_t>(pmin - 1, 0);
+    out[2 * k + 1] = (int)std::min<int64_t>(pmax + 1, D - 1);
+  }
+  return true;
+}
+
+bool parse_raw_name(const std::string &path, int64_t dims[3], int &fmt) {
+  // rawFile.cpp:36-84
+  dims[0] = dims[1] = dims[2] = 0;
+  fmt = MDWT_FMT_UINT8;
+  std::istringstream st(path);
+  std::string tok;
+  while (std::getline(st, tok, '_')) {
+    const size_t dp = tok.find('.');
+    if (dp != std::string::npos) tok = tok.substr(0, dp);
+    int x = 0, y = 0, z = 0;
+    if (std::sscanf(tok.c_str(), "%dx%dx%d", &x, &y, &z) == 3) {
+      dims[0] = x; dims[1] = y; dims[2] = z;
+      continue;
+    }
+    if (tok == "int8") fmt = MDWT_FMT_INT8;
+    else if (tok == "int16") fmt = MDWT_FMT_INT16;
+    else if (tok == "int32") fmt = MDWT_FMT_INT32;
+    else if (tok == "uint8") fmt = MDWT_FMT_UINT8;
+    else if (tok == "uint16") fmt = MDWT_FMT_UINT16;
+    else if (tok == "uint32") fmt = MDWT_FMT_UINT32;
+    else if (tok == "float32") fmt = MDWT_FMT_FLOAT32;
+    else if (tok == "double64") fmt = MDWT_FMT_DOUBLE64;
+    else fmt = MDWT_FMT_UNSPECIFIED;
+  }
+  return dims[0] > 0 && dims[1] > 0 && dims[2] > 0;
+}
+
+// RawR conversion (rawFile.cpp:94-121) and value range.
+void convert_channel(Channel &h, const void *buf, int fmt, size_t n) {
+  h.lo[0] = h.lo[1] = h.lo[2] = h.lo[3] = 0.f;
+  h.hi[0] = h.hi[1] = h.hi[2] = h.hi[3] = 1.f;
+  if (fmt == MDWT_FMT_UINT8) {
+    h.store = kStoreU8;
+    h.u8.assign((const uint8_t *)buf, (const uint8_t *)buf + n);
+    uint8_t bmin = 255, bmax = 0;
+    for (size_t i = 0; i < n; i++) { bmin = std::min(bmin, h.u8[i]); bmax = std::max(bmax, h.u8[i]); }
+    if (n) {
+      const float vmin = (float)bmin * 255, vmax = (float)bmax * 255;
+      if (vmax > h.hi[3]) h.hi[3] = vmax;
+      if (vmin < h.lo[3]) h.lo[3] = vmin;
+    }
+    return;
+  }
+  h.store = kStoreF32;
+  h.f32.resize(n);
+  for (size_t i = 0; i < n; i++) {
+    float v = 0.f;
+    switch (fmt) {
+      case MDWT_FMT_INT8: v = (float)((const int8_t *)buf)[i] * 255 - 128; break;
+      case MDWT_FMT_INT16: v = (float)((const int16_t *)buf)[i] * 65535 - 32768; break;
+      case MDWT_FMT_INT32: v = (float)((const int32_t *)buf)[i] * 4294967295.0f - 2147483648.0f; break;
+      case MDWT_FMT_UINT16: v = (float)((const uint16_t *)buf)[i] * 65535; break;
+      case MDWT_FMT_UINT32: v = (float)((const uint32_t *)buf)[i] * 4294967295.0f; break;
+      case MDWT_FMT_FLOAT32: v = ((const float *)buf)[i]; break;
+      case MDWT_FMT_DOUBLE64: v = (float)((const double *)buf)[i]; break;
+      default: v = 0.f;
+    }
+    h.f32[i] = v;
+    if (v > h.hi[3]) h.hi[3] = v;
+    if (v < h.lo[3]) h.lo[3] = v;
+  }
+}
+
+mdwt_status push_common(mdwt_ctx *c, const void *buf, int fmt, const int64_t dims[3]) {
+  if ((int)c->ch.size() >= MDWT_MAX_CHANNELS)
+    return fail(c, MDWT_ERR_TOO_MANY_CHANNELS, "at most 12 channels (deviceCode.h:13)");
+  if (c->inited) return fail(c, MDWT_ERR_STATE, "channels must be pushed before mdwt_init");
+  const size_t n = (size_t)(dims[0] * dims[1] * dims[2]);
+  Channel h;
+  for (int a = 0; a < 3; a++) h.dims[a] = dims[a];
+  try {
+    convert_channel(h, buf, fmt, n);
+  } catch (const std::bad_alloc &) {
+    return fail(c, MDWT_ERR_OOM, "host allocation failed");
+  }
+  c->ch.push_back(std::move(h));
+  return MDWT_OK;
+}
+
+mdwt_status check_ch(mdwt_ctx *c, int ch) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (ch < 0 || ch >= (int)c->ch.size()) return fail(c, MDWT_ERR_BAD_ARG, "channel id out of range");
+  return MDWT_OK;
+}
+
+void free_device(mdwt_ctx *c) {
+  for (auto &h : c->ch) { if (h.dVol) cudaFree(h.dVol); h.dVol = nullptr; }
+  for (auto &t : c->tf) {
+    if (t.dAlpha) cudaFree(t.dAlpha);
+    if (t.dRgba) cudaFree(t.dRgba);
+    t.dAlpha = t.dRgba = nullptr;
+  }
+  if (c->dAccum) cudaFree(c->dAccum);
+  if (c->dFb) cudaFree(c->dFb);
+  if (c->dStats) cudaFree(c->dStats);
+  if (c->dCounters) cudaFree(c->dCounters);
+  if (c->dWork) cudaFree(c->dWork);
+  if (c->dRanges) cudaFree(c->dRanges);
+  if (c->dMaj) cudaFree(c->dMaj);
+  c->dAccum = nullptr; c->dFb = nullptr; c->dStats = nullptr; c->dCounters = nullptr;
+  c->dWork = nullptr; c->dRanges = nullptr; c->dMaj = nullptr;
+}
+
+mdwt_status alloc_frame(mdwt_ctx *c) {
+  if (c->dAccum) cudaFree(c->dAccum);
+  if (c->dFb) cudaFree(c->dFb);
+  if (c->dStats) cudaFree(c->dStats);
+  c->dAccum = nullptr; c->dFb = nullptr; c->dStats = nullptr;
+  const size_t np = (size_t)c->W * c->H;
+  CK(cudaMalloc(&c->dAccum, np * 16), "cudaMalloc accum");
+  CK(cudaMalloc(&c->dFb, np * 4), "cudaMalloc framebuffer");
+  CK(cudaMemsetAsync(c->dAccum, 0, np * 16, c->stream), "memset accum");
+  CK(cudaMemsetAsync(c->dFb, 0, np * 4, c->stream), "memset framebuffer");
+  if (c->statsOn) {
+    CK(cudaMalloc(&c->dStats, np * 16), "cudaMalloc stats");
+    CK(cudaMemsetAsync(c->dStats, 0, np * 16, c->stream), "memset stats");
+  }
+  return MDWT_OK;
+}
+
+// RecalculateDensityRanges (renderer.cu:206-274)
+mdwt_status recalc(mdwt_ctx *c) {
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  MajorantParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.ranges = c->dRanges;
+  p.majorants = c->dMaj;
+  p.C = (int)c->ch.size();
+  p.mode = c->mode;
+  p.M = c->M;
+  for (int i = 0; i < p.C; i++) {
+    const TFState &t = c->tf[i];
+    p.tfAlpha[i] = t.dAlpha;
+    p.tfN[i] = t.n;
+    p.vd[i][0] = t.vd[0]; p.vd[i][1] = t.vd[1];
+    p.xd[i][0] = t.xd[0]; p.xd[i][1] = t.xd[1];
+    p.os[i] = t.os;
+  }
+  CKI(launch_majorants(p, c->stream, &c->launches), "majorant kernel");
+  return MDWT_OK;
+}
+
+// Macrocell counts per side: the requested ones, zero components from
+// CalculateMCGridDims(4) (renderer.cpp:641-647, 1342-1355).
+void resolve_mc(const mdwt_ctx *c, uint32_t out[3]) {
+  uint32_t acc[3] = {0, 0, 0};
+  for (auto &h : c->ch)
+    for (int a = 0; a < 3; a++) acc[a] += (uint32_t)((float)(uint32_t)h.dims[a] / 4.0f);
+  if (!c->ch.empty())
+    for (int a = 0; a < 3; a++) acc[a] = (uint32_t)((float)acc[a] / (float)c->ch.size());
+  for (int a = 0; a < 3; a++) out[a] = c->mcReq[a] ? c->mcReq[a] : acc[a];
+}
+
+mdwt_status build_ranges(mdwt_ctx *c) {
+  const int C = (int)c->ch.size();
+  const size_t M = c->M;
+  CKI(launch_ranges_init(c->dRanges, M * C, c->stream, &c->launches), "range init kernel");
+  size_t scratch = 0;
+  for (auto &h : c->ch) scratch = std::max(scratch, (size_t)h.dims[2] * c->mc[1] * c->mc[0]);
+  float *dA = nullptr;
+  int *dIv = nullptr;
+  CK(cudaMalloc(&dA, scratch * 8), "cudaMalloc range scratch");
+  const size_t ivn = 2 * ((size_t)c->mc[0] + c->mc[1] + c->mc[2]);
+  cudaError_t e = cudaMalloc(&dIv, ivn * sizeof(int) * C);
+  if (e != cudaSuccess) { cudaFree(dA); return cuda_fail(c, e, "cudaMalloc intervals"); }
+  std::vector<int> all;
+  all.reserve(ivn * C);
+  for (int i = 0; i < C; i++) {
+    const Channel &h = c->ch[i];
+    for (int a = 0; a < 3; a++) {
+      std::vector<int> iv;
+      if (!axis_intervals(h.dims[a], (int)c->mc[a], c->rootLo[a], c->rootHi[a], iv)) {
+        cudaFree(dA); cudaFree(dIv);
+        return fail(c, MDWT_ERR_UNSUPPORTED, "degenerate channel bounds: macrocell projection is not monotone");
+      }
+      all.insert(all.end(), iv.begin(), iv.end());
+    }
+  }
+  e = cudaMemcpyAsync(dIv, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) { cudaFree(dA); cudaFree(dIv); return cuda_fail(c, e, "copy intervals"); }
+  size_t off = 0;
+  for (int i = 0; i < C; i++) {
+    const Channel &h = c->ch[i];
+    const int dims[3] = {(int)h.dims[0], (int)h.dims[1], (int)h.dims[2]};
+    const int *ivx = dIv + off;
+    const int *ivy = ivx + 2 * c->mc[0];
+    const int *ivz = ivy + 2 * c->mc[1];
+    off += ivn;
+    int rc = launch_ranges(h.dVol, c->store, dims, c->mc, ivx, ivy, ivz, C, i, c->dRanges, dA, nullptr, c->stream, &c->launches);
+    if (rc != 0) { cudaFree(dA); cudaFree(dIv); return cuda_fail(c, (cudaError_t)rc, "range kernels"); }
+  }
+  e = cudaStreamSynchronize(c->stream);
+  cudaFree(dA);
+  cudaFree(dIv);
+  if (e != cudaSuccess) return cuda_fail(c, e, "range build");
+  return MDWT_OK;
+}
+
+}  // namespace
+
+// ========================================================================= C ABI
+extern "C" {
+
+int mdwt_version(void) { return (1 << 16) | 0; }
+
+const char *mdwt_status_string(mdwt_status s) {
+  switch (s) {
+    case MDWT_OK: return "ok";
+    case MDWT_ERR_BAD_ARG: return "bad argument";
+    case MDWT_ERR_CUDA: return "CUDA error";
+    case MDWT_ERR_IO: return "I/O error";
+    case MDWT_ERR_TOO_MANY_CHANNELS: return "too many channels";
+    case MDWT_ERR_UNSUPPORTED: return "unsupported";
+    case MDWT_ERR_STATE: return "wrong call order";
+    case MDWT_ERR_OOM: return "out of memory";
+    case MDWT_ERR_TIMEOUT: return "device wait timed out";
+    case MDWT_ERR_FORMAT: return "bad raw file name";
+    case MDWT_ERR_NUMERIC: return "sample step cap reached";
+  }
+  return "unknown status";
+}
+
+const char *mdwt_last_error(const mdwt_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+mdwt_status mdwt_create(mdwt_ctx **out, int device) {
+  if (!out) return MDWT_ERR_BAD_ARG;
+  *out = nullptr;
+  if (device == MDWT_HOST_ONLY) {
+    mdwt_ctx *h = new (std::nothrow) mdwt_ctx();
+    if (!h) return MDWT_ERR_OOM;
+    h->device = MDWT_HOST_ONLY;
+    *out = h;
+    return MDWT_OK;
+  }
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n <= 0) { cudaGetLastError(); return MDWT_ERR_CUDA; }
+  if (device < 0 || device >= n) return MDWT_ERR_BAD_ARG;
+  mdwt_ctx *c = new (std::nothrow) mdwt_ctx();
+  if (!c) return MDWT_ERR_OOM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->numSMs, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->dCounters, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->dWork, 64) != cudaSuccess ||
+      cudaMemset(c->dCounters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->dCounters) cudaFree(c->dCounters);
+    if (c->dWork) cudaFree(c->dWork);
+    delete c;
+    return MDWT_ERR_CUDA;
+  }
+  *out = c;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_destroy(mdwt_ctx *c) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (c->device == MDWT_HOST_ONLY) { delete c; return MDWT_OK; }
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_device(c);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_push_channel(mdwt_ctx *c, const void *data, int fmt, const int64_t dims[3]) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!data || !dims || dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0)
+    return fail(c, MDWT_ERR_BAD_ARG, "null data or non-positive dims");
+  if (dims[0] > (1 << 20) || dims[1] > (1 << 20) || dims[2] > (1 << 20))
+    return fail(c, MDWT_ERR_BAD_ARG, "dimension above 2^20");
+  if (fmt_bytes(fmt) == 0) return fail(c, MDWT_ERR_UNSUPPORTED, "unspecified voxel format");
+  return push_common(c, data, fmt, dims);
+}
+
+mdwt_status mdwt_push_channel_raw(mdwt_ctx *c, const char *path) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!path) return fail(c, MDWT_ERR_BAD_ARG, "null path");
+  int64_t dims[3];
+  int fmt;
+  if (!parse_raw_name(path, dims, fmt)) return fail(c, MDWT_ERR_FORMAT, std::string("no <X>x<Y>x<Z> token in ") + path);
+  const int bpv = fmt_bytes(fmt);
+  if (bpv == 0) return fail(c, MDWT_ERR_FORMAT, std::string("no voxel type token in ") + path);
+  const size_t n = (size_t)(dims[0] * dims[1] * dims[2]);
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(c, MDWT_ERR_IO, std::string("cannot open ") + path);
+  std::vector<char> buf;
+  try {
+    buf.resize(n * bpv);
+  } catch (const std::bad_alloc &) {
+    std::fclose(f);
+    return fail(c, MDWT_ERR_OOM, "host allocation failed");
+  }
+  const size_t got = std::fread(buf.data(), 1, buf.size(), f);
+  std::fclose(f);
+  if (got != buf.size()) return fail(c, MDWT_ERR_IO, std::string("truncated raw file ") + path);
+  return push_common(c, buf.data(), fmt, dims);
+}
+
+mdwt_status mdwt_reshape_bounds(mdwt_ctx *c, int chn, const float *scale3) {
+  mdwt_status s = check_ch(c, chn);
+  if (s) return s;
+  if (c->inited) return fail(c, MDWT_ERR_STATE, "reshape bounds before mdwt_init");
+  Channel &h = c->ch[chn];
+  for (int a = 0; a < 3; a++) {
+    const float k = scale3 ? scale3[a] : (float)h.dims[a];
+    h.lo[a] = h.lo[a] * k;
+    h.hi[a] = h.hi[a] * k;
+  }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_num_channels(const mdwt_ctx *c, int *n) {
+  if (!c || !n) return MDWT_ERR_BAD_ARG;
+  *n = (int)c->ch.size();
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_channel_info(const mdwt_ctx *c, int chn, int64_t dims[3], float b8[8]) {
+  if (!c || chn < 0 || chn >= (int)c->ch.size() || !dims || !b8) return MDWT_ERR_BAD_ARG;
+  for (int a = 0; a < 3; a++) dims[a] = c->ch[chn].dims[a];
+  for (int a = 0; a < 4; a++) { b8[a] = c->ch[chn].lo[a]; b8[4 + a] = c->ch[chn].hi[a]; }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_macrocells(mdwt_ctx *c, const uint32_t d[3]) {
+  if (!c || !d) return MDWT_ERR_BAD_ARG;
+  if (c->inited) return fail(c, MDWT_ERR_STATE, "macrocells before mdwt_init");
+  for (int a = 0; a < 3; a++) c->mcReq[a] = d[a];
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (c->inited) return fail(c, MDWT_ERR_STATE, "already initialised");
+  if (c->ch.empty()) return fail(c, MDWT_ERR_STATE, "No data source specified (renderer.cpp:326-330)");
+  if (mode != MDWT_MODE_NDDA && mode != MDWT_MODE_SYNCDDA)
+    return fail(c, MDWT_ERR_UNSUPPORTED, "mode not supported by the GPU tracker (0 and 2 are)");
+  if (c->device == MDWT_HOST_ONLY) return fail(c, MDWT_ERR_STATE, "host-only context: no device to initialise");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  c->mode = mode;
+  resolve_mc(c, c->mc);
+  if (c->mc[0] == 0 || c->mc[1] == 0 || c->mc[2] == 0) return fail(c, MDWT_ERR_BAD_ARG, "zero macrocell dims");
+  if ((uint64_t)c->mc[0] * c->mc[1] * c->mc[2] > (1ull << 30)) return fail(c, MDWT_ERR_BAD_ARG, "macrocell grid above 2^30 cells");
+  c->M = (size_t)c->mc[0] * c->mc[1] * c->mc[2];
+  // root box = union of bounds (renderer.cpp:698-716); trackers use the last channel's
+  // bounds (globalBoundsLo/Hi are set in the per-channel loop, renderer.cpp:748-754)
+  for (int a = 0; a < 3; a++) {
+    float lo = std::numeric_limits<float>::infinity(), hi = -std::numeric_limits<float>::infinity();
+    for (auto &h : c->ch) { lo = std::fmin(lo, h.lo[a]); hi = std::fmax(hi, h.hi[a]); }
+    c->rootLo[a] = lo; c->rootHi[a] = hi;
+  }
+  for (int a = 0; a < 4; a++) { c->gLo[a] = c->ch.back().lo[a]; c->gHi[a] = c->ch.back().hi[a]; }
+  // one storage kind for all channels: native uint8 only when every channel is uint8
+  bool allU8 = true;
+  for (auto &h : c->ch) allU8 = allU8 && h.store == kStoreU8;
+  c->store = allU8 ? kStoreU8 : kStoreF32;
+  for (auto &h : c->ch) {
+    const size_t n = (size_t)(h.dims[0] * h.dims[1] * h.dims[2]);
+    if (!allU8 && h.store == kStoreU8) {
+      h.f32.resize(n);
+      for (size_t i = 0; i < n; i++) h.f32[i] = (float)h.u8[i] * 255;
+      h.u8.clear(); h.u8.shrink_to_fit();
+      h.store = kStoreF32;
+    }
+    const size_t bytes = n * (c->store == kStoreU8 ? 1 : 4);
+    CK(cudaMalloc(&h.dVol, bytes), "cudaMalloc volume");
+    CK(cudaMemcpyAsync(h.dVol, c->store == kStoreU8 ? (const void *)h.u8.data() : (const void *)h.f32.data(), bytes,
+                       cudaMemcpyHostToDevice, c->stream), "upload volume");
+  }
+  const int C = (int)c->ch.size();
+  CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
+  CK(cudaMalloc(&c->dMaj, c->M * (mode == 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  c->inited = true;
+  mdwt_status s = build_ranges(c);
+  if (s) { c->inited = false; return s; }
+  // host copies are no longer needed (the reference frees its scalar buffers too)
+  for (auto &h : c->ch) { h.u8.clear(); h.u8.shrink_to_fit(); h.f32.clear(); h.f32.shrink_to_fit(); }
+  c->tf.assign(C, TFState());
+  c->mats.assign(C, Material());
+  for (int i = 0; i < C; i++) { c->tf[i].vd[0] = c->ch[i].lo[3]; c->tf[i].vd[1] = c->ch[i].hi[3]; }
+  s = recalc(c);
+  if (s) return s;
+  if (auto_camera) {
+    const V3 center = v3(0.5f, 0.5f, 0.5f);
+    const V3 eye = v3(center.x, center.y, center.z + 2.5f);
+    c->cam.setOrientation(eye, center, v3(0, 1, 0), 45.0f);
+  }
+  update_camera(c);
+  s = alloc_frame(c);
+  if (s) return s;
+  c->frameID = 0; c->frameParam = 0;
+  reset_accum_ids(c);
+  reset_dt(c);
+  CK(cudaStreamSynchronize(c->stream), "init");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_macrocell_dims(const mdwt_ctx *c, uint32_t d[3]) {
+  if (!c || !d) return MDWT_ERR_BAD_ARG;
+  if (c->inited) for (int a = 0; a < 3; a++) d[a] = c->mc[a];
+  else resolve_mc(c, d);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_tf(mdwt_ctx *c, int chn, const float *rgba, int n) {
+  mdwt_status s = check_ch(c, chn);
+  if (s) return s;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  if (!rgba || n <= 0 || n > (1 << 20)) return fail(c, MDWT_ERR_BAD_ARG, "bad colormap");
+  for (int i = 0; i < 4 * n; i++)
+    if (!std::isfinite(rgba[i])) return fail(c, MDWT_ERR_BAD_ARG, "colormap values must be finite");
+  TFState &t = c->tf[chn];
+  t.rgba.assign(rgba, rgba + 4 * (size_t)n);
+  std::vector<float> alpha((size_t)n);
+  for (int i = 0; i < n; i++) {
+    t.rgba[4 * i + 3] = std::pow(t.rgba[4 * i + 3], 3.f);  // renderer.cpp:1100
+    alpha[i] = t.rgba[4 * i + 3];
+  }
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  if (t.cap < n) {
+    if (t.dAlpha) cudaFree(t.dAlpha);
+    if (t.dRgba) cudaFree(t.dRgba);
+    t.dAlpha = t.dRgba = nullptr;
+    t.cap = 0;
+    CK(cudaMalloc(&t.dAlpha, (size_t)n * 4), "cudaMalloc tf");
+    CK(cudaMalloc(&t.dRgba, (size_t)n * 16), "cudaMalloc tf");
+    t.cap = n;
+  }
+  CK(cudaMemcpyAsync(t.dAlpha, alpha.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->stream), "upload tf");
+  CK(cudaMemcpyAsync(t.dRgba, t.rgba.data(), (size_t)n * 16, cudaMemcpyHostToDevice, c->stream), "upload tf");
+  CK(cudaStreamSynchronize(c->stream), "upload tf");
+  t.n = n;
+  reset_accum_ids(c);
+  return recalc(c);
+}
+
+mdwt_status mdwt_set_opacity_scale(mdwt_ctx *c, int chn, float scale) {
+  mdwt_status s = check_ch(c, chn);
+  if (s) return s;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  if (!std::isfinite(scale)) return fail(c, MDWT_ERR_BAD_ARG, "opacity scale must be finite");
+  c->tf[chn].os = scale;
+  reset_accum_ids(c);
+  return recalc(c);
+}
+
+mdwt_status mdwt_set_tf_range(mdwt_ctx *c, int chn, float lo, float hi) {
+  mdwt_status s = check_ch(c, chn);
+  if (s) return s;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  c->tf[chn].xd[0] = lo;
+  c->tf[chn].xd[1] = hi;
+  reset_accum_ids(c);
+  return recalc(c);
+}
+
+mdwt_status mdwt_recalculate_majorants(mdwt_ctx *c) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  return recalc(c);
+}
+
+mdwt_status mdwt_set_dt(mdwt_ctx *c, float dt) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!(dt == dt)) return fail(c, MDWT_ERR_BAD_ARG, "dt is NaN");
+  c->dt = std::max(dt, 1e-4f);
+  reset_accum_ids(c);
+  return MDWT_OK;
+}
+mdwt_status mdwt_reset_dt(mdwt_ctx *c) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (c->ch.empty()) return fail(c, MDWT_ERR_STATE, "no channels");
+  reset_dt(c);
+  return MDWT_OK;
+}
+mdwt_status mdwt_get_dt(const mdwt_ctx *c, float *dt) {
+  if (!c || !dt) return MDWT_ERR_BAD_ARG;
+  *dt = c->dt;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_camera(mdwt_ctx *c, const float f[3], const float at[3], const float up[3], float fovy) {
+  if (!c || !f || !at || !up) return MDWT_ERR_BAD_ARG;
+  c->cam.setOrientation(v3(f[0], f[1], f[2]), v3(at[0], at[1], at[2]), v3(up[0], up[1], up[2]), fovy);
+  update_camera(c);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_camera_basis(const mdwt_ctx *c, float out[12]) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  const V3 v[4] = {c->cOrg, c->cLlc, c->cHor, c->cVer};
+  for (int i = 0; i < 4; i++) { out[3 * i] = v[i].x; out[3 * i + 1] = v[i].y; out[3 * i + 2] = v[i].z; }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_resize(mdwt_ctx *c, int w, int h) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (w <= 0 || h <= 0 || (int64_t)w * h > (1ll << 28)) return fail(c, MDWT_ERR_BAD_ARG, "bad resolution");
+  c->W = w;
+  c->H = h;
+  if (c->inited) {
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(c->stream), "resize");
+    mdwt_status s = alloc_frame(c);
+    if (s) return s;
+  }
+  update_camera(c);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_spp(mdwt_ctx *c, int spp) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (spp <= 0) return fail(c, MDWT_ERR_BAD_ARG, "spp must be positive");
+  c->spp = spp;
+  return MDWT_OK;
+}
+mdwt_status mdwt_set_accumulation(mdwt_ctx *c, int e) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  c->accum = e != 0;
+  return MDWT_OK;
+}
+mdwt_status mdwt_set_background(mdwt_ctx *c, const float rgb[3]) {
+  if (!c || !rgb) return MDWT_ERR_BAD_ARG;
+  c->bg = v3(rgb[0], rgb[1], rgb[2]);
+  return MDWT_OK;
+}
+mdwt_status mdwt_set_light(mdwt_ctx *c, int shadows, int gradient, const float dir[3], float intensity, float ambient) {
+  if (!c || !dir) return MDWT_ERR_BAD_ARG;
+  if (shadows || gradient) return fail(c, MDWT_ERR_UNSUPPORTED, "shadow rays and gradient shading are not in the GPU tracker yet");
+  c->shadows = false;
+  c->gradient = false;
+  c->lightDir = v3(dir[0], dir[1], dir[2]);
+  c->lightIntensity = intensity;
+  c->ambient = ambient;
+  reset_accum_ids(c);
+  return MDWT_OK;
+}
+mdwt_status mdwt_set_material(mdwt_ctx *c, int chn, float di, float sp, float sh, float gs, const float rgb[3]) {
+  mdwt_status s = check_ch(c, chn);
+  if (s) return s;
+  if (!rgb) return fail(c, MDWT_ERR_BAD_ARG, "null colour");
+  if (chn >= (int)c->mats.size()) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  Material &m = c->mats[chn];
+  m.diffuse = di; m.specular = sp; m.shininess = sh; m.gradStep = gs;
+  m.spec = v3(rgb[0], rgb[1], rgb[2]);
+  reset_accum_ids(c);
+  return MDWT_OK;
+}
+mdwt_status mdwt_set_mirror(mdwt_ctx *c, int e) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  c->mirror = e != 0;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  TrackParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.W = c->W; p.H = c->H; p.spp = c->spp;
+  p.frameParam = (uint32_t)c->frameParam;
+  p.accumParam = (uint32_t)c->accumParam;
+  p.accumulate = c->accum ? 1 : 0;
+  p.mirror = c->mirror ? 1 : 0;
+  p.bg = f3(c->bg);
+  p.camOrg = f3(c->cOrg); p.camLlc = f3(c->cLlc); p.camHor = f3(c->cHor); p.camVer = f3(c->cVer);
+  p.rootLo = {c->rootLo[0], c->rootLo[1], c->rootLo[2]};
+  p.rootHi = {c->rootHi[0], c->rootHi[1], c->rootHi[2]};
+  p.gLo = {c->gLo[0], c->gLo[1], c->gLo[2]};
+  p.w2u = {1.f / (c->gHi[0] - c->gLo[0]), 1.f / (c->gHi[1] - c->gLo[1]), 1.f / (c->gHi[2] - c->gLo[2])};
+  p.gScale = {(float)c->mc[0] * p.w2u.x, (float)c->mc[1] * p.w2u.y, (float)c->mc[2] * p.w2u.z};
+  for (int a = 0; a < 3; a++) p.mc[a] = c->mc[a];
+  p.C = (int)c->ch.size();
+  p.mode = c->mode;
+  p.dt = c->dt;
+  p.majorants = c->dMaj;
+  for (int i = 0; i < p.C; i++) {
+    p.vol[i] = c->ch[i].dVol;
+    for (int a = 0; a < 3; a++) p.dims[i][a] = (int)c->ch[i].dims[a];
+    const TFState &t = c->tf[i];
+    p.tfAlpha[i] = t.dAlpha;
+    p.tfRgba[i] = t.dRgba;
+    p.tfN[i] = t.n;
+    p.vd[i][0] = t.vd[0]; p.vd[i][1] = t.vd[1];
+    p.xd[i][0] = t.xd[0]; p.xd[i][1] = t.xd[1];
+    p.os[i] = t.os;
+    p.matSpec[i] = f3(c->mats[i].spec);
+  }
+  p.lightIntensity = c->lightIntensity;
+  p.ambient = c->ambient;
+  p.accum = c->dAccum;
+  p.fb = c->dFb;
+  p.stats = c->statsOn ? c->dStats : nullptr;
+  p.counters = c->dCounters;
+  p.workCounter = c->dWork;
+  p.tilesX = (c->W + 7) / 8;
+  p.numTiles = p.tilesX * ((c->H + 3) / 4);
+  CK(cudaMemsetAsync(c->dWork, 0, sizeof(unsigned int), st), "reset work counter");
+  CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock), "tracker kernel");
+  // Renderer::Render (renderer.cpp:957-958): the ids the next frame sees are the
+  // pre-increment values
+  c->accumParam = c->accumID++;
+  c->frameParam = c->frameID++;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_sync(mdwt_ctx *c) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(c->stream), "stream");
+  CK(cudaDeviceSynchronize(), "device");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_reset_accumulation(mdwt_ctx *c) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  reset_accum_ids(c);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_frame_ids(const mdwt_ctx *c, int out[4]) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  out[0] = c->frameID; out[1] = c->accumID; out[2] = c->frameParam; out[3] = c->accumParam;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_framebuffer(mdwt_ctx *c, uint32_t *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(out, c->dFb, (size_t)c->W * c->H * 4, cudaMemcpyDeviceToHost), "copy framebuffer");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_accum(mdwt_ctx *c, float *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(out, c->dAccum, (size_t)c->W * c->H * 16, cudaMemcpyDeviceToHost), "copy accum");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_device_buffers(mdwt_ctx *c, void **accum, void **fb) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (accum) *accum = c->dAccum;
+  if (fb) *fb = c->dFb;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_counters(mdwt_ctx *c, uint64_t out[4]) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  unsigned long long h[8];
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(h, c->dCounters, sizeof(h), cudaMemcpyDeviceToHost), "copy counters");
+  for (int i = 0; i < 4; i++) out[i] = h[i];
+  if (h[4]) return fail(c, MDWT_ERR_NUMERIC, "samples reached the per-sample step cap");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_reset_counters(mdwt_ctx *c) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaMemsetAsync(c->dCounters, 0, 8 * sizeof(unsigned long long), c->stream), "reset counters");
+  CK(cudaStreamSynchronize(c->stream), "reset counters");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_enable_pixel_stats(mdwt_ctx *c, int e) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  c->statsOn = e != 0;
+  if (c->inited) {
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    if (c->statsOn && !c->dStats) {
+      const size_t np = (size_t)c->W * c->H;
+      CK(cudaMalloc(&c->dStats, np * 16), "cudaMalloc stats");
+      CK(cudaMemsetAsync(c->dStats, 0, np * 16, c->stream), "memset stats");
+    }
+  }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_pixel_stats(mdwt_ctx *c, uint32_t *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->statsOn || !c->dStats) return fail(c, MDWT_ERR_STATE, "pixel stats are off");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(out, c->dStats, (size_t)c->W * c->H * 16, cudaMemcpyDeviceToHost), "copy stats");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_render_info(const mdwt_ctx *c, int64_t out[4]) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  out[0] = c->launches;
+  out[1] = (int64_t)sizeof(TrackParams);
+  out[2] = c->lastGrid;
+  out[3] = c->lastBlock;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_majorants(mdwt_ctx *c, float *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  const size_t n = c->M * (c->mode == 3 ? 1 : c->ch.size());
+  CK(cudaMemcpy(out, c->dMaj, n * 4, cudaMemcpyDeviceToHost), "copy majorants");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_ranges(mdwt_ctx *c, float *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(out, c->dRanges, c->M * c->ch.size() * 8, cudaMemcpyDeviceToHost), "copy ranges");
+  return MDWT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,296 @@
+"""Python mirror of ``dtracker::Renderer`` (renderer.h:52-222) over the C ABI.
+
+The methods keep the reference names and argument meanings (``PushMesh``, ``Init``,
+``Render``, ``SetXFColormap``, ``SetXFOpacityScale``, ``SetXFRange``, ``Setdt``,
+``Resetdt``, ``ResetAccumulation``, ``Resize``, ``UpdateCamera``...), so a script written
+against the reference reads the same.  Two differences in error behaviour: a failing
+call raises :class:`MdwtError` (the reference prints and returns, or calls ``exit``), and
+member writes (``spp``, ``enableAccumulation``...) take effect at once instead of at
+the next ``Update()``.
+
+The binding is generic over a ctypes library and a symbol prefix so that the CPU
+oracle, which exposes the same entry points with the ``orc_`` prefix, can be driven by
+the very same test scripts; the product library is ``libmdwt.so`` with ``mdwt_``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmdwt.so")
+
+STATUS = {
+    0: "ok", 1: "bad argument", 2: "CUDA error", 3: "I/O error", 4: "too many channels",
+    5: "unsupported", 6: "wrong call order", 7: "out of memory", 8: "device wait timed out",
+    9: "bad raw file name", 10: "sample step cap reached",
+}
+MDWT_HOST_ONLY = -1
+
+# raw::DataFormat numbering (rawFile.h:21-35)
+FORMATS = {
+    np.dtype(np.int8): 1, np.dtype(np.int16): 2, np.dtype(np.int32): 3, np.dtype(np.uint8): 4,
+    np.dtype(np.uint16): 5, np.dtype(np.uint32): 6, np.dtype(np.float32): 7, np.dtype(np.float64): 8,
+}
+
+
+class MdwtError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({message})")
+
+
+_lib_cache = {}
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libmdwt.so.  There is no fallback: a missing library is an error."""
+    if path in _lib_cache:
+        return _lib_cache[path]
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is not built; run `make -C mdwtracker_b200` or __graft_entry__.build()")
+    lib = C.CDLL(path)
+    _lib_cache[path] = lib
+    return lib
+
+
+def _f3(v) -> C.Array:
+    return (C.c_float * 3)(*[float(x) for x in v])
+
+
+class Renderer:
+    """Headless renderer on one device (``device=MDWT_HOST_ONLY`` for a host-only context)."""
+
+    _prefix = "mdwt_"
+
+    def __init__(self, device: int = 0, lib: Optional[C.CDLL] = None):
+        self._lib = lib if lib is not None else load_library()
+        self._ctx = C.c_void_p()
+        self._create(device)
+        self.fbSize = (1024, 1024)
+        self.mode = None
+
+    # ---------------------------------------------------------------- plumbing
+    def _fn(self, name: str):
+        return getattr(self._lib, self._prefix + name)
+
+    def _create(self, device: int):
+        st = self._fn("create")(C.byref(self._ctx), C.c_int(device))
+        if st != 0:
+            raise MdwtError(st, "create", f"device {device}")
+
+    def _call(self, name: str, *args):
+        st = self._fn(name)(self._ctx, *args)
+        if st != 0:
+            err = self._fn("last_error")
+            err.restype = C.c_char_p
+            raise MdwtError(st, name, (err(self._ctx) or b"").decode())
+        return st
+
+    def close(self):
+        if self._ctx:
+            self._fn("destroy")(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---------------------------------------------------------------- data
+    def PushMesh(self, data, dims: Optional[Sequence[int]] = None) -> bool:
+        """PushMesh(shared_ptr<RawR>) (renderer.cpp:1031-1044).
+
+        ``data`` is a raw-file path (parsed like raw::RawR) or a numpy array of shape
+        (Z, Y, X) (x fastest, as in the raw files)."""
+        if isinstance(data, (str, os.PathLike)):
+            self._call("push_channel_raw", C.c_char_p(os.fsencode(data)))
+            return True
+        arr = np.ascontiguousarray(data)
+        if arr.dtype not in FORMATS:
+            raise MdwtError(5, "push_channel", f"dtype {arr.dtype}")
+        if dims is None:
+            if arr.ndim != 3:
+                raise MdwtError(1, "push_channel", "need a (Z, Y, X) array or explicit dims")
+            dims = (arr.shape[2], arr.shape[1], arr.shape[0])
+        d = (C.c_int64 * 3)(*[int(x) for x in dims])
+        self._call("push_channel", arr.ctypes.data_as(C.c_void_p), C.c_int(FORMATS[arr.dtype]), d)
+        return True
+
+    def reshapeBounds(self, channel: int, scale: Optional[Sequence[float]] = None):
+        """raw::RawR::reshapeBounds (rawFile.cpp:217-237), viewer ``-cb``."""
+        self._call("reshape_bounds", C.c_int(channel), _f3(scale) if scale is not None else None)
+
+    @property
+    def numChannels(self) -> int:
+        n = C.c_int()
+        self._call("num_channels", C.byref(n))
+        return n.value
+
+    def channelInfo(self, channel: int):
+        dims = (C.c_int64 * 3)()
+        b = (C.c_float * 8)()
+        self._call("get_channel_info", C.c_int(channel), dims, b)
+        return tuple(dims), np.array(b[:], dtype=np.float32)
+
+    # ---------------------------------------------------------------- set-up
+    @property
+    def macrocellDims(self):
+        d = (C.c_uint32 * 3)()
+        self._call("get_macrocell_dims", d)
+        return tuple(d)
+
+    @macrocellDims.setter
+    def macrocellDims(self, dims):
+        if isinstance(dims, int):
+            dims = (dims, dims, dims)
+        self._call("set_macrocells", (C.c_uint32 * 3)(*[int(x) for x in dims]))
+
+    def Init(self, mode: int = 0, autoSetCamera: bool = True):
+        """Renderer::Init (renderer.cpp:324-942)."""
+        self._call("init", C.c_int(mode), C.c_int(1 if autoSetCamera else 0))
+        self.mode = mode
+
+    # ---------------------------------------------------------------- TF
+    def SetXFColormap(self, colormap, tfID: int = 0):
+        cm = np.ascontiguousarray(np.asarray(colormap, dtype=np.float32).reshape(-1, 4))
+        self._call("set_tf", C.c_int(tfID), cm.ctypes.data_as(C.POINTER(C.c_float)), C.c_int(cm.shape[0]))
+
+    def SetXFOpacityScale(self, opacityScale: float, tfID: int = 0):
+        self._call("set_opacity_scale", C.c_int(tfID), C.c_float(opacityScale))
+
+    def SetXFRange(self, xfDomain, tfID: int = 0):
+        self._call("set_tf_range", C.c_int(tfID), C.c_float(xfDomain[0]), C.c_float(xfDomain[1]))
+
+    def RecalculateDensityRanges(self):
+        self._call("recalculate_majorants")
+
+    # ---------------------------------------------------------------- parameters
+    def Setdt(self, dt: float):
+        self._call("set_dt", C.c_float(dt))
+
+    def Resetdt(self):
+        self._call("reset_dt")
+
+    @property
+    def dt(self) -> float:
+        v = C.c_float()
+        self._call("get_dt", C.byref(v))
+        return v.value
+
+    def setCamera(self, lookFrom, lookAt, lookUp, fovy: float):
+        """camera.setOrientation + UpdateCamera (viewer ``-c``)."""
+        self._call("set_camera", _f3(lookFrom), _f3(lookAt), _f3(lookUp), C.c_float(fovy))
+
+    def cameraBasis(self) -> np.ndarray:
+        out = (C.c_float * 12)()
+        self._call("get_camera_basis", out)
+        return np.array(out[:], dtype=np.float32).reshape(4, 3)
+
+    def Resize(self, newSize):
+        self._call("resize", C.c_int(int(newSize[0])), C.c_int(int(newSize[1])))
+        self.fbSize = (int(newSize[0]), int(newSize[1]))
+
+    def setSpp(self, spp: int):
+        self._call("set_spp", C.c_int(spp))
+
+    def setAccumulation(self, enable: bool):
+        self._call("set_accumulation", C.c_int(1 if enable else 0))
+
+    def setBackground(self, rgb):
+        self._call("set_background", _f3(rgb))
+
+    def setLight(self, shadows: bool, gradient: bool, direction, intensity: float = 1.0, ambient: float = 0.1):
+        self._call("set_light", C.c_int(int(shadows)), C.c_int(int(gradient)), _f3(direction),
+                   C.c_float(intensity), C.c_float(ambient))
+
+    def setMaterial(self, channel: int, diffuse=0.8, specular=0.3, shininess=8.0, gradientStep=0.01,
+                    specularColor=(1.0, 1.0, 1.0)):
+        self._call("set_material", C.c_int(channel), C.c_float(diffuse), C.c_float(specular),
+                   C.c_float(shininess), C.c_float(gradientStep), _f3(specularColor))
+
+    def setMirror(self, enable: bool):
+        self._call("set_mirror", C.c_int(1 if enable else 0))
+
+    # ---------------------------------------------------------------- frames
+    def Render(self, stream: Optional[int] = None):
+        """Renderer::Render (renderer.cpp:944-973); asynchronous on ``stream``."""
+        self._call("render", C.c_void_p(stream) if stream else None)
+
+    def sync(self):
+        self._call("sync")
+
+    def ResetAccumulation(self):
+        self._call("reset_accumulation")
+
+    def frameIds(self):
+        out = (C.c_int * 4)()
+        self._call("get_frame_ids", out)
+        return tuple(out)
+
+    def framebuffer(self) -> np.ndarray:
+        w, h = self.fbSize
+        out = np.empty(w * h, dtype=np.uint32)
+        self._call("get_framebuffer", out.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return out.reshape(h, w)
+
+    def accum(self) -> np.ndarray:
+        w, h = self.fbSize
+        out = np.empty(w * h * 4, dtype=np.float32)
+        self._call("get_accum", out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out.reshape(h, w, 4)
+
+    def counters(self) -> np.ndarray:
+        out = (C.c_uint64 * 4)()
+        self._call("get_counters", out)
+        return np.array(out[:], dtype=np.uint64)
+
+    def resetCounters(self):
+        self._call("reset_counters")
+
+    def enablePixelStats(self, enable: bool = True):
+        self._call("enable_pixel_stats", C.c_int(1 if enable else 0))
+
+    def pixelStats(self) -> np.ndarray:
+        w, h = self.fbSize
+        out = np.empty(w * h * 4, dtype=np.uint32)
+        self._call("get_pixel_stats", out.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return out.reshape(h, w, 4)
+
+    # ---------------------------------------------------------------- majorants
+    def _num_cells(self) -> int:
+        d = self.macrocellDims
+        return int(d[0]) * int(d[1]) * int(d[2])
+
+    def majorants(self) -> np.ndarray:
+        n = self._num_cells() * (1 if self.mode == 3 else self.numChannels)
+        out = np.empty(n, dtype=np.float32)
+        self._call("get_majorants", out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def ranges(self) -> np.ndarray:
+        n = self._num_cells() * self.numChannels
+        out = np.empty(2 * n, dtype=np.float32)
+        self._call("get_ranges", out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out.reshape(n, 2)
+
+    def renderInfo(self):
+        """(kernels launched so far, per-frame parameter bytes, last grid, last block)."""
+        out = (C.c_int64 * 4)()
+        self._call("get_render_info", out)
+        return tuple(out)
+
+    def deviceBuffers(self):
+        a, f = C.c_void_p(), C.c_void_p()
+        self._call("get_device_buffers", C.byref(a), C.byref(f))
+        return a.value, f.value

@@ -1,0 +1,162 @@
+"""Seeded synthetic scenes with the shapes of the benchmark configurations.
+
+The reference's experiment scripts render external datasets (nyx, zebrafish,
+hurricane, miranda; ``mcSizeExps/*.sh``, ``numChanExps/*.sh``) that are not available
+here.  These generators produce volumes with the configured shapes, dtypes and value
+distributions instead:
+
+* ``blobs``  -- 64^3 uint8: 16 isotropic Gaussians (sigma 4-12 voxels, amplitude
+  0-255) plus uniform noise of +-8, clamped to [0, 255].
+* ``value_noise_sparse`` -- N^3 uint8: 4-octave value noise thresholded so that a
+  given fraction (10-30 %) of the voxels is non-zero.
+* ``lognormal`` -- N^3 float32: 5-octave noise, exp-mapped into [1e-3, 1e3].
+
+Transfer functions are 256-entry RGBA tables with linear opacity ramps 0 -> 1 (the
+renderer cubes alpha, renderer.cpp:1100).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+
+def _upsample(lattice: np.ndarray, n: int) -> np.ndarray:
+    from scipy.ndimage import zoom
+    z = n / lattice.shape[0]
+    out = zoom(lattice, z, order=1, mode="nearest", grid_mode=True)
+    return out[:n, :n, :n]
+
+
+def blobs(n: int = 64, nblobs: int = 16, seed: int = 1) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    sig = rng.uniform(4.0, 12.0, nblobs)
+    amp = rng.uniform(0.0, 255.0, nblobs)
+    ctr = rng.uniform(0.0, n, (nblobs, 3))
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    vol = np.zeros((n, n, n), dtype=np.float64)
+    for k in range(nblobs):
+        d2 = (x - ctr[k, 0]) ** 2 + (y - ctr[k, 1]) ** 2 + (z - ctr[k, 2]) ** 2
+        vol += amp[k] * np.exp(-d2 / (2.0 * sig[k] ** 2))
+    vol += rng.uniform(-8.0, 8.0, vol.shape)
+    return np.clip(np.rint(vol), 0, 255).astype(np.uint8)
+
+
+def value_noise(n: int, octaves: int, seed: int, base: int = 4) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, n, n), dtype=np.float32)
+    amp = 1.0
+    for o in range(octaves):
+        res = min(base * (2 ** o), n)
+        lattice = rng.random((res, res, res), dtype=np.float32)
+        out += amp * _upsample(lattice, n)
+        amp *= 0.5
+    return out
+
+
+def value_noise_sparse(n: int = 256, occupancy: float = 0.2, seed: int = 2, octaves: int = 4) -> np.ndarray:
+    f = value_noise(n, octaves, seed)
+    t = np.quantile(f, 1.0 - occupancy)
+    hi = float(f.max())
+    v = np.where(f > t, 1.0 + 254.0 * (f - t) / max(hi - t, 1e-6), 0.0)
+    return np.clip(np.rint(v), 0, 255).astype(np.uint8)
+
+
+def lognormal(n: int = 512, seed: int = 3, octaves: int = 5) -> np.ndarray:
+    f = value_noise(n, octaves, seed)
+    f = (f - f.mean()) / max(float(f.std()), 1e-6)
+    v = np.exp(np.clip(f / 3.0, -1.0, 1.0) * np.log(1e3))
+    return v.astype(np.float32)
+
+
+def ramp_tf(rgb: Sequence[float], n: int = 256, alpha_max: float = 1.0) -> np.ndarray:
+    """n RGBA texels: colour fades in with the ramp, opacity rises linearly 0 -> alpha_max."""
+    x = np.linspace(0.0, 1.0, n, dtype=np.float32)
+    tf = np.empty((n, 4), dtype=np.float32)
+    for k in range(3):
+        tf[:, k] = rgb[k] * (0.35 + 0.65 * x)
+    tf[:, 3] = alpha_max * x
+    return tf
+
+
+def viridis_like(n: int = 256) -> np.ndarray:
+    x = np.linspace(0.0, 1.0, n, dtype=np.float32)
+    tf = np.empty((n, 4), dtype=np.float32)
+    tf[:, 0] = np.clip(1.6 * x - 0.4, 0, 1)
+    tf[:, 1] = np.clip(0.1 + 0.85 * x, 0, 1)
+    tf[:, 2] = np.clip(0.55 + 0.3 * np.sin(3.0 * x), 0, 1)
+    tf[:, 3] = x
+    return tf
+
+
+HUES = [(1.0, 0.2, 0.15), (0.2, 1.0, 0.25), (0.2, 0.35, 1.0), (1.0, 0.85, 0.2), (0.9, 0.3, 1.0), (0.2, 0.95, 0.95),
+        (1.0, 0.55, 0.1), (0.6, 0.6, 0.6), (0.5, 1.0, 0.5), (1.0, 0.5, 0.7), (0.4, 0.4, 1.0), (0.8, 0.8, 0.3)]
+
+
+@dataclass
+class Scene:
+    """One render configuration: channels, TFs, grid, method and frame settings."""
+    name: str
+    volumes: List[np.ndarray]
+    tfs: List[np.ndarray]
+    mode: int
+    macrocells: Tuple[int, int, int]
+    resolution: Tuple[int, int]
+    spp: int
+    frames: int = 1
+    opacity: List[float] = field(default_factory=list)
+    xf_range: List[Tuple[float, float]] = field(default_factory=list)
+    camera: Optional[Tuple] = None   # (from, at, up, fovy) or None for the default camera
+    dt: Optional[float] = None
+
+    def setup(self, r, resolution: Optional[Tuple[int, int]] = None, spp: Optional[int] = None):
+        """Configure a Renderer (product or oracle) like viewer.cpp:486-509 does."""
+        for v in self.volumes:
+            r.PushMesh(v)
+        r.macrocellDims = self.macrocells
+        res = resolution or self.resolution
+        r.Resize(res)
+        r.Init(self.mode, self.camera is None)
+        if self.dt is not None:
+            r.Setdt(self.dt)
+        if self.camera is not None:
+            r.setCamera(*self.camera)
+        for i, tf in enumerate(self.tfs):
+            r.SetXFColormap(tf, i)
+            r.SetXFOpacityScale(self.opacity[i] if self.opacity else 1.0, i)
+            r.SetXFRange(self.xf_range[i] if self.xf_range else (0.0, 1.0), i)
+        r.setSpp(spp or self.spp)
+        return r
+
+    @property
+    def nbytes(self) -> int:
+        return int(sum(v.nbytes for v in self.volumes))
+
+
+def scene_c1(seed: int = 1) -> Scene:
+    """N-DDA, 1 channel 64^3 uint8 blobs, macrocell 8^3, 512x512, 1 spp x 16 frames."""
+    return Scene("c1_ndda_64u8", [blobs(64, 16, seed)], [viridis_like()], mode=0, macrocells=(8, 8, 8),
+                 resolution=(512, 512), spp=1, frames=16)
+
+
+def scene_c2(seed: int = 2, n: int = 256) -> Scene:
+    """syncDDA, 3 channels n^3 uint8 sparse value noise (10/20/30 %), macrocell 16^3 voxels,
+    1024x1024, 64 spp."""
+    occ = [0.10, 0.20, 0.30]
+    vols = [value_noise_sparse(n, occ[i], seed * 17 + i) for i in range(3)]
+    tfs = [ramp_tf(HUES[i]) for i in range(3)]
+    mc = max(1, n // 16)
+    return Scene(f"c2_syncdda_3x{n}u8", vols, tfs, mode=2, macrocells=(mc, mc, mc), resolution=(1024, 1024), spp=64)
+
+
+def scene_c3(seed: int = 3, n: int = 512, channels: int = 6, edge: int = 16, mode: int = 2) -> Scene:
+    """N-DDA / syncDDA, `channels` x n^3 float32 log-normal, macrocell edge `edge` voxels,
+    1920x1080, 256 spp.  The TF range maps [1e-3, ~15] of the [0, 1e3] value domain, so
+    the opacity ramp covers the log-normal bulk."""
+    vols = [lognormal(n, seed * 31 + i) for i in range(channels)]
+    tfs = [ramp_tf(HUES[i % len(HUES)], alpha_max=0.5) for i in range(channels)]
+    mc = max(1, n // edge)
+    return Scene(f"c3_{'syncdda' if mode == 2 else 'ndda'}_{channels}x{n}f32_e{edge}", vols, tfs, mode=mode,
+                 macrocells=(mc, mc, mc), resolution=(1920, 1080), spp=256,
+                 xf_range=[(0.0, 0.015)] * channels)

@@ -1,0 +1,77 @@
+"""ctypes binding of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for libmdwt.so.  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module.
+
+The oracle exposes the renderer entry points of include/mdwt.h with the ``orc_``
+prefix, so :class:`OracleRenderer` reuses the product's Python mirror of the reference
+``dtracker::Renderer`` API and a test script drives both the same way.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from mdwtracker_b200.renderer import Renderer, MdwtError
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+
+_lib = None
+
+
+def build_oracle(force: bool = False) -> str:
+    if force or not os.path.exists(ORACLE_LIB):
+        subprocess.run(["make", "-C", HERE], check=True, stdout=subprocess.DEVNULL)
+    return ORACLE_LIB
+
+
+def load_oracle() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build_oracle()
+        _lib = C.CDLL(ORACLE_LIB)
+        _lib.orc_log.restype = C.c_float
+        _lib.orc_log.argtypes = [C.c_float]
+        _lib.orc_capped_samples.restype = C.c_uint64
+        _lib.orc_rng_stream.argtypes = [C.c_uint32, C.c_uint32, C.c_int, C.POINTER(C.c_float)]
+    return _lib
+
+
+def set_threads(n: int) -> int:
+    return load_oracle().orc_set_threads(C.c_int(n))
+
+
+def oracle_log(x: float) -> float:
+    return load_oracle().orc_log(C.c_float(x))
+
+
+def rng_stream(v0: int, v1: int, n: int) -> np.ndarray:
+    out = np.empty(n, dtype=np.float32)
+    load_oracle().orc_rng_stream(C.c_uint32(v0), C.c_uint32(v1), C.c_int(n),
+                                 out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+class OracleRenderer(Renderer):
+    """The reference renderer restated on the CPU (OpenMP)."""
+
+    _prefix = "orc_"
+
+    def __init__(self):
+        super().__init__(device=0, lib=load_oracle())
+
+    def _create(self, device: int):
+        st = self._lib.orc_create(C.byref(self._ctx))
+        if st != 0:
+            raise MdwtError(st, "orc_create")
+
+    def renderRows(self, row0: int, row1: int):
+        """One frame restricted to pixel rows [row0, row1) (frame ids still advance)."""
+        self._call("render_rows", C.c_int(row0), C.c_int(row1))
+
+    def cappedSamples(self) -> int:
+        return int(self._lib.orc_capped_samples(self._ctx))

@@ -1,0 +1,90 @@
+"""The C ABI: libmdwt.so loads, exports every entry point of include/mdwt.h, and its
+host-side logic answers without a GPU (host-only contexts)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from mdwtracker_b200 import MDWT_HOST_ONLY, MdwtError, Renderer
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "mdwt.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mdwt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_renderer_surface():
+    syms = header_symbols()
+    for must in ["mdwt_create", "mdwt_destroy", "mdwt_push_channel_raw", "mdwt_push_channel", "mdwt_init",
+                 "mdwt_set_tf", "mdwt_set_opacity_scale", "mdwt_set_tf_range", "mdwt_set_dt", "mdwt_reset_dt",
+                 "mdwt_set_camera", "mdwt_resize", "mdwt_render", "mdwt_reset_accumulation",
+                 "mdwt_get_framebuffer", "mdwt_get_accum", "mdwt_get_majorants"]:
+        assert must in syms
+
+
+def test_library_exports_every_declared_symbol(mdwt_lib):
+    missing = [s for s in header_symbols() if not hasattr(mdwt_lib, s)]
+    assert not missing, missing
+
+
+def test_status_strings(mdwt_lib):
+    mdwt_lib.mdwt_status_string.restype = C.c_char_p
+    assert mdwt_lib.mdwt_status_string(0) == b"ok"
+    assert mdwt_lib.mdwt_status_string(4) == b"too many channels"
+    assert mdwt_lib.mdwt_version() >> 16 == 1
+
+
+def test_null_arguments_are_rejected(mdwt_lib):
+    assert mdwt_lib.mdwt_create(None, 0) == 1
+    assert mdwt_lib.mdwt_destroy(None) == 1
+    assert mdwt_lib.mdwt_render(None, None) == 1
+
+
+def test_host_only_context_refuses_init():
+    r = Renderer(MDWT_HOST_ONLY)
+    r.PushMesh(np.zeros((4, 4, 4), np.uint8))
+    with pytest.raises(MdwtError) as e:
+        r.Init(0)
+    assert e.value.status == 6
+
+
+def test_too_many_channels():
+    r = Renderer(MDWT_HOST_ONLY)
+    for _ in range(12):
+        r.PushMesh(np.zeros((2, 2, 2), np.uint8))
+    with pytest.raises(MdwtError) as e:
+        r.PushMesh(np.zeros((2, 2, 2), np.uint8))
+    assert e.value.status == 4
+
+
+def test_bad_arguments():
+    r = Renderer(MDWT_HOST_ONLY)
+    with pytest.raises(MdwtError):
+        r.PushMesh(np.zeros((4, 4, 4), np.complex64))
+    with pytest.raises(MdwtError):
+        r.setSpp(0)
+    with pytest.raises(MdwtError):
+        r.Resize((0, 10))
+    with pytest.raises(MdwtError):
+        r.channelInfo(0)
+    with pytest.raises(MdwtError) as e:
+        r.PushMesh("/nonexistent/vol_8x8x8_uint8.raw")
+    assert e.value.status == 3
+    with pytest.raises(MdwtError) as e:
+        r.PushMesh("/nonexistent/volume_uint8.raw")
+    assert e.value.status == 9
+
+
+def test_gpu_absent_is_an_error_not_a_fallback():
+    """Without a device the product refuses to create a render context."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(MdwtError) as e:
+        Renderer(0)
+    assert e.value.status == 2

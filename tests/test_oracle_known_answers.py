@@ -1,0 +1,159 @@
+"""Known-answer tests that pin the CPU oracle.
+
+The reference ships no tests or golden vectors and cannot be built here, so the oracle
+is pinned against answers derived from the domain and from published algorithms:
+  * the RNG's TEA hash and LCG against their published test vectors;
+  * the project log against libm;
+  * an empty volume renders the background exactly;
+  * a constant-density slab gives the Beer-Lambert collision probability 1-exp(-alpha*L/dt)
+    (Woodcock tracking is unbiased; the reference's dt scales every free-flight step,
+    deviceCode.cu:800-806, so the world extinction is alpha/dt);
+  * a single bright voxel gives the hand-derived macrocell ranges and majorants
+    (renderer.cu:387-392, 487-519, 835-893, 159-203);
+  * a transfer function with zero opacity gives zero majorants.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+
+def test_tea_published_vector(oracle):
+    lib = oracle.load_oracle()
+    k = (C.c_uint32 * 4)(0, 0, 0, 0)
+    out = (C.c_uint32 * 2)()
+    lib.orc_tea(C.c_uint32(0), C.c_uint32(0), k, 32, out)
+    # TEA, 32 cycles, key 0, plaintext 0 (Wheeler & Needham reference cipher)
+    assert (out[0], out[1]) == (0x41EA3A0A, 0x94BAA940)
+
+
+def test_lcg_numerical_recipes_sequence(oracle):
+    lib = oracle.load_oracle()
+    out = (C.c_uint32 * 5)()
+    lib.orc_lcg_states(C.c_uint32(0), 5, out)
+    # Numerical Recipes in C (2nd ed.) sec. 7.1, quick-and-dirty generator from idum = 0
+    assert list(out) == [0x3C6EF35F, 0x47502932, 0xD1CCF6E9, 0xAAF95334, 0x6252E503]
+
+
+def test_rng_stream_is_uniform(oracle):
+    xs = np.concatenate([oracle.rng_stream(i, 7 * i + 1, 256) for i in range(64)])
+    assert xs.min() >= 0.0 and xs.max() < 1.0
+    hist, _ = np.histogram(xs, bins=16, range=(0, 1))
+    exp = len(xs) / 16
+    chi2 = float(((hist - exp) ** 2 / exp).sum())
+    assert chi2 < 40.0  # 15 dof, p ~ 5e-4
+
+
+def test_log_accuracy(oracle):
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([rng.random(2000).astype(np.float32), np.float32(2.0) ** -np.arange(1, 25, dtype=np.float32),
+                         np.float32(1) - np.arange(1, 200, dtype=np.float32) * np.float32(2 ** -24)])
+    xs = xs[xs > 0]
+    for x in xs:
+        got = oracle.oracle_log(float(x))
+        ref = math.log(float(x))
+        assert abs(got - ref) <= 3e-7 * max(abs(ref), 1e-30) + 1e-12, (x, got, ref)
+    assert oracle.oracle_log(1.0) == 0.0
+
+
+def _scene(oracle, vol, tf, res=(32, 32), spp=1, mode=0, mc=(4, 4, 4), bg=(0.0, 0.0, 0.0)):
+    o = oracle.OracleRenderer()
+    vols = vol if isinstance(vol, list) else [vol]
+    for v in vols:
+        o.PushMesh(v)
+    o.macrocellDims = mc
+    o.Resize(res)
+    o.Init(mode)
+    for i in range(len(vols)):
+        o.SetXFColormap(tf, i)
+        o.SetXFOpacityScale(1.0, i)
+        o.SetXFRange((0.0, 1.0), i)
+    o.setSpp(spp)
+    o.setBackground(bg)
+    return o
+
+
+def ramp(n=256):
+    tf = np.zeros((n, 4), np.float32)
+    tf[:, 0] = 1.0
+    tf[:, 3] = np.linspace(0, 1, n)
+    return tf
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_empty_volume_renders_background(oracle, mode):
+    vol = np.zeros((16, 16, 16), np.uint8)
+    bg = (0.25, 0.5, 0.75)
+    o = _scene(oracle, [vol, vol], ramp(), spp=4, mode=mode, bg=bg)
+    assert np.all(o.majorants() == 0.0)
+    o.Render()
+    acc = o.accum()
+    np.testing.assert_array_equal(acc[..., :3], np.broadcast_to(np.float32(bg), acc[..., :3].shape))
+    # alpha: finalColor starts at 1 and gains 1 per sample (deviceCode.cu:289, 433): (spp+1)/spp
+    np.testing.assert_array_equal(acc[..., 3], np.float32(1.25))
+    assert o.counters()[0] == 0
+
+
+def test_zero_alpha_tf_gives_zero_majorants(oracle):
+    from mdwtracker_b200.synthetic import blobs
+    tf = ramp()
+    tf[:, 3] = 0.0
+    o = _scene(oracle, blobs(32, 6, 3), tf)
+    assert np.all(o.majorants() == 0.0)
+
+
+def test_single_voxel_ranges_and_majorants(oracle):
+    vol = np.zeros((16, 16, 16), np.uint8)
+    vol[5, 5, 5] = 255
+    o = _scene(oracle, vol, ramp(), mc=(4, 4, 4))
+    rng = o.ranges().reshape(4, 4, 4, 2)     # [cz, cy, cx]
+    # voxels 4, 5, 6 have voxel 5 in their 3x3x3 neighbourhood; their boxes
+    # [p-1, p+1]/16 project onto cells {0,1} (voxel 4) and {1} (voxels 5, 6)
+    hot = np.zeros((4, 4, 4), bool)
+    hot[:2, :2, :2] = True
+    assert np.all(rng[..., 0] == 0.0)
+    np.testing.assert_array_equal(rng[..., 1][hot], 65025.0)
+    np.testing.assert_array_equal(rng[..., 1][~hot], 0.0)
+    maj = o.majorants().reshape(4, 4, 4)
+    np.testing.assert_array_equal(maj[hot], 1.0)       # full texel range: max alpha = 1^3
+    np.testing.assert_array_equal(maj[~hot], 0.0)      # texel 0: alpha 0
+
+
+def test_beer_lambert_slab(oracle):
+    """Constant density alpha over the unit cube: P(hit) = 1 - exp(-alpha * L / dt)."""
+    alpha = 0.004
+    tf = np.zeros((256, 4), np.float32)
+    tf[:, 0] = 1.0
+    tf[:, 3] = np.float32(alpha) ** (1.0 / 3.0)   # cubed on upload
+    vol = np.full((32, 32, 32), 128, np.uint8)
+    res = (33, 33)
+    o = _scene(oracle, vol, tf, res=res, spp=2048, mode=2, mc=(4, 4, 4))
+    o.enablePixelStats(True)
+    o.Render()
+    st = o.pixelStats()
+    dt = o.dt                                   # 0.5 / 32
+    basis = o.cameraBasis()
+    org = basis[0].astype(np.float64)
+    n = 0
+    for (py, px) in [(16, 16), (14, 18), (10, 12), (20, 22)]:
+        # expected path length through [0,1]^3 of the (jitter-averaged) pixel ray
+        hits = st[py, px, 2]
+        ps = []
+        for j in np.linspace(0.0, 1.0, 33)[:-1] + 1.0 / 64:
+            s = (np.array([px, py]) + j) / np.array(res)
+            d = basis[1] + s[0] * basis[2] + s[1] * basis[3] - org
+            d /= np.linalg.norm(d)
+            with np.errstate(divide="ignore"):
+                t0 = (0.0 - org) / d
+                t1 = (1.0 - org) / d
+            tn = np.max(np.minimum(t0, t1))
+            tf_ = np.min(np.maximum(t0, t1))
+            L = max(0.0, tf_ - tn)
+            ps.append(1.0 - math.exp(-alpha * L / dt))
+        p = float(np.mean(ps))
+        phat = hits / 2048.0
+        sigma = math.sqrt(p * (1 - p) / 2048.0)
+        assert abs(phat - p) < 4.5 * sigma, (px, py, phat, p, sigma)
+        n += 1
+    assert n == 4
