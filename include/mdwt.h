@@ -39,7 +39,8 @@ enum {
   MDWT_ERR_OOM = 7,                /* device or host allocation failed */
   MDWT_ERR_TIMEOUT = 8,            /* a device-side bounded wait gave up */
   MDWT_ERR_FORMAT = 9,             /* raw file name carries no dims / unknown type */
-  MDWT_ERR_NUMERIC = 10            /* a sample hit the per-sample step cap (NaN/inf input) */
+  MDWT_ERR_NUMERIC = 10,           /* a sample hit the per-sample step cap (NaN/inf input) */
+  MDWT_ERR_SCRATCH_LIMIT = 11      /* input larger than the fixed scratch of mdwt_build_ranges_noalloc */
 };
 
 #define MDWT_MAX_CHANNELS 12       /* deviceCode.h:13 */
@@ -192,6 +193,25 @@ mdwt_status mdwt_get_render_info(const mdwt_ctx *ctx, int64_t out4[4]);
 mdwt_status mdwt_get_majorants(mdwt_ctx *ctx, float *host_out);
 /* macrocellsBuffer (renderer.cu:1116-1179): per (cell, channel) value range, 2*M*C floats. */
 mdwt_status mdwt_get_ranges(mdwt_ctx *ctx, float *host_out);
+
+/* No counterpart in the reference.  The value ranges of ONE channel, built on the GPU
+ * without allocating any memory, for callers that may not allocate device memory: code
+ * that runs inside an application's own memory pool or under an allocator that forbids
+ * cudaMalloc, and plug-ins that are handed device buffers and a stream but no right to
+ * allocate.  The caller passes the channel's voxels on the device (`format`
+ * MDWT_FMT_UINT8, value = byte * 255, or MDWT_FMT_FLOAT32; x fastest), its dims, the
+ * macrocell counts, the box the grid spans (the union of the channel bounds,
+ * renderer.cpp:698-716) and a device output of 2 * mc[0]*mc[1]*mc[2] floats (min, max per
+ * cell, cell-major).  The result equals the ranges mdwt_init builds for that channel.
+ * Work is enqueued on `cuda_stream` (a cudaStream_t; NULL = legacy default stream).
+ * Limits: at most 1024 macrocells per axis and dims[2] * mc[1] * mc[0] <= 2^20, else
+ * MDWT_ERR_SCRATCH_LIMIT.  The scratch is fixed device memory inside the library (8 MiB +
+ * 24 KiB, held by every GPU that loads the library until the process exits); the first
+ * call on a device looks up its address, so make that first call before any stream
+ * capture.  Calls share the scratch: calls that overlap on the GPU race. */
+mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int format, const int64_t dims[3],
+                                      const uint32_t macrocells[3], const float world_lo[3],
+                                      const float world_hi[3], float *d_ranges_out, void *cuda_stream);
 
 #ifdef __cplusplus
 }

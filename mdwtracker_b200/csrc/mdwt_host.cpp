@@ -475,6 +475,7 @@ const char *mdwt_status_string(mdwt_status s) {
     case MDWT_ERR_TIMEOUT: return "device wait timed out";
     case MDWT_ERR_FORMAT: return "bad raw file name";
     case MDWT_ERR_NUMERIC: return "sample step cap reached";
+    case MDWT_ERR_SCRATCH_LIMIT: return "input exceeds the fixed scratch of a no-alloc entry point";
   }
   return "unknown status";
 }

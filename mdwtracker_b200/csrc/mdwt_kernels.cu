@@ -17,6 +17,11 @@
 //       state machine so that a lane that finishes a path starts its next path at once.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <cmath>
+#include <mutex>
+
+#include "../../include/mdwt.h"
 #include "mdwt_internal.h"
 
 namespace mdwt {
@@ -622,4 +627,131 @@ int launch_majorants(const MajorantParams &p, void *stream, int *launches) {
   return (int)cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ range build without allocation
+// Scratch of mdwt_build_ranges_noalloc: the per-(z, cell-y, cell-x) partial ranges and
+// the voxel intervals.  Module globals: every device that loads the library holds them
+// (8 MiB + 24 KiB) until the process exits.
+namespace {
+constexpr size_t kNoAllocPairs = size_t(1) << 20;
+constexpr int kNoAllocMaxCells = 1024;
+static __device__ __align__(256) float2 g_noalloc_pairs[kNoAllocPairs];
+static __device__ __align__(256) int g_noalloc_iv[3 * 2 * kNoAllocMaxCells];
+
+__device__ __forceinline__ int project_d(float f, float lo, float hi, int dim) {
+  int v = f2i((float)dim * (f - lo) / (hi - lo));
+  v = v < dim - 1 ? v : dim - 1;
+  return v > 0 ? v : 0;
+}
+
+// Cells [clo, chi] that the 27-neighbour box of voxel p touches on one axis.
+__device__ __forceinline__ void voxel_cells(int p, int D, int md, float wlo, float whi, float len, int &clo, int &chi) {
+  const float vlo = fmaf((float)p, len, wlo);
+  float blo = vlo, bhi = vlo + len;
+  if (p - 1 >= 0) { const float nl = fmaf((float)(p - 1), len, wlo); blo = fminf(blo, nl); bhi = fmaxf(bhi, nl); }
+  if (p + 1 < D) { const float nl = fmaf((float)(p + 1), len, wlo); blo = fminf(blo, nl); bhi = fmaxf(bhi, nl); }
+  clo = project_d(blo, wlo, whi, md);
+  const int h = project_d(bhi, wlo, whi, md);
+  chi = h < md - 1 ? h : md - 1;
+}
+
+// One thread per (axis, cell index): the voxel interval of the separable range build,
+// found by binary search (clo and chi are non-decreasing in p for these bounds).
+__global__ void noalloc_intervals_kernel(int dx, int dy, int dz, int mx, int my, int mz, float lx, float ly, float lz,
+                                         float hx, float hy, float hz, int *iv) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int D, md, off;
+  float wlo, whi;
+  if (t < mx) { D = dx; md = mx; wlo = lx; whi = hx; off = 0; }
+  else if (t < mx + my) { t -= mx; D = dy; md = my; wlo = ly; whi = hy; off = 2 * mx; }
+  else if (t < mx + my + mz) { t -= mx + my; D = dz; md = mz; wlo = lz; whi = hz; off = 2 * (mx + my); }
+  else return;
+  const int k = t;
+  const float len = (whi - wlo) / (float)D;
+  int lo = 0, hi = D;
+  while (lo < hi) {  // first p with chi(p) >= k
+    const int mid = (lo + hi) >> 1;
+    int cl, ch;
+    voxel_cells(mid, D, md, wlo, whi, len, cl, ch);
+    if (ch >= k) hi = mid; else lo = mid + 1;
+  }
+  const int pmin = lo;
+  lo = 0; hi = D;
+  while (lo < hi) {  // first p with clo(p) > k
+    const int mid = (lo + hi) >> 1;
+    int cl, ch;
+    voxel_cells(mid, D, md, wlo, whi, len, cl, ch);
+    if (cl > k) hi = mid; else lo = mid + 1;
+  }
+  const int pmax = lo - 1;
+  if (pmin > pmax) { iv[off + 2 * k] = 1; iv[off + 2 * k + 1] = 0; return; }
+  iv[off + 2 * k] = pmin - 1 > 0 ? pmin - 1 : 0;
+  iv[off + 2 * k + 1] = pmax + 1 < D - 1 ? pmax + 1 : D - 1;
+}
+
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 64;
+void *g_noalloc_pairs_ptr[kNoAllocMaxDevices];
+int *g_noalloc_iv_ptr[kNoAllocMaxDevices];
+bool g_noalloc_ready[kNoAllocMaxDevices];
+
+bool bounds_ok(float lo, float hi, int64_t D) {
+  if (!std::isfinite(lo) || !std::isfinite(hi) || !(hi > lo)) return false;
+  const float scale = std::fmax(std::fabs(lo), std::fabs(hi));
+  return (hi - lo) / (float)D >= 1e-6f * scale;
+}
+}  // namespace
+
 }  // namespace mdwt
+
+// Value ranges of one channel computed without allocating any memory.  For callers that
+// must not allocate device memory: code running inside an application's own memory pool
+// or under an allocator that forbids cudaMalloc, or plug-ins that are handed device
+// buffers and a stream but no allocation rights.  The scratch is the module-global
+// g_noalloc_pairs / g_noalloc_iv; the first call on a device looks up their addresses
+// (cudaGetSymbolAddress), so make that first call before any stream capture.  All calls
+// share the scratch: calls that overlap on the GPU (two streams, two threads) race.
+extern "C" mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int format, const int64_t dims[3],
+                                                 const uint32_t macrocells[3], const float world_lo[3],
+                                                 const float world_hi[3], float *d_ranges_out, void *cuda_stream) {
+  using namespace mdwt;
+  if (!d_volume || !dims || !macrocells || !world_lo || !world_hi || !d_ranges_out) return MDWT_ERR_BAD_ARG;
+  if (format != MDWT_FMT_UINT8 && format != MDWT_FMT_FLOAT32) return MDWT_ERR_UNSUPPORTED;
+  for (int a = 0; a < 3; a++) {
+    if (dims[a] <= 0 || dims[a] > (1 << 20) || macrocells[a] == 0) return MDWT_ERR_BAD_ARG;
+    if (macrocells[a] > (uint32_t)kNoAllocMaxCells) return MDWT_ERR_SCRATCH_LIMIT;
+    if (!bounds_ok(world_lo[a], world_hi[a], dims[a])) return MDWT_ERR_UNSUPPORTED;
+  }
+  if ((size_t)dims[2] * macrocells[1] * macrocells[0] > kNoAllocPairs) return MDWT_ERR_SCRATCH_LIMIT;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) { cudaGetLastError(); return MDWT_ERR_CUDA; }
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ready[dev]) {
+      void *p = nullptr, *q = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_pairs) != cudaSuccess ||
+          cudaGetSymbolAddress(&q, g_noalloc_iv) != cudaSuccess) {
+        cudaGetLastError();
+        return MDWT_ERR_CUDA;
+      }
+      g_noalloc_pairs_ptr[dev] = p;
+      g_noalloc_iv_ptr[dev] = (int *)q;
+      g_noalloc_ready[dev] = true;
+    }
+  }
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  const int mx = (int)macrocells[0], my = (int)macrocells[1], mz = (int)macrocells[2];
+  int *iv = g_noalloc_iv_ptr[dev];
+  noalloc_intervals_kernel<<<(mx + my + mz + 127) / 128, 128, 0, st>>>(
+      (int)dims[0], (int)dims[1], (int)dims[2], mx, my, mz, world_lo[0], world_lo[1], world_lo[2],
+      world_hi[0], world_hi[1], world_hi[2], iv);
+  if (cudaGetLastError() != cudaSuccess) return MDWT_ERR_CUDA;
+  const size_t M = (size_t)mx * my * mz;
+  if (launch_ranges_init(d_ranges_out, M, st, nullptr) != 0) return MDWT_ERR_CUDA;
+  const int d3[3] = {(int)dims[0], (int)dims[1], (int)dims[2]};
+  const uint32_t mc3[3] = {macrocells[0], macrocells[1], macrocells[2]};
+  const int sk = format == MDWT_FMT_UINT8 ? kStoreU8 : kStoreF32;
+  if (launch_ranges(d_volume, sk, d3, mc3, iv, iv + 2 * mx, iv + 2 * (mx + my), 1, 0, d_ranges_out,
+                    (float *)g_noalloc_pairs_ptr[dev], nullptr, st, nullptr) != 0)
+    return MDWT_ERR_CUDA;
+  return MDWT_OK;
+}

@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(_HERE, "libmdwt.so")
 STATUS = {
     0: "ok", 1: "bad argument", 2: "CUDA error", 3: "I/O error", 4: "too many channels",
     5: "unsupported", 6: "wrong call order", 7: "out of memory", 8: "device wait timed out",
-    9: "bad raw file name", 10: "sample step cap reached",
+    9: "bad raw file name", 10: "sample step cap reached", 11: "scratch limit of a no-alloc entry point",
 }
 MDWT_HOST_ONLY = -1
 
