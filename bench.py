@@ -42,20 +42,28 @@ def parse_args():
     ap.add_argument("--flush-mib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--res", type=int, nargs=2, default=None, help="override the resolution (smaller profiling cases)")
+    ap.add_argument("--spp", type=int, default=None, help="override samples per pixel")
     return ap.parse_args()
 
 
-def make_scene(name):
+def make_scene(name, res=None, spp=None):
     from mdwtracker_b200 import synthetic as syn
     if name == "c1":
-        return syn.scene_c1()
-    if name == "c2":
-        return syn.scene_c2()
-    if name == "c3":
-        return syn.scene_c3(mode=2)
-    if name == "c3ndda":
-        return syn.scene_c3(mode=0)
-    raise ValueError(name)
+        sc = syn.scene_c1()
+    elif name == "c2":
+        sc = syn.scene_c2()
+    elif name == "c3":
+        sc = syn.scene_c3(mode=2)
+    elif name == "c3ndda":
+        sc = syn.scene_c3(mode=0)
+    else:
+        raise ValueError(name)
+    if res is not None:
+        sc.resolution = (int(res[0]), int(res[1]))
+    if spp is not None:
+        sc.spp = int(spp)
+    return sc
 
 
 def workload_name(sc):
@@ -151,7 +159,7 @@ class ClockSampler:
 def cpu_baseline(sc, budget_s, full=False):
     """Oracle on the host cores over a band of rows of the same frame."""
     from oracle import oracle as orc
-    threads = orc.set_threads(os.cpu_count() or 1)
+    threads = orc.set_threads(len(os.sched_getaffinity(0)))
     o = sc.setup(orc.OracleRenderer())
     w, h = sc.resolution
     # calibrate on 1 row, then size the band for the budget
@@ -173,9 +181,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sc = make_scene(args.config)
+    sc = make_scene(args.config, args.res, args.spp)
     from oracle import oracle as orc
-    threads = orc.set_threads(os.cpu_count() or 1)
+    threads = orc.set_threads(len(os.sched_getaffinity(0)))
     o = sc.setup(orc.OracleRenderer())
     w, h = sc.resolution
     t0 = time.perf_counter()
@@ -230,7 +238,7 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    sc = make_scene(args.config)
+    sc = make_scene(args.config, args.res, args.spp)
     r = sc.setup(Renderer(local))
     w, h = sc.resolution
     stream = torch.cuda.Stream(dev)
