@@ -181,6 +181,14 @@ mdwt_status mdwt_reset_counters(mdwt_ctx *ctx);
 mdwt_status mdwt_enable_pixel_stats(mdwt_ctx *ctx, int enable);
 mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
 
+/* Tracker tuning knobs (no reference counterpart; results do not depend on them).
+ * MDWT_TUNE_POOL: a warp starts new paths only when at least `value` (1..32) of its
+ * lanes wait for one, or when no lane is busy.
+ * MDWT_TUNE_BATCH: at most `value` samples per pixel per trace pass (0 = as many as the
+ * 1 GiB path-record budget allows); the per-pixel sums still run in sample order. */
+enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1 };
+mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
+
 /* Launch bookkeeping: out[0] = kernels launched by this context so far, out[1] = bytes
  * of per-frame parameters a render sends host->device, out[2] = grid and out[3] = block
  * size of the last tracker launch. */

@@ -136,14 +136,21 @@ struct mdwt_ctx {
   bool statsOn = false;
   unsigned long long *dCounters = nullptr;
   unsigned int *dWork = nullptr;
+  uint32_t *dRec = nullptr, *dRecStats = nullptr;   // per-path records of one sample batch
+  float *dPartial = nullptr;                          // running sums between batches
+  uint32_t *dPartialStats = nullptr;
+  size_t recCap = 0, recStatsCap = 0, partialCap = 0, partialStatsCap = 0;
   float *dRanges = nullptr;
   float *dMaj = nullptr;
+  uint16_t *dMask = nullptr;    // per-cell non-zero-majorant channel mask
   size_t M = 0;
   float rootLo[3] = {0, 0, 0}, rootHi[3] = {1, 1, 1};
   float gLo[4] = {0, 0, 0, 0}, gHi[4] = {1, 1, 1, 1};
   std::string err;
   int launches = 0;
   int lastGrid = 0, lastBlock = 0;
+  int pool = 8;       // regeneration pool of the tracker (MDWT_TUNE_POOL)
+  int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
 };
 
 namespace {
@@ -208,6 +215,78 @@ void reset_dt(mdwt_ctx *c) {
   }
   c->dt = std::max(minVoxelSideLength * 0.5f, 1e-4f);
   reset_accum_ids(c);
+}
+
+// Grow a context-owned device buffer to at least `bytes` (contents are not kept).
+mdwt_status grow(mdwt_ctx *c, void **buf, size_t &cap, size_t bytes, const char *what) {
+  if (bytes <= cap && *buf) return MDWT_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc(buf, bytes);
+  if (e != cudaSuccess) return cuda_fail(c, e, what);
+  cap = bytes;
+  return MDWT_OK;
+}
+
+// Conservative screen-space rectangle {x0, y0, x1, y1} (inclusive pixel indices) of the
+// root box: a pixel's rays pass through screen points ((px+j)/W, (py+j)/H), j in [0,1),
+// and hit the box only inside the convex hull of its projected corners.  With a corner
+// at or behind the eye plane the whole frame is traced.  Margin: 3 pixels.
+void cull_rect(const mdwt_ctx *c, int out[4]) {
+  const int W = c->W, H = c->H;
+  out[0] = 0; out[1] = 0; out[2] = W - 1; out[3] = H - 1;
+  const double o[3] = {c->cOrg.x, c->cOrg.y, c->cOrg.z};
+  const double l[3] = {c->cLlc.x, c->cLlc.y, c->cLlc.z};
+  const double h[3] = {c->cHor.x, c->cHor.y, c->cHor.z};
+  const double v[3] = {c->cVer.x, c->cVer.y, c->cVer.z};
+  double n[3], nn = 0, hh = 0, vv = 0, dp = 0;
+  for (int a = 0; a < 3; a++) {
+    n[a] = l[a] + 0.5 * h[a] + 0.5 * v[a] - o[a];
+    nn += n[a] * n[a]; hh += h[a] * h[a]; vv += v[a] * v[a];
+  }
+  nn = std::sqrt(nn);
+  if (!(nn > 0) || !(hh > 0) || !(vv > 0)) return;
+  for (int a = 0; a < 3; a++) { n[a] /= nn; dp += (l[a] - o[a]) * n[a]; }
+  if (!(dp > 0)) return;
+  double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+  for (int k = 0; k < 8; k++) {
+    const double P[3] = {(k & 1) ? c->rootHi[0] : c->rootLo[0], (k & 2) ? c->rootHi[1] : c->rootLo[1],
+                         (k & 4) ? c->rootHi[2] : c->rootLo[2]};
+    double e[3], z = 0, el = 0;
+    for (int a = 0; a < 3; a++) { e[a] = P[a] - o[a]; z += e[a] * n[a]; el += e[a] * e[a]; }
+    if (!std::isfinite(z) || !(z > 1e-3 * std::sqrt(el))) return;
+    const double lam = dp / z;
+    double qa = 0, qb = 0;
+    for (int a = 0; a < 3; a++) {
+      const double q = o[a] + lam * e[a] - l[a];
+      qa += q * h[a];
+      qb += q * v[a];
+    }
+    const double X = qa / hh * W, Y = qb / vv * H;
+    xmin = std::min(xmin, X); xmax = std::max(xmax, X);
+    ymin = std::min(ymin, Y); ymax = std::max(ymax, Y);
+  }
+  if (!std::isfinite(xmin + xmax + ymin + ymax)) return;
+  const double x0 = std::floor(xmin) - 3, x1 = std::floor(xmax) + 3;
+  const double y0 = std::floor(ymin) - 3, y1 = std::floor(ymax) + 3;
+  out[0] = (int)std::max(0.0, std::min((double)W, x0));
+  out[2] = (int)std::max(-1.0, std::min((double)(W - 1), x1));
+  out[1] = (int)std::max(0.0, std::min((double)H, y0));
+  out[3] = (int)std::max(-1.0, std::min((double)(H - 1), y1));
+}
+
+// Per-pixel result of a pixel whose every sample misses: finalColor starts at (0,0,0,1)
+// and gains over((0,0,0,0), (bg,1)) = (bg, 1) per sample (deviceCode.cu:289, 433),
+// summed in sample order, then / spp (deviceCode.cu:435).
+void background_result(const mdwt_ctx *c, float out[4]) {
+  float f[4] = {0.f, 0.f, 0.f, 1.f};
+  const float bg[3] = {c->bg.x, c->bg.y, c->bg.z};
+  for (int s = 0; s < c->spp; s++) {
+    for (int k = 0; k < 3; k++) f[k] += std::fma(bg[k] * 1.0f, 1.0f - 0.0f, 0.0f);
+    f[3] += std::fma(1.0f - 0.0f, 1.0f, 0.0f);
+  }
+  for (int k = 0; k < 4; k++) out[k] = f[k] / (float)c->spp;
 }
 
 // project (renderer.cu:387-392)
@@ -356,6 +435,15 @@ void free_device(mdwt_ctx *c) {
   if (c->dWork) cudaFree(c->dWork);
   if (c->dRanges) cudaFree(c->dRanges);
   if (c->dMaj) cudaFree(c->dMaj);
+  if (c->dMask) cudaFree(c->dMask);
+  c->dMask = nullptr;
+  if (c->dRec) cudaFree(c->dRec);
+  if (c->dRecStats) cudaFree(c->dRecStats);
+  if (c->dPartial) cudaFree(c->dPartial);
+  if (c->dPartialStats) cudaFree(c->dPartialStats);
+  c->dRec = c->dRecStats = c->dPartialStats = nullptr;
+  c->dPartial = nullptr;
+  c->recCap = c->recStatsCap = c->partialCap = c->partialStatsCap = 0;
   c->dAccum = nullptr; c->dFb = nullptr; c->dStats = nullptr; c->dCounters = nullptr;
   c->dWork = nullptr; c->dRanges = nullptr; c->dMaj = nullptr;
 }
@@ -384,6 +472,7 @@ mdwt_status recalc(mdwt_ctx *c) {
   std::memset(&p, 0, sizeof(p));
   p.ranges = c->dRanges;
   p.majorants = c->dMaj;
+  p.mask = c->dMask;
   p.C = (int)c->ch.size();
   p.mode = c->mode;
   p.M = c->M;
@@ -635,6 +724,7 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (mode == 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
   c->inited = true;
   mdwt_status s = build_ranges(c);
   if (s) { c->inited = false; return s; }
@@ -671,7 +761,7 @@ mdwt_status mdwt_set_tf(mdwt_ctx *c, int chn, const float *rgba, int n) {
   mdwt_status s = check_ch(c, chn);
   if (s) return s;
   if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
-  if (!rgba || n <= 0 || n > (1 << 20)) return fail(c, MDWT_ERR_BAD_ARG, "bad colormap");
+  if (!rgba || n <= 0 || n > kMaxTexels) return fail(c, MDWT_ERR_BAD_ARG, "colormap needs 1..16384 texels");
   for (int i = 0; i < 4 * n; i++)
     if (!std::isfinite(rgba[i])) return fail(c, MDWT_ERR_BAD_ARG, "colormap values must be finite");
   TFState &t = c->tf[chn];
@@ -841,6 +931,7 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   p.mode = c->mode;
   p.dt = c->dt;
   p.majorants = c->dMaj;
+  p.mask = c->dMask;
   for (int i = 0; i < p.C; i++) {
     p.vol[i] = c->ch[i].dVol;
     for (int a = 0; a < 3; a++) p.dims[i][a] = (int)c->ch[i].dims[a];
@@ -860,10 +951,44 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   p.stats = c->statsOn ? c->dStats : nullptr;
   p.counters = c->dCounters;
   p.workCounter = c->dWork;
-  p.tilesX = (c->W + 7) / 8;
-  p.numTiles = p.tilesX * ((c->H + 3) / 4);
-  CK(cudaMemsetAsync(c->dWork, 0, sizeof(unsigned int), st), "reset work counter");
-  CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock), "tracker kernel");
+  int rect[4];
+  cull_rect(c, rect);
+  p.cullX0 = rect[0]; p.cullY0 = rect[1]; p.cullX1 = rect[2]; p.cullY1 = rect[3];
+  const int rw = rect[2] - rect[0] + 1, rh = rect[3] - rect[1] + 1;
+  p.tilesX = rw > 0 ? (rw + 7) / 8 : 0;
+  p.numTiles = (rw > 0 && rh > 0) ? p.tilesX * ((rh + 3) / 4) : 0;
+  background_result(c, p.bgFin);
+  p.gOrg = {p.gScale.x * (c->cOrg.x - p.gLo.x), p.gScale.y * (c->cOrg.y - p.gLo.y), p.gScale.z * (c->cOrg.z - p.gLo.z)};
+  p.pool = c->pool;
+  p.vol32 = 1;
+  for (auto &h : c->ch)
+    if ((uint64_t)h.dims[0] * h.dims[1] * h.dims[2] >= (1ull << 32)) p.vol32 = 0;
+  // samples in batches whose path records fit the record budget; the resolve pass
+  // carries the per-pixel running sums across batches in sample order
+  const size_t nrect = p.numTiles > 0 ? (size_t)rw * (size_t)rh : 0;
+  int batch = c->spp;
+  if (nrect > 0 && (size_t)batch * nrect > kRecordBudget) batch = (int)std::max<size_t>(1, kRecordBudget / nrect);
+  if (c->batchCap > 0) batch = std::min(batch, c->batchCap);
+  const bool stats = c->statsOn;
+  mdwt_status s = MDWT_OK;
+  if (nrect > 0) {
+    if ((s = grow(c, (void **)&c->dRec, c->recCap, (size_t)batch * nrect * 4, "records")) != MDWT_OK) return s;
+    if (stats && (s = grow(c, (void **)&c->dRecStats, c->recStatsCap, (size_t)batch * nrect * 4, "record stats")) != MDWT_OK) return s;
+    if (batch < c->spp) {
+      if ((s = grow(c, (void **)&c->dPartial, c->partialCap, nrect * 16, "partial sums")) != MDWT_OK) return s;
+      if (stats && (s = grow(c, (void **)&c->dPartialStats, c->partialStatsCap, nrect * 16, "partial stats")) != MDWT_OK) return s;
+    }
+  }
+  p.records = c->dRec;
+  p.recStats = stats ? c->dRecStats : nullptr;
+  p.partial = c->dPartial;
+  p.partialStats = stats ? c->dPartialStats : nullptr;
+  for (int s0 = 0; s0 < c->spp; s0 += batch) {
+    p.sBase = s0;
+    p.sCount = std::min(batch, c->spp - s0);
+    CK(cudaMemsetAsync(c->dWork, 0, sizeof(unsigned int), st), "reset work counter");
+    CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock), "tracker kernels");
+  }
   // Renderer::Render (renderer.cpp:957-958): the ids the next frame sees are the
   // pre-increment values
   c->accumParam = c->accumID++;
@@ -956,6 +1081,21 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *c, uint32_t *out) {
   CK(cudaDeviceSynchronize(), "sync");
   CK(cudaMemcpy(out, c->dStats, (size_t)c->W * c->H * 16, cudaMemcpyDeviceToHost), "copy stats");
   return MDWT_OK;
+}
+
+mdwt_status mdwt_set_tuning(mdwt_ctx *c, int key, int value) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (key == MDWT_TUNE_POOL) {
+    if (value < 1 || value > 32) return fail(c, MDWT_ERR_BAD_ARG, "pool must be in 1..32");
+    c->pool = value;
+    return MDWT_OK;
+  }
+  if (key == MDWT_TUNE_BATCH) {
+    if (value < 0) return fail(c, MDWT_ERR_BAD_ARG, "batch must be >= 0");
+    c->batchCap = value;
+    return MDWT_OK;
+  }
+  return fail(c, MDWT_ERR_BAD_ARG, "unknown tuning key");
 }
 
 mdwt_status mdwt_get_render_info(const mdwt_ctx *c, int64_t out[4]) {

@@ -37,6 +37,7 @@ struct TrackParams {
   int C, mode;
   float dt;
   const float *majorants;      // [cell*C + ch] (modes 0..2) or [cell] (mode 3)
+  const uint16_t *mask;        // per cell: bit c set when majorants[cell*C + c] != 0
   // channels
   const void *vol[kMaxChannels];
   int dims[kMaxChannels][3];
@@ -56,9 +57,29 @@ struct TrackParams {
   uint32_t *stats;               // 4 per pixel or null
   unsigned long long *counters;  // [0]=samples [1]=rejections [2]=cells [3]=path-samples [4]=capped
   unsigned int *workCounter;     // pixel dispenser, zeroed before the launch
-  int numTiles;                  // 8x4 pixel tiles covering the image
+  // Pixels outside [cullX0, cullX1] x [cullY0, cullY1] certainly miss the root box
+  // (conservative screen-space bound of its 8 corners, 3 px margin): each of their
+  // samples composites the background, so their per-pixel result is the constant
+  // bgFin (sum over spp of the background, / spp), computed on the host.
+  int cullX0, cullY0, cullX1, cullY1;
+  float bgFin[4];
+  int numTiles;                  // 8x4 pixel tiles covering the traced rectangle
   int tilesX;
+  F3 gOrg;                       // gScale * (camOrg - gLo): grid-space ray origin
+  int pool;                      // regenerate paths when this many lanes of a warp wait
+  int chunk;                     // work items a warp takes from the dispenser at once
+  int vol32;                     // every channel has < 2^32 voxels: 32-bit voxel offsets
+  // sample batch [sBase, sBase + sCount) of the frame; one 4-byte record per traced
+  // path, [k * nrect + rect-local pixel], nrect = pixels of the traced rectangle
+  int sBase, sCount;
+  uint32_t *records;
+  uint32_t *recStats;            // per-path density samples | rejections << 16 (stats only)
+  float *partial;                // float4 running sums per rect pixel between batches
+  uint32_t *partialStats;        // uint4 per rect pixel between batches (stats only)
 };
+
+constexpr int kMaxTexels = 16384;          // TF texels addressable by a path record
+constexpr size_t kRecordBudget = size_t(1) << 28;   // records per batch (1 GiB)
 
 // Per-axis voxel intervals of the separable range build: for macrocell index k on
 // one axis, voxels [lo[k], hi[k]] (empty when lo > hi) enter its value range.
@@ -69,7 +90,6 @@ struct AxisIntervals {
 
 // ---- launchers implemented in mdwt_kernels.cu (return cudaError_t as int) ----
 int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block);
-int track_occupancy(int storeKind, int mode, int *blocksPerSM, int *threadsPerBlock);
 
 // Value ranges of one channel into ranges[(cell*C + ch)*2 + {0,1}].
 //   vol: channel voxels; dims; mc grid; intervals per axis (device arrays);
@@ -83,6 +103,7 @@ int launch_ranges_init(float *ranges, size_t count, void *stream, int *launches)
 struct MajorantParams {
   const float *ranges;
   float *majorants;
+  uint16_t *mask;              // per cell: bit c set when channel c's majorant is non-zero
   int C, mode;
   size_t M;
   const float *tfAlpha[kMaxChannels];

@@ -1,0 +1,79 @@
+// mdwt_math.cuh -- device side of the arithmetic specification shared with the CPU
+// oracle: float->int conversion, the TEA-seeded LCG, the project log, and the
+// software texture filter (8-bit fractional weights, clamp addressing).  Every
+// translation unit that includes it is compiled with --fmad=false; fused
+// multiply-adds appear only as explicit fmaf().
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "mdwt_internal.h"
+
+namespace mdwt {
+namespace {
+
+// ------------------------------------------------------------------ arithmetic spec
+__device__ __forceinline__ int f2i(float x) {
+  if (!(x == x)) return 0;
+  if (x >= 2147483648.0f) return 2147483647;
+  if (x <= -2147483648.0f) return (-2147483647 - 1);
+  return (int)x;
+}
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// 4-round TEA of the seed words (Wheeler & Needham 1994), key = SHA-256 IV words 0..3.
+__device__ __forceinline__ uint32_t tea4(uint32_t v0, uint32_t v1) {
+  uint32_t sum = 0;
+#pragma unroll
+  for (int n = 0; n < 4; n++) {
+    sum += 0x9E3779B9u;
+    v0 += ((v1 << 4) + 0x6a09e667u) ^ (v1 + sum) ^ ((v1 >> 5) + 0xbb67ae85u);
+    v1 += ((v0 << 4) + 0x3c6ef372u) ^ (v0 + sum) ^ ((v0 >> 5) + 0xa54ff53au);
+  }
+  return v0;
+}
+// LCG with the Numerical Recipes constants; a draw is the top 24 bits times 2^-24.
+__device__ __forceinline__ float rng_next(uint32_t &s) {
+  s = 1664525u * s + 1013904223u;
+  return (float)(s >> 8) * (1.0f / 16777216.0f);
+}
+
+// log(x) for positive normal x: e*ln2 + 2*atanh(s), s = (m-1)/(m+1), m in (sqrt(1/2), sqrt(2)].
+__device__ __forceinline__ float mlog(float x) {
+  uint32_t b = __float_as_uint(x);
+  int e = (int)((b >> 23) & 0xffu) - 127;
+  float m = __uint_as_float((b & 0x007fffffu) | 0x3f800000u);
+  if (m > 1.41421353816986083984375f) { m = m * 0.5f; e = e + 1; }
+  float s = (m - 1.0f) / (m + 1.0f);
+  float z = s * s;
+  float p = fmaf(z, 1.0f / 9.0f, 1.0f / 7.0f);
+  p = fmaf(z, p, 1.0f / 5.0f);
+  p = fmaf(z, p, 1.0f / 3.0f);
+  float s2 = s + s;
+  float r = fmaf(s2 * z, p, s2);
+  float fe = (float)e;
+  return fmaf(fe, 0.693145751953125f, fmaf(fe, 1.428606765330187e-06f, r));
+}
+
+__device__ __forceinline__ float quant(float a) { return rintf(a * 256.0f) * (1.0f / 256.0f); }
+__device__ __forceinline__ float lerpf(float a, float p, float q) { return fmaf(a, q, (1.0f - a) * p); }
+
+struct Axis { int i0, i1; float a; };
+__device__ __forceinline__ Axis axis(float u, int n) {
+  const float x = fmaf(u, (float)n, -0.5f);
+  const float fl = floorf(x);
+  Axis r;
+  r.a = quant(x - fl);
+  const int i = f2i(fl);
+  r.i0 = clampi(i, 0, n - 1);
+  r.i1 = clampi(i, -1, n - 2) + 1;
+  return r;
+}
+
+template <int SK>
+__device__ __forceinline__ float vox(const void *base, size_t idx) {
+  if (SK == kStoreU8) return (float)__ldg(reinterpret_cast<const uint8_t *>(base) + idx) * 255.0f;
+  return __ldg(reinterpret_cast<const float *>(base) + idx);
+}
+
+}  // namespace
+}  // namespace mdwt

@@ -1,0 +1,570 @@
+// mdwt_track.cu -- the sm_100a tracker: mainRG + baseLineDTCH (-m 0, N-DDA) and
+// altMultiMajDTCH (-m 2, syncDDA) of the reference (deviceCode.cu:283-471, 747-970) with
+// dda3 (dda.h:81-202), as two kernels per batch of samples.
+//
+// trace_kernel: one path-sample per lane at a time.  Work items are (8x4 pixel tile,
+//   sample) pairs, a warp's 32 consecutive items being one tile at one sample; warps take
+//   items in chunks from a global dispenser.  The warp loop has three lane states:
+//   NEED lanes start their next path (TEA seed, jitter, ray, root box, grid transform,
+//   DDA start) together, once `pool` lanes wait or nothing else runs; TRANS lanes walk
+//   channels and macrocells to the next non-zero majorant; STEP lanes take one
+//   Woodcock step (free flight, world-exit test, null-collision test with the trilinear
+//   fetch and the TF).  A finished path writes a 4-byte record: hit flag, channel, TF
+//   texel index and quantized weight -- everything its shaded colour depends on.
+// resolve_kernel: per pixel, the records of the batch in sample order -> shading,
+//   over(colour, background), running sum; after the last batch /spp, the running
+//   mean into the accumulation buffer and RGBA8 (deviceCode.cu:323-471).  Keeping the
+//   reference's per-pixel summation order makes the result bit-identical to a
+//   sequential spp loop.
+// Pixels whose rays certainly miss the root box (outside a conservative screen-space
+// rectangle) are not traced; resolve gives them the background result.
+// Compiled with --fmad=false; fused multiply-adds are the explicit fmaf() of the
+// arithmetic specification shared with the CPU oracle.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mdwt_internal.h"
+#include "mdwt_math.cuh"
+
+namespace mdwt {
+namespace {
+
+constexpr int kTPB = 128;
+constexpr int kMinBlocks = 6;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Path record: bit 31 hit, bits 27..30 channel, bits 13..26 TF texel i0, bit 12 set when
+// i1 == i0 (clamped edge), bits 0..8 quantized weight * 256.  0 = miss.
+__device__ __forceinline__ uint32_t make_record(int ch, const Axis &a) {
+  const uint32_t k = (uint32_t)(a.a * 256.0f);
+  return 0x80000000u | ((uint32_t)ch << 27) | ((uint32_t)a.i0 << 13) | ((a.i1 == a.i0) ? (1u << 12) : 0u) | k;
+}
+
+// Texture axis of a coordinate known to be finite and in [0, 1] (so x in [-0.5, n-0.5]):
+// the same values as axis(), with floor and conversion in one instruction.
+__device__ __forceinline__ Axis axis_in_range(float u, int n) {
+  const float x = fmaf(u, (float)n, -0.5f);
+  const int i = __float2int_rd(x);
+  Axis r;
+  r.a = quant(x - (float)i);
+  r.i0 = i < 0 ? 0 : i;
+  r.i1 = (i < n - 1 ? i : n - 2) + 1;
+  return r;
+}
+
+template <int SK, typename IDX>
+__device__ __forceinline__ float trilinear(const void *base, int X, int Y, const Axis &ax, const Axis &ay, const Axis &az) {
+  const IDX sXY = (IDX)X * (IDX)Y;
+  const IDX z0 = (IDX)az.i0 * sXY, z1 = (IDX)az.i1 * sXY;
+  const IDX y0 = (IDX)ay.i0 * (IDX)X, y1 = (IDX)ay.i1 * (IDX)X;
+  const float v000 = vox<SK>(base, z0 + y0 + ax.i0), v100 = vox<SK>(base, z0 + y0 + ax.i1);
+  const float v010 = vox<SK>(base, z0 + y1 + ax.i0), v110 = vox<SK>(base, z0 + y1 + ax.i1);
+  const float v001 = vox<SK>(base, z1 + y0 + ax.i0), v101 = vox<SK>(base, z1 + y0 + ax.i1);
+  const float v011 = vox<SK>(base, z1 + y1 + ax.i0), v111 = vox<SK>(base, z1 + y1 + ax.i1);
+  const float c00 = lerpf(ax.a, v000, v100);
+  const float c10 = lerpf(ax.a, v010, v110);
+  const float c01 = lerpf(ax.a, v001, v101);
+  const float c11 = lerpf(ax.a, v011, v111);
+  const float c0 = lerpf(ay.a, c00, c10);
+  const float c1 = lerpf(ay.a, c01, c11);
+  return lerpf(az.a, c0, c1);
+}
+
+// Per-channel parameters, staged in shared memory at kernel start: lanes index them by
+// their own channel, which in the constant bank would serialise on divergent indices.
+struct ChanSm {
+  const void *vol;
+  const float *tfAlpha;
+  int X, Y, Z, n;
+  float vd0, vd1, xd0, xd1, os;
+};
+
+// sampleVolumeTexture (deviceCode.cu:122-132): NaN outside [0,1]^3, else trilinear.
+template <int SK>
+__device__ __forceinline__ float sample_volume(const TrackParams &P, const ChanSm &cs, float px, float py, float pz) {
+  if (px < 0.0f || px > 1.0f || py < 0.0f || py > 1.0f || pz < 0.0f || pz > 1.0f) return __int_as_float(0x7fc00000);
+  const Axis ax = axis_in_range(px, cs.X), ay = axis_in_range(py, cs.Y), az = axis_in_range(pz, cs.Z);
+  if (P.vol32) return trilinear<SK, uint32_t>(cs.vol, cs.X, cs.Y, ax, ay, az);
+  return trilinear<SK, size_t>(cs.vol, cs.X, cs.Y, ax, ay, az);
+}
+
+// transferFunction (deviceCode.cu:27-42), alpha part; the lookup axis is returned for
+// the colour of a hit.
+__device__ __forceinline__ float tf_alpha(const ChanSm &cs, float f, Axis &ax) {
+  if (cs.n <= 0) return 0.f;
+  if (f < cs.vd0 || f > cs.vd1) return 0.f;
+  const float r1 = (f - cs.vd0) / (cs.vd1 - cs.vd0);
+  const float r2 = (r1 - cs.xd0) / (cs.xd1 - cs.xd0);
+  ax = axis(r2, cs.n);
+  return lerpf(ax.a, __ldg(cs.tfAlpha + ax.i0), __ldg(cs.tfAlpha + ax.i1)) * cs.os;
+}
+
+__device__ __forceinline__ uint32_t q8(float c) {
+  const float v = fminf(fmaxf(c, 0.f), 1.f);
+  return (uint32_t)f2i(v * 255.0f + 0.5f);
+}
+
+// ------------------------------------------------------------------ 3D-DDA (dda.h:81-202)
+struct DDA {
+  float tnx, tny, tnz;   // t_next
+  float tsx, tsy, tsz;   // t_step
+  int cx, cy, cz;        // cell
+  float rt0, ncb;        // ray_t0, next_cell_begin
+  uint32_t visits;
+};
+
+__device__ __forceinline__ bool dda_init(const TrackParams &P, float dx, float dy, float dz, DDA &d) {
+  const float ox = P.gOrg.x, oy = P.gOrg.y, oz = P.gOrg.z;
+  const float fsx = (float)P.mc[0], fsy = (float)P.mc[1], fsz = (float)P.mc[2];
+  const float rx = 1.0f / dx, ry = 1.0f / dy, rz = 1.0f / dz;
+  const float tlx = (0.0f - ox) * rx, thx = (fsx - ox) * rx;
+  const float tly = (0.0f - oy) * ry, thy = (fsy - oy) * ry;
+  const float tlz = (0.0f - oz) * rz, thz = (fsz - oz) * rz;
+  float nrx = fminf(tlx, thx), nry = fminf(tly, thy), nrz = fminf(tlz, thz);
+  const float frx = fmaxf(tlx, thx), fry = fmaxf(tly, thy), frz = fmaxf(tlz, thz);
+  const float inf = __int_as_float(0x7f800000);
+  if (dx == 0.f) { if (ox < 0.f || ox > fsx) return false; nrx = inf; }   // dda.h:100-101 (t_nr set twice)
+  if (dy == 0.f) { if (oy < 0.f || oy > fsy) return false; nry = inf; }
+  if (dz == 0.f) { if (oz < 0.f || oz > fsz) return false; nrz = inf; }
+  const float rt0 = fmaxf(0.f, fmaxf(fmaxf(nrx, nry), nrz));
+  const float rt1 = fminf(1e20f, fminf(fminf(frx, fry), frz));
+  if (rt0 > rt1) return false;
+  const float ivx = fmaf(rt0, dx, ox), ivy = fmaf(rt0, dy, oy), ivz = fmaf(rt0, dz, oz);
+  const float fcx = fmaxf(0.f, fminf(fsx - 1.f, floorf(ivx)));
+  const float fcy = fmaxf(0.f, fminf(fsy - 1.f, floorf(ivy)));
+  const float fcz = fmaxf(0.f, fminf(fsz - 1.f, floorf(ivz)));
+  const float ex = dx > 0.f ? fcx + 1.f : fcx;
+  const float ey = dy > 0.f ? fcy + 1.f : fcy;
+  const float ez = dz > 0.f ? fcz + 1.f : fcz;
+  d.tsx = fabsf(rx); d.tsy = fabsf(ry); d.tsz = fabsf(rz);
+  d.tnx = (dx == 0.f) ? inf : fabsf(ex - ivx) * d.tsx;
+  d.tny = (dy == 0.f) ? inf : fabsf(ey - ivy) * d.tsy;
+  d.tnz = (dz == 0.f) ? inf : fabsf(ez - ivz) * d.tsz;
+  d.cx = (int)fcx; d.cy = (int)fcy; d.cz = (int)fcz;
+  d.rt0 = rt0;
+  d.ncb = 0.f;
+  d.visits = 0;
+  return true;
+}
+
+// Advance past the current cell (the step direction per axis is the sign of the ray
+// direction, which the world and grid directions share); false when the walk leaves.
+__device__ __forceinline__ bool dda_advance(const TrackParams &P, DDA &d, float wdx, float wdy, float wdz,
+                                            uint32_t maxCells) {
+  const float tc = fminf(fminf(d.tnx, d.tny), d.tnz);
+  d.ncb = tc;
+  if (d.tnx == tc) {
+    d.tnx += d.tsx;
+    if (wdx > 0.f) { if (++d.cx == (int)P.mc[0]) return false; } else { if (--d.cx == -1) return false; }
+  }
+  if (d.tny == tc) {
+    d.tny += d.tsy;
+    if (wdy > 0.f) { if (++d.cy == (int)P.mc[1]) return false; } else { if (--d.cy == -1) return false; }
+  }
+  if (d.tnz == tc) {
+    d.tnz += d.tsz;
+    if (wdz > 0.f) { if (++d.cz == (int)P.mc[2]) return false; } else { if (--d.cz == -1) return false; }
+  }
+  return d.visits < maxCells;
+}
+
+// Normalised grid-space direction of a world direction (deviceCode.cu:773-778).
+__device__ __forceinline__ void grid_dir(const TrackParams &P, float wdx, float wdy, float wdz, float &gx, float &gy,
+                                         float &gz, float &w2g, float &g2w) {
+  gx = P.gScale.x * wdx; gy = P.gScale.y * wdy; gz = P.gScale.z * wdz;
+  const float n2 = fmaf(gz, gz, fmaf(gy, gy, gx * gx));
+  w2g = sqrtf(n2);
+  g2w = 1.f / w2g;
+  const float inv = 1.0f / sqrtf(n2);
+  gx = gx * inv; gy = gy * inv; gz = gz * inv;
+}
+
+enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_DONE = 3 };
+enum : int { A_CHAN = 0, A_ADVANCE = 1, A_NEWDDA = 2 };
+
+template <int MODE, int SK, bool STATS>
+__global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_constant__ TrackParams P) {
+  const int C = P.C;
+  const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned total = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
+  const int rw = P.cullX1 - P.cullX0 + 1;
+  const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
+  uint32_t totSamp = 0, totRej = 0, totCell = 0, totPaths = 0, totCap = 0;
+
+  __shared__ ChanSm sch[kMaxChannels];
+  if (threadIdx.x < (unsigned)C) {
+    const int c = threadIdx.x;
+    ChanSm cs;
+    cs.vol = P.vol[c];
+    cs.tfAlpha = P.tfAlpha[c];
+    cs.X = P.dims[c][0]; cs.Y = P.dims[c][1]; cs.Z = P.dims[c][2];
+    cs.n = P.tfN[c];
+    cs.vd0 = P.vd[c][0]; cs.vd1 = P.vd[c][1];
+    cs.xd0 = P.xd[c][0]; cs.xd1 = P.xd[c][1];
+    cs.os = P.os[c];
+    sch[c] = cs;
+  }
+  __syncthreads();
+
+  unsigned qNext = 0, qEnd = 0;                // this warp's share of the item dispenser
+  int st = S_NEED, act = A_CHAN;
+  size_t recIdx = 0;
+  uint32_t pSamp = 0, pRej = 0;                // per-path event counts (STATS)
+  uint32_t rng = 0, steps = 0, record = 0;
+  float wdx = 1.f, wdy = 1.f, wdz = 1.f, t1w = 0.f, w2g = 0.f, g2w = 0.f;
+  DDA d;
+  d.visits = 0;
+  int ch = 0, cellID = 0;
+  uint32_t cmask = 0;                          // non-zero-majorant channels of the current cell
+  float maj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f;
+  bool capped = false;
+
+  auto enter_cell = [&]() {  // cell_t0 / cell_t1 of the DDA lambda call (dda.h:164-170)
+    const float tc = fminf(fminf(d.tnx, d.tny), d.tnz);
+    ct0 = d.rt0 + d.ncb;
+    ct1 = d.rt0 + fminf(tc, 1e20f);
+    d.visits++;
+    totCell++;
+    cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
+    cmask = __ldg(P.mask + cellID);
+  };
+  auto finish = [&]() {
+    P.records[recIdx] = capped ? 0u : record;
+    if (STATS) P.recStats[recIdx] = (pSamp < 0xffffu ? pSamp : 0xffffu) | ((pRej < 0xffffu ? pRej : 0xffffu) << 16);
+    totPaths++;
+    if (capped) totCap++;
+    st = S_NEED;
+  };
+
+  while (true) {
+    // ---------------- pooled path start: waiting lanes take consecutive items together
+    const unsigned need = __ballot_sync(kFull, st == S_NEED);
+    const unsigned busy = __ballot_sync(kFull, st == S_TRANS || st == S_STEP);
+    if (need == 0u && busy == 0u) break;  // every lane is done
+    if (need != 0u && (busy == 0u || __popc(need) >= P.pool)) {
+      const unsigned n = __popc(need);
+      const unsigned rank = __popc(need & ((1u << lane) - 1u));
+      unsigned avail = qEnd - qNext, base = 0;
+      if (avail < n) {
+        if (lane == 0) base = atomicAdd(P.workCounter, (unsigned)P.chunk);
+        base = __shfl_sync(kFull, base, 0);
+      }
+      unsigned item = rank < avail ? qNext + rank : base + (rank - avail);
+      if (avail < n) { qNext = base + (n - avail); qEnd = base + (unsigned)P.chunk; }
+      else qNext += n;
+      if (st == S_NEED) {
+        if (item >= total) {
+          st = S_DONE;
+        } else {
+          const unsigned tile = item / (32u * (unsigned)P.sCount);
+          const unsigned rem = item - tile * 32u * (unsigned)P.sCount;
+          const int k = (int)(rem >> 5), w = (int)(rem & 31u);
+          const int lx = (int)(tile % (unsigned)P.tilesX) * 8 + (w & 7);
+          const int ly = (int)(tile / (unsigned)P.tilesX) * 4 + (w >> 3);
+          const int px = P.cullX0 + lx, py = P.cullY0 + ly;
+          if (px <= P.cullX1 && py <= P.cullY1) {
+            const int s = P.sBase + k;
+            recIdx = (size_t)k * nrect + (size_t)ly * rw + lx;
+            record = 0;
+            capped = false;
+            steps = 0;
+            pSamp = pRej = 0;
+            // seeding, jitter, generateRay (deviceCode.cu:293-298, 61-76)
+            const uint32_t seed = (uint32_t)P.W * (uint32_t)P.H * (P.frameParam + 1u) * (uint32_t)(s + 1);
+            rng = tea4((uint32_t)px + seed, (uint32_t)py + seed);
+            const float jit = rng_next(rng);
+            const float sxf = ((float)px + jit) / (float)P.W;
+            const float syf = ((float)py + jit) / (float)P.H;
+            float dx = fmaf(syf, P.camVer.x, fmaf(sxf, P.camHor.x, P.camLlc.x));
+            float dy = fmaf(syf, P.camVer.y, fmaf(sxf, P.camHor.y, P.camLlc.y));
+            float dz = fmaf(syf, P.camVer.z, fmaf(sxf, P.camHor.z, P.camLlc.z));
+            if (fabsf(dx) < 1e-5f) dx = 1e-5f;
+            if (fabsf(dy) < 1e-5f) dy = 1e-5f;
+            if (fabsf(dz) < 1e-5f) dz = 1e-5f;
+            dx = dx - P.camOrg.x; dy = dy - P.camOrg.y; dz = dz - P.camOrg.z;
+            const float inv = 1.0f / sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+            wdx = dx * inv; wdy = dy * inv; wdz = dz * inv;
+            // volumeIntersection against the union box (deviceCode.cu:1676-1726)
+            const float frx = 1.0f / wdx, fry = 1.0f / wdy, frz = 1.0f / wdz;
+            const float t1 = (P.rootLo.x - P.camOrg.x) * frx, t2 = (P.rootHi.x - P.camOrg.x) * frx;
+            const float t3 = (P.rootLo.y - P.camOrg.y) * fry, t4 = (P.rootHi.y - P.camOrg.y) * fry;
+            const float t5 = (P.rootLo.z - P.camOrg.z) * frz, t6 = (P.rootHi.z - P.camOrg.z) * frz;
+            const float th0 = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
+            const float th1 = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
+            if (th1 < 0 || th0 >= th1) {
+              finish();
+            } else {
+              t1w = fminf(1e20f, th1);
+              float gx, gy, gz;
+              grid_dir(P, wdx, wdy, wdz, gx, gy, gz, w2g, g2w);
+              ch = 0;
+              st = S_TRANS;
+              if (MODE == 2) {
+                if (dda_init(P, gx, gy, gz, d)) {
+                  enter_cell();
+                  lim = ct1;
+                  act = A_CHAN;
+                } else {
+                  finish();
+                }
+              } else {
+                lim = 1e20f;
+                act = A_NEWDDA;
+              }
+            }
+          }
+        }
+      }
+    }
+
+    // ---------------- transitions: walk channels / cells to the next non-zero majorant
+    if (st == S_TRANS) {
+      bool stepping = false;
+      while (true) {
+        if (MODE == 2) {
+          if (act == A_ADVANCE) {
+            if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) break;
+            enter_cell();
+            lim = ct1;
+            ch = 0;
+            act = A_CHAN;
+          }
+          // next channel of this cell with a non-zero majorant (zero ones are skipped
+          // without draws, deviceCode.cu:794-797)
+          const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
+          if (rem == 0u) {  // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
+            if (record) break;
+            act = A_ADVANCE;
+            continue;
+          }
+          ch += __ffs(rem) - 1;
+          maj = __ldg(P.majorants + (size_t)cellID * C + ch);
+          t = ct0;
+          stepping = true;
+          break;
+        } else {
+          if (act == A_NEWDDA) {  // one full traversal per channel (deviceCode.cu:965-969)
+            if (ch >= C) break;
+            float gx, gy, gz, a, b;
+            grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
+            if (!dda_init(P, gx, gy, gz, d)) { ch++; continue; }
+            enter_cell();
+          } else if (act == A_ADVANCE) {
+            if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; act = A_NEWDDA; continue; }
+            enter_cell();
+          }
+          act = A_CHAN;
+          if ((cmask >> ch) & 1u) {  // zero-majorant cells are skipped (deviceCode.cu:893-894)
+            maj = __ldg(P.majorants + (size_t)cellID * C + ch);
+            t = ct0;
+            stepping = true;
+            break;
+          }
+          act = A_ADVANCE;
+        }
+      }
+      if (stepping) st = S_STEP;
+      else finish();
+    }
+
+    // ---------------- one Woodcock step
+    if (st == S_STEP) {
+      if (++steps >= kMaxStepsPerSample) {
+        capped = true;
+        finish();
+      } else {
+        const float u = rng_next(rng);
+        t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+        if (MODE == 2 ? (t >= lim) : (t >= ct1)) {
+          if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
+          st = S_TRANS;
+        } else if (MODE == 0 && lim < t) {
+          ch++; act = A_NEWDDA; st = S_TRANS;
+        } else {
+          const float tW = t * g2w;
+          const float xs = fmaf(tW, wdx, P.camOrg.x) * P.w2u.x;
+          const float ys = fmaf(tW, wdy, P.camOrg.y) * P.w2u.y;
+          const float zs = fmaf(tW, wdz, P.camOrg.z) * P.w2u.z;
+          if (tW >= t1w) {
+            if (STATS) pRej++;
+            totRej++;
+            if (MODE == 2 && ch == C - 1) finish();
+            else { ch++; act = MODE == 2 ? A_CHAN : A_NEWDDA; st = S_TRANS; }
+          } else {
+            const float thr = rng_next(rng) * maj;
+            const ChanSm &cs = sch[ch];
+            const float v = sample_volume<SK>(P, cs, xs, ys, zs);
+            if (STATS) pSamp++;
+            totSamp++;
+            bool rejected = MODE == 2;
+            if (v == v) {
+              Axis tax;
+              const float a = tf_alpha(cs, v, tax);
+              if (a > 0.0f && thr < a) {
+                record = make_record(ch, tax);
+                lim = fminf(t, lim);
+                if (MODE == 0) { ch++; act = A_NEWDDA; st = S_TRANS; }
+              } else {
+                rejected = true;
+              }
+            }
+            if (rejected) {
+              if (STATS) pRej++;
+              totRej++;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // ---------------- counters: warp reduction, one atomic per warp and counter
+  unsigned long long v[5] = {totSamp, totRej, totCell, totPaths, totCap};
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(kFull, v[k], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+      if (v[k]) atomicAdd(P.counters + k, v[k]);
+  }
+}
+
+// Running mean into the accumulation buffer, RGBA8 write (deviceCode.cu:435, 463-471).
+template <bool STATS>
+__device__ __forceinline__ void write_pixel(const TrackParams &P, int px, int py, float o0, float o1, float o2, float o3,
+                                            uint4 st) {
+  const size_t pix = (size_t)px + (size_t)P.W * (size_t)py;
+  if (P.accumulate) {
+    float4 *ap = reinterpret_cast<float4 *>(P.accum) + pix;
+    const float4 prev = *ap;
+    const float k = (float)P.accumParam, k1 = (float)(P.accumParam + 1u);
+    o0 = fmaf(k, prev.x, o0) / k1;
+    o1 = fmaf(k, prev.y, o1) / k1;
+    o2 = fmaf(k, prev.z, o2) / k1;
+    o3 = fmaf(k, prev.w, o3) / k1;
+    *ap = make_float4(o0, o1, o2, o3);
+  }
+  const int fx = P.mirror ? (P.W - 1 - px) : px;
+  P.fb[(size_t)fx + (size_t)P.W * (size_t)py] = q8(o0) | (q8(o1) << 8) | (q8(o2) << 16) | (q8(o3) << 24);
+  if (STATS) reinterpret_cast<uint4 *>(P.stats)[pix] = st;
+}
+
+template <bool STATS>
+__global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ TrackParams P) {
+  const unsigned npix = (unsigned)P.W * (unsigned)P.H;
+  const int rw = P.cullX1 - P.cullX0 + 1;
+  const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
+  const bool last = P.sBase + P.sCount == P.spp;
+  const float kd = (1.0f * 1.0f) * P.lightIntensity;   // diffuse * shadow * lightIntensity (defaults)
+  const float ks = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
+  uint32_t culledPaths = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+    const int px = (int)(i % (unsigned)P.W), py = (int)(i / (unsigned)P.W);
+    if (px < P.cullX0 || px > P.cullX1 || py < P.cullY0 || py > P.cullY1) {
+      if (last) {
+        write_pixel<STATS>(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], P.bgFin[3], make_uint4(0u, 0u, 0u, 0u));
+        culledPaths += (uint32_t)P.spp;
+      }
+      continue;
+    }
+    const size_t q = (size_t)(py - P.cullY0) * rw + (px - P.cullX0);
+    float4 f = make_float4(0.f, 0.f, 0.f, 1.f);
+    uint4 sv = make_uint4(0u, 0u, 0u, 0u);
+    if (P.sBase > 0) {
+      f = reinterpret_cast<const float4 *>(P.partial)[q];
+      if (STATS) sv = reinterpret_cast<const uint4 *>(P.partialStats)[q];
+    }
+    for (int k = 0; k < P.sCount; k++) {
+      const uint32_t r = P.records[(size_t)k * nrect + q];
+      float cr = 0.f, cg = 0.f, cb = 0.f, ca = 0.f;
+      if (r) {
+        const int ch = (int)((r >> 27) & 15u);
+        const int i0 = (int)((r >> 13) & 0x3fffu);
+        const int i1 = ((r >> 12) & 1u) ? i0 : i0 + 1;
+        const float a = (float)(r & 0x1ffu) * (1.0f / 256.0f);
+        const float *R = P.tfRgba[ch];
+        const float ar = lerpf(a, __ldg(R + 4 * i0 + 0), __ldg(R + 4 * i1 + 0));
+        const float ag = lerpf(a, __ldg(R + 4 * i0 + 1), __ldg(R + 4 * i1 + 1));
+        const float ab = lerpf(a, __ldg(R + 4 * i0 + 2), __ldg(R + 4 * i1 + 2));
+        const F3 sc = P.matSpec[ch];
+        const float mr = fmaf(ar, 0.75f, sc.x * 0.25f);
+        const float mg = fmaf(ag, 0.75f, sc.y * 0.25f);
+        const float mb = fmaf(ab, 0.75f, sc.z * 0.25f);
+        cr = fmaf(P.ambient, mr, fmaf(ks, mr, kd * ar));
+        cg = fmaf(P.ambient, mg, fmaf(ks, mg, kd * ag));
+        cb = fmaf(P.ambient, mb, fmaf(ks, mb, kd * ab));
+        ca = 1.0f;
+        if (STATS) { sv.z++; sv.w ^= (uint32_t)(ch + 1) << ((P.sBase + k) & 15); }
+      }
+      if (STATS) {
+        const uint32_t e = P.recStats[(size_t)k * nrect + q];
+        sv.x += e & 0xffffu;
+        sv.y += e >> 16;
+      }
+      const float oma = 1.0f - ca;
+      f.x += fmaf(P.bg.x * 1.0f, oma, cr);
+      f.y += fmaf(P.bg.y * 1.0f, oma, cg);
+      f.z += fmaf(P.bg.z * 1.0f, oma, cb);
+      f.w += fmaf(oma, 1.0f, ca);
+    }
+    if (last) {
+      const float fs = (float)P.spp;
+      write_pixel<STATS>(P, px, py, f.x / fs, f.y / fs, f.z / fs, f.w / fs, sv);
+    } else {
+      reinterpret_cast<float4 *>(P.partial)[q] = f;
+      if (STATS) reinterpret_cast<uint4 *>(P.partialStats)[q] = sv;
+    }
+  }
+  unsigned long long cp = culledPaths;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cp += __shfl_down_sync(kFull, cp, o);
+  if ((threadIdx.x & 31) == 0 && cp) atomicAdd(P.counters + 3, cp);
+}
+
+template <int MODE, int SK, bool STATS>
+int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
+  int bps = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_kernel<MODE, SK, STATS>, kTPB, 0);
+  if (e != cudaSuccess) return (int)e;
+  if (bps < 1) bps = 1;
+  *grid = numSMs * bps;
+  // dispenser chunk: about 8 chunks per warp, 32..256 items (multiples of a tile)
+  TrackParams q = p;
+  const size_t items = (size_t)p.numTiles * 32u * (size_t)p.sCount;
+  size_t chunk = items / ((size_t)*grid * (kTPB / 32) * 8);
+  chunk = chunk < 32 ? 32 : (chunk > 256 ? 256 : chunk & ~(size_t)31);
+  q.chunk = (int)chunk;
+  if (p.numTiles > 0) trace_kernel<MODE, SK, STATS><<<*grid, kTPB, 0, st>>>(q);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  const size_t npix = (size_t)p.W * p.H;
+  size_t g = (npix + 255) / 256;
+  if (g > (size_t)numSMs * 8) g = (size_t)numSMs * 8;
+  resolve_kernel<STATS><<<(unsigned)g, 256, 0, st>>>(p);
+  return (int)cudaGetLastError();
+}
+
+template <int MODE, int SK>
+int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
+  return p.stats ? launch_t<MODE, SK, true>(p, st, numSMs, grid) : launch_t<MODE, SK, false>(p, st, numSMs, grid);
+}
+
+}  // namespace
+
+// One batch of samples [sBase, sBase + sCount): trace + resolve on `stream`.
+int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block) {
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (p.mode == 2) rc = storeKind == kStoreU8 ? launch_s<2, kStoreU8>(p, st, numSMs, grid) : launch_s<2, kStoreF32>(p, st, numSMs, grid);
+  else if (p.mode == 0) rc = storeKind == kStoreU8 ? launch_s<0, kStoreU8>(p, st, numSMs, grid) : launch_s<0, kStoreF32>(p, st, numSMs, grid);
+  else return (int)cudaErrorInvalidValue;
+  *block = kTPB;
+  if (launches) *launches += p.numTiles > 0 ? 2 : 1;
+  return rc;
+}
+
+}  // namespace mdwt

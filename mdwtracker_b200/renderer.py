@@ -284,6 +284,10 @@ class Renderer:
         self._call("get_ranges", out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.reshape(n, 2)
 
+    def setTuning(self, key: int, value: int):
+        """Tracker tuning knob (0 = regeneration pool); results do not depend on it."""
+        self._call("set_tuning", C.c_int(key), C.c_int(value))
+
     def renderInfo(self):
         """(kernels launched so far, per-frame parameter bytes, last grid, last block)."""
         out = (C.c_int64 * 4)()

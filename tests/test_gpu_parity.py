@@ -180,6 +180,18 @@ def test_camera_edge_cases(oracle, cam):
         run_frames(p, o, 1)
 
 
+@pytest.mark.parametrize("mode,batch,pool", [(2, 3, 1), (0, 5, 32), (2, 1, 8), (0, 0, 4)])
+def test_sample_batches_and_pool_sizes(oracle, mode, batch, pool):
+    """Path records resolved over several sample batches (running sums carried between
+    passes) and any regeneration pool give the oracle's sequential spp loop exactly."""
+    vols = [noise_u8(32, 0.25, 90), noise_u8(32, 0.2, 91)]
+    tfs = [syn.ramp_tf(syn.HUES[0]), syn.ramp_tf(syn.HUES[1])]
+    p, o = make_pair(oracle, vols, tfs, mode, (4, 4, 4), (40, 36), 11)
+    p.setTuning(1, batch)
+    p.setTuning(0, pool)
+    run_frames(p, o, 2)
+
+
 def test_no_tf_and_empty_volume(oracle):
     """A channel without a colour map is invisible; an all-zero volume renders the background."""
     vols = [np.zeros((16, 16, 16), np.uint8), noise_u8(16, 0.3, 80)]
