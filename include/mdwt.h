@@ -185,8 +185,10 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * MDWT_TUNE_POOL: a warp starts new paths only when at least `value` (1..32) of its
  * lanes wait for one, or when no lane is busy.
  * MDWT_TUNE_BATCH: at most `value` samples per pixel per trace pass (0 = as many as the
- * 1 GiB path-record budget allows); the per-pixel sums still run in sample order. */
-enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1 };
+ * 1 GiB path-record budget allows); the per-pixel sums still run in sample order.
+ * MDWT_TUNE_TRIPS: transition/free-flight trips (1..64) a warp takes per round before
+ * it evaluates its pending density samples together. */
+enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2 };
 mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
 
 /* Launch bookkeeping: out[0] = kernels launched by this context so far, out[1] = bytes

@@ -151,6 +151,7 @@ struct mdwt_ctx {
   int lastGrid = 0, lastBlock = 0;
   int pool = 8;       // regeneration pool of the tracker (MDWT_TUNE_POOL)
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
+  int trips = 2;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
 };
 
 namespace {
@@ -960,6 +961,7 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   background_result(c, p.bgFin);
   p.gOrg = {p.gScale.x * (c->cOrg.x - p.gLo.x), p.gScale.y * (c->cOrg.y - p.gLo.y), p.gScale.z * (c->cOrg.z - p.gLo.z)};
   p.pool = c->pool;
+  p.trips = c->trips;
   p.vol32 = 1;
   for (auto &h : c->ch)
     if ((uint64_t)h.dims[0] * h.dims[1] * h.dims[2] >= (1ull << 32)) p.vol32 = 0;
@@ -1088,6 +1090,11 @@ mdwt_status mdwt_set_tuning(mdwt_ctx *c, int key, int value) {
   if (key == MDWT_TUNE_POOL) {
     if (value < 1 || value > 32) return fail(c, MDWT_ERR_BAD_ARG, "pool must be in 1..32");
     c->pool = value;
+    return MDWT_OK;
+  }
+  if (key == MDWT_TUNE_TRIPS) {
+    if (value < 1 || value > 64) return fail(c, MDWT_ERR_BAD_ARG, "trips must be in 1..64");
+    c->trips = value;
     return MDWT_OK;
   }
   if (key == MDWT_TUNE_BATCH) {

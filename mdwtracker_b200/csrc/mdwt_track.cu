@@ -179,7 +179,7 @@ __device__ __forceinline__ void grid_dir(const TrackParams &P, float wdx, float 
   gx = gx * inv; gy = gy * inv; gz = gz * inv;
 }
 
-enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_DONE = 3 };
+enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_SAMPLE = 3, S_DONE = 4 };
 enum : int { A_CHAN = 0, A_ADVANCE = 1, A_NEWDDA = 2 };
 
 template <int MODE, int SK, bool STATS>
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
   d.visits = 0;
   int ch = 0, cellID = 0;
   uint32_t cmask = 0;                          // non-zero-majorant channels of the current cell
-  float maj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f;
+  float maj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f, tW = 0.f;
   bool capped = false;
 
   auto enter_cell = [&]() {  // cell_t0 / cell_t1 of the DDA lambda call (dda.h:164-170)
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
   while (true) {
     // ---------------- pooled path start: waiting lanes take consecutive items together
     const unsigned need = __ballot_sync(kFull, st == S_NEED);
-    const unsigned busy = __ballot_sync(kFull, st == S_TRANS || st == S_STEP);
+    const unsigned busy = __ballot_sync(kFull, st == S_TRANS || st == S_STEP || st == S_SAMPLE);
     if (need == 0u && busy == 0u) break;  // every lane is done
     if (need != 0u && (busy == 0u || __popc(need) >= P.pool)) {
       const unsigned n = __popc(need);
@@ -318,105 +318,118 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
       }
     }
 
-    // ---------------- transitions: walk channels / cells to the next non-zero majorant
-    if (st == S_TRANS) {
-      bool stepping = false;
-      while (true) {
-        if (MODE == 2) {
-          if (act == A_ADVANCE) {
-            if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) break;
-            enter_cell();
-            lim = ct1;
-            ch = 0;
-            act = A_CHAN;
-          }
-          // next channel of this cell with a non-zero majorant (zero ones are skipped
-          // without draws, deviceCode.cu:794-797)
-          const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
-          if (rem == 0u) {  // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
-            if (record) break;
-            act = A_ADVANCE;
-            continue;
-          }
-          ch += __ffs(rem) - 1;
-          maj = __ldg(P.majorants + (size_t)cellID * C + ch);
-          t = ct0;
-          stepping = true;
-          break;
-        } else {
-          if (act == A_NEWDDA) {  // one full traversal per channel (deviceCode.cu:965-969)
-            if (ch >= C) break;
-            float gx, gy, gz, a, b;
-            grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
-            if (!dda_init(P, gx, gy, gz, d)) { ch++; continue; }
-            enter_cell();
-          } else if (act == A_ADVANCE) {
-            if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; act = A_NEWDDA; continue; }
-            enter_cell();
-          }
-          act = A_CHAN;
-          if ((cmask >> ch) & 1u) {  // zero-majorant cells are skipped (deviceCode.cu:893-894)
+    // ---------------- phase 1: each lane transitions and draws until it holds a
+    // tentative collision inside the volume (a pending density sample) or its path ends;
+    // a few trips per round, the lanes that are ready wait
+    for (int trip = 0; trip < P.trips; trip++) {
+      if (!__any_sync(kFull, st == S_TRANS || st == S_STEP)) break;
+      // transitions: walk channels / cells to the next non-zero majorant
+      if (st == S_TRANS) {
+        bool stepping = false;
+        while (true) {
+          if (MODE == 2) {
+            if (act == A_ADVANCE) {
+              if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) break;
+              enter_cell();
+              lim = ct1;
+              ch = 0;
+              act = A_CHAN;
+            }
+            // next channel of this cell with a non-zero majorant (zero ones are skipped
+            // without draws, deviceCode.cu:794-797)
+            const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
+            if (rem == 0u) {  // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
+              if (record) break;
+              act = A_ADVANCE;
+              continue;
+            }
+            ch += __ffs(rem) - 1;
             maj = __ldg(P.majorants + (size_t)cellID * C + ch);
             t = ct0;
             stepping = true;
             break;
-          }
-          act = A_ADVANCE;
-        }
-      }
-      if (stepping) st = S_STEP;
-      else finish();
-    }
-
-    // ---------------- one Woodcock step
-    if (st == S_STEP) {
-      if (++steps >= kMaxStepsPerSample) {
-        capped = true;
-        finish();
-      } else {
-        const float u = rng_next(rng);
-        t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
-        if (MODE == 2 ? (t >= lim) : (t >= ct1)) {
-          if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
-          st = S_TRANS;
-        } else if (MODE == 0 && lim < t) {
-          ch++; act = A_NEWDDA; st = S_TRANS;
-        } else {
-          const float tW = t * g2w;
-          const float xs = fmaf(tW, wdx, P.camOrg.x) * P.w2u.x;
-          const float ys = fmaf(tW, wdy, P.camOrg.y) * P.w2u.y;
-          const float zs = fmaf(tW, wdz, P.camOrg.z) * P.w2u.z;
-          if (tW >= t1w) {
-            if (STATS) pRej++;
-            totRej++;
-            if (MODE == 2 && ch == C - 1) finish();
-            else { ch++; act = MODE == 2 ? A_CHAN : A_NEWDDA; st = S_TRANS; }
           } else {
-            const float thr = rng_next(rng) * maj;
-            const ChanSm &cs = sch[ch];
-            const float v = sample_volume<SK>(P, cs, xs, ys, zs);
-            if (STATS) pSamp++;
-            totSamp++;
-            bool rejected = MODE == 2;
-            if (v == v) {
-              Axis tax;
-              const float a = tf_alpha(cs, v, tax);
-              if (a > 0.0f && thr < a) {
-                record = make_record(ch, tax);
-                lim = fminf(t, lim);
-                if (MODE == 0) { ch++; act = A_NEWDDA; st = S_TRANS; }
-              } else {
-                rejected = true;
-              }
+            if (act == A_NEWDDA) {  // one full traversal per channel (deviceCode.cu:965-969)
+              if (ch >= C) break;
+              float gx, gy, gz, a, b;
+              grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
+              if (!dda_init(P, gx, gy, gz, d)) { ch++; continue; }
+              enter_cell();
+            } else if (act == A_ADVANCE) {
+              if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; act = A_NEWDDA; continue; }
+              enter_cell();
             }
-            if (rejected) {
+            act = A_CHAN;
+            if ((cmask >> ch) & 1u) {  // zero-majorant cells are skipped (deviceCode.cu:893-894)
+              maj = __ldg(P.majorants + (size_t)cellID * C + ch);
+              t = ct0;
+              stepping = true;
+              break;
+            }
+            act = A_ADVANCE;
+          }
+        }
+        if (stepping) st = S_STEP;
+        else finish();
+      }
+      // free-flight draw (deviceCode.cu:800-820, 908-930)
+      if (st == S_STEP) {
+        if (++steps >= kMaxStepsPerSample) {
+          capped = true;
+          finish();
+        } else {
+          const float u = rng_next(rng);
+          t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+          if (MODE == 2 ? (t >= lim) : (t >= ct1)) {
+            if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
+            st = S_TRANS;
+          } else if (MODE == 0 && lim < t) {
+            ch++; act = A_NEWDDA; st = S_TRANS;
+          } else {
+            tW = t * g2w;
+            if (tW >= t1w) {  // world exit
               if (STATS) pRej++;
               totRej++;
+              if (MODE == 2 && ch == C - 1) finish();
+              else { ch++; act = MODE == 2 ? A_CHAN : A_NEWDDA; st = S_TRANS; }
+            } else {
+              st = S_SAMPLE;
             }
           }
         }
       }
     }
+    __syncwarp();
+
+    // ---------------- phase 2: the pending density samples, together
+    if (st == S_SAMPLE) {
+      const float xs = fmaf(tW, wdx, P.camOrg.x) * P.w2u.x;
+      const float ys = fmaf(tW, wdy, P.camOrg.y) * P.w2u.y;
+      const float zs = fmaf(tW, wdz, P.camOrg.z) * P.w2u.z;
+      const float thr = rng_next(rng) * maj;
+      const ChanSm &cs = sch[ch];
+      const float v = sample_volume<SK>(P, cs, xs, ys, zs);
+      if (STATS) pSamp++;
+      totSamp++;
+      st = S_STEP;
+      bool rejected = MODE == 2;
+      if (v == v) {
+        Axis tax;
+        const float a = tf_alpha(cs, v, tax);
+        if (a > 0.0f && thr < a) {
+          record = make_record(ch, tax);
+          lim = fminf(t, lim);
+          if (MODE == 0) { ch++; act = A_NEWDDA; st = S_TRANS; }
+        } else {
+          rejected = true;
+        }
+      }
+      if (rejected) {
+        if (STATS) pRej++;
+        totRej++;
+      }
+    }
+    __syncwarp();
   }
 
   // ---------------- counters: warp reduction, one atomic per warp and counter
