@@ -17,16 +17,43 @@ renderer cubes alpha, renderer.cpp:1100).
 from __future__ import annotations
 
 from dataclasses import dataclass, field
+import os
+import tempfile
 from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
 
-def _upsample(lattice: np.ndarray, n: int) -> np.ndarray:
-    from scipy.ndimage import zoom
-    z = n / lattice.shape[0]
-    out = zoom(lattice, z, order=1, mode="nearest", grid_mode=True)
-    return out[:n, :n, :n]
+def _upsample(lattice: np.ndarray, n: int):
+    """Trilinear upsampling of a cubic lattice to n^3 (torch on the CPU: deterministic,
+    independent of the thread count)."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(lattice, dtype=np.float32))[None, None]
+    return torch.nn.functional.interpolate(t, size=(n, n, n), mode="trilinear", align_corners=False)[0, 0]
+
+
+_CACHE_DIR = os.environ.get("MDWT_SYNTH_CACHE", os.path.join(tempfile.gettempdir(), "mdwt_synth_cache"))
+
+
+def _cached(key: str, make):
+    """Large generated volumes are kept in a temp-dir cache (keyed by generator and
+    parameters) so that runs on one machine share identical inputs."""
+    path = os.path.join(_CACHE_DIR, key + ".npy")
+    if os.path.exists(path):
+        try:
+            return np.load(path)
+        except Exception:
+            pass
+    v = make()
+    if v.nbytes >= (64 << 20):
+        try:
+            os.makedirs(_CACHE_DIR, exist_ok=True)
+            tmp = path + f".{os.getpid()}.tmp"
+            np.save(tmp, v)
+            os.replace(tmp + ".npy" if not tmp.endswith(".npy") else tmp, path)
+        except Exception:
+            pass
+    return v
 
 
 def blobs(n: int = 64, nblobs: int = 16, seed: int = 1) -> np.ndarray:
@@ -44,39 +71,52 @@ def blobs(n: int = 64, nblobs: int = 16, seed: int = 1) -> np.ndarray:
 
 
 def value_noise(n: int, octaves: int, seed: int, base: int = 4) -> np.ndarray:
+    """Sum of `octaves` trilinearly upsampled random lattices (4, 8, 16, ... per side),
+    amplitude halving per octave."""
+    import torch
     rng = np.random.default_rng(seed)
-    out = np.zeros((n, n, n), dtype=np.float32)
+    out = torch.zeros((n, n, n), dtype=torch.float32)
     amp = 1.0
     for o in range(octaves):
         res = min(base * (2 ** o), n)
         lattice = rng.random((res, res, res), dtype=np.float32)
         out += amp * _upsample(lattice, n)
         amp *= 0.5
-    return out
+    return out.numpy()
 
 
 def value_noise_sparse(n: int = 256, occupancy: float = 0.2, seed: int = 2, octaves: int = 4) -> np.ndarray:
-    f = value_noise(n, octaves, seed)
-    t = np.quantile(f, 1.0 - occupancy)
-    hi = float(f.max())
-    v = np.where(f > t, 1.0 + 254.0 * (f - t) / max(hi - t, 1e-6), 0.0)
-    return np.clip(np.rint(v), 0, 255).astype(np.uint8)
+    def make():
+        f = value_noise(n, octaves, seed)
+        t = np.quantile(f, 1.0 - occupancy)
+        hi = float(f.max())
+        v = np.where(f > t, 1.0 + 254.0 * (f - t) / max(hi - t, 1e-6), 0.0)
+        return np.clip(np.rint(v), 0, 255).astype(np.uint8)
+    return _cached(f"vns_{n}_{occupancy}_{seed}_{octaves}", make)
 
 
 def lognormal(n: int = 512, seed: int = 3, octaves: int = 5) -> np.ndarray:
-    f = value_noise(n, octaves, seed)
-    f = (f - f.mean()) / max(float(f.std()), 1e-6)
-    v = np.exp(np.clip(f / 3.0, -1.0, 1.0) * np.log(1e3))
-    return v.astype(np.float32)
+    """Log-normal field in [1e-3, 1e3]: normalised noise, exp-mapped."""
+    def make():
+        f = value_noise(n, octaves, seed)
+        f = (f - f.mean()) / max(float(f.std()), 1e-6)
+        return np.exp(np.clip(f / 3.0, -1.0, 1.0) * np.log(1e3)).astype(np.float32)
+    return _cached(f"lgn_{n}_{seed}_{octaves}", make)
 
 
-def ramp_tf(rgb: Sequence[float], n: int = 256, alpha_max: float = 1.0) -> np.ndarray:
-    """n RGBA texels: colour fades in with the ramp, opacity rises linearly 0 -> alpha_max."""
+def lognormal_log10(n: int = 512, seed: int = 3, octaves: int = 5) -> np.ndarray:
+    """The log-normal field log-scaled into the TF domain: log10 of `lognormal`, [-3, 3]."""
+    return _cached(f"lgl_{n}_{seed}_{octaves}", lambda: np.log10(lognormal(n, seed, octaves)).astype(np.float32))
+
+
+def ramp_tf(rgb: Sequence[float], n: int = 256, alpha_max: float = 1.0, start: float = 0.0) -> np.ndarray:
+    """n RGBA texels: colour fades in with the ramp, opacity rises linearly from 0 at
+    `start` to alpha_max at the top of the range."""
     x = np.linspace(0.0, 1.0, n, dtype=np.float32)
     tf = np.empty((n, 4), dtype=np.float32)
     for k in range(3):
         tf[:, k] = rgb[k] * (0.35 + 0.65 * x)
-    tf[:, 3] = alpha_max * x
+    tf[:, 3] = alpha_max * np.clip((x - start) / max(1.0 - start, 1e-6), 0.0, 1.0)
     return tf
 
 
@@ -151,12 +191,12 @@ def scene_c2(seed: int = 2, n: int = 256) -> Scene:
 
 
 def scene_c3(seed: int = 3, n: int = 512, channels: int = 6, edge: int = 16, mode: int = 2) -> Scene:
-    """N-DDA / syncDDA, `channels` x n^3 float32 log-normal, macrocell edge `edge` voxels,
-    1920x1080, 256 spp.  The TF range maps [1e-3, ~15] of the [0, 1e3] value domain, so
-    the opacity ramp covers the log-normal bulk."""
-    vols = [lognormal(n, seed * 31 + i) for i in range(channels)]
-    tfs = [ramp_tf(HUES[i % len(HUES)], alpha_max=0.5) for i in range(channels)]
+    """N-DDA / syncDDA, `channels` x n^3 float32 log-normal fields log-scaled into the
+    TF domain (log10, [-3, 3]), macrocell edge `edge` voxels, 1920x1080, 256 spp.  The
+    opacity ramps start at the middle of the range (the upper half of each field is
+    visible), alpha_max 0.25 before cubing: a semi-transparent turbulent medium."""
+    vols = [lognormal_log10(n, seed * 31 + i) for i in range(channels)]
+    tfs = [ramp_tf(HUES[i % len(HUES)], alpha_max=0.25, start=0.5) for i in range(channels)]
     mc = max(1, n // edge)
     return Scene(f"c3_{'syncdda' if mode == 2 else 'ndda'}_{channels}x{n}f32_e{edge}", vols, tfs, mode=mode,
-                 macrocells=(mc, mc, mc), resolution=(1920, 1080), spp=256,
-                 xf_range=[(0.0, 0.015)] * channels)
+                 macrocells=(mc, mc, mc), resolution=(1920, 1080), spp=256)
