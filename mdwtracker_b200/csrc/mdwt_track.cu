@@ -30,7 +30,7 @@ namespace mdwt {
 namespace {
 
 constexpr int kTPB = 128;
-constexpr int kMinBlocks = 6;
+constexpr int kMinBlocks = 8;   // 64 registers: 32 warps per SM (measured fastest)
 constexpr unsigned kFull = 0xffffffffu;
 
 // Path record: bit 31 hit, bits 27..30 channel, bits 13..26 TF texel i0, bit 12 set when
