@@ -688,8 +688,8 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   if (!c) return MDWT_ERR_BAD_ARG;
   if (c->inited) return fail(c, MDWT_ERR_STATE, "already initialised");
   if (c->ch.empty()) return fail(c, MDWT_ERR_STATE, "No data source specified (renderer.cpp:326-330)");
-  if (mode != MDWT_MODE_NDDA && mode != MDWT_MODE_SYNCDDA)
-    return fail(c, MDWT_ERR_UNSUPPORTED, "mode not supported by the GPU tracker (0 and 2 are)");
+  if (mode < MDWT_MODE_NDDA || mode > MDWT_MODE_CUMULATIVE)
+    return fail(c, MDWT_ERR_UNSUPPORTED, "mode not supported (0..3 are; 4..9 are the blending modes and ray marchers)");
   if (c->device == MDWT_HOST_ONLY) return fail(c, MDWT_ERR_STATE, "host-only context: no device to initialise");
   CK(cudaSetDevice(c->device), "cudaSetDevice");
   c->mode = mode;

@@ -218,6 +218,8 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
   int ch = 0, cellID = 0;
   uint32_t cmask = 0;                          // non-zero-majorant channels of the current cell
   float maj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f, tW = 0.f;
+  float rnd = 0.f;                              // -m 1: the draw taken before a selection
+  float majs[MODE == 1 ? kMaxChannels : 1], ts[MODE == 1 ? kMaxChannels : 1];   // -m 1 per-channel state
   bool capped = false;
 
   auto enter_cell = [&]() {  // cell_t0 / cell_t1 of the DDA lambda call (dda.h:164-170)
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
               grid_dir(P, wdx, wdy, wdz, gx, gy, gz, w2g, g2w);
               ch = 0;
               st = S_TRANS;
-              if (MODE == 2) {
+              if (MODE != 0) {
                 if (dda_init(P, gx, gy, gz, d)) {
                   enter_cell();
                   lim = ct1;
@@ -327,7 +329,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
       if (st == S_TRANS) {
         bool stepping = false;
         while (true) {
-          if (MODE == 2) {
+          if constexpr (MODE == 2) {
             if (act == A_ADVANCE) {
               if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) break;
               enter_cell();
@@ -348,7 +350,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
             t = ct0;
             stepping = true;
             break;
-          } else {
+          } else if constexpr (MODE == 0) {
             if (act == A_NEWDDA) {  // one full traversal per channel (deviceCode.cu:965-969)
               if (ch >= C) break;
               float gx, gy, gz, a, b;
@@ -367,30 +369,71 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
               break;
             }
             act = A_ADVANCE;
+          } else {  // MODE 1 and 3: one traversal, the cell entered or advanced past
+            if (act == A_ADVANCE) {
+              if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) break;
+              enter_cell();
+              act = A_CHAN;
+            }
+            if constexpr (MODE == 3) {  // summed majorant (deviceCode.cu:541-548)
+              if (cmask & 1u) {
+                maj = __ldg(P.majorants + cellID);
+                t = ct0;
+                stepping = true;
+                break;
+              }
+              act = A_ADVANCE;
+            } else {  // MODE 1: per-channel free flights from the cell entry (deviceCode.cu:652-674)
+              float sum = 0.0f;
+              for (int i = 0; i < C; i++) {
+                majs[i] = __ldg(P.majorants + (size_t)cellID * C + i);
+                sum += majs[i];
+                ts[i] = ct0;
+              }
+              if (sum <= 0.0000001f) { act = A_ADVANCE; continue; }
+              for (int i = 0; i < C; i++)
+                ts[i] = majs[i] > 0.0f ? fmaf(-((mlog(1.0f - rng_next(rng)) / majs[i]) * P.dt), w2g, ts[i]) : 1e20f;
+              stepping = true;
+              break;
+            }
           }
         }
         if (stepping) st = S_STEP;
         else finish();
       }
-      // free-flight draw (deviceCode.cu:800-820, 908-930)
+      // free-flight draw (deviceCode.cu:568-583, 677-703, 800-820, 908-930)
       if (st == S_STEP) {
         if (++steps >= kMaxStepsPerSample) {
           capped = true;
           finish();
         } else {
-          const float u = rng_next(rng);
-          t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
-          if (MODE == 2 ? (t >= lim) : (t >= ct1)) {
+          bool exitCell, skipChannel = false;
+          if constexpr (MODE == 1) {
+            rnd = rng_next(rng);  // drawn before the selection (deviceCode.cu:681)
+            float minT = ts[0];
+            int sel = 0;
+            for (int i = 1; i < C; i++)
+              if (ts[i] < minT && majs[i] > 0.f) { sel = i; minT = ts[i]; }
+            ch = sel;
+            t = minT;
+            exitCell = minT >= ct1;
+          } else {
+            const float u = rng_next(rng);
+            t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+            exitCell = MODE == 2 ? (t >= lim) : (t >= ct1);
+            if (MODE == 0 && !exitCell && lim < t) skipChannel = true;
+          }
+          if (exitCell) {
             if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
             st = S_TRANS;
-          } else if (MODE == 0 && lim < t) {
+          } else if (skipChannel) {
             ch++; act = A_NEWDDA; st = S_TRANS;
           } else {
             tW = t * g2w;
             if (tW >= t1w) {  // world exit
               if (STATS) pRej++;
               totRej++;
-              if (MODE == 2 && ch == C - 1) finish();
+              if ((MODE == 2 && ch == C - 1) || MODE == 1 || MODE == 3) finish();
               else { ch++; act = MODE == 2 ? A_CHAN : A_NEWDDA; st = S_TRANS; }
             } else {
               st = S_SAMPLE;
@@ -406,27 +449,59 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
       const float xs = fmaf(tW, wdx, P.camOrg.x) * P.w2u.x;
       const float ys = fmaf(tW, wdy, P.camOrg.y) * P.w2u.y;
       const float zs = fmaf(tW, wdz, P.camOrg.z) * P.w2u.z;
-      const float thr = rng_next(rng) * maj;
-      const ChanSm &cs = sch[ch];
-      const float v = sample_volume<SK>(P, cs, xs, ys, zs);
-      if (STATS) pSamp++;
-      totSamp++;
       st = S_STEP;
-      bool rejected = MODE == 2;
-      if (v == v) {
-        Axis tax;
-        const float a = tf_alpha(cs, v, tax);
-        if (a > 0.0f && thr < a) {
-          record = make_record(ch, tax);
-          lim = fminf(t, lim);
-          if (MODE == 0) { ch++; act = A_NEWDDA; st = S_TRANS; }
-        } else {
-          rejected = true;
+      if constexpr (MODE == 3) {  // one threshold walked down through the channels (deviceCode.cu:590-613)
+        float thr = rng_next(rng) * maj;
+        bool hitNow = false;
+        for (int c = 0; c < C; c++) {
+          const ChanSm &cs = sch[c];
+          const float v = sample_volume<SK>(P, cs, xs, ys, zs);
+          if (STATS) pSamp++;
+          totSamp++;
+          if (!(v == v)) continue;
+          Axis tax;
+          const float a = tf_alpha(cs, v, tax);
+          if (a > 0.0f && thr < a) {
+            record = make_record(c, tax);
+            hitNow = true;
+            break;
+          }
+          thr -= a;
         }
-      }
-      if (rejected) {
-        if (STATS) pRej++;
-        totRej++;
+        if (hitNow) {
+          finish();
+        } else {
+          if (STATS) pRej++;
+          totRej++;
+        }
+      } else {
+        const float mj = MODE == 1 ? majs[ch] : maj;
+        const float thr = rng_next(rng) * mj;
+        const ChanSm &cs = sch[ch];
+        const float v = sample_volume<SK>(P, cs, xs, ys, zs);
+        if (STATS) pSamp++;
+        totSamp++;
+        bool rejected = MODE != 0;
+        if (v == v) {
+          Axis tax;
+          const float a = tf_alpha(cs, v, tax);
+          if (a > 0.0f && thr < a) {
+            record = make_record(ch, tax);
+            if constexpr (MODE == 2) lim = fminf(t, lim);
+            if constexpr (MODE == 0) { lim = fminf(t, lim); ch++; act = A_NEWDDA; st = S_TRANS; }
+            if constexpr (MODE == 1) finish();
+            rejected = MODE == 2;
+          } else {
+            rejected = true;
+          }
+        }
+        if (rejected) {
+          if (STATS) pRej++;
+          totRej++;
+        }
+        if constexpr (MODE == 1) {
+          if (st == S_STEP) ts[ch] = fmaf(-((mlog(1.0f - rnd) / majs[ch]) * P.dt), w2g, ts[ch]);
+        }
       }
     }
     __syncwarp();
@@ -572,9 +647,14 @@ int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
 int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block) {
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
-  if (p.mode == 2) rc = storeKind == kStoreU8 ? launch_s<2, kStoreU8>(p, st, numSMs, grid) : launch_s<2, kStoreF32>(p, st, numSMs, grid);
-  else if (p.mode == 0) rc = storeKind == kStoreU8 ? launch_s<0, kStoreU8>(p, st, numSMs, grid) : launch_s<0, kStoreF32>(p, st, numSMs, grid);
-  else return (int)cudaErrorInvalidValue;
+  const bool u8 = storeKind == kStoreU8;
+  switch (p.mode) {
+    case 0: rc = u8 ? launch_s<0, kStoreU8>(p, st, numSMs, grid) : launch_s<0, kStoreF32>(p, st, numSMs, grid); break;
+    case 1: rc = u8 ? launch_s<1, kStoreU8>(p, st, numSMs, grid) : launch_s<1, kStoreF32>(p, st, numSMs, grid); break;
+    case 2: rc = u8 ? launch_s<2, kStoreU8>(p, st, numSMs, grid) : launch_s<2, kStoreF32>(p, st, numSMs, grid); break;
+    case 3: rc = u8 ? launch_s<3, kStoreU8>(p, st, numSMs, grid) : launch_s<3, kStoreF32>(p, st, numSMs, grid); break;
+    default: return (int)cudaErrorInvalidValue;
+  }
   *block = kTPB;
   if (launches) *launches += p.numTiles > 0 ? 2 : 1;
   return rc;

@@ -88,7 +88,7 @@ def test_c1_like_ndda(oracle):
     assert c[0] > 0 and c[3] == 96 * 80 * 5
 
 
-@pytest.mark.parametrize("mode", [0, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_c2_like_three_channels(oracle, mode):
     vols = [noise_u8(48, occ, 10 + i) for i, occ in enumerate([0.1, 0.2, 0.3])]
     tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(3)]
@@ -97,7 +97,7 @@ def test_c2_like_three_channels(oracle, mode):
     run_frames(p, o, 2)
 
 
-@pytest.mark.parametrize("mode", [0, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_float32_lognormal(oracle, mode):
     vols = [syn.lognormal(40, 5 + i, octaves=4) for i in range(2)]
     tfs = [syn.ramp_tf(syn.HUES[i], alpha_max=0.7) for i in range(2)]
@@ -113,7 +113,7 @@ def test_mixed_formats_and_ragged_dims(oracle):
     b = (syn.value_noise(24, 3, 4) * 40.0).astype(np.float32)[:, :20, :]  # dims (24, 20, 24)
     c = rng.integers(-20, 60, (17, 23, 29)).astype(np.int8)          # dims (29, 23, 17)
     tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(3)]
-    for mode in (0, 2):
+    for mode in (0, 1, 2, 3):
         p, o = make_pair(oracle, [a, b, c], tfs, mode, (7, 5, 3), (45, 37), 3, opacity=[1.0, 0.6, 2.0])
         assert_same_grid(p, o)
         run_frames(p, o, 2)
@@ -122,7 +122,7 @@ def test_mixed_formats_and_ragged_dims(oracle):
 def test_twelve_channels(oracle):
     vols = [noise_u8(12, 0.25, 40 + i) for i in range(12)]
     tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(12)]
-    for mode in (0, 2):
+    for mode in (0, 1, 2, 3):
         p, o = make_pair(oracle, vols, tfs, mode, (3, 3, 3), (24, 24), 2)
         assert_same_grid(p, o)
         run_frames(p, o, 1)
@@ -174,13 +174,13 @@ def test_state_changes_between_frames(oracle):
     ((-2.0, 0.5, 0.5), (0.5, 0.5, 0.5), (0.0, 0.0, 1.0), 40.0),    # along +x
 ])
 def test_camera_edge_cases(oracle, cam):
-    vols = [noise_u8(24, 0.3, 70)]
-    for mode in (0, 2):
+    vols = [noise_u8(24, 0.3, 70), noise_u8(24, 0.2, 71)]
+    for mode in (0, 1, 2, 3):
         p, o = make_pair(oracle, vols, [syn.viridis_like()], mode, (3, 3, 3), (33, 31), 3, camera=cam)
         run_frames(p, o, 1)
 
 
-@pytest.mark.parametrize("mode,batch,pool", [(2, 3, 1), (0, 5, 32), (2, 1, 8), (0, 0, 4)])
+@pytest.mark.parametrize("mode,batch,pool", [(2, 3, 1), (0, 5, 32), (2, 1, 8), (0, 0, 4), (1, 4, 8), (3, 2, 16)])
 def test_sample_batches_and_pool_sizes(oracle, mode, batch, pool):
     """Path records resolved over several sample batches (running sums carried between
     passes) and any regeneration pool give the oracle's sequential spp loop exactly."""
