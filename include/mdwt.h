@@ -159,6 +159,16 @@ mdwt_status mdwt_set_mirror(mdwt_ctx *ctx, int enable);
  * frame/accumulation ids; afterwards they advance exactly like the reference
  * (owlParamsSet1i(.., accumID++) after the launch). */
 mdwt_status mdwt_render(mdwt_ctx *ctx, void *cuda_stream);
+/* No reference counterpart: render only the rows [row0, row1) of the frame (other rows
+ * keep their contents; row1 <= row0 = all rows).  Frame and accumulation ids advance
+ * as for a full frame, so N contexts rendering disjoint bands of the same frame
+ * together produce exactly the single-context frame (multi-GPU row split). */
+mdwt_status mdwt_set_render_rows(mdwt_ctx *ctx, int row0, int row1);
+/* Copy rows [row0, row1) of the accumulation (float4) and RGBA8 buffers to caller
+ * memory (device or pinned/pageable host; either pointer may be NULL), enqueued on
+ * `cuda_stream` (NULL = the context's stream). */
+mdwt_status mdwt_copy_frame_rows(mdwt_ctx *ctx, int row0, int row1, float *accum_dst, uint32_t *fb_dst,
+                                 void *cuda_stream);
 /* Wait for every frame issued on the context's streams; reports device-side errors. */
 mdwt_status mdwt_sync(mdwt_ctx *ctx);
 /* Renderer::ResetAccumulation (renderer.cpp:1488-1495). */

@@ -152,6 +152,7 @@ struct mdwt_ctx {
   int pool = 8;       // regeneration pool of the tracker (MDWT_TUNE_POOL)
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
   int trips = 2;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
+  int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
 };
 
 namespace {
@@ -954,6 +955,12 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   p.workCounter = c->dWork;
   int rect[4];
   cull_rect(c, rect);
+  // a row band (mdwt_set_render_rows) restricts tracing and resolve to its rows
+  p.rowLo = std::max(0, std::min(c->H, c->rowLo));
+  p.rowHi = c->rowHi > c->rowLo ? std::max(p.rowLo, std::min(c->H, c->rowHi)) : c->H;
+  if (c->rowHi <= c->rowLo) p.rowLo = 0;
+  rect[1] = std::max(rect[1], p.rowLo);
+  rect[3] = std::min(rect[3], p.rowHi - 1);
   p.cullX0 = rect[0]; p.cullY0 = rect[1]; p.cullX1 = rect[2]; p.cullY1 = rect[3];
   const int rw = rect[2] - rect[0] + 1, rh = rect[3] - rect[1] + 1;
   p.tilesX = rw > 0 ? (rw + 7) / 8 : 0;
@@ -1082,6 +1089,26 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *c, uint32_t *out) {
   CK(cudaSetDevice(c->device), "cudaSetDevice");
   CK(cudaDeviceSynchronize(), "sync");
   CK(cudaMemcpy(out, c->dStats, (size_t)c->W * c->H * 16, cudaMemcpyDeviceToHost), "copy stats");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_render_rows(mdwt_ctx *c, int row0, int row1) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (row0 < 0 || row1 < 0) return fail(c, MDWT_ERR_BAD_ARG, "negative row");
+  c->rowLo = row0;
+  c->rowHi = row1;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_copy_frame_rows(mdwt_ctx *c, int row0, int row1, float *accum_dst, uint32_t *fb_dst, void *stream) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  if (row0 < 0 || row1 > c->H || row0 > row1) return fail(c, MDWT_ERR_BAD_ARG, "row range outside the frame");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const size_t off = (size_t)row0 * c->W, n = (size_t)(row1 - row0) * c->W;
+  if (accum_dst) CK(cudaMemcpyAsync(accum_dst, c->dAccum + 4 * off, n * 16, cudaMemcpyDefault, st), "copy accum rows");
+  if (fb_dst) CK(cudaMemcpyAsync(fb_dst, c->dFb + off, n * 4, cudaMemcpyDefault, st), "copy framebuffer rows");
   return MDWT_OK;
 }
 

@@ -62,6 +62,7 @@ struct TrackParams {
   // samples composites the background, so their per-pixel result is the constant
   // bgFin (sum over spp of the background, / spp), computed on the host.
   int cullX0, cullY0, cullX1, cullY1;
+  int rowLo, rowHi;              // rows [rowLo, rowHi) of the frame are rendered (a band)
   float bgFin[4];
   int numTiles;                  // 8x4 pixel tiles covering the traced rectangle
   int tilesX;

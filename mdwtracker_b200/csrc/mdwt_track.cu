@@ -543,7 +543,7 @@ __device__ __forceinline__ void write_pixel(const TrackParams &P, int px, int py
 
 template <bool STATS>
 __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ TrackParams P) {
-  const unsigned npix = (unsigned)P.W * (unsigned)P.H;
+  const unsigned npix = (unsigned)P.W * (unsigned)(P.rowHi - P.rowLo);   // the rendered row band
   const int rw = P.cullX1 - P.cullX0 + 1;
   const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
   const bool last = P.sBase + P.sCount == P.spp;
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
   const float ks = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
   uint32_t culledPaths = 0;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
-    const int px = (int)(i % (unsigned)P.W), py = (int)(i / (unsigned)P.W);
+    const int px = (int)(i % (unsigned)P.W), py = P.rowLo + (int)(i / (unsigned)P.W);
     if (px < P.cullX0 || px > P.cullX1 || py < P.cullY0 || py > P.cullY1) {
       if (last) {
         write_pixel<STATS>(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], P.bgFin[3], make_uint4(0u, 0u, 0u, 0u));
@@ -629,7 +629,8 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
   if (p.numTiles > 0) trace_kernel<MODE, SK, STATS><<<*grid, kTPB, 0, st>>>(q);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  const size_t npix = (size_t)p.W * p.H;
+  const size_t npix = (size_t)p.W * (size_t)(p.rowHi - p.rowLo);
+  if (npix == 0) return (int)cudaGetLastError();
   size_t g = (npix + 255) / 256;
   if (g > (size_t)numSMs * 8) g = (size_t)numSMs * 8;
   resolve_kernel<STATS><<<(unsigned)g, 256, 0, st>>>(p);

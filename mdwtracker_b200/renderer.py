@@ -284,6 +284,17 @@ class Renderer:
         self._call("get_ranges", out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.reshape(n, 2)
 
+    def setRenderRows(self, row0: int, row1: int):
+        """Render only rows [row0, row1) (row1 <= row0: all rows); ids advance per frame."""
+        self._call("set_render_rows", C.c_int(row0), C.c_int(row1))
+
+    def copyFrameRows(self, row0: int, row1: int, accum_ptr: Optional[int], fb_ptr: Optional[int],
+                      stream: Optional[int] = None):
+        """Copy rows [row0, row1) of the accumulation / RGBA8 buffers to raw (device or
+        host) pointers."""
+        self._call("copy_frame_rows", C.c_int(row0), C.c_int(row1), C.c_void_p(accum_ptr), C.c_void_p(fb_ptr),
+                   C.c_void_p(stream) if stream else None)
+
     def setTuning(self, key: int, value: int):
         """Tracker tuning knob (0 = regeneration pool); results do not depend on it."""
         self._call("set_tuning", C.c_int(key), C.c_int(value))

@@ -73,5 +73,13 @@ class OracleRenderer(Renderer):
         """One frame restricted to pixel rows [row0, row1) (frame ids still advance)."""
         self._call("render_rows", C.c_int(row0), C.c_int(row1))
 
+    _band = (0, 0)
+
+    def setRenderRows(self, row0: int, row1: int):
+        self._band = (row0, row1)
+
+    def Render(self, stream=None):
+        self.renderRows(*self._band)
+
     def cappedSamples(self) -> int:
         return int(self._lib.orc_capped_samples(self._ctx))

@@ -198,3 +198,27 @@ def test_no_tf_and_empty_volume(oracle):
     p, o = make_pair(oracle, vols, [syn.viridis_like()], 2, (4, 4, 4), (32, 32), 2, bg=(0.25, 0.5, 0.75))
     assert_same_grid(p, o)
     run_frames(p, o, 1)
+
+
+def test_row_bands_assemble_the_full_frame(oracle):
+    """Contexts rendering disjoint row bands (mdwt_set_render_rows) give the full frame,
+    read back band by band through mdwt_copy_frame_rows (the multi-GPU row split)."""
+    import torch
+    vols = [noise_u8(32, 0.25, 110), noise_u8(32, 0.2, 111)]
+    tfs = [syn.ramp_tf(syn.HUES[0]), syn.ramp_tf(syn.HUES[1])]
+    full, o = make_pair(oracle, vols, tfs, 2, (4, 4, 4), (40, 37), 4)
+    bands = [(0, 13), (13, 25), (25, 37)]
+    parts = [make_pair(oracle, vols, tfs, 2, (4, 4, 4), (40, 37), 4)[0] for _ in bands]
+    for f in range(2):
+        full.Render()
+        acc = torch.empty((37, 40, 4), dtype=torch.float32, device="cuda")
+        fb = torch.empty((37, 40), dtype=torch.int32, device="cuda")
+        for r, (a, b) in zip(parts, bands):
+            r.setRenderRows(a, b)
+            r.Render()
+            r.copyFrameRows(a, b, acc[a:b].data_ptr(), fb[a:b].data_ptr())
+            r.sync()
+        np.testing.assert_array_equal(acc.cpu().numpy().view(np.uint32), full.accum().view(np.uint32))
+        np.testing.assert_array_equal(fb.cpu().numpy().view(np.uint32), full.framebuffer())
+    tot = sum(np.asarray(r.counters(), dtype=np.uint64) for r in parts)
+    np.testing.assert_array_equal(tot, full.counters())
