@@ -1084,6 +1084,7 @@ int orc_render_rows(Oracle *o, int row0, int row1) {
   return ORC_OK;
 }
 int orc_render(Oracle *o) { return orc_render_rows(o, 0, 0); }
+int orc_sync(Oracle *) { return ORC_OK; }
 int orc_reset_accumulation(Oracle *o) { o->accumID = 0; o->accumParam = 0; return ORC_OK; }
 int orc_get_frame_ids(Oracle *o, int out[4]) {
   out[0] = o->frameID; out[1] = o->accumID; out[2] = o->frameParam; out[3] = o->accumParam; return ORC_OK;

@@ -222,3 +222,23 @@ def test_row_bands_assemble_the_full_frame(oracle):
         np.testing.assert_array_equal(fb.cpu().numpy().view(np.uint32), full.framebuffer())
     tot = sum(np.asarray(r.counters(), dtype=np.uint64) for r in parts)
     np.testing.assert_array_equal(tot, full.counters())
+
+
+def test_cli_on_the_gpu_matches_the_oracle(tmp_path, oracle):
+    """The headless front end end to end on libmdwt.so: final PNG equals the oracle's."""
+    from mdwtracker_b200 import cli, imageio
+    vol = noise_u8(24, 0.3, 5)
+    raw = str(tmp_path / "vol_24x24x24_uint8.raw")
+    vol.tofile(raw)
+    tf = str(tmp_path / "a.tf")
+    imageio.save_tf(tf, syn.ramp_tf(syn.HUES[0]), 1.5, (0.0, 0.9))
+    args = ["-fr", raw, raw, "-t", tf, tf, "-mc", "3", "-r", "20", "16", "-m", "2", "-spp", "2", "-n", "3", "-wu", "1",
+            "-mf", "1"]
+    a = cli.build_parser().parse_args(args + ["-o", str(tmp_path / "gpu")])
+    p = cli.setup(a, Renderer(0))
+    cli.run(a, p)
+    b = cli.build_parser().parse_args(args + ["-o", str(tmp_path / "cpu")])
+    o = cli.setup(b, oracle.OracleRenderer())
+    cli.run(b, o)
+    np.testing.assert_array_equal(imageio.read_png(str(tmp_path / "gpu_AMMB_w_3_shadows_off_frames.png")),
+                                  imageio.read_png(str(tmp_path / "cpu_AMMB_w_3_shadows_off_frames.png")))
