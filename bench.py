@@ -28,6 +28,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -98,7 +100,7 @@ def measured_peak_hbm():
 
 def profiled_traffic(workload):
     """DRAM bytes per tracker launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"track_kernel_{workload}.md")
+    p = os.path.join(ROOT, "profiles", f"trace_kernel_{workload}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -259,18 +261,26 @@ def main():
             r.Render(sptr)
     torch.cuda.synchronize(dev)
     r.resetCounters()
+    timed = True
+    try:
+        r.setTiming(True)
+    except Exception:
+        timed = False
     launches0 = r.renderInfo()[0]
     clocks = ClockSampler(torch.cuda.get_device_properties(dev).uuid and f"GPU-{torch.cuda.get_device_properties(dev).uuid}")
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
+    trace_ms = []
     with torch.cuda.stream(stream):
         for k in range(args.steps):
             flush.fill_(k & 0xff)
             ev[k][0].record(stream)
             r.Render(sptr)
             ev[k][1].record(stream)
+            if timed:
+                trace_ms.append(r.kernelTimes()[0])  # trace kernel, CUDA events on the render stream
     torch.cuda.synchronize(dev)
     barrier()
     clk = clocks.stop()
@@ -285,14 +295,15 @@ def main():
     paths = w * h * sc.spp
     value = world * paths / (ms / 1e3) / 1e9
 
-    # algorithmic bytes of the tracker (per launch): 8*bpv per density sample,
-    # 4*C_read per macrocell visit, 36 per pixel (accum read+write, RGBA8 write)
-    bpv = sc.volumes[0].dtype.itemsize if all(v.dtype == sc.volumes[0].dtype for v in sc.volumes) else 4
-    bpv = 1 if bpv == 1 else 4
+    # algorithmic bytes of the dominant kernel (trace_kernel) per launch: 8*bpv per
+    # density sample (trilinear footprint), 4*C_read per macrocell visit (majorants;
+    # C for syncDDA, 1 otherwise); the resolve pass (36 B per pixel) is timed apart
+    bpv = 1 if all(v.dtype == np.uint8 for v in sc.volumes) else 4
     creads = len(sc.volumes) if sc.mode == 2 else 1
     steps = args.steps
-    alg_bytes = (8.0 * bpv * float(cnt[0]) + 4.0 * creads * float(cnt[2]) + 36.0 * w * h * steps) / steps
-    achieved = alg_bytes / (statistics.mean(step_ms) / 1e3) / 1e9
+    alg_bytes = (8.0 * bpv * float(cnt[0]) + 4.0 * creads * float(cnt[2])) / steps
+    kernel_ms = statistics.mean(trace_ms) if trace_ms else statistics.mean(step_ms)
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
 
     # ---- end to end through the C ABI with host buffers
@@ -340,8 +351,8 @@ def main():
         "config": scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profiled_traffic(workload_name(sc)),
-                     "peak_source": peak_kind, "kernel": "track_kernel",
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "peak_source": peak_kind, "kernel": "trace_kernel",
+                     "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
         "cpu_baseline": cpu,
         "e2e": {"value": world * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": w * h * 4, "ms_per_step": e2e},

@@ -201,6 +201,13 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
 enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2 };
 mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
 
+/* No reference counterpart: CUDA events on the render stream around the trace kernel
+ * (with the work-counter reset before it) and the resolve kernel of each frame whose
+ * samples fit one trace pass; mdwt_get_kernel_times returns the last frame's
+ * {trace, resolve} milliseconds (it waits for that frame). */
+mdwt_status mdwt_set_timing(mdwt_ctx *ctx, int enable);
+mdwt_status mdwt_get_kernel_times(mdwt_ctx *ctx, float out_ms2[2]);
+
 /* Launch bookkeeping: out[0] = kernels launched by this context so far, out[1] = bytes
  * of per-frame parameters a render sends host->device, out[2] = grid and out[3] = block
  * size of the last tracker launch. */

@@ -153,6 +153,9 @@ struct mdwt_ctx {
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
   int trips = 2;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
   int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
+  bool timing = false;        // CUDA events around the trace and resolve kernels
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  bool timed = false;
 };
 
 namespace {
@@ -612,6 +615,8 @@ mdwt_status mdwt_destroy(mdwt_ctx *c) {
   if (c->device == MDWT_HOST_ONLY) { delete c; return MDWT_OK; }
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
   free_device(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -992,11 +997,24 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   p.recStats = stats ? c->dRecStats : nullptr;
   p.partial = c->dPartial;
   p.partialStats = stats ? c->dPartialStats : nullptr;
+  // kernel timing: events around the trace and the resolve pass of a one-batch frame
+  const bool timeIt = c->timing && batch >= c->spp;
+  c->timed = false;
+  if (timeIt) {
+    for (auto &e : c->ev)
+      if (!e) CK(cudaEventCreate(&e), "cudaEventCreate");
+    CK(cudaEventRecord(c->ev[0], st), "event");
+  }
   for (int s0 = 0; s0 < c->spp; s0 += batch) {
     p.sBase = s0;
     p.sCount = std::min(batch, c->spp - s0);
     CK(cudaMemsetAsync(c->dWork, 0, sizeof(unsigned int), st), "reset work counter");
-    CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock), "tracker kernels");
+    CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock, timeIt ? c->ev[1] : nullptr),
+        "tracker kernels");
+  }
+  if (timeIt) {
+    CK(cudaEventRecord(c->ev[2], st), "event");
+    c->timed = true;
   }
   // Renderer::Render (renderer.cpp:957-958): the ids the next frame sees are the
   // pre-increment values
@@ -1109,6 +1127,21 @@ mdwt_status mdwt_copy_frame_rows(mdwt_ctx *c, int row0, int row1, float *accum_d
   const size_t off = (size_t)row0 * c->W, n = (size_t)(row1 - row0) * c->W;
   if (accum_dst) CK(cudaMemcpyAsync(accum_dst, c->dAccum + 4 * off, n * 16, cudaMemcpyDefault, st), "copy accum rows");
   if (fb_dst) CK(cudaMemcpyAsync(fb_dst, c->dFb + off, n * 4, cudaMemcpyDefault, st), "copy framebuffer rows");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_timing(mdwt_ctx *c, int enable) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  c->timing = enable != 0;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_kernel_times(mdwt_ctx *c, float out_ms[2]) {
+  if (!c || !out_ms) return MDWT_ERR_BAD_ARG;
+  if (!c->timed) return fail(c, MDWT_ERR_STATE, "no timed frame (enable timing; frames of one sample batch)");
+  CK(cudaEventSynchronize(c->ev[2]), "event sync");
+  CK(cudaEventElapsedTime(&out_ms[0], c->ev[0], c->ev[1]), "elapsed");
+  CK(cudaEventElapsedTime(&out_ms[1], c->ev[1], c->ev[2]), "elapsed");
   return MDWT_OK;
 }
 

@@ -91,7 +91,9 @@ struct AxisIntervals {
 };
 
 // ---- launchers implemented in mdwt_kernels.cu (return cudaError_t as int) ----
-int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block);
+// trace + resolve of one sample batch; evMid (a cudaEvent_t or null) is recorded between them
+int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block,
+                 void *evMid);
 
 // Value ranges of one channel into ranges[(cell*C + ch)*2 + {0,1}].
 //   vol: channel voxels; dims; mc grid; intervals per axis (device arrays);

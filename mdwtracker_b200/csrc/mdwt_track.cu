@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
 }
 
 template <int MODE, int SK, bool STATS>
-int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
+int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
   int bps = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_kernel<MODE, SK, STATS>, kTPB, 0);
   if (e != cudaSuccess) return (int)e;
@@ -627,6 +627,7 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
   chunk = chunk < 32 ? 32 : (chunk > 256 ? 256 : chunk & ~(size_t)31);
   q.chunk = (int)chunk;
   if (p.numTiles > 0) trace_kernel<MODE, SK, STATS><<<*grid, kTPB, 0, st>>>(q);
+  if (evMid) cudaEventRecord((cudaEvent_t)evMid, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   const size_t npix = (size_t)p.W * (size_t)(p.rowHi - p.rowLo);
@@ -638,22 +639,23 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
 }
 
 template <int MODE, int SK>
-int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid) {
-  return p.stats ? launch_t<MODE, SK, true>(p, st, numSMs, grid) : launch_t<MODE, SK, false>(p, st, numSMs, grid);
+int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
+  return p.stats ? launch_t<MODE, SK, true>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false>(p, st, numSMs, grid, evMid);
 }
 
 }  // namespace
 
 // One batch of samples [sBase, sBase + sCount): trace + resolve on `stream`.
-int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block) {
+int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block,
+                 void *evMid) {
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
   const bool u8 = storeKind == kStoreU8;
   switch (p.mode) {
-    case 0: rc = u8 ? launch_s<0, kStoreU8>(p, st, numSMs, grid) : launch_s<0, kStoreF32>(p, st, numSMs, grid); break;
-    case 1: rc = u8 ? launch_s<1, kStoreU8>(p, st, numSMs, grid) : launch_s<1, kStoreF32>(p, st, numSMs, grid); break;
-    case 2: rc = u8 ? launch_s<2, kStoreU8>(p, st, numSMs, grid) : launch_s<2, kStoreF32>(p, st, numSMs, grid); break;
-    case 3: rc = u8 ? launch_s<3, kStoreU8>(p, st, numSMs, grid) : launch_s<3, kStoreF32>(p, st, numSMs, grid); break;
+    case 0: rc = u8 ? launch_s<0, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<0, kStoreF32>(p, st, numSMs, grid, evMid); break;
+    case 1: rc = u8 ? launch_s<1, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<1, kStoreF32>(p, st, numSMs, grid, evMid); break;
+    case 2: rc = u8 ? launch_s<2, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<2, kStoreF32>(p, st, numSMs, grid, evMid); break;
+    case 3: rc = u8 ? launch_s<3, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<3, kStoreF32>(p, st, numSMs, grid, evMid); break;
     default: return (int)cudaErrorInvalidValue;
   }
   *block = kTPB;

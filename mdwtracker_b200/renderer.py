@@ -295,6 +295,15 @@ class Renderer:
         self._call("copy_frame_rows", C.c_int(row0), C.c_int(row1), C.c_void_p(accum_ptr), C.c_void_p(fb_ptr),
                    C.c_void_p(stream) if stream else None)
 
+    def setTiming(self, enable: bool = True):
+        self._call("set_timing", C.c_int(1 if enable else 0))
+
+    def kernelTimes(self):
+        """(trace ms, resolve ms) of the last frame (timing on, one sample batch)."""
+        out = (C.c_float * 2)()
+        self._call("get_kernel_times", out)
+        return float(out[0]), float(out[1])
+
     def setTuning(self, key: int, value: int):
         """Tracker tuning knob (0 = regeneration pool); results do not depend on it."""
         self._call("set_tuning", C.c_int(key), C.c_int(value))
