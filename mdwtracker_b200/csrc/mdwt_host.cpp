@@ -140,6 +140,8 @@ struct mdwt_ctx {
   float *dPartial = nullptr;                          // running sums between batches
   uint32_t *dPartialStats = nullptr;
   size_t recCap = 0, recStatsCap = 0, partialCap = 0, partialStatsCap = 0;
+  float *dRecT = nullptr;                             // per-path primary hit t (gradient shading)
+  size_t recTCap = 0;
   float *dRanges = nullptr;
   float *dMaj = nullptr;
   uint16_t *dMask = nullptr;    // per-cell non-zero-majorant channel mask
@@ -444,6 +446,9 @@ void free_device(mdwt_ctx *c) {
   c->dMask = nullptr;
   if (c->dRec) cudaFree(c->dRec);
   if (c->dRecStats) cudaFree(c->dRecStats);
+  if (c->dRecT) cudaFree(c->dRecT);
+  c->dRecT = nullptr;
+  c->recTCap = 0;
   if (c->dPartial) cudaFree(c->dPartial);
   if (c->dPartialStats) cudaFree(c->dPartialStats);
   c->dRec = c->dRecStats = c->dPartialStats = nullptr;
@@ -888,9 +893,13 @@ mdwt_status mdwt_set_background(mdwt_ctx *c, const float rgb[3]) {
 }
 mdwt_status mdwt_set_light(mdwt_ctx *c, int shadows, int gradient, const float dir[3], float intensity, float ambient) {
   if (!c || !dir) return MDWT_ERR_BAD_ARG;
-  if (shadows || gradient) return fail(c, MDWT_ERR_UNSUPPORTED, "shadow rays and gradient shading are not in the GPU tracker yet");
-  c->shadows = false;
-  c->gradient = false;
+  // a shadow ray along a zero or non-finite direction would walk NaN distances until the
+  // step cap of every sample
+  const float n2 = dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2];
+  if (shadows && !(n2 > 0.0f && std::isfinite(n2)))
+    return fail(c, MDWT_ERR_BAD_ARG, "light direction must be finite and non-zero with shadows on");
+  c->shadows = shadows != 0;
+  c->gradient = gradient != 0;
   c->lightDir = v3(dir[0], dir[1], dir[2]);
   c->lightIntensity = intensity;
   c->ambient = ambient;
@@ -950,9 +959,16 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
     p.xd[i][0] = t.xd[0]; p.xd[i][1] = t.xd[1];
     p.os[i] = t.os;
     p.matSpec[i] = f3(c->mats[i].spec);
+    p.matDiffuse[i] = c->mats[i].diffuse;
+    p.matSpecular[i] = c->mats[i].specular;
+    p.matShininess[i] = c->mats[i].shininess;
+    p.matGradStep[i] = c->mats[i].gradStep;
   }
   p.lightIntensity = c->lightIntensity;
   p.ambient = c->ambient;
+  p.shadows = c->shadows ? 1 : 0;
+  p.gradient = c->gradient ? 1 : 0;
+  p.lightDir = f3(c->lightDir);
   p.accum = c->dAccum;
   p.fb = c->dFb;
   p.stats = c->statsOn ? c->dStats : nullptr;
@@ -988,6 +1004,7 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   if (nrect > 0) {
     if ((s = grow(c, (void **)&c->dRec, c->recCap, (size_t)batch * nrect * 4, "records")) != MDWT_OK) return s;
     if (stats && (s = grow(c, (void **)&c->dRecStats, c->recStatsCap, (size_t)batch * nrect * 4, "record stats")) != MDWT_OK) return s;
+    if (c->gradient && (s = grow(c, (void **)&c->dRecT, c->recTCap, (size_t)batch * nrect * 4, "hit distances")) != MDWT_OK) return s;
     if (batch < c->spp) {
       if ((s = grow(c, (void **)&c->dPartial, c->partialCap, nrect * 16, "partial sums")) != MDWT_OK) return s;
       if (stats && (s = grow(c, (void **)&c->dPartialStats, c->partialStatsCap, nrect * 16, "partial stats")) != MDWT_OK) return s;
@@ -995,6 +1012,7 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   }
   p.records = c->dRec;
   p.recStats = stats ? c->dRecStats : nullptr;
+  p.recT = c->gradient ? c->dRecT : nullptr;
   p.partial = c->dPartial;
   p.partialStats = stats ? c->dPartialStats : nullptr;
   // kernel timing: events around the trace and the resolve pass of a one-batch frame

@@ -51,6 +51,9 @@ struct TrackParams {
   // shading (defaults of renderer.h:125-130 unless set)
   float lightIntensity, ambient;
   F3 matSpec[kMaxChannels];
+  int shadows, gradient;         // shadow rays; gradient (Blinn-Phong) shading
+  F3 lightDir;
+  float matDiffuse[kMaxChannels], matSpecular[kMaxChannels], matShininess[kMaxChannels], matGradStep[kMaxChannels];
   // outputs
   float *accum;                  // float4 per pixel
   uint32_t *fb;                  // RGBA8 per pixel
@@ -76,6 +79,7 @@ struct TrackParams {
   int sBase, sCount;
   uint32_t *records;
   uint32_t *recStats;            // per-path density samples | rejections << 16 (stats only)
+  float *recT;                   // per-path world t of the primary hit (gradient shading only)
   float *partial;                // float4 running sums per rect pixel between batches
   uint32_t *partialStats;        // uint4 per rect pixel between batches (stats only)
 };

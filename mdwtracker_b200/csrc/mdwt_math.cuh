@@ -54,6 +54,32 @@ __device__ __forceinline__ float mlog(float x) {
   return fmaf(fe, 0.693145751953125f, fmaf(fe, 1.428606765330187e-06f, r));
 }
 
+// exp(z): z = k*ln2 + r (Cody-Waite reduction with ln2 split hi/lo), |r| <= ln2/2, the
+// degree-7 Taylor polynomial of e^r, times 2^k built in the exponent field; 0 below 2^-126.
+__device__ __forceinline__ float mexp(float z) {
+  if (!(z == z)) return z;
+  if (z > 88.0f) return __int_as_float(0x7f800000);
+  if (z < -87.0f) return 0.0f;
+  const float kf = rintf(z * 1.44269502162933349609375f);
+  float r = fmaf(-kf, 0.693145751953125f, z);
+  r = fmaf(-kf, 1.428606765330187e-06f, r);
+  float p = fmaf(r, 1.0f / 5040.0f, 1.0f / 720.0f);
+  p = fmaf(r, p, 1.0f / 120.0f);
+  p = fmaf(r, p, 1.0f / 24.0f);
+  p = fmaf(r, p, 1.0f / 6.0f);
+  p = fmaf(r, p, 0.5f);
+  p = fmaf(r, p, 1.0f);
+  p = fmaf(r, p, 1.0f);
+  const int k = (int)kf;
+  if (k < -126) return 0.0f;
+  return p * __uint_as_float((uint32_t)(k + 127) << 23);
+}
+// pow(x, y) for x >= 0: exp(y * log(x)), pow(0, y) = 0.
+__device__ __forceinline__ float mpow(float x, float y) {
+  if (x == 0.0f) return 0.0f;
+  return mexp(y * mlog(x));
+}
+
 __device__ __forceinline__ float quant(float a) { return rintf(a * 256.0f) * (1.0f / 256.0f); }
 __device__ __forceinline__ float lerpf(float a, float p, float q) { return fmaf(a, q, (1.0f - a) * p); }
 

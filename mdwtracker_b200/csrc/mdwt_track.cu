@@ -113,8 +113,8 @@ struct DDA {
   uint32_t visits;
 };
 
-__device__ __forceinline__ bool dda_init(const TrackParams &P, float dx, float dy, float dz, DDA &d) {
-  const float ox = P.gOrg.x, oy = P.gOrg.y, oz = P.gOrg.z;
+__device__ __forceinline__ bool dda_init(const TrackParams &P, float ox, float oy, float oz, float dx, float dy, float dz,
+                                         DDA &d) {
   const float fsx = (float)P.mc[0], fsy = (float)P.mc[1], fsz = (float)P.mc[2];
   const float rx = 1.0f / dx, ry = 1.0f / dy, rz = 1.0f / dz;
   const float tlx = (0.0f - ox) * rx, thx = (fsx - ox) * rx;
@@ -179,10 +179,33 @@ __device__ __forceinline__ void grid_dir(const TrackParams &P, float wdx, float 
   gx = gx * inv; gy = gy * inv; gz = gz * inv;
 }
 
+// Seeding, jitter and generateRay of one path-sample (deviceCode.cu:293-298, 61-76):
+// the normalised world direction; returns the generator state after the jitter draw.
+__device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, int py, int s, float &wdx, float &wdy,
+                                                float &wdz) {
+  const uint32_t seed = (uint32_t)P.W * (uint32_t)P.H * (P.frameParam + 1u) * (uint32_t)(s + 1);
+  uint32_t rng = tea4((uint32_t)px + seed, (uint32_t)py + seed);
+  const float jit = rng_next(rng);
+  const float sxf = ((float)px + jit) / (float)P.W;
+  const float syf = ((float)py + jit) / (float)P.H;
+  float dx = fmaf(syf, P.camVer.x, fmaf(sxf, P.camHor.x, P.camLlc.x));
+  float dy = fmaf(syf, P.camVer.y, fmaf(sxf, P.camHor.y, P.camLlc.y));
+  float dz = fmaf(syf, P.camVer.z, fmaf(sxf, P.camHor.z, P.camLlc.z));
+  if (fabsf(dx) < 1e-5f) dx = 1e-5f;
+  if (fabsf(dy) < 1e-5f) dy = 1e-5f;
+  if (fabsf(dz) < 1e-5f) dz = 1e-5f;
+  dx = dx - P.camOrg.x; dy = dy - P.camOrg.y; dz = dz - P.camOrg.z;
+  const float inv = 1.0f / sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+  wdx = dx * inv; wdy = dy * inv; wdz = dz * inv;
+  return rng;
+}
+
 enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_SAMPLE = 3, S_DONE = 4 };
 enum : int { A_CHAN = 0, A_ADVANCE = 1, A_NEWDDA = 2 };
 
-template <int MODE, int SK, bool STATS>
+// SH: shading variant -- shadow rays (when P.shadows) and the hit distance of every path
+// for gradient shading (when P.recT).
+template <int MODE, int SK, bool STATS, bool SH>
 __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_constant__ TrackParams P) {
   const int C = P.C;
   const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
@@ -221,6 +244,12 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
   float rnd = 0.f;                              // -m 1: the draw taken before a selection
   float majs[MODE == 1 ? kMaxChannels : 1], ts[MODE == 1 ? kMaxChannels : 1];   // -m 1 per-channel state
   bool capped = false;
+  float tHitW = 0.f;                            // world t of the recorded hit
+  // the current leg's world origin: the camera, or the hit point for a shadow ray
+  float lox = P.camOrg.x, loy = P.camOrg.y, loz = P.camOrg.z;
+  int leg = 0;                                  // 0 primary, 1 shadow ray (SH)
+  uint32_t primRec = 0, pxy = 0;
+  float primT = 0.f;
 
   auto enter_cell = [&]() {  // cell_t0 / cell_t1 of the DDA lambda call (dda.h:164-170)
     const float tc = fminf(fminf(d.tnx, d.tny), d.tnz);
@@ -231,11 +260,75 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
     cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
     cmask = __ldg(P.mask + cellID);
   };
+  // Start a tracking leg (volumeIntersection + the tracker's set-up, deviceCode.cu:759-778,
+  // 1676-1726) from the leg origin along (dx, dy, dz); false when it misses the volume.
+  auto start_leg = [&](float dx, float dy, float dz) -> bool {
+    wdx = dx; wdy = dy; wdz = dz;
+    const float frx = 1.0f / wdx, fry = 1.0f / wdy, frz = 1.0f / wdz;
+    const float ox = SH ? lox : P.camOrg.x, oy = SH ? loy : P.camOrg.y, oz = SH ? loz : P.camOrg.z;
+    const float t1 = (P.rootLo.x - ox) * frx, t2 = (P.rootHi.x - ox) * frx;
+    const float t3 = (P.rootLo.y - oy) * fry, t4 = (P.rootHi.y - oy) * fry;
+    const float t5 = (P.rootLo.z - oz) * frz, t6 = (P.rootHi.z - oz) * frz;
+    const float th0 = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
+    const float th1 = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
+    if (th1 < 0 || th0 >= th1) return false;
+    t1w = fminf(1e20f, th1);
+    float gx, gy, gz;
+    grid_dir(P, wdx, wdy, wdz, gx, gy, gz, w2g, g2w);
+    ch = 0;
+    record = 0;
+    steps = 0;
+    capped = false;
+    st = S_TRANS;
+    if (MODE != 0) {
+      const float gox = SH ? P.gScale.x * (lox - P.gLo.x) : P.gOrg.x;
+      const float goy = SH ? P.gScale.y * (loy - P.gLo.y) : P.gOrg.y;
+      const float goz = SH ? P.gScale.z * (loz - P.gLo.z) : P.gOrg.z;
+      if (!dda_init(P, gox, goy, goz, gx, gy, gz, d)) return false;
+      enter_cell();
+      lim = ct1;
+      act = A_CHAN;
+    } else {
+      lim = 1e20f;
+      act = A_NEWDDA;
+    }
+    return true;
+  };
+  // End of a leg: a primary hit with shadows on continues as the shadow ray
+  // (deviceCode.cu:380-397), otherwise the path record is written.
   auto finish = [&]() {
-    P.records[recIdx] = capped ? 0u : record;
+    bool shadowed = false;
+    if constexpr (SH) {
+      if (P.shadows && leg == 0 && record != 0u && !capped) {
+        primRec = record;
+        primT = tHitW;
+        leg = 1;
+        lox = fmaf(tHitW, wdx, P.camOrg.x);
+        loy = fmaf(tHitW, wdy, P.camOrg.y);
+        loz = fmaf(tHitW, wdz, P.camOrg.z);
+        const uint32_t sseed = (uint32_t)P.W * (uint32_t)P.H * P.frameParam;
+        rng = tea4((pxy & 0xffffu) + sseed + 1u, (pxy >> 16) + sseed + 1u);
+        if (start_leg(-P.lightDir.x, -P.lightDir.y, -P.lightDir.z)) return;
+        record = 0u;
+        capped = false;
+      }
+      if (leg == 1) {
+        shadowed = record != 0u && !capped;
+        if (capped) totCap++;
+        record = primRec;
+        tHitW = primT;
+        capped = false;
+      }
+    }
+    P.records[recIdx] = capped ? 0u : (record | (shadowed ? (1u << 9) : 0u));
+    if (SH && P.recT) P.recT[recIdx] = tHitW;
     if (STATS) P.recStats[recIdx] = (pSamp < 0xffffu ? pSamp : 0xffffu) | ((pRej < 0xffffu ? pRej : 0xffffu) << 16);
     totPaths++;
     if (capped) totCap++;
+    if constexpr (SH) {
+      leg = 0;
+      lox = P.camOrg.x; loy = P.camOrg.y; loz = P.camOrg.z;
+    }
     st = S_NEED;
   };
 
@@ -268,53 +361,15 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
           if (px <= P.cullX1 && py <= P.cullY1) {
             const int s = P.sBase + k;
             recIdx = (size_t)k * nrect + (size_t)ly * rw + lx;
+            pxy = (uint32_t)px | ((uint32_t)py << 16);
             record = 0;
             capped = false;
             steps = 0;
+            tHitW = 0.f;
             pSamp = pRej = 0;
-            // seeding, jitter, generateRay (deviceCode.cu:293-298, 61-76)
-            const uint32_t seed = (uint32_t)P.W * (uint32_t)P.H * (P.frameParam + 1u) * (uint32_t)(s + 1);
-            rng = tea4((uint32_t)px + seed, (uint32_t)py + seed);
-            const float jit = rng_next(rng);
-            const float sxf = ((float)px + jit) / (float)P.W;
-            const float syf = ((float)py + jit) / (float)P.H;
-            float dx = fmaf(syf, P.camVer.x, fmaf(sxf, P.camHor.x, P.camLlc.x));
-            float dy = fmaf(syf, P.camVer.y, fmaf(sxf, P.camHor.y, P.camLlc.y));
-            float dz = fmaf(syf, P.camVer.z, fmaf(sxf, P.camHor.z, P.camLlc.z));
-            if (fabsf(dx) < 1e-5f) dx = 1e-5f;
-            if (fabsf(dy) < 1e-5f) dy = 1e-5f;
-            if (fabsf(dz) < 1e-5f) dz = 1e-5f;
-            dx = dx - P.camOrg.x; dy = dy - P.camOrg.y; dz = dz - P.camOrg.z;
-            const float inv = 1.0f / sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
-            wdx = dx * inv; wdy = dy * inv; wdz = dz * inv;
-            // volumeIntersection against the union box (deviceCode.cu:1676-1726)
-            const float frx = 1.0f / wdx, fry = 1.0f / wdy, frz = 1.0f / wdz;
-            const float t1 = (P.rootLo.x - P.camOrg.x) * frx, t2 = (P.rootHi.x - P.camOrg.x) * frx;
-            const float t3 = (P.rootLo.y - P.camOrg.y) * fry, t4 = (P.rootHi.y - P.camOrg.y) * fry;
-            const float t5 = (P.rootLo.z - P.camOrg.z) * frz, t6 = (P.rootHi.z - P.camOrg.z) * frz;
-            const float th0 = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
-            const float th1 = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
-            if (th1 < 0 || th0 >= th1) {
-              finish();
-            } else {
-              t1w = fminf(1e20f, th1);
-              float gx, gy, gz;
-              grid_dir(P, wdx, wdy, wdz, gx, gy, gz, w2g, g2w);
-              ch = 0;
-              st = S_TRANS;
-              if (MODE != 0) {
-                if (dda_init(P, gx, gy, gz, d)) {
-                  enter_cell();
-                  lim = ct1;
-                  act = A_CHAN;
-                } else {
-                  finish();
-                }
-              } else {
-                lim = 1e20f;
-                act = A_NEWDDA;
-              }
-            }
+            float dx, dy, dz;
+            rng = primary_ray(P, px, py, s, dx, dy, dz);
+            if (!start_leg(dx, dy, dz)) finish();
           }
         }
       }
@@ -355,7 +410,10 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
               if (ch >= C) break;
               float gx, gy, gz, a, b;
               grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
-              if (!dda_init(P, gx, gy, gz, d)) { ch++; continue; }
+              const float gox = SH ? P.gScale.x * (lox - P.gLo.x) : P.gOrg.x;
+              const float goy = SH ? P.gScale.y * (loy - P.gLo.y) : P.gOrg.y;
+              const float goz = SH ? P.gScale.z * (loz - P.gLo.z) : P.gOrg.z;
+              if (!dda_init(P, gox, goy, goz, gx, gy, gz, d)) { ch++; continue; }
               enter_cell();
             } else if (act == A_ADVANCE) {
               if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; act = A_NEWDDA; continue; }
@@ -446,9 +504,9 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
 
     // ---------------- phase 2: the pending density samples, together
     if (st == S_SAMPLE) {
-      const float xs = fmaf(tW, wdx, P.camOrg.x) * P.w2u.x;
-      const float ys = fmaf(tW, wdy, P.camOrg.y) * P.w2u.y;
-      const float zs = fmaf(tW, wdz, P.camOrg.z) * P.w2u.z;
+      const float xs = fmaf(tW, wdx, SH ? lox : P.camOrg.x) * P.w2u.x;
+      const float ys = fmaf(tW, wdy, SH ? loy : P.camOrg.y) * P.w2u.y;
+      const float zs = fmaf(tW, wdz, SH ? loz : P.camOrg.z) * P.w2u.z;
       st = S_STEP;
       if constexpr (MODE == 3) {  // one threshold walked down through the channels (deviceCode.cu:590-613)
         float thr = rng_next(rng) * maj;
@@ -463,6 +521,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
           const float a = tf_alpha(cs, v, tax);
           if (a > 0.0f && thr < a) {
             record = make_record(c, tax);
+            if constexpr (SH) tHitW = tW;
             hitNow = true;
             break;
           }
@@ -487,6 +546,7 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
           const float a = tf_alpha(cs, v, tax);
           if (a > 0.0f && thr < a) {
             record = make_record(ch, tax);
+            if constexpr (SH) tHitW = tW;
             if constexpr (MODE == 2) lim = fminf(t, lim);
             if constexpr (MODE == 0) { lim = fminf(t, lim); ch++; act = A_NEWDDA; st = S_TRANS; }
             if constexpr (MODE == 1) finish();
@@ -541,14 +601,100 @@ __device__ __forceinline__ void write_pixel(const TrackParams &P, int px, int py
   if (STATS) reinterpret_cast<uint4 *>(P.stats)[pix] = st;
 }
 
-template <bool STATS>
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+  return fmaf(az, bz, fmaf(ay, by, ax * bx));
+}
+__device__ __forceinline__ void normalize3(float &x, float &y, float &z) {
+  const float s = 1.0f / sqrtf(fmaf(z, z, fmaf(y, y, x * x)));
+  x = s * x; y = s * y; z = s * z;
+}
+
+// transferFunction(sampleVolumeTexture(p, c), c).w (deviceCode.cu:27-42, 122-132) for any
+// position, outside positions giving NaN.
+template <int SK>
+__device__ __forceinline__ float alpha_at(const ChanSm &cs, float x, float y, float z) {
+  float v;
+  if (x < 0.0f || x > 1.0f || y < 0.0f || y > 1.0f || z < 0.0f || z > 1.0f) {
+    v = __int_as_float(0x7fc00000);
+  } else {
+    const Axis ax = axis(x, cs.X), ay = axis(y, cs.Y), az = axis(z, cs.Z);
+    v = trilinear<SK, size_t>(cs.vol, cs.X, cs.Y, ax, ay, az);
+  }
+  Axis t;
+  return tf_alpha(cs, v, t);
+}
+
+// Gradient (Blinn-Phong) shading of a hit (deviceCode.cu:327-378, calculateGradient
+// deviceCode.cu:243-281): diffuse and specular factors.
+template <int SK>
+__device__ void gradient_shading(const TrackParams &P, int ch, float tHit, float dx, float dy, float dz, float &diffuse,
+                                 float &specular) {
+  ChanSm cs;
+  cs.vol = P.vol[ch];
+  cs.tfAlpha = P.tfAlpha[ch];
+  cs.X = P.dims[ch][0]; cs.Y = P.dims[ch][1]; cs.Z = P.dims[ch][2];
+  cs.n = P.tfN[ch];
+  cs.vd0 = P.vd[ch][0]; cs.vd1 = P.vd[ch][1];
+  cs.xd0 = P.xd[ch][0]; cs.xd1 = P.xd[ch][1];
+  cs.os = P.os[ch];
+  const float tp[3] = {fmaf(tHit, dx, P.camOrg.x) * P.w2u.x, fmaf(tHit, dy, P.camOrg.y) * P.w2u.y,
+                       fmaf(tHit, dz, P.camOrg.z) * P.w2u.z};
+  const float eps = P.matGradStep[ch];
+  float g[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    float p1[3] = {tp[0], tp[1], tp[2]}, p2[3] = {tp[0], tp[1], tp[2]};
+    p1[i] -= eps;
+    p2[i] += eps;
+    float den;
+    if (p1[i] < 0.0f) {          // forward difference at the lower boundary
+      p1[i] = tp[i];
+      p2[i] = tp[i] + eps;
+      den = eps;
+    } else if (p2[i] > 1.0f) {   // backward difference at the upper boundary
+      p1[i] = tp[i] - eps;
+      p2[i] = tp[i];
+      den = eps;
+    } else {
+      den = 2.0f * eps;
+    }
+    const float a1 = alpha_at<SK>(cs, p1[0], p1[1], p1[2]);
+    const float a2 = alpha_at<SK>(cs, p2[0], p2[1], p2[2]);
+    g[i] = (a2 - a1) / den;
+  }
+  if (sqrtf(fmaf(g[2], g[2], fmaf(g[1], g[1], g[0] * g[0]))) > 1e-6f) {
+    float nx = -g[0], ny = -g[1], nz = -g[2];
+    normalize3(nx, ny, nz);
+    float lx = P.lightDir.x, ly = P.lightDir.y, lz = P.lightDir.z;
+    normalize3(lx, ly, lz);
+    float vx = -dx, vy = -dy, vz = -dz;
+    normalize3(vx, vy, vz);
+    float hx = lx + vx, hy = ly + vy, hz = lz + vz;
+    normalize3(hx, hy, hz);
+    const float NdotL = fmaxf(dot3(nx, ny, nz, lx, ly, lz), 0.0f);
+    const float NdotH = fmaxf(dot3(nx, ny, nz, hx, hy, hz), 0.0f);
+    diffuse = P.matDiffuse[ch] * NdotL;
+    if (NdotL > 0.0f && NdotH > 0.001f) {
+      const float sh = P.matShininess[ch];
+      const float normalization = (sh + 8.0f) / (8.0f * 3.14159265f);
+      specular = (P.matSpecular[ch] * normalization) * mpow(NdotH, sh);
+    } else {
+      specular = 0.0f;
+    }
+  } else {
+    diffuse = P.matDiffuse[ch];
+    specular = 0.0f;
+  }
+}
+
+template <bool STATS, bool SHADE, int SK>
 __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ TrackParams P) {
   const unsigned npix = (unsigned)P.W * (unsigned)(P.rowHi - P.rowLo);   // the rendered row band
   const int rw = P.cullX1 - P.cullX0 + 1;
   const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
   const bool last = P.sBase + P.sCount == P.spp;
-  const float kd = (1.0f * 1.0f) * P.lightIntensity;   // diffuse * shadow * lightIntensity (defaults)
-  const float ks = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
+  const float kd0 = (1.0f * 1.0f) * P.lightIntensity;   // diffuse * shadow * lightIntensity (unshaded)
+  const float ks0 = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
   uint32_t culledPaths = 0;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
     const int px = (int)(i % (unsigned)P.W), py = P.rowLo + (int)(i / (unsigned)P.W);
@@ -578,6 +724,18 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
         const float ar = lerpf(a, __ldg(R + 4 * i0 + 0), __ldg(R + 4 * i1 + 0));
         const float ag = lerpf(a, __ldg(R + 4 * i0 + 1), __ldg(R + 4 * i1 + 1));
         const float ab = lerpf(a, __ldg(R + 4 * i0 + 2), __ldg(R + 4 * i1 + 2));
+        float kd = kd0, ks = ks0;
+        if constexpr (SHADE) {
+          float diffuse = 1.0f, specular = 0.0f, shadow = 1.0f;
+          if (P.gradient && sqrtf(fmaf(ab, ab, fmaf(ag, ag, ar * ar))) > 0.001f) {
+            float dx, dy, dz;
+            primary_ray(P, px, py, P.sBase + k, dx, dy, dz);
+            gradient_shading<SK>(P, ch, P.recT[(size_t)k * nrect + q], dx, dy, dz, diffuse, specular);
+          }
+          if (P.shadows) shadow = (1.f - P.ambient) * (1.f - (((r >> 9) & 1u) ? 1.0f : 0.0f));
+          kd = (diffuse * shadow) * P.lightIntensity;
+          ks = (specular * shadow) * P.lightIntensity;
+        }
         const F3 sc = P.matSpec[ch];
         const float mr = fmaf(ar, 0.75f, sc.x * 0.25f);
         const float mg = fmaf(ag, 0.75f, sc.y * 0.25f);
@@ -613,10 +771,10 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
   if ((threadIdx.x & 31) == 0 && cp) atomicAdd(P.counters + 3, cp);
 }
 
-template <int MODE, int SK, bool STATS>
+template <int MODE, int SK, bool STATS, bool SH>
 int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
   int bps = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_kernel<MODE, SK, STATS>, kTPB, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_kernel<MODE, SK, STATS, SH>, kTPB, 0);
   if (e != cudaSuccess) return (int)e;
   if (bps < 1) bps = 1;
   *grid = numSMs * bps;
@@ -626,7 +784,7 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void 
   size_t chunk = items / ((size_t)*grid * (kTPB / 32) * 8);
   chunk = chunk < 32 ? 32 : (chunk > 256 ? 256 : chunk & ~(size_t)31);
   q.chunk = (int)chunk;
-  if (p.numTiles > 0) trace_kernel<MODE, SK, STATS><<<*grid, kTPB, 0, st>>>(q);
+  if (p.numTiles > 0) trace_kernel<MODE, SK, STATS, SH><<<*grid, kTPB, 0, st>>>(q);
   if (evMid) cudaEventRecord((cudaEvent_t)evMid, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
@@ -634,13 +792,15 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void 
   if (npix == 0) return (int)cudaGetLastError();
   size_t g = (npix + 255) / 256;
   if (g > (size_t)numSMs * 8) g = (size_t)numSMs * 8;
-  resolve_kernel<STATS><<<(unsigned)g, 256, 0, st>>>(p);
+  if (p.shadows || p.gradient) resolve_kernel<STATS, true, SK><<<(unsigned)g, 256, 0, st>>>(p);
+  else resolve_kernel<STATS, false, SK><<<(unsigned)g, 256, 0, st>>>(p);
   return (int)cudaGetLastError();
 }
 
 template <int MODE, int SK>
 int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
-  return p.stats ? launch_t<MODE, SK, true>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false>(p, st, numSMs, grid, evMid);
+  if (p.shadows || p.gradient) return p.stats ? launch_t<MODE, SK, true, true>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false, true>(p, st, numSMs, grid, evMid);
+  return p.stats ? launch_t<MODE, SK, true, false>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false, false>(p, st, numSMs, grid, evMid);
 }
 
 }  // namespace

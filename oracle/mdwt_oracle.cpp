@@ -126,6 +126,34 @@ static inline float mlog(float x) {
   return std::fma(fe, 0.693145751953125f, std::fma(fe, 1.428606765330187e-06f, r));
 }
 
+// exp(z): z = k*ln2 + r (Cody-Waite, ln2 split hi/lo), |r| <= ln2/2, degree-7 Taylor
+// polynomial of e^r, times 2^k built in the exponent field; 0 below 2^-126.
+static inline float mexp(float z) {
+  if (!(z == z)) return z;
+  if (z > 88.0f) return INFINITY;
+  if (z < -87.0f) return 0.0f;
+  const float kf = std::rint(z * 1.44269502162933349609375f);
+  float r = std::fma(-kf, 0.693145751953125f, z);
+  r = std::fma(-kf, 1.428606765330187e-06f, r);
+  float p = std::fma(r, 1.0f / 5040.0f, 1.0f / 720.0f);
+  p = std::fma(r, p, 1.0f / 120.0f);
+  p = std::fma(r, p, 1.0f / 24.0f);
+  p = std::fma(r, p, 1.0f / 6.0f);
+  p = std::fma(r, p, 0.5f);
+  p = std::fma(r, p, 1.0f);
+  p = std::fma(r, p, 1.0f);
+  const int k = (int)kf;
+  if (k < -126) return 0.0f;
+  uint32_t sb = (uint32_t)(k + 127) << 23;
+  float scale; std::memcpy(&scale, &sb, 4);
+  return p * scale;
+}
+// pow(x, y) for x > 0: exp(y * log(x)); pow(0, y > 0) = 0.
+static inline float mpow(float x, float y) {
+  if (x == 0.0f) return 0.0f;
+  return mexp(y * mlog(x));
+}
+
 // ---------------------------------------------------------------- filtering (S4-S6)
 static inline float quant(float a) { return std::rint(a * 256.0f) * (1.0f / 256.0f); }
 static inline float lerpf(float a, float p, float q) { return std::fma(a, q, (1.0f - a) * p); }
@@ -406,6 +434,17 @@ static inline float tf_eval(const TFData &t, float f, float *rgb) {
   return lerpf(a.a, t.rgba[4 * a.i0 + 3], t.rgba[4 * a.i1 + 3]) * t.os;
 }
 
+// transferFunction(...).w for any input, NaN included (gradient samples may fall outside
+// the volume): the domain test fails for NaN, so the remap and lookup run on NaN.
+static inline float tf_eval_any(const TFData &t, float f) {
+  if (t.n <= 0) return 0.f;
+  if (f < t.vd[0] || f > t.vd[1]) return 0.f;
+  float r1 = (f - t.vd[0]) / (t.vd[1] - t.vd[0]);
+  float r2 = (r1 - t.xd[0]) / (t.xd[1] - t.xd[0]);
+  Axis a = axis(r2, t.n);
+  return lerpf(a.a, t.rgba[4 * a.i0 + 3], t.rgba[4 * a.i1 + 3]) * t.os;
+}
+
 // ---------------------------------------------------------------- majorants (M)
 static float channel_majorant(const TFData &t, float mn, float mx) {
   // renderer.cu:159-203 body for one (cell, channel)
@@ -534,6 +573,38 @@ static void dda3(V3 org, V3 dir, float tMax, const uint32_t gs[3], L &&lam) {
       }
     }
   }
+}
+
+// device-side dot / normalize (x*x+y*y+z*z contracted like nvcc)
+static inline float dot_d(V3 a, V3 b) { return std::fma(a.z, b.z, std::fma(a.y, b.y, a.x * b.x)); }
+static inline V3 normalize_d(V3 v) { const float s = 1.0f / std::sqrt(len2_d(v)); return muls(s, v); }
+
+// calculateGradient (deviceCode.cu:243-281): central differences of the TF opacity,
+// one-sided at the [0,1] boundary.
+static V3 gradient_at(const Oracle &o, V3 p, float eps, int c) {
+  const float pp[3] = {p.x, p.y, p.z};
+  float g[3];
+  auto alpha_at = [&](const float q[3]) {
+    const float v = sample_volume(o, c, v3(q[0], q[1], q[2]));
+    return tf_eval_any(o.tf[c], v);
+  };
+  for (int i = 0; i < 3; i++) {
+    float p1[3] = {pp[0], pp[1], pp[2]}, p2[3] = {pp[0], pp[1], pp[2]};
+    p1[i] -= eps;
+    p2[i] += eps;
+    if (p1[i] < 0.0f) {
+      p1[i] = pp[i];
+      p2[i] = pp[i] + eps;
+      g[i] = (alpha_at(p2) - alpha_at(p1)) / eps;
+    } else if (p2[i] > 1.0f) {
+      p1[i] = pp[i] - eps;
+      p2[i] = pp[i];
+      g[i] = (alpha_at(p2) - alpha_at(p1)) / eps;
+    } else {
+      g[i] = (alpha_at(p2) - alpha_at(p1)) / (2.0f * eps);
+    }
+  }
+  return v3(g[0], g[1], g[2]);
 }
 
 // ---------------------------------------------------------------- trackers (W)
@@ -826,7 +897,59 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
       chx ^= (uint32_t)(prd.channelID + 1) << (sampleID & 15);
       const float *alb = prd.rgb;
       const Material &m = o.mats[prd.channelID];
-      const float diffuse = 1.0f, specular = 0.0f, shadow = 1.0f;
+      float diffuse = 1.0f, specular = 0.0f, shadow = 1.0f;
+      // deviceCode.cu:327-403: gradient (Blinn-Phong) shading and the shadow ray
+      const bool calcShading = o.gradient && o.mode < 6 &&
+                               std::sqrt(len2_d(v3(alb[0], alb[1], alb[2]))) > 0.001f;
+      const bool calcShadows = o.shadows && o.mode < 6;
+      if (calcShading) {
+        const V3 w2u = v3(1.f / (o.gHi[0] - o.gLo[0]), 1.f / (o.gHi[1] - o.gLo[1]), 1.f / (o.gHi[2] - o.gLo[2]));
+        V3 tp;
+        tp.x = std::fma(prd.tHit, dir.x, o.cOrg.x) * w2u.x;
+        tp.y = std::fma(prd.tHit, dir.y, o.cOrg.y) * w2u.y;
+        tp.z = std::fma(prd.tHit, dir.z, o.cOrg.z) * w2u.z;
+        const V3 g = gradient_at(o, tp, m.gradStep, prd.channelID);
+        if (std::sqrt(len2_d(g)) > 1e-6f) {
+          const V3 N = normalize_d(neg(g));
+          const V3 L = normalize_d(o.lightDir);
+          const V3 Vv = normalize_d(neg(dir));
+          const V3 Hh = normalize_d(add(L, Vv));
+          const float NdotL = std::fmax(dot_d(N, L), 0.0f);
+          const float NdotH = std::fmax(dot_d(N, Hh), 0.0f);
+          diffuse = m.diffuse * NdotL;
+          if (NdotL > 0.0f && NdotH > 0.001f) {
+            const float normalization = (m.shininess + 8.0f) / (8.0f * 3.14159265f);
+            specular = (m.specular * normalization) * mpow(NdotH, m.shininess);
+          } else {
+            specular = 0.0f;
+          }
+        } else {
+          diffuse = m.diffuse;
+          specular = 0.0f;
+        }
+      }
+      if (calcShadows) {
+        // shadow payload: t0 0, t1 1e20, LCG seeded from the frame (not the sample) and
+        // pixel + 1 (deviceCode.cu:380-397)
+        RayPayload sh;
+        sh.samples = sh.rejections = sh.cells = 0;
+        sh.t0 = 0.f;
+        sh.t1 = 1e20f;
+        const uint32_t sseed = (uint32_t)o.W * (uint32_t)o.H * (uint32_t)o.frameParam;
+        sh.rng.init((uint32_t)px + sseed + 1u, (uint32_t)py + sseed + 1u);
+        sh.steps = 0;
+        sh.capped = false;
+        V3 so;
+        so.x = std::fma(prd.tHit, dir.x, o.cOrg.x);
+        so.y = std::fma(prd.tHit, dir.y, o.cOrg.y);
+        so.z = std::fma(prd.tHit, dir.z, o.cOrg.z);
+        trace_volume(o, so, neg(o.lightDir), sh);
+        shadow = (1.f - o.ambient) * (1.f - (sh.missed ? 0.0f : 1.0f));
+        prd.samples += sh.samples;
+        prd.rejections += sh.rejections;
+        prd.cells += sh.cells;
+        if (sh.capped) capped++;
+      }
       const float kd = (diffuse * shadow) * o.lightIntensity;
       const float ks = (specular * shadow) * o.lightIntensity;
       const float sc[3] = {m.spec.x, m.spec.y, m.spec.z};
@@ -1046,7 +1169,7 @@ int orc_set_light(Oracle *o, int sh, int gr, const float d[3], float in, float a
   o->shadows = sh != 0; o->gradient = gr != 0;
   o->lightDir = v3(d[0], d[1], d[2]); o->lightIntensity = in; o->ambient = amb;
   o->accumID = 0; o->accumParam = 0;
-  return (sh || gr) ? ORC_UNSUP : ORC_OK;
+  return ORC_OK;
 }
 int orc_set_material(Oracle *o, int c, float di, float sp, float shin, float gs, const float rgb[3]) {
   if (c < 0 || c >= (int)o->mats.size()) return ORC_BAD;

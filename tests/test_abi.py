@@ -78,6 +78,11 @@ def test_bad_arguments():
     with pytest.raises(MdwtError) as e:
         r.PushMesh("/nonexistent/volume_uint8.raw")
     assert e.value.status == 9
+    with pytest.raises(MdwtError) as e:
+        r.setLight(True, False, (0.0, 0.0, 0.0))
+    assert e.value.status == 1
+    r.setLight(False, True, (0.0, 0.0, 0.0))      # gradient alone: NdotL clamps to 0
+    r.setLight(True, True, (0.0, -1.0, 0.0))
 
 
 def test_gpu_absent_is_an_error_not_a_fallback():

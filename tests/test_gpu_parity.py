@@ -242,3 +242,36 @@ def test_cli_on_the_gpu_matches_the_oracle(tmp_path, oracle):
     cli.run(b, o)
     np.testing.assert_array_equal(imageio.read_png(str(tmp_path / "gpu_AMMB_w_3_shadows_off_frames.png")),
                                   imageio.read_png(str(tmp_path / "cpu_AMMB_w_3_shadows_off_frames.png")))
+
+
+def _shade(r, shadows, gradient, light, nch):
+    r.setLight(shadows, gradient, light, 1.3, 0.15)
+    for i in range(nch):
+        r.setMaterial(i, diffuse=0.6 + 0.1 * i, specular=0.4, shininess=4.0 + 6.0 * i,
+                      gradientStep=(0.01, 0.2, 0.05)[i % 3], specularColor=(1.0, 0.9 - 0.2 * i, 0.8))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("shadows,gradient", [(True, False), (False, True), (True, True)])
+def test_shadows_and_gradient_shading(oracle, mode, shadows, gradient):
+    """Shadow rays traced by the same tracker from the hit point towards -lightDir
+    (deviceCode.cu:380-397) and Blinn-Phong shading from the opacity gradient
+    (deviceCode.cu:243-281, 327-378), bit for bit."""
+    vols = [noise_u8(40, occ, 30 + i) for i, occ in enumerate([0.15, 0.3])]
+    tfs = [syn.ramp_tf(syn.HUES[i], alpha_max=0.9) for i in range(2)]
+    p, o = make_pair(oracle, vols, tfs, mode, (5, 5, 5), (48, 40), 4)
+    for r in (p, o):
+        _shade(r, shadows, gradient, (0.35, -0.8, 0.25), 2)
+    run_frames(p, o, 3)
+
+
+@pytest.mark.parametrize("mode", [0, 2])
+def test_shading_float_channels_and_batches(oracle, mode):
+    """Float channels, an axis-aligned light (zero direction components), sample batches."""
+    vols = [syn.lognormal(36, 21 + i, octaves=4) for i in range(3)]
+    tfs = [syn.ramp_tf(syn.HUES[i], alpha_max=0.8) for i in range(3)]
+    p, o = make_pair(oracle, vols, tfs, mode, (4, 6, 5), (41, 33), 5, xf=[(0.0, 0.05)] * 3)
+    for r in (p, o):
+        _shade(r, True, True, (0.0, 0.0, -1.0), 3)
+    p.setTuning(1, 2)   # two samples per batch
+    run_frames(p, o, 2)

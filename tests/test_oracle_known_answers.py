@@ -157,3 +157,84 @@ def test_beer_lambert_slab(oracle):
         assert abs(phat - p) < 4.5 * sigma, (px, py, phat, p, sigma)
         n += 1
     assert n == 4
+
+
+def _shading_scene(oracle, light_dir, shadows, gradient, spp, value=0.5, alpha=1.0, dt=None, res=(9, 9)):
+    """Constant float volume over [0,1]^3 seen along +z from z = -2, one flat-colour TF."""
+    tf = np.zeros((64, 4), np.float32)
+    tf[:, :3] = (0.6, 0.3, 0.2)
+    tf[:, 3] = np.float32(alpha) ** (1.0 / 3.0)   # cubed on upload
+    o = oracle.OracleRenderer()
+    o.PushMesh(np.full((16, 16, 16), value, np.float32))
+    o.macrocellDims = (4, 4, 4)
+    o.Resize(res)
+    o.Init(2, False)
+    o.setCamera((0.5, 0.5, -2.0), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0), 8.0)
+    if dt is not None:
+        o.Setdt(dt)
+    o.SetXFColormap(tf, 0)
+    o.SetXFOpacityScale(1.0, 0)
+    o.SetXFRange((0.0, 1.0), 0)
+    o.setMaterial(0, diffuse=0.5, specular=0.3, shininess=8.0, gradientStep=0.01)
+    o.setLight(shadows, gradient, light_dir, 1.0, 0.1)
+    o.setSpp(spp)
+    o.setBackground((0.0, 0.0, 0.0))
+    o.enablePixelStats(True)
+    return o
+
+
+def _hit_colour(diffuse_times_shadow, ambient=0.1):
+    alb = np.float32([0.6, 0.3, 0.2])
+    mix = alb * np.float32(0.75) + np.float32(0.25)
+    return np.float32(ambient) * mix + np.float32(diffuse_times_shadow) * alb
+
+
+def test_gradient_of_constant_volume_is_material_diffuse(oracle):
+    """Zero opacity gradient -> diffuse = material diffuse, no specular (deviceCode.cu:372-376)."""
+    spp = 16
+    o = _shading_scene(oracle, (0.3, -1.0, 0.2), False, True, spp, alpha=0.5)
+    o.Render()
+    acc, st = o.accum(), o.pixelStats()
+    hits = st[..., 2].astype(np.float64)
+    assert hits.sum() > 0
+    want = hits[..., None] * _hit_colour(0.5)[None, None, :] / spp
+    np.testing.assert_allclose(acc[..., :3], want, rtol=2e-6, atol=1e-7)
+
+
+def test_shadow_rays_into_a_dense_medium_are_always_blocked(oracle):
+    """Light from behind the volume: the shadow ray crosses ~1 unit of a medium with
+    extinction 64 per unit, so every hit is shadowed: colour = ambient * mix only."""
+    spp = 16
+    o = _shading_scene(oracle, (0.0001, 0.0001, -1.0), True, False, spp, dt=1.0 / 64)
+    o.Render()
+    acc, st = o.accum(), o.pixelStats()
+    hits = st[..., 2].astype(np.float64)
+    assert hits.sum() > 0.9 * spp * acc.shape[0] * acc.shape[1] * 0.5
+    want = hits[..., None] * _hit_colour(0.0)[None, None, :] / spp
+    np.testing.assert_allclose(acc[..., :3], want, rtol=2e-6, atol=1e-7)
+
+
+def test_shadow_rays_back_towards_the_camera_follow_the_shared_shadow_seed(oracle):
+    """Light from the camera side.  Every shadow ray of a pixel in one frame starts from the
+    same generator state, seeded from the frame and pixel only (deviceCode.cu:385-386).
+    In a constant medium (majorant = density, every tentative collision is real) the shadow
+    ray's first free flight s = -ln(1 - u1) / sigma, u1 the generator's first draw, ends the
+    walk unless it leaves the front macrocell -- which here is leaving the volume.  A hit at
+    depth d (density sigma*exp(-sigma*d)) is lit iff d < s, so the lit fraction of the
+    pixel's samples is 1 - exp(-sigma*s) = u1."""
+    spp = 2048
+    o = _shading_scene(oracle, (0.0001, 0.0001, 1.0), True, False, spp, dt=1.0 / 64, res=(5, 5))
+    o.Render()
+    acc, st = o.accum(), o.pixelStats()
+    lit, dark = _hit_colour(0.9), _hit_colour(0.0)
+    us = []
+    for (py, px) in [(2, 2), (1, 2), (2, 3), (3, 1)]:
+        hits = float(st[py, px, 2])
+        assert hits > 0.99 * spp
+        # red channel: hits * (dark + u * (lit - dark)) / spp, u = lit fraction
+        u = (acc[py, px, 0] * spp / hits - dark[0]) / (lit[0] - dark[0])
+        u1 = float(oracle.rng_stream(px + 1, py + 1, 1)[0])    # frame 0: seed W*H*0
+        sigma = math.sqrt(max(u1 * (1 - u1), 1e-4) / hits)
+        assert abs(u - u1) < 4.5 * sigma + 0.01, (px, py, u, u1)
+        us.append(u1)
+    assert max(us) - min(us) > 0.05    # the pixels' generators differ
