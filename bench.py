@@ -16,6 +16,11 @@ device), frame, framebuffer copy to pinned host memory.  Under torchrun every ra
 renders its own frames (different frame seeds) with no collective: per-GPU work is
 fixed, `scaling` is weak, and time is the max over ranks.
 
+time_to_rmse (rank 0, one GPU; --no-ttr skips it): the first part of the headline metric
+-- how long plain accumulation takes at 1920x1080 (the 6 x 512^3 float32 log-normal scene,
+syncDDA) until the accumulation buffer is within RMSE 0.01 of the FP64 expected image of
+the estimator (libmdwt's mdwt_render_expected).
+
 --impl reference times the reference's path restated on the CPU (the OpenMP oracle,
 the reference itself cannot be built: no OptiX/OWL) on the same scene, on all host
 cores, each step a band of image rows; rank 0 only.
@@ -46,6 +51,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--res", type=int, nargs=2, default=None, help="override the resolution (smaller profiling cases)")
     ap.add_argument("--spp", type=int, default=None, help="override samples per pixel")
+    ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-RMSE measurement")
+    ap.add_argument("--ttr-config", default="c3", choices=["c1", "c2", "c3", "c3ndda"])
+    ap.add_argument("--ttr-target", type=float, default=0.01)
     return ap.parse_args()
 
 
@@ -177,6 +185,60 @@ def cpu_baseline(sc, budget_s, full=False):
     return {"value": ps / el / 1e9, "unit": "Gpath-samples/s", "cores": threads, "kind": "port",
             "sample": f"rows {r0}..{r0 + rows - 1} of the {w}x{h} frame at {sc.spp} spp "
                       f"({ps} path-samples, {el:.1f} s)"}, o
+
+
+def time_to_rmse(name, target, device_index, max_frames=20000):
+    """Plain accumulation until the accumulation buffer's RGB is within `target` RMSE of
+    the FP64 expected image: one sample per frame (frame f draws with seed factor f+1, so
+    no two samples of the run share a seed), the RMSE checked on the device after every
+    frame (first 16) and every 8th frame after that.  Time = device time of the frames
+    (CUDA events on the render stream) up to the first frame that meets the target."""
+    import torch
+    from mdwtracker_b200 import Renderer
+    sc = make_scene(name)
+    r = sc.setup(Renderer(device_index))
+    w, h = sc.resolution
+    t0 = time.perf_counter()
+    coarse = r.expectedImage(4, 0.5)
+    ref = r.expectedImage(8, 0.25)          # stays on the device for accumRmse
+    t_ref = time.perf_counter() - t0
+    quad = float(np.sqrt(np.mean((coarse - ref) ** 2)))
+    r.setSpp(1)
+    r.ResetAccumulation()
+    stream = torch.cuda.Stream(torch.device("cuda", device_index))
+    evs, trace = [], []
+    frames, rmse = 0, None
+    torch.cuda.synchronize()
+    tw = time.perf_counter()
+    while frames < max_frames:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r.Render(stream.cuda_stream)
+        b.record(stream)
+        evs.append((a, b))
+        frames += 1
+        if frames <= 16 or frames % 8 == 0:
+            torch.cuda.synchronize()
+            rmse = r.accumRmse()
+            if frames in (1, 4, 16, 64) or frames % 256 == 0:
+                trace.append([frames, rmse])
+            if rmse <= target:
+                break
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - tw
+    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    r.close()
+    return {
+        "target": target, "metric": "RMSE of linear RGB (accumulation buffer) vs the FP64 expected image",
+        "workload": workload_name(sc).replace(f"_{sc.spp}spp", ""), "resolution": [w, h], "mode": sc.mode,
+        "reference": {"kind": "FP64 expected image of the estimator (mdwt_render_expected)",
+                      "jitter_points": 8, "step_voxels": 0.25, "seconds": t_ref,
+                      "rmse_vs_4_jitter_0.5_voxel": quad},
+        "plain": {"reached": rmse is not None and rmse <= target, "frames": frames, "spp_total": frames,
+                  "rmse": rmse, "device_ms": dev_ms, "wall_ms": 1e3 * wall,
+                  "path_samples": frames * w * h, "trace": trace},
+        "denoised": None,
+    }
 
 
 def run_reference(args):
@@ -334,6 +396,13 @@ def main():
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "error": str(ex)}
 
+    ttr = None
+    if rank == 0 and world == 1 and not args.no_ttr:
+        try:
+            ttr = time_to_rmse(args.ttr_config, args.ttr_target, local)
+        except Exception as ex:  # reported beside the throughput line, never required
+            ttr = {"error": str(ex)}
+
     l2note = f"flushed between timed steps ({args.flush_mib} MiB write, outside the timed events)"
     line = {
         "metric": "Gpath-samples/s",
@@ -356,6 +425,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": world * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": w * h * 4, "ms_per_step": e2e},
+        "time_to_rmse": ttr,
         "gpu_launches": int(launches),
         "clocks": clk,
         "counters": {"density_samples": int(cnt[0]), "rejections": int(cnt[1]), "cells": int(cnt[2]),

@@ -221,6 +221,22 @@ mdwt_status mdwt_get_majorants(mdwt_ctx *ctx, float *host_out);
 /* macrocellsBuffer (renderer.cu:1116-1179): per (cell, channel) value range, 2*M*C floats. */
 mdwt_status mdwt_get_ranges(mdwt_ctx *ctx, float *host_out);
 
+/* ---- FP64 ground truth (no counterpart in the reference: the convergence measurement
+ * "RMSE of the accumulation buffer against an FP64 expected image")
+ * mdwt_render_expected: per pixel, the expected value of the unshaded estimator in double
+ * precision -- the integral over the root-box segment of T(t) * sum_c (alpha_c / dt) *
+ * colour_c plus T(exit) * background (every tracker -m 0..3 samples this first-collision
+ * distribution), midpoint rule with `step_voxels` of the smallest voxel edge, averaged over
+ * `jitter` points of the pixel's diagonal jitter.  Asynchronous on `stream` (NULL: the
+ * context's).  MDWT_ERR_UNSUPPORTED with shadows or gradient shading on.
+ * mdwt_get_expected: copy of the last expected image, W*H*3 doubles (row py*W + px, like
+ * the accumulation buffer).
+ * mdwt_accum_rmse: sqrt(mean over pixels and R, G, B of (accum - expected)^2), in double,
+ * synchronous. */
+mdwt_status mdwt_render_expected(mdwt_ctx *ctx, int jitter, float step_voxels, void *stream);
+mdwt_status mdwt_get_expected(mdwt_ctx *ctx, double *host_out);
+mdwt_status mdwt_accum_rmse(mdwt_ctx *ctx, double *rmse);
+
 /* No counterpart in the reference.  The value ranges of ONE channel, built on the GPU
  * without allocating any memory, for callers that may not allocate device memory: code
  * that runs inside an application's own memory pool or under an allocator that forbids

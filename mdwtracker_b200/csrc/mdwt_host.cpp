@@ -142,6 +142,11 @@ struct mdwt_ctx {
   size_t recCap = 0, recStatsCap = 0, partialCap = 0, partialStatsCap = 0;
   float *dRecT = nullptr;                             // per-path primary hit t (gradient shading)
   size_t recTCap = 0;
+  double *dExpected = nullptr;                        // FP64 expected image, W*H*3
+  size_t expectedCap = 0;
+  bool expectedValid = false;                         // matches the current W x H
+  double *dSqSum = nullptr;                           // RMSE reduction target
+  int expW = 0, expH = 0;
   float *dRanges = nullptr;
   float *dMaj = nullptr;
   uint16_t *dMask = nullptr;    // per-cell non-zero-majorant channel mask
@@ -449,6 +454,12 @@ void free_device(mdwt_ctx *c) {
   if (c->dRecT) cudaFree(c->dRecT);
   c->dRecT = nullptr;
   c->recTCap = 0;
+  if (c->dExpected) cudaFree(c->dExpected);
+  if (c->dSqSum) cudaFree(c->dSqSum);
+  c->dExpected = nullptr;
+  c->dSqSum = nullptr;
+  c->expectedCap = 0;
+  c->expectedValid = false;
   if (c->dPartial) cudaFree(c->dPartial);
   if (c->dPartialStats) cudaFree(c->dPartialStats);
   c->dRec = c->dRecStats = c->dPartialStats = nullptr;
@@ -923,12 +934,8 @@ mdwt_status mdwt_set_mirror(mdwt_ctx *c, int e) {
   return MDWT_OK;
 }
 
-mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
-  if (!c) return MDWT_ERR_BAD_ARG;
-  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
-  CK(cudaSetDevice(c->device), "cudaSetDevice");
-  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-  TrackParams p;
+// Scene, camera, transfer functions and shading of the next frame.
+static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   std::memset(&p, 0, sizeof(p));
   p.W = c->W; p.H = c->H; p.spp = c->spp;
   p.frameParam = (uint32_t)c->frameParam;
@@ -940,6 +947,7 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   p.rootLo = {c->rootLo[0], c->rootLo[1], c->rootLo[2]};
   p.rootHi = {c->rootHi[0], c->rootHi[1], c->rootHi[2]};
   p.gLo = {c->gLo[0], c->gLo[1], c->gLo[2]};
+  p.gHi = {c->gHi[0], c->gHi[1], c->gHi[2]};
   p.w2u = {1.f / (c->gHi[0] - c->gLo[0]), 1.f / (c->gHi[1] - c->gLo[1]), 1.f / (c->gHi[2] - c->gLo[2])};
   p.gScale = {(float)c->mc[0] * p.w2u.x, (float)c->mc[1] * p.w2u.y, (float)c->mc[2] * p.w2u.z};
   for (int a = 0; a < 3; a++) p.mc[a] = c->mc[a];
@@ -969,6 +977,15 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   p.shadows = c->shadows ? 1 : 0;
   p.gradient = c->gradient ? 1 : 0;
   p.lightDir = f3(c->lightDir);
+}
+
+mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  TrackParams p;
+  fill_scene(c, p);
   p.accum = c->dAccum;
   p.fb = c->dFb;
   p.stats = c->statsOn ? c->dStats : nullptr;
@@ -1038,6 +1055,56 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   // pre-increment values
   c->accumParam = c->accumID++;
   c->frameParam = c->frameID++;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_render_expected(mdwt_ctx *c, int jitter, float step_voxels, void *stream) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  if (jitter <= 0 || jitter > 1024 || !(step_voxels > 0.0f) || !std::isfinite(step_voxels))
+    return fail(c, MDWT_ERR_BAD_ARG, "jitter in [1, 1024] and a positive step");
+  if (c->shadows || c->gradient) return fail(c, MDWT_ERR_UNSUPPORTED, "expected image of the unshaded estimator only");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  TrackParams p;
+  fill_scene(c, p);
+  double h0 = 1e300;   // step: step_voxels times the smallest voxel edge in world units
+  for (auto &h : c->ch)
+    for (int a = 0; a < 3; a++) h0 = std::min(h0, ((double)h.hi[a] - (double)h.lo[a]) / (double)h.dims[a]);
+  h0 *= (double)step_voxels;
+  const size_t bytes = (size_t)c->W * c->H * 3 * sizeof(double);
+  mdwt_status s = grow(c, (void **)&c->dExpected, c->expectedCap, bytes, "expected image");
+  if (s != MDWT_OK) return s;
+  CKI(launch_expected(p, c->store, jitter, h0, c->dExpected, st, c->numSMs, &c->launches), "expected image kernel");
+  c->expectedValid = true;
+  c->expW = c->W;
+  c->expH = c->H;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_expected(mdwt_ctx *c, double *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->expectedValid || c->expW != c->W || c->expH != c->H)
+    return fail(c, MDWT_ERR_STATE, "mdwt_render_expected first (at the current size)");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(out, c->dExpected, (size_t)c->W * c->H * 3 * sizeof(double), cudaMemcpyDeviceToHost), "copy expected");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_accum_rmse(mdwt_ctx *c, double *rmse) {
+  if (!c || !rmse) return MDWT_ERR_BAD_ARG;
+  if (!c->expectedValid || c->expW != c->W || c->expH != c->H)
+    return fail(c, MDWT_ERR_STATE, "mdwt_render_expected first (at the current size)");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  if (!c->dSqSum) CK(cudaMalloc((void **)&c->dSqSum, sizeof(double)), "rmse scratch");
+  CK(cudaMemsetAsync(c->dSqSum, 0, sizeof(double), c->stream), "rmse scratch");
+  const size_t npix = (size_t)c->W * c->H;
+  CKI(launch_rmse(c->dAccum, c->dExpected, npix, c->dSqSum, c->stream, c->numSMs, &c->launches), "rmse kernel");
+  double sum = 0.0;
+  CK(cudaMemcpyAsync(&sum, c->dSqSum, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "rmse copy");
+  CK(cudaStreamSynchronize(c->stream), "rmse sync");
+  *rmse = std::sqrt(sum / (3.0 * (double)npix));
   return MDWT_OK;
 }
 

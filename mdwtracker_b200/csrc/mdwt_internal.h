@@ -31,6 +31,7 @@ struct TrackParams {
   F3 rootLo, rootHi;
   // grid transform of the trackers (deviceCode.cu:759-778), bounds of the last channel
   F3 gLo;        // worlddim.lower
+  F3 gHi;        // worlddim.upper
   F3 w2u;        // 1 / (upper - lower)
   F3 gScale;     // unitToGrid * worldToUnit (== worldToUnit * unitToGrid)
   uint32_t mc[3];
@@ -106,6 +107,13 @@ int launch_ranges(const void *vol, int storeKind, const int dims[3], const uint3
                   const int *ivx, const int *ivy, const int *ivz, int C, int ch,
                   float *ranges, float *scratchA, float *scratchB, void *stream, int *launches);
 // ranges initialised to (1e20, -1e20) (sizeMCs, renderer.cu:330-347)
+// FP64 expected image (W*H*3 doubles) of the unshaded estimator; J jitter points, world
+// step h0.  RMSE helper: *sum += sum over pixels of |accum.rgb - ref|^2 (sum zeroed by
+// the caller).
+int launch_expected(const TrackParams &p, int storeKind, int J, double h0, double *out, void *stream, int numSMs,
+                    int *launches);
+int launch_rmse(const float *accum, const double *ref, size_t npix, double *sum, void *stream, int numSMs,
+                int *launches);
 int launch_ranges_init(float *ranges, size_t count, void *stream, int *launches);
 
 struct MajorantParams {

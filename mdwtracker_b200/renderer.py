@@ -284,6 +284,26 @@ class Renderer:
         self._call("get_ranges", out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.reshape(n, 2)
 
+    # ---------------------------------------------------------------- FP64 ground truth
+    def renderExpected(self, jitter: int = 4, stepVoxels: float = 0.5, stream: Optional[int] = None):
+        """Compute the FP64 expected image of the unshaded estimator (asynchronous)."""
+        self._call("render_expected", C.c_int(jitter), C.c_float(stepVoxels),
+                   C.c_void_p(stream) if stream else None)
+
+    def expectedImage(self, jitter: int = 4, stepVoxels: float = 0.5) -> np.ndarray:
+        """(H, W, 3) float64 expected image (row 0 = framebuffer row 0)."""
+        self.renderExpected(jitter, stepVoxels)
+        w, h = self.fbSize
+        out = np.empty(w * h * 3, dtype=np.float64)
+        self._call("get_expected", out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out.reshape(h, w, 3)
+
+    def accumRmse(self) -> float:
+        """RMSE of the accumulation buffer's RGB against the last expected image."""
+        out = C.c_double()
+        self._call("accum_rmse", C.byref(out))
+        return out.value
+
     def setRenderRows(self, row0: int, row1: int):
         """Render only rows [row0, row1) (row1 <= row0: all rows); ids advance per frame."""
         self._call("set_render_rows", C.c_int(row0), C.c_int(row1))

@@ -985,6 +985,127 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
   }
 }
 
+// ---------------------------------------------------------------- FP64 expected image
+// The expected value of the tracker's per-sample estimate (unshaded: no shadow rays, no
+// gradient shading), per pixel, in double precision.  Every tracker (-m 0..3) samples
+// the first collision of the superposed channels: a channel-c collision at world
+// distance t has density T(t) * mu_c(t), mu_c = alpha_c / dt (dt scales every free
+// flight, deviceCode.cu:800-806), T the transmittance exp(-integral of sum_c mu_c), and
+// shows channel c's shaded TF colour (deviceCode.cu:408-433); no collision before the
+// root-box exit shows the background.  So
+//   E = mean over the pixel's jitter j of
+//       integral_{t0}^{t1} T(t) sum_c mu_c(t) C_c(t) dt + T(t1) bg,
+// j on the pixel diagonal (one jitter draw for x and y, deviceCode.cu:298).  The
+// integral is a midpoint rule in `stepVoxels` of the smallest voxel edge with the
+// extinction held constant over each step (exact exponential attenuation per step);
+// the jitter average is a J-point midpoint rule.  Opacity and colour use the tracker's
+// filtering semantics (8-bit fractional weights, clamp) evaluated in double.
+struct AxisD { int i0, i1; double a; };
+static inline AxisD axis_d(double u, int n) {
+  const double x = u * (double)n - 0.5;
+  const double fl = std::floor(x);
+  AxisD r;
+  r.a = std::rint((x - fl) * 256.0) / 256.0;
+  const long long i = (long long)fl;
+  r.i0 = (int)std::min<long long>(std::max<long long>(i, 0), n - 1);
+  r.i1 = (int)std::min<long long>(std::max<long long>(i, -1), n - 2) + 1;
+  return r;
+}
+static inline double lerp_d(double a, double p, double q) { return (1.0 - a) * p + a * q; }
+
+static double volume_d(const Oracle &o, int c, const double p[3]) {
+  for (int a = 0; a < 3; a++)
+    if (!(p[a] >= 0.0 && p[a] <= 1.0)) return NAN;
+  const Channel &h = o.ch[c];
+  const int X = (int)h.dims[0], Y = (int)h.dims[1], Z = (int)h.dims[2];
+  const AxisD ax = axis_d(p[0], X), ay = axis_d(p[1], Y), az = axis_d(p[2], Z);
+  auto at = [&](int x, int y, int z) { return (double)h.data[((size_t)z * Y + y) * X + x]; };
+  const double c00 = lerp_d(ax.a, at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0));
+  const double c10 = lerp_d(ax.a, at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0));
+  const double c01 = lerp_d(ax.a, at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1));
+  const double c11 = lerp_d(ax.a, at(ax.i0, ay.i1, az.i1), at(ax.i1, ay.i1, az.i1));
+  return lerp_d(az.a, lerp_d(ay.a, c00, c10), lerp_d(ay.a, c01, c11));
+}
+
+// alpha (times opacity scale) and rgb of channel c's TF at value f, in double
+static double tf_d(const TFData &t, double f, double rgb[3]) {
+  rgb[0] = rgb[1] = rgb[2] = 0.0;
+  if (t.n <= 0 || !(f >= (double)t.vd[0] && f <= (double)t.vd[1])) return 0.0;
+  const double r1 = (f - (double)t.vd[0]) / ((double)t.vd[1] - (double)t.vd[0]);
+  const double r2 = (r1 - (double)t.xd[0]) / ((double)t.xd[1] - (double)t.xd[0]);
+  const AxisD a = axis_d(r2, t.n);
+  for (int k = 0; k < 3; k++) rgb[k] = lerp_d(a.a, t.rgba[4 * a.i0 + k], t.rgba[4 * a.i1 + k]);
+  return lerp_d(a.a, t.rgba[4 * a.i0 + 3], t.rgba[4 * a.i1 + 3]) * (double)t.os;
+}
+
+static void expected_pixel(const Oracle &o, int px, int py, int J, double stepVoxels, double out[3]) {
+  const int C = (int)o.ch.size();
+  double h0 = 1e300;
+  for (auto &h : o.ch)
+    for (int a = 0; a < 3; a++) h0 = std::min(h0, ((double)h.hi[a] - (double)h.lo[a]) / (double)h.dims[a]);
+  h0 *= stepVoxels;
+  const double org[3] = {o.cOrg.x, o.cOrg.y, o.cOrg.z};
+  const double llc[3] = {o.cLlc.x, o.cLlc.y, o.cLlc.z}, hor[3] = {o.cHor.x, o.cHor.y, o.cHor.z};
+  const double ver[3] = {o.cVer.x, o.cVer.y, o.cVer.z};
+  const double w2u[3] = {1.0 / ((double)o.gHi[0] - o.gLo[0]), 1.0 / ((double)o.gHi[1] - o.gLo[1]),
+                         1.0 / ((double)o.gHi[2] - o.gLo[2])};
+  const double bg[3] = {o.bg.x, o.bg.y, o.bg.z};
+  const double dt = o.dt, amb = o.ambient, li = o.lightIntensity;
+  double acc[3] = {0, 0, 0};
+  for (int m = 0; m < J; m++) {
+    const double j = (m + 0.5) / J;
+    const double sx = (px + j) / o.W, sy = (py + j) / o.H;
+    double d[3];
+    for (int a = 0; a < 3; a++) {
+      d[a] = llc[a] + sx * hor[a] + sy * ver[a];
+      if (std::fabs(d[a]) < 1e-5) d[a] = 1e-5;   // generateRay clamps the point (deviceCode.cu:70-72)
+      d[a] -= org[a];
+    }
+    const double inv = 1.0 / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int a = 0; a < 3; a++) d[a] *= inv;
+    // root box and macrocell-grid box clip
+    double ta = 0.0, tb = 1e300;
+    for (int a = 0; a < 3; a++) {
+      const double lo[2] = {(double)o.rootLo[a], (double)o.gLo[a]}, hi[2] = {(double)o.rootHi[a], (double)o.gHi[a]};
+      for (int b = 0; b < 2; b++) {
+        const double t1 = (lo[b] - org[a]) / d[a], t2 = (hi[b] - org[a]) / d[a];
+        ta = std::max(ta, std::min(t1, t2));
+        tb = std::min(tb, std::max(t1, t2));
+      }
+    }
+    double L[3] = {0, 0, 0}, T = 1.0;
+    if (tb > ta) {
+      const long long n = (long long)std::ceil((tb - ta) / h0);
+      const double h = (tb - ta) / (double)n;
+      for (long long i = 0; i < n && T > 1e-300; i++) {
+        const double t = ta + (i + 0.5) * h;
+        double p[3];
+        for (int a = 0; a < 3; a++) p[a] = (org[a] + t * d[a]) * w2u[a];
+        double mu = 0.0, cw[3] = {0, 0, 0};
+        for (int c = 0; c < C; c++) {
+          const double v = volume_d(o, c, p);
+          if (v != v) continue;
+          double alb[3];
+          const double al = tf_d(o.tf[c], v, alb);
+          if (!(al > 0.0)) continue;
+          const double mc = al / dt;
+          mu += mc;
+          const Material &mt = o.mats[c];
+          const double sc[3] = {mt.spec.x, mt.spec.y, mt.spec.z};
+          for (int k = 0; k < 3; k++) cw[k] += mc * (amb * (0.75 * alb[k] + 0.25 * sc[k]) + li * alb[k]);
+        }
+        if (mu > 0.0) {
+          const double att = std::exp(-mu * h);
+          for (int k = 0; k < 3; k++) L[k] += T * (1.0 - att) * (cw[k] / mu);
+          T *= att;
+        }
+      }
+    }
+    for (int k = 0; k < 3; k++) acc[k] += L[k] + T * bg[k];
+  }
+  for (int k = 0; k < 3; k++) out[k] = acc[k] / J;
+}
+
 }  // namespace orc
 
 // ======================================================================= C ABI
@@ -1207,6 +1328,17 @@ int orc_render_rows(Oracle *o, int row0, int row1) {
   return ORC_OK;
 }
 int orc_render(Oracle *o) { return orc_render_rows(o, 0, 0); }
+// FP64 expected image (W*H*3 doubles, row-major like the accumulation buffer).
+int orc_expected_image(Oracle *o, int J, double stepVoxels, double *out) {
+  if (!o->inited) return ORC_STATE;
+  if (J <= 0 || !(stepVoxels > 0.0) || !out) return ORC_BAD;
+  if (o->shadows || o->gradient) { o->err = "expected image: unshaded only"; return ORC_UNSUP; }
+  const int W = o->W;
+  const int64_t n = (int64_t)o->W * o->H;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < n; i++) expected_pixel(*o, (int)(i % W), (int)(i / W), J, stepVoxels, out + 3 * i);
+  return ORC_OK;
+}
 int orc_sync(Oracle *) { return ORC_OK; }
 int orc_reset_accumulation(Oracle *o) { o->accumID = 0; o->accumParam = 0; return ORC_OK; }
 int orc_get_frame_ids(Oracle *o, int out[4]) {

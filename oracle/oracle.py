@@ -81,5 +81,24 @@ class OracleRenderer(Renderer):
     def Render(self, stream=None):
         self.renderRows(*self._band)
 
+    _expected = None
+
+    def renderExpected(self, jitter: int = 4, stepVoxels: float = 0.5, stream=None):
+        w, h = self.fbSize
+        out = np.empty(w * h * 3, dtype=np.float64)
+        self._call("expected_image", C.c_int(jitter), C.c_double(stepVoxels),
+                   out.ctypes.data_as(C.POINTER(C.c_double)))
+        self._expected = out.reshape(h, w, 3)
+
+    def expectedImage(self, jitter: int = 4, stepVoxels: float = 0.5) -> np.ndarray:
+        self.renderExpected(jitter, stepVoxels)
+        return self._expected.copy()
+
+    def accumRmse(self) -> float:
+        if self._expected is None:
+            raise MdwtError(6, "renderExpected first")
+        d = self.accum()[..., :3].astype(np.float64) - self._expected
+        return float(np.sqrt(np.mean(d * d)))
+
     def cappedSamples(self) -> int:
         return int(self._lib.orc_capped_samples(self._ctx))
