@@ -221,6 +221,16 @@ mdwt_status mdwt_get_majorants(mdwt_ctx *ctx, float *host_out);
 /* macrocellsBuffer (renderer.cu:1116-1179): per (cell, channel) value range, 2*M*C floats. */
 mdwt_status mdwt_get_ranges(mdwt_ctx *ctx, float *host_out);
 
+/* ---- denoiser features (no counterpart in the reference: the input of the learned
+ * denoiser).  With features on, every frame also writes 16 floats per pixel: the frame's
+ * mean radiance RGB, the first-collision depth (mean hit distance / (camera-to-box-centre
+ * distance + box diagonal), 0 without hits), the miss fraction (transmittance estimate),
+ * the hit fractions of channels 0..7 and three zeros.  Needs the frame in one sample batch
+ * and spp < 65536 (MDWT_ERR_UNSUPPORTED otherwise). */
+mdwt_status mdwt_set_features(mdwt_ctx *ctx, int enable);
+mdwt_status mdwt_get_features(mdwt_ctx *ctx, float *host_out);        /* W*H*16 */
+mdwt_status mdwt_get_device_features(mdwt_ctx *ctx, void **d_features);
+
 /* ---- FP64 ground truth (no counterpart in the reference: the convergence measurement
  * "RMSE of the accumulation buffer against an FP64 expected image")
  * mdwt_render_expected: per pixel, the expected value of the unshaded estimator in double

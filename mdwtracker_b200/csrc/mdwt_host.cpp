@@ -142,6 +142,9 @@ struct mdwt_ctx {
   size_t recCap = 0, recStatsCap = 0, partialCap = 0, partialStatsCap = 0;
   float *dRecT = nullptr;                             // per-path primary hit t (gradient shading)
   size_t recTCap = 0;
+  bool featOn = false;                                // denoiser features per frame
+  float *dFeat = nullptr;                             // W*H*16 floats
+  size_t featCap = 0;
   double *dExpected = nullptr;                        // FP64 expected image, W*H*3
   size_t expectedCap = 0;
   bool expectedValid = false;                         // matches the current W x H
@@ -454,6 +457,9 @@ void free_device(mdwt_ctx *c) {
   if (c->dRecT) cudaFree(c->dRecT);
   c->dRecT = nullptr;
   c->recTCap = 0;
+  if (c->dFeat) cudaFree(c->dFeat);
+  c->dFeat = nullptr;
+  c->featCap = 0;
   if (c->dExpected) cudaFree(c->dExpected);
   if (c->dSqSum) cudaFree(c->dSqSum);
   c->dExpected = nullptr;
@@ -934,6 +940,16 @@ mdwt_status mdwt_set_mirror(mdwt_ctx *c, int e) {
   return MDWT_OK;
 }
 
+// Depth-feature scale: 1 / (distance from the camera to the root-box centre + the box
+// diagonal), so that hit distances map into [0, 1].
+static float feature_scale(const mdwt_ctx *c) {
+  const float cx = (c->rootLo[0] + c->rootHi[0]) * 0.5f, cy = (c->rootLo[1] + c->rootHi[1]) * 0.5f,
+              cz = (c->rootLo[2] + c->rootHi[2]) * 0.5f;
+  const float dx = c->cOrg.x - cx, dy = c->cOrg.y - cy, dz = c->cOrg.z - cz;
+  const float ex = c->rootHi[0] - c->rootLo[0], ey = c->rootHi[1] - c->rootLo[1], ez = c->rootHi[2] - c->rootLo[2];
+  return 1.0f / (std::sqrt(dx * dx + dy * dy + dz * dz) + std::sqrt(ex * ex + ey * ey + ez * ez));
+}
+
 // Scene, camera, transfer functions and shading of the next frame.
 static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   std::memset(&p, 0, sizeof(p));
@@ -1021,7 +1037,9 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   if (nrect > 0) {
     if ((s = grow(c, (void **)&c->dRec, c->recCap, (size_t)batch * nrect * 4, "records")) != MDWT_OK) return s;
     if (stats && (s = grow(c, (void **)&c->dRecStats, c->recStatsCap, (size_t)batch * nrect * 4, "record stats")) != MDWT_OK) return s;
-    if (c->gradient && (s = grow(c, (void **)&c->dRecT, c->recTCap, (size_t)batch * nrect * 4, "hit distances")) != MDWT_OK) return s;
+    if ((c->gradient || c->featOn) &&
+        (s = grow(c, (void **)&c->dRecT, c->recTCap, (size_t)batch * nrect * 4, "hit distances")) != MDWT_OK)
+      return s;
     if (batch < c->spp) {
       if ((s = grow(c, (void **)&c->dPartial, c->partialCap, nrect * 16, "partial sums")) != MDWT_OK) return s;
       if (stats && (s = grow(c, (void **)&c->dPartialStats, c->partialStatsCap, nrect * 16, "partial stats")) != MDWT_OK) return s;
@@ -1029,7 +1047,15 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   }
   p.records = c->dRec;
   p.recStats = stats ? c->dRecStats : nullptr;
-  p.recT = c->gradient ? c->dRecT : nullptr;
+  p.recT = (c->gradient || c->featOn) ? c->dRecT : nullptr;
+  if (c->featOn) {
+    if (batch < c->spp || c->spp > 65535)
+      return fail(c, MDWT_ERR_UNSUPPORTED, "denoiser features need the frame in one sample batch and spp < 65536");
+    if ((s = grow(c, (void **)&c->dFeat, c->featCap, (size_t)c->W * c->H * 16 * sizeof(float), "features")) != MDWT_OK)
+      return s;
+    p.feat = c->dFeat;
+    p.featScale = feature_scale(c);
+  }
   p.partial = c->dPartial;
   p.partialStats = stats ? c->dPartialStats : nullptr;
   // kernel timing: events around the trace and the resolve pass of a one-batch frame
@@ -1055,6 +1081,27 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   // pre-increment values
   c->accumParam = c->accumID++;
   c->frameParam = c->frameID++;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_features(mdwt_ctx *c, int enable) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  c->featOn = enable != 0;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_features(mdwt_ctx *c, float *out) {
+  if (!c || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->featOn || !c->dFeat) return fail(c, MDWT_ERR_STATE, "mdwt_set_features(1) and a frame first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaDeviceSynchronize(), "sync");
+  CK(cudaMemcpy(out, c->dFeat, (size_t)c->W * c->H * 16 * sizeof(float), cudaMemcpyDeviceToHost), "copy features");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_get_device_features(mdwt_ctx *c, void **feat) {
+  if (!c || !feat) return MDWT_ERR_BAD_ARG;
+  *feat = c->featOn ? c->dFeat : nullptr;
   return MDWT_OK;
 }
 

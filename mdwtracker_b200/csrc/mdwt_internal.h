@@ -80,7 +80,9 @@ struct TrackParams {
   int sBase, sCount;
   uint32_t *records;
   uint32_t *recStats;            // per-path density samples | rejections << 16 (stats only)
-  float *recT;                   // per-path world t of the primary hit (gradient shading only)
+  float *recT;                   // per-path world t of the primary hit (gradient shading, features)
+  float *feat;                   // 16 floats per pixel of denoiser features, or null
+  float featScale;               // depth feature = mean hit distance * featScale
   float *partial;                // float4 running sums per rect pixel between batches
   uint32_t *partialStats;        // uint4 per rect pixel between batches (stats only)
 };

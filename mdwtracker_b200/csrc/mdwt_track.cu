@@ -203,8 +203,8 @@ __device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, in
 enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_SAMPLE = 3, S_DONE = 4 };
 enum : int { A_CHAN = 0, A_ADVANCE = 1, A_NEWDDA = 2 };
 
-// SH: shading variant -- shadow rays (when P.shadows) and the hit distance of every path
-// for gradient shading (when P.recT).
+// SH: extended variant -- shadow rays (when P.shadows) and the hit distance of every path
+// (when P.recT: gradient shading, denoiser features).
 template <int MODE, int SK, bool STATS, bool SH>
 __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_constant__ TrackParams P) {
   const int C = P.C;
@@ -582,6 +582,22 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
 }
 
 // Running mean into the accumulation buffer, RGBA8 write (deviceCode.cu:435, 463-471).
+// Denoiser input features of a pixel for this frame (16 floats): mean radiance RGB,
+// first-collision depth (mean hit distance times featScale, 0 without hits), the
+// transmittance estimate (miss fraction), the hit fractions of channels 0..7, zeros.
+__device__ __forceinline__ void write_features(const TrackParams &P, int px, int py, float r, float g, float b,
+                                               uint32_t hits, float sT, uint4 cnt) {
+  const float fs = (float)P.spp;
+  float4 *o = reinterpret_cast<float4 *>(P.feat) + 4 * ((size_t)px + (size_t)P.W * (size_t)py);
+  const float depth = hits ? (sT / (float)hits) * P.featScale : 0.f;
+  o[0] = make_float4(r, g, b, depth);
+  o[1] = make_float4((float)((uint32_t)P.spp - hits) / fs, (float)(cnt.x & 0xffffu) / fs, (float)(cnt.x >> 16) / fs,
+                     (float)(cnt.y & 0xffffu) / fs);
+  o[2] = make_float4((float)(cnt.y >> 16) / fs, (float)(cnt.z & 0xffffu) / fs, (float)(cnt.z >> 16) / fs,
+                     (float)(cnt.w & 0xffffu) / fs);
+  o[3] = make_float4((float)(cnt.w >> 16) / fs, 0.f, 0.f, 0.f);
+}
+
 template <bool STATS>
 __device__ __forceinline__ void write_pixel(const TrackParams &P, int px, int py, float o0, float o1, float o2, float o3,
                                             uint4 st) {
@@ -696,15 +712,20 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
   const float kd0 = (1.0f * 1.0f) * P.lightIntensity;   // diffuse * shadow * lightIntensity (unshaded)
   const float ks0 = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
   uint32_t culledPaths = 0;
+  const bool feat = P.feat != nullptr;   // denoiser features (one batch per frame)
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
     const int px = (int)(i % (unsigned)P.W), py = P.rowLo + (int)(i / (unsigned)P.W);
     if (px < P.cullX0 || px > P.cullX1 || py < P.cullY0 || py > P.cullY1) {
       if (last) {
         write_pixel<STATS>(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], P.bgFin[3], make_uint4(0u, 0u, 0u, 0u));
+        if (feat) write_features(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], 0u, 0.f, make_uint4(0u, 0u, 0u, 0u));
         culledPaths += (uint32_t)P.spp;
       }
       continue;
     }
+    uint32_t hits = 0;
+    uint4 cnt = make_uint4(0u, 0u, 0u, 0u);   // hits of channels 0..7, 16 bits each
+    float sT = 0.f;                           // sum of the hits' world t, in sample order
     const size_t q = (size_t)(py - P.cullY0) * rw + (px - P.cullX0);
     float4 f = make_float4(0.f, 0.f, 0.f, 1.f);
     uint4 sv = make_uint4(0u, 0u, 0u, 0u);
@@ -745,6 +766,16 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
         cb = fmaf(P.ambient, mb, fmaf(ks, mb, kd * ab));
         ca = 1.0f;
         if (STATS) { sv.z++; sv.w ^= (uint32_t)(ch + 1) << ((P.sBase + k) & 15); }
+        if (feat) {
+          hits++;
+          sT += P.recT[(size_t)k * nrect + q];
+          const uint32_t inc = ch < 8 ? (1u << ((ch & 1) * 16)) : 0u;
+          const int w = ch >> 1;
+          cnt.x += w == 0 ? inc : 0u;
+          cnt.y += w == 1 ? inc : 0u;
+          cnt.z += w == 2 ? inc : 0u;
+          cnt.w += w == 3 ? inc : 0u;
+        }
       }
       if (STATS) {
         const uint32_t e = P.recStats[(size_t)k * nrect + q];
@@ -760,6 +791,7 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
     if (last) {
       const float fs = (float)P.spp;
       write_pixel<STATS>(P, px, py, f.x / fs, f.y / fs, f.z / fs, f.w / fs, sv);
+      if (feat) write_features(P, px, py, f.x / fs, f.y / fs, f.z / fs, hits, sT, cnt);
     } else {
       reinterpret_cast<float4 *>(P.partial)[q] = f;
       if (STATS) reinterpret_cast<uint4 *>(P.partialStats)[q] = sv;
@@ -799,7 +831,7 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void 
 
 template <int MODE, int SK>
 int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
-  if (p.shadows || p.gradient) return p.stats ? launch_t<MODE, SK, true, true>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false, true>(p, st, numSMs, grid, evMid);
+  if (p.shadows || p.recT) return p.stats ? launch_t<MODE, SK, true, true>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false, true>(p, st, numSMs, grid, evMid);
   return p.stats ? launch_t<MODE, SK, true, false>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false, false>(p, st, numSMs, grid, evMid);
 }
 

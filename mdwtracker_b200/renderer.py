@@ -284,6 +284,23 @@ class Renderer:
         self._call("get_ranges", out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.reshape(n, 2)
 
+    # ---------------------------------------------------------------- denoiser features
+    def setFeatures(self, enable: bool):
+        """Write the 16 denoiser input features per pixel with every frame."""
+        self._call("set_features", C.c_int(1 if enable else 0))
+
+    def features(self) -> np.ndarray:
+        """(H, W, 16) float32 features of the last frame."""
+        w, h = self.fbSize
+        out = np.empty(w * h * 16, dtype=np.float32)
+        self._call("get_features", out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out.reshape(h, w, 16)
+
+    def deviceFeatures(self) -> int:
+        p = C.c_void_p()
+        self._call("get_device_features", C.byref(p))
+        return p.value or 0
+
     # ---------------------------------------------------------------- FP64 ground truth
     def renderExpected(self, jitter: int = 4, stepVoxels: float = 0.5, stream: Optional[int] = None):
         """Compute the FP64 expected image of the unshaded estimator (asynchronous)."""

@@ -242,6 +242,9 @@ struct Oracle {
   std::vector<uint32_t> fb;
   bool statsOn = false;
   std::vector<uint32_t> stats;
+  bool featOn = false;
+  std::vector<float> feat;       // 16 per pixel
+  float featScale = 1.0f;
   uint64_t counters[4] = {0, 0, 0, 0};
   uint64_t capped = 0;
   float rootLo[3], rootHi[3];    // union of channel bounds (renderer.cpp:698-716)
@@ -865,6 +868,8 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
   RayPayload prd;
   prd.samples = prd.rejections = prd.cells = 0;
   uint32_t hits = 0, chx = 0;
+  uint32_t chcnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  float sT = 0.f;
   for (int sampleID = 0; sampleID < o.spp; sampleID++) {
     uint32_t seed = (uint32_t)o.W * (uint32_t)o.H * (uint32_t)(o.frameParam + 1) * (uint32_t)(sampleID + 1);
     Rng rng;
@@ -895,6 +900,8 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
     if (!prd.missed) {
       hits++;
       chx ^= (uint32_t)(prd.channelID + 1) << (sampleID & 15);
+      sT += prd.tHit;
+      if (prd.channelID < 8) chcnt[prd.channelID]++;
       const float *alb = prd.rgb;
       const Material &m = o.mats[prd.channelID];
       float diffuse = 1.0f, specular = 0.0f, shadow = 1.0f;
@@ -966,6 +973,15 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
     fin[3] += std::fma(oneMinusA, 1.0f, color[3]);
   }
   for (int k = 0; k < 4; k++) fin[k] = fin[k] / (float)o.spp;
+  if (o.featOn) {
+    float *f = &o.feat[16 * (size_t)fbOfs];
+    const float fs = (float)o.spp;
+    f[0] = fin[0]; f[1] = fin[1]; f[2] = fin[2];
+    f[3] = hits ? (sT / (float)hits) * o.featScale : 0.f;
+    f[4] = (float)((uint32_t)o.spp - hits) / fs;
+    for (int c = 0; c < 8; c++) f[5 + c] = (float)chcnt[c] / fs;
+    f[13] = f[14] = f[15] = 0.f;
+  }
   float *acc = &o.accumBuf[4 * (size_t)fbOfs];
   float out[4];
   if (o.accum) {
@@ -1310,6 +1326,15 @@ int orc_enable_pixel_stats(Oracle *o, int e) {
 int orc_render_rows(Oracle *o, int row0, int row1) {
   if (!o->inited) return ORC_STATE;
   if (row1 <= row0) { row0 = 0; row1 = o->H; }
+  if (o->featOn) {
+    // depth-feature scale: 1 / (camera-to-root-box-centre distance + box diagonal)
+    const float cx = (o->rootLo[0] + o->rootHi[0]) * 0.5f, cy = (o->rootLo[1] + o->rootHi[1]) * 0.5f,
+                cz = (o->rootLo[2] + o->rootHi[2]) * 0.5f;
+    const float dx = o->cOrg.x - cx, dy = o->cOrg.y - cy, dz = o->cOrg.z - cz;
+    const float ex = o->rootHi[0] - o->rootLo[0], ey = o->rootHi[1] - o->rootLo[1], ez = o->rootHi[2] - o->rootLo[2];
+    o->featScale = 1.0f / (std::sqrt(dx * dx + dy * dy + dz * dz) + std::sqrt(ex * ex + ey * ey + ez * ez));
+    o->feat.resize(16 * (size_t)o->W * o->H, 0.f);
+  }
   uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0, cap = 0;
   const int W = o->W;
   const int64_t n = (int64_t)(row1 - row0) * W;
@@ -1328,6 +1353,12 @@ int orc_render_rows(Oracle *o, int row0, int row1) {
   return ORC_OK;
 }
 int orc_render(Oracle *o) { return orc_render_rows(o, 0, 0); }
+int orc_set_features(Oracle *o, int e) { o->featOn = e != 0; return ORC_OK; }
+int orc_get_features(Oracle *o, float *out) {
+  if (!o->featOn || o->feat.empty()) return ORC_STATE;
+  std::memcpy(out, o->feat.data(), o->feat.size() * 4);
+  return ORC_OK;
+}
 // FP64 expected image (W*H*3 doubles, row-major like the accumulation buffer).
 int orc_expected_image(Oracle *o, int J, double stepVoxels, double *out) {
   if (!o->inited) return ORC_STATE;

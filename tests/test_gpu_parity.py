@@ -275,3 +275,22 @@ def test_shading_float_channels_and_batches(oracle, mode):
         _shade(r, True, True, (0.0, 0.0, -1.0), 3)
     p.setTuning(1, 2)   # two samples per batch
     run_frames(p, o, 2)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_denoiser_features(oracle, mode):
+    """Per-pixel denoiser features (radiance, depth, transmittance, channel hit fractions),
+    bit for bit, and the accumulation unchanged by turning them on."""
+    vols = [noise_u8(40, occ, 50 + i) for i, occ in enumerate([0.15, 0.25, 0.3])]
+    tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(3)]
+    p, o = make_pair(oracle, vols, tfs, mode, (5, 5, 5), (52, 36), 6)
+    for r in (p, o):
+        r.setFeatures(True)
+    for f in range(2):
+        p.Render()
+        o.Render()
+        assert_same_frame(p, o, f"frame {f}")
+        fp, fo = p.features(), o.features()
+        np.testing.assert_array_equal(fp.view(np.uint32), fo.view(np.uint32))
+    st = p.pixelStats()
+    np.testing.assert_allclose(fp[..., 4] * 6 + st[..., 2], 6, atol=1e-5)
