@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/mdwt.h"
+#include "../../include/mdwt_denoiser.h"
 #include "mdwt_internal.h"
 
 using namespace mdwt;
@@ -1148,6 +1149,31 @@ mdwt_status mdwt_accum_rmse(mdwt_ctx *c, double *rmse) {
   CK(cudaMemsetAsync(c->dSqSum, 0, sizeof(double), c->stream), "rmse scratch");
   const size_t npix = (size_t)c->W * c->H;
   CKI(launch_rmse(c->dAccum, c->dExpected, npix, c->dSqSum, c->stream, c->numSMs, &c->launches), "rmse kernel");
+  double sum = 0.0;
+  CK(cudaMemcpyAsync(&sum, c->dSqSum, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "rmse copy");
+  CK(cudaStreamSynchronize(c->stream), "rmse sync");
+  *rmse = std::sqrt(sum / (3.0 * (double)npix));
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoise(mdwt_ctx *c, mdwt_denoiser *d, float *out) {
+  if (!c || !d || !out) return MDWT_ERR_BAD_ARG;
+  if (!c->featOn || !c->dFeat) return fail(c, MDWT_ERR_STATE, "mdwt_set_features(1) and a frame first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  const mdwt_status s = mdwt_denoiser_infer(d, c->dFeat, out, 1, c->H, c->W, c->stream);
+  if (s != MDWT_OK) return fail(c, s, std::string("denoiser: ") + mdwt_denoiser_last_error(d));
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_image_rmse(mdwt_ctx *c, const float *img, double *rmse) {
+  if (!c || !img || !rmse) return MDWT_ERR_BAD_ARG;
+  if (!c->expectedValid || c->expW != c->W || c->expH != c->H)
+    return fail(c, MDWT_ERR_STATE, "mdwt_render_expected first (at the current size)");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  if (!c->dSqSum) CK(cudaMalloc((void **)&c->dSqSum, sizeof(double)), "rmse scratch");
+  CK(cudaMemsetAsync(c->dSqSum, 0, sizeof(double), c->stream), "rmse scratch");
+  const size_t npix = (size_t)c->W * c->H;
+  CKI(launch_rmse(img, c->dExpected, npix, c->dSqSum, c->stream, c->numSMs, &c->launches), "rmse kernel");
   double sum = 0.0;
   CK(cudaMemcpyAsync(&sum, c->dSqSum, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "rmse copy");
   CK(cudaStreamSynchronize(c->stream), "rmse sync");

@@ -1,0 +1,41 @@
+// mdwt_nn.h -- launchers of the denoiser kernels (mdwt_nn.cu).  Activations are BF16
+// NHWC, weights BF16 [tap][co][ci] (forward) / [tap][ci][co] with flipped taps (data
+// gradient), master weights, gradients and optimizer state FP32.  Every launcher returns
+// a cudaError_t value.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+namespace mdwt {
+namespace nn {
+
+// Y = act(conv3x3(X, Wt) + bias), zero padding; Cin % 16 == 0, Cout % 8 == 0;
+// bias may be null; Y is FP32 when outF32, else BF16.
+int conv3x3_fwd(const void *X, const void *Wt, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
+                int relu, int outF32, void *stream);
+// dW[tap][co][ci] += sum over pixels of dY[p][co] * X[p shifted by tap][ci] (dW zeroed by the caller)
+int conv3x3_wgrad(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin, int Cout, void *stream);
+int relu_bwd(void *dY, const void *Y, size_t n, int numSMs, void *stream);
+int avgpool2(const void *X, void *Y, int N, int H, int W, int C, int numSMs, void *stream);
+// dX (N x H x W x C) += upsampled dY / 4
+int avgpool2_bwd_add(const void *dY, void *dX, int N, int H, int W, int C, int numSMs, void *stream);
+// out (N x H x W x (Cu + Cs)) = concat(nearest-2x(coarse), skip)
+int up2_concat(const void *coarse, const void *skip, void *out, int N, int H, int W, int Cu, int Cs, int numSMs,
+               void *stream);
+int up2_concat_bwd(const void *dOut, void *dCoarse, void *dSkip, int N, int H, int W, int Cu, int Cs, int numSMs,
+                   void *stream);
+// db[c] += sum over P pixels of dY[p][c] (db zeroed by the caller), C <= 256
+int bias_grad(const void *dY, float *db, size_t P, int C, int numSMs, void *stream);
+// X [N][Hp][Wp][16] bf16 = F [N][H][W][16] fp32, zero outside H x W
+int pack_features(const float *F, void *X, int N, int H, int W, int Hp, int Wp, int numSMs, void *stream);
+// over the N x H x W pixels (O, dO padded to Hp x Wp): out4 (optional) = F.rgb + O[.., 0:3]
+// as RGBA (alpha 1); with target4: *lossSum += sum of squared RGB errors and
+// dO[.., 0:3] = 2 (out - target) * invCount (the rest of dO zeroed by the caller)
+int residual_out(const float *F, const float *O, int Co, float *out4, const float *target4, void *dO, double *lossSum,
+                 int N, int H, int W, int Hp, int Wp, float invCount, int numSMs, void *stream);
+int adam(float *Wm, float *mW, float *vW, const float *gW, void *Wf, void *Wd, int Cin, int Cout, float *b, float *mb,
+         float *vb, const float *gb, float lr, float b1, float b2, float eps, int step, int numSMs, void *stream);
+int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int numSMs, void *stream);
+
+}  // namespace nn
+}  // namespace mdwt

@@ -1,0 +1,93 @@
+"""Python binding of the learned denoiser (include/mdwt_denoiser.h).
+
+Buffers are device pointers (ints) or CUDA torch tensors on the denoiser's device:
+features [n][h][w][16] float32 (the tracker's per-pixel features, Renderer.setFeatures),
+targets and outputs [n][h][w][4] float32 RGBA.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from .renderer import MdwtError, load_library
+
+
+def _ptr(x) -> C.c_void_p:
+    if hasattr(x, "data_ptr"):
+        if not x.is_cuda or not x.is_contiguous() or str(x.dtype) != "torch.float32":
+            raise ValueError("denoiser buffers are contiguous float32 CUDA tensors")
+        return C.c_void_p(x.data_ptr())
+    return C.c_void_p(int(x))
+
+
+class Denoiser:
+    def __init__(self, device: int = 0, seed: int = 0, lib: Optional[C.CDLL] = None):
+        self._lib = lib if lib is not None else load_library()
+        self._lib.mdwt_denoiser_num_params.restype = C.c_int64
+        self._lib.mdwt_denoiser_last_error.restype = C.c_char_p
+        self._d = C.c_void_p()
+        st = self._lib.mdwt_denoiser_create(C.byref(self._d), C.c_int(device), C.c_uint64(seed))
+        if st != 0:
+            raise MdwtError(st, "denoiser_create", f"device {device}")
+
+    @staticmethod
+    def numParams(lib: Optional[C.CDLL] = None) -> int:
+        lib = lib if lib is not None else load_library()
+        lib.mdwt_denoiser_num_params.restype = C.c_int64
+        return int(lib.mdwt_denoiser_num_params())
+
+    def _call(self, name: str, *args):
+        st = getattr(self._lib, "mdwt_denoiser_" + name)(self._d, *args)
+        if st != 0:
+            raise MdwtError(st, "denoiser_" + name, (self._lib.mdwt_denoiser_last_error(self._d) or b"").decode())
+
+    def close(self):
+        if self._d:
+            self._lib.mdwt_denoiser_destroy(self._d)
+            self._d = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.numParams(self._lib), np.float32)
+        self._call("get_params", out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def setParams(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        if p.size != self.numParams(self._lib):
+            raise ValueError(f"expected {self.numParams(self._lib)} parameters, got {p.size}")
+        self._call("set_params", p.ctypes.data_as(C.POINTER(C.c_float)))
+
+    def grads(self) -> np.ndarray:
+        out = np.empty(self.numParams(self._lib), np.float32)
+        self._call("get_grads", out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def infer(self, features, out, n: int, h: int, w: int, stream: int = 0) -> None:
+        self._call("infer", _ptr(features), _ptr(out), C.c_int(n), C.c_int(h), C.c_int(w), C.c_void_p(stream or None))
+
+    def backward(self, features, target, n: int, h: int, w: int, stream: int = 0) -> float:
+        loss = C.c_double()
+        self._call("backward", _ptr(features), _ptr(target), C.c_int(n), C.c_int(h), C.c_int(w), C.byref(loss),
+                   C.c_void_p(stream or None))
+        return loss.value
+
+    def trainStep(self, features, target, n: int, h: int, w: int, lr: float, stream: int = 0,
+                  want_loss: bool = True) -> Optional[float]:
+        loss = C.c_double()
+        self._call("train_step", _ptr(features), _ptr(target), C.c_int(n), C.c_int(h), C.c_int(w), C.c_float(lr),
+                   C.byref(loss) if want_loss else None, C.c_void_p(stream or None))
+        return loss.value if want_loss else None
+
+    def save(self, path: str) -> None:
+        np.save(path, self.params())
+
+    def load(self, path: str) -> None:
+        self.setParams(np.load(path))

@@ -301,6 +301,18 @@ class Renderer:
         self._call("get_device_features", C.byref(p))
         return p.value or 0
 
+    def denoise(self, denoiser, out) -> None:
+        """Denoise the last frame's features into `out` ([H][W][4] float32 on the device)."""
+        from .denoiser import _ptr
+        self._call("denoise", denoiser._d, _ptr(out))
+
+    def imageRmse(self, img) -> float:
+        """RMSE of a device RGBA image [H][W][4] against the last expected image."""
+        from .denoiser import _ptr
+        out = C.c_double()
+        self._call("image_rmse", _ptr(img), C.byref(out))
+        return out.value
+
     # ---------------------------------------------------------------- FP64 ground truth
     def renderExpected(self, jitter: int = 4, stepVoxels: float = 0.5, stream: Optional[int] = None):
         """Compute the FP64 expected image of the unshaded estimator (asynchronous)."""

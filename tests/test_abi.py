@@ -13,9 +13,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def header_symbols():
-    text = open(os.path.join(ROOT, "include", "mdwt.h")).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(mdwt_[a-z0-9_]+)\s*\(", text)))
+    syms = set()
+    for h in ("mdwt.h", "mdwt_denoiser.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        syms |= set(re.findall(r"\b(mdwt_[a-z0-9_]+)\s*\(", text))
+    return sorted(syms)
 
 
 def test_header_declares_the_renderer_surface():
@@ -28,8 +31,18 @@ def test_header_declares_the_renderer_surface():
 
 
 def test_library_exports_every_declared_symbol(mdwt_lib):
-    missing = [s for s in header_symbols() if not hasattr(mdwt_lib, s)]
+    syms = header_symbols()
+    for must in ["mdwt_denoiser_create", "mdwt_denoiser_train_step", "mdwt_denoiser_infer", "mdwt_denoise",
+                 "mdwt_render_expected", "mdwt_accum_rmse", "mdwt_set_features"]:
+        assert must in syms
+    missing = [s for s in syms if not hasattr(mdwt_lib, s)]
     assert not missing, missing
+
+
+def test_denoiser_parameter_count_matches_the_reference_layout(mdwt_lib):
+    from mdwtracker_b200 import Denoiser
+    from oracle import denoiser_ref
+    assert Denoiser.numParams(mdwt_lib) == denoiser_ref.num_params()
 
 
 def test_status_strings(mdwt_lib):

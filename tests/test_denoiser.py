@@ -1,0 +1,117 @@
+"""The learned denoiser: the GPU forward pass and gradients against the NumPy restatement
+(oracle/denoiser_ref.py, float64 with BF16 rounding at the GPU's storage points), and
+training on the GPU by the library's own kernels.
+
+Tolerances: the GPU accumulates in FP32 in a different order and rounds activations to
+BF16, so an element near a BF16 rounding boundary can land one BF16 ulp (2^-8 relative)
+apart and carry that through later layers; outputs are compared within 1e-2 relative
+(norm) and every layer's weight gradient within 3e-2 relative (norm).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import denoiser_ref as R
+
+
+def test_reference_backward_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    p = R.init_params(3).astype(np.float64)
+    F = rng.random((1, 8, 8, 16)).astype(np.float32)
+    T = rng.random((1, 8, 8, 4)).astype(np.float32)
+    _, g = R.backward(p, F, T, bf16=False)
+    for i in rng.choice(len(p), 25, replace=False):
+        e = 1e-5 * max(1.0, abs(p[i]))
+        pp, pm = p.copy(), p.copy()
+        pp[i] += e
+        pm[i] -= e
+        fd = (R.backward(pp, F, T, bf16=False)[0] - R.backward(pm, F, T, bf16=False)[0]) / (2 * e)
+        assert abs(fd - g[i]) < 1e-8 + 1e-5 * abs(g[i]), (i, fd, g[i])
+
+
+def _features(rng, n, h, w):
+    f = np.zeros((n, h, w, 16), np.float32)
+    f[..., :3] = rng.random((n, h, w, 3))
+    f[..., 3] = rng.random((n, h, w))
+    f[..., 4] = rng.random((n, h, w))
+    f[..., 5:9] = rng.random((n, h, w, 4)) * 0.3
+    return f
+
+
+def _layer_slices():
+    out, k = [], 0
+    for ci, co, _ in R.SPEC:
+        out.append(slice(k, k + 9 * ci * co))
+        k += 9 * ci * co + co
+    return out
+
+
+@pytest.mark.gpu
+def test_gpu_forward_matches_the_reference():
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(5)
+    d = Denoiser(0, seed=1)
+    p = R.init_params(7)
+    d.setParams(p)
+    n, h, w = 2, 18, 26      # padded to 20 x 28 inside
+    F = _features(rng, n, h, w)
+    out = torch.empty((n, h, w, 4), dtype=torch.float32, device="cuda")
+    d.infer(torch.from_numpy(F).cuda(), out, n, h, w)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()[..., :3]
+    hp, wp = 20, 28
+    Fp = np.zeros((n, hp, wp, 16), np.float32)
+    Fp[:, :h, :w] = F
+    ref, _ = R.forward(p, Fp, bf16=True)
+    ref = ref[:, :h, :w]
+    rel = np.linalg.norm(got - ref) / np.linalg.norm(ref - F[..., :3])
+    assert rel < 1e-2, rel
+    assert np.all(out.cpu().numpy()[..., 3] == 1.0)
+
+
+@pytest.mark.gpu
+def test_gpu_gradients_match_the_reference():
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(9)
+    d = Denoiser(0)
+    p = R.init_params(11)
+    d.setParams(p)
+    n, h, w = 2, 16, 24
+    F = _features(rng, n, h, w)
+    T = rng.random((n, h, w, 4)).astype(np.float32)
+    loss = d.backward(torch.from_numpy(F).cuda(), torch.from_numpy(T).cuda(), n, h, w)
+    g = d.grads()
+    rloss, rg = R.backward(p, F, T, bf16=True)
+    assert abs(loss - rloss) < 1e-3 * rloss
+    for i, sl in enumerate(_layer_slices()):
+        a, b = g[sl].astype(np.float64), rg[sl]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert rel < 3e-2, (i, rel)
+    # biases
+    k = 0
+    for i, (ci, co, _) in enumerate(R.SPEC):
+        k += 9 * ci * co
+        a, b = g[k:k + co].astype(np.float64), rg[k:k + co]
+        assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b) + 1e-7, i
+        k += co
+
+
+@pytest.mark.gpu
+def test_gpu_training_fits_a_fixed_batch():
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(2)
+    d = Denoiser(0, seed=3)
+    n, h, w = 4, 32, 32
+    F = _features(rng, n, h, w)
+    # target: a smooth function of the features the network can learn
+    T = np.zeros((n, h, w, 4), np.float32)
+    T[..., :3] = 0.5 * F[..., :3] + 0.25 * F[..., 3:4]
+    Ft, Tt = torch.from_numpy(F).cuda(), torch.from_numpy(T).cuda()
+    first = d.trainStep(Ft, Tt, n, h, w, 1e-3)
+    for _ in range(150):
+        last = d.trainStep(Ft, Tt, n, h, w, 1e-3)
+    assert math.isfinite(last) and last < 0.1 * first, (first, last)
