@@ -19,7 +19,9 @@ fixed, `scaling` is weak, and time is the max over ranks.
 time_to_rmse (rank 0, one GPU; --no-ttr skips it): the first part of the headline metric
 -- how long plain accumulation takes at 1920x1080 (the 6 x 512^3 float32 log-normal scene,
 syncDDA) until the accumulation buffer is within RMSE 0.01 of the FP64 expected image of
-the estimator (libmdwt's mdwt_render_expected).
+the estimator (libmdwt's mdwt_render_expected) -- and how long one low-spp frame plus the
+learned denoiser (weights in mdwtracker_b200/weights, trained by
+mdwtracker_b200/train_denoiser.py) takes to get there.
 
 --impl reference times the reference's path restated on the CPU (the OpenMP oracle,
 the reference itself cannot be built: no OptiX/OWL) on the same scene, on all host
@@ -227,7 +229,14 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     torch.cuda.synchronize()
     wall = time.perf_counter() - tw
     dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    denoised = None
+    try:
+        denoised = denoised_time_to_rmse(r, target, stream)
+    except Exception as ex:  # reported, never required
+        denoised = {"error": str(ex)}
     r.close()
+    if denoised and denoised.get("device_ms"):
+        denoised["speedup_vs_plain"] = dev_ms / denoised["device_ms"]
     return {
         "target": target, "metric": "RMSE of linear RGB (accumulation buffer) vs the FP64 expected image",
         "workload": workload_name(sc).replace(f"_{sc.spp}spp", ""), "resolution": [w, h], "mode": sc.mode,
@@ -237,8 +246,64 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
         "plain": {"reached": rmse is not None and rmse <= target, "frames": frames, "spp_total": frames,
                   "rmse": rmse, "device_ms": dev_ms, "wall_ms": 1e3 * wall,
                   "path_samples": frames * w * h, "trace": trace},
-        "denoised": None,
+        "denoised": denoised,
     }
+
+
+DENOISER_WEIGHTS = os.path.join(ROOT, "mdwtracker_b200", "weights", "denoiser_c3_syncdda.npy")
+
+
+def denoised_time_to_rmse(r, target, stream, spps=(1, 2, 4, 8, 16, 32, 64), reps=3):
+    """One k-spp frame with the denoiser features, then the learned denoiser; the smallest
+    k whose denoised image is within `target` RMSE of the FP64 expected image.  Time =
+    device time of the frame + the denoiser (CUDA events on the render stream, best of
+    `reps` runs after a warm-up of the same k, fresh sample seeds per run)."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    if not os.path.exists(DENOISER_WEIGHTS):
+        return {"error": f"no trained weights at {os.path.relpath(DENOISER_WEIGHTS, ROOT)}"}
+    den = Denoiser(torch.cuda.current_device())
+    den.load(DENOISER_WEIGHTS)
+    w, h = r.fbSize
+    out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
+    r.setFeatures(True)
+    tried = []
+    found = None
+    frame = 5_000_000
+    for k in spps:
+        r.setSpp(k)
+        best = None
+        for rep in range(reps + 1):
+            frame += 1
+            r.setFrameId(frame)
+            r.ResetAccumulation()
+            torch.cuda.synchronize()
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record(stream)
+            r.Render(stream.cuda_stream)
+            b.record(stream)
+            den.infer(r.deviceFeatures(), out, 1, h, w, stream.cuda_stream)
+            c.record(stream)
+            torch.cuda.synchronize()
+            if rep == 0:
+                continue   # warm-up: buffer growth for this k
+            rec = {"render_ms": a.elapsed_time(b), "denoise_ms": b.elapsed_time(c), "rmse": r.imageRmse(out),
+                   "plain_rmse_same_frame": r.accumRmse()}
+            if best is None or rec["render_ms"] + rec["denoise_ms"] < best["render_ms"] + best["denoise_ms"]:
+                best = rec
+        best["spp"] = k
+        tried.append(best)
+        if best["rmse"] <= target:
+            found = best
+            break
+    r.setFeatures(False)
+    den.close()
+    res = {"weights": os.path.relpath(DENOISER_WEIGHTS, ROOT), "tried": tried,
+           "reached": found is not None}
+    if found:
+        res.update({"spp": found["spp"], "rmse": found["rmse"], "device_ms": found["render_ms"] + found["denoise_ms"],
+                    "render_ms": found["render_ms"], "denoise_ms": found["denoise_ms"]})
+    return res
 
 
 def run_reference(args):

@@ -175,6 +175,10 @@ mdwt_status mdwt_sync(mdwt_ctx *ctx);
 mdwt_status mdwt_reset_accumulation(mdwt_ctx *ctx);
 /* frameID, accumID (host counters) and the values the next frame uses. */
 mdwt_status mdwt_get_frame_ids(const mdwt_ctx *ctx, int out4[4]);
+/* Writes the reference's public Renderer::frameID member (renderer.h:110): the next frame
+ * renders with frame id `frame_id` (seed factor frame_id + 1), the one after with
+ * frame_id + 1, and so on.  Sample seeds of frames far apart do not repeat. */
+mdwt_status mdwt_set_frame_id(mdwt_ctx *ctx, int frame_id);
 /* RGBA8 framebuffer (LaunchParams::fbPtr), W*H words, row-major from the bottom row. */
 mdwt_status mdwt_get_framebuffer(mdwt_ctx *ctx, uint32_t *host_out);
 /* Accumulation buffer (LaunchParams::accumBuffer), 4*W*H floats. */
@@ -225,11 +229,13 @@ mdwt_status mdwt_get_ranges(mdwt_ctx *ctx, float *host_out);
  * denoiser).  With features on, every frame also writes 16 floats per pixel: the frame's
  * mean radiance RGB, the first-collision depth (mean hit distance / (camera-to-box-centre
  * distance + box diagonal), 0 without hits), the miss fraction (transmittance estimate),
- * the hit fractions of channels 0..7 and three zeros.  Needs the frame in one sample batch
+ * the hit fractions of channels 0..7, the noise level 1/sqrt(spp) and two zeros.  Needs the frame in one sample batch
  * and spp < 65536 (MDWT_ERR_UNSUPPORTED otherwise). */
 mdwt_status mdwt_set_features(mdwt_ctx *ctx, int enable);
 mdwt_status mdwt_get_features(mdwt_ctx *ctx, float *host_out);        /* W*H*16 */
 mdwt_status mdwt_get_device_features(mdwt_ctx *ctx, void **d_features);
+/* Device-to-device copy of the last frame's features (W*H*16 floats) on `stream`. */
+mdwt_status mdwt_copy_features(mdwt_ctx *ctx, void *d_dst, void *stream);
 
 /* ---- FP64 ground truth (no counterpart in the reference: the convergence measurement
  * "RMSE of the accumulation buffer against an FP64 expected image")

@@ -1100,6 +1100,16 @@ mdwt_status mdwt_get_features(mdwt_ctx *c, float *out) {
   return MDWT_OK;
 }
 
+mdwt_status mdwt_copy_features(mdwt_ctx *c, void *dst, void *stream) {
+  if (!c || !dst) return MDWT_ERR_BAD_ARG;
+  if (!c->featOn || !c->dFeat) return fail(c, MDWT_ERR_STATE, "mdwt_set_features(1) and a frame first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaMemcpyAsync(dst, c->dFeat, (size_t)c->W * c->H * 16 * sizeof(float), cudaMemcpyDeviceToDevice,
+                     stream ? (cudaStream_t)stream : c->stream),
+     "copy features");
+  return MDWT_OK;
+}
+
 mdwt_status mdwt_get_device_features(mdwt_ctx *c, void **feat) {
   if (!c || !feat) return MDWT_ERR_BAD_ARG;
   *feat = c->featOn ? c->dFeat : nullptr;
@@ -1192,6 +1202,13 @@ mdwt_status mdwt_sync(mdwt_ctx *c) {
 mdwt_status mdwt_reset_accumulation(mdwt_ctx *c) {
   if (!c) return MDWT_ERR_BAD_ARG;
   reset_accum_ids(c);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_set_frame_id(mdwt_ctx *c, int f) {
+  if (!c || f < 0 || f == INT32_MAX) return MDWT_ERR_BAD_ARG;
+  c->frameParam = f;
+  c->frameID = f + 1;
   return MDWT_OK;
 }
 

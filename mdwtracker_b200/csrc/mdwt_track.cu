@@ -584,7 +584,8 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
 // Running mean into the accumulation buffer, RGBA8 write (deviceCode.cu:435, 463-471).
 // Denoiser input features of a pixel for this frame (16 floats): mean radiance RGB,
 // first-collision depth (mean hit distance times featScale, 0 without hits), the
-// transmittance estimate (miss fraction), the hit fractions of channels 0..7, zeros.
+// transmittance estimate (miss fraction), the hit fractions of channels 0..7, the noise
+// level 1/sqrt(spp), zeros.
 __device__ __forceinline__ void write_features(const TrackParams &P, int px, int py, float r, float g, float b,
                                                uint32_t hits, float sT, uint4 cnt) {
   const float fs = (float)P.spp;
@@ -595,7 +596,7 @@ __device__ __forceinline__ void write_features(const TrackParams &P, int px, int
                      (float)(cnt.y & 0xffffu) / fs);
   o[2] = make_float4((float)(cnt.y >> 16) / fs, (float)(cnt.z & 0xffffu) / fs, (float)(cnt.z >> 16) / fs,
                      (float)(cnt.w & 0xffffu) / fs);
-  o[3] = make_float4((float)(cnt.w >> 16) / fs, 0.f, 0.f, 0.f);
+  o[3] = make_float4((float)(cnt.w >> 16) / fs, 1.0f / sqrtf(fs), 0.f, 0.f);
 }
 
 template <bool STATS>

@@ -233,6 +233,10 @@ class Renderer:
     def ResetAccumulation(self):
         self._call("reset_accumulation")
 
+    def setFrameId(self, frame_id: int):
+        """The next frame renders with frame id `frame_id` (the reference's public frameID)."""
+        self._call("set_frame_id", C.c_int(frame_id))
+
     def frameIds(self):
         out = (C.c_int * 4)()
         self._call("get_frame_ids", out)
@@ -295,6 +299,11 @@ class Renderer:
         out = np.empty(w * h * 16, dtype=np.float32)
         self._call("get_features", out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.reshape(h, w, 16)
+
+    def copyFeatures(self, dst, stream: int = 0):
+        """Device-to-device copy of the last frame's features into `dst` (pointer or tensor)."""
+        from .denoiser import _ptr
+        self._call("copy_features", _ptr(dst), C.c_void_p(stream or None))
 
     def deviceFeatures(self) -> int:
         p = C.c_void_p()

@@ -980,7 +980,8 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
     f[3] = hits ? (sT / (float)hits) * o.featScale : 0.f;
     f[4] = (float)((uint32_t)o.spp - hits) / fs;
     for (int c = 0; c < 8; c++) f[5 + c] = (float)chcnt[c] / fs;
-    f[13] = f[14] = f[15] = 0.f;
+    f[13] = 1.0f / std::sqrt(fs);
+    f[14] = f[15] = 0.f;
   }
   float *acc = &o.accumBuf[4 * (size_t)fbOfs];
   float out[4];
@@ -1372,6 +1373,12 @@ int orc_expected_image(Oracle *o, int J, double stepVoxels, double *out) {
 }
 int orc_sync(Oracle *) { return ORC_OK; }
 int orc_reset_accumulation(Oracle *o) { o->accumID = 0; o->accumParam = 0; return ORC_OK; }
+int orc_set_frame_id(Oracle *o, int f) {
+  if (f < 0 || f == 2147483647) return ORC_BAD;
+  o->frameParam = f;
+  o->frameID = f + 1;
+  return ORC_OK;
+}
 int orc_get_frame_ids(Oracle *o, int out[4]) {
   out[0] = o->frameID; out[1] = o->accumID; out[2] = o->frameParam; out[3] = o->accumParam; return ORC_OK;
 }
