@@ -51,6 +51,13 @@ mdwt_status mdwt_denoiser_get_grads(mdwt_denoiser *d, float *host_out);
 mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *d_features, const float *d_target_rgba, int n,
                                      int h, int w, float lr, double *loss, void *stream);
 
+/* Convolution path: 1 (default) = tcgen05 tensor-core kernels (TMA operand loads, TMEM
+ * accumulator) wherever the layer shapes allow, 0 = the mma.sync kernels everywhere. */
+mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode);
+/* Wait for the denoiser's work; MDWT_ERR_TIMEOUT when a tensor-core kernel's bounded
+ * wait for its operands gave up (its output is then invalid). */
+mdwt_status mdwt_denoiser_check(mdwt_denoiser *d);
+
 /* Denoise the last frame of a render context (its features must be on) into
  * d_out_rgba [H][W][4] on the context's stream. */
 mdwt_status mdwt_denoise(mdwt_ctx *ctx, mdwt_denoiser *d, float *d_out_rgba);

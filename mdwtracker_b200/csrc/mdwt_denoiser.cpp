@@ -35,6 +35,7 @@ struct Layer {
   float *mW = nullptr, *vW = nullptr, *mb = nullptr, *vb = nullptr;
   float *gW = nullptr, *gb = nullptr;   // gradients
   void *Wf = nullptr, *Wd = nullptr;    // BF16 forward / data-gradient weights
+  void *Wuf = nullptr, *Wud = nullptr;  // the same in the tensor-core operand layout
   size_t nW() const { return (size_t)9 * cin * cout; }
 };
 
@@ -58,6 +59,8 @@ struct mdwt_denoiser {
   Layer L[kLayers];
   Acts A;
   int step = 0;
+  int useTC = 1;          // tcgen05 convolutions where the shapes allow
+  int *dErr = nullptr;    // set by a tensor-core kernel whose bounded wait gave up
   std::string err;
 };
 
@@ -127,7 +130,18 @@ mdwt_status ensure_acts(mdwt_denoiser *d, int N, int Hp, int Wp) {
 }
 
 mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st) {
-  DCKI(mdwt::nn::conv3x3_fwd(x, l.Wf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, st), "conv forward");
+  if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout))
+    DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st),
+         "conv forward (tcgen05)");
+  else
+    DCKI(mdwt::nn::conv3x3_fwd(x, l.Wf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, st), "conv forward");
+  return MDWT_OK;
+}
+
+// operand-layout copies of both weight layouts (after every weight change)
+mdwt_status umma_copies(mdwt_denoiser *d, const Layer &l, void *st) {
+  DCKI(mdwt::nn::umma_weights(l.Wf, l.Wuf, l.cin, l.cout, d->numSMs, st), "operand layout");
+  DCKI(mdwt::nn::umma_weights(l.Wd, l.Wud, l.cout, l.cin, d->numSMs, st), "operand layout");
   return MDWT_OK;
 }
 
@@ -161,7 +175,13 @@ mdwt_status layer_bwd(mdwt_denoiser *d, const Layer &l, const void *x, const voi
                       void *st) {
   DCKI(mdwt::nn::conv3x3_wgrad(x, dy, l.gW, N, H, W, l.cin, l.cout, st), "weight gradient");
   DCKI(mdwt::nn::bias_grad(dy, l.gb, (size_t)N * H * W, l.cout, d->numSMs, st), "bias gradient");
-  if (dx) DCKI(mdwt::nn::conv3x3_fwd(dy, l.Wd, nullptr, dx, N, H, W, l.cout, l.cin, 0, 0, st), "data gradient");
+  if (dx) {
+    if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cout, l.cin))
+      DCKI(mdwt::nn::conv3x3_tc(dy, l.Wud, nullptr, dx, N, H, W, l.cout, l.cin, 0, 0, d->dErr, st),
+           "data gradient (tcgen05)");
+    else
+      DCKI(mdwt::nn::conv3x3_fwd(dy, l.Wd, nullptr, dx, N, H, W, l.cout, l.cin, 0, 0, st), "data gradient");
+  }
   return MDWT_OK;
 }
 
@@ -210,7 +230,11 @@ mdwt_status backward(mdwt_denoiser *d, const float *F, const float *T, int N, in
 }
 
 mdwt_status refresh_copies(mdwt_denoiser *d) {
-  for (auto &l : d->L) DCKI(mdwt::nn::weight_copies(l.W, l.Wf, l.Wd, l.cin, l.cout, d->numSMs, nullptr), "weights");
+  for (auto &l : d->L) {
+    DCKI(mdwt::nn::weight_copies(l.W, l.Wf, l.Wd, l.cin, l.cout, d->numSMs, nullptr), "weights");
+    mdwt_status s = umma_copies(d, l, nullptr);
+    if (s) return s;
+  }
   DCK(cudaDeviceSynchronize(), "weights");
   return MDWT_OK;
 }
@@ -237,6 +261,10 @@ mdwt_status mdwt_denoiser_create(mdwt_denoiser **out, int device, uint64_t seed)
   d->device = device;
   if (cudaSetDevice(device) != cudaSuccess) { delete d; return MDWT_ERR_CUDA; }
   cudaDeviceGetAttribute(&d->numSMs, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMalloc((void **)&d->dErr, sizeof(int)) != cudaSuccess || cudaMemset(d->dErr, 0, sizeof(int)) != cudaSuccess) {
+    delete d;
+    return MDWT_ERR_CUDA;
+  }
   SplitMix rng{seed};
   for (int i = 0; i < kLayers; i++) {
     Layer &l = d->L[i];
@@ -250,7 +278,8 @@ mdwt_status mdwt_denoiser_create(mdwt_denoiser **out, int device, uint64_t seed)
         return MDWT_ERR_CUDA;
       }
     }
-    if (cudaMalloc(&l.Wf, nW * 2) != cudaSuccess || cudaMalloc(&l.Wd, nW * 2) != cudaSuccess) {
+    if (cudaMalloc(&l.Wf, nW * 2) != cudaSuccess || cudaMalloc(&l.Wd, nW * 2) != cudaSuccess ||
+        cudaMalloc(&l.Wuf, nW * 2) != cudaSuccess || cudaMalloc(&l.Wud, nW * 2) != cudaSuccess) {
       mdwt_denoiser_destroy(d);
       return MDWT_ERR_CUDA;
     }
@@ -277,7 +306,10 @@ mdwt_status mdwt_denoiser_destroy(mdwt_denoiser *d) {
       if (b) cudaFree(b);
     if (l.Wf) cudaFree(l.Wf);
     if (l.Wd) cudaFree(l.Wd);
+    if (l.Wuf) cudaFree(l.Wuf);
+    if (l.Wud) cudaFree(l.Wud);
   }
+  if (d->dErr) cudaFree(d->dErr);
   if (d->A.base) cudaFree(d->A.base);
   delete d;
   return MDWT_OK;
@@ -362,10 +394,32 @@ mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *F, const flo
   mdwt_status s = mdwt_denoiser_backward(d, F, T, n, h, w, loss, stream);
   if (s) return s;
   d->step++;
-  for (auto &l : d->L)
+  for (auto &l : d->L) {
     DCKI(mdwt::nn::adam(l.W, l.mW, l.vW, l.gW, l.Wf, l.Wd, l.cin, l.cout, l.b, l.mb, l.vb, l.gb, lr, 0.9f, 0.999f,
                         1e-8f, d->step, d->numSMs, stream),
          "Adam");
+    if (d->useTC && (s = umma_copies(d, l, stream))) return s;
+  }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode) {
+  if (!d || mode < 0 || mode > 1) return MDWT_ERR_BAD_ARG;
+  if (mode && !d->useTC) {   // operand copies may be stale after mma.sync-path training
+    d->useTC = 1;
+    return refresh_copies(d);
+  }
+  d->useTC = mode;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoiser_check(mdwt_denoiser *d) {
+  if (!d) return MDWT_ERR_BAD_ARG;
+  DCK(cudaSetDevice(d->device), "cudaSetDevice");
+  DCK(cudaDeviceSynchronize(), "sync");
+  int e = 0;
+  DCK(cudaMemcpy(&e, d->dErr, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+  if (e) return fail(d, MDWT_ERR_TIMEOUT, "a tensor-core convolution gave up waiting for its operands");
   return MDWT_OK;
 }
 

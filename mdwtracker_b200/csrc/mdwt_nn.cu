@@ -227,55 +227,104 @@ __global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16 *__restri
 }
 
 // ------------------------------------------------------------------ elementwise
-__global__ void relu_bwd_kernel(bf16 *dY, const bf16 *Y, size_t n) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    if (!(__bfloat162float(Y[i]) > 0.f)) dY[i] = __float2bfloat16(0.f);
+// Channel counts are multiples of 8: one thread moves 8 channels (16 bytes) at a time.
+__device__ __forceinline__ void unpack8(const uint4 &u, float f[8]) {
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const float2 t = __bfloat1622float2(h[j]);
+    f[2 * j] = t.x;
+    f[2 * j + 1] = t.y;
+  }
+}
+__device__ __forceinline__ uint4 pack8(const float f[8]) {
+  uint4 u;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+  for (int j = 0; j < 4; j++) h[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+  return u;
+}
+
+__global__ void relu_bwd_kernel(bf16 *dY, const bf16 *Y, size_t n8) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n8; i += (size_t)gridDim.x * blockDim.x) {
+    const uint4 y = reinterpret_cast<const uint4 *>(Y)[i];
+    uint4 d = reinterpret_cast<uint4 *>(dY)[i];
+    const uint32_t *yw = &y.x;
+    uint32_t *dw = &d.x;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      // keep each BF16 half of d where the matching half of y is > 0: sign clear and the
+      // magnitude bits in (0, +inf] (NaN compares false)
+      const uint32_t ml = yw[j] & 0xffffu, mh = yw[j] >> 16;
+      const uint32_t lo = ml >= 0x0001u && ml <= 0x7f80u ? 0x0000ffffu : 0u;
+      const uint32_t hi = mh >= 0x0001u && mh <= 0x7f80u ? 0xffff0000u : 0u;
+      dw[j] &= lo | hi;
+    }
+    reinterpret_cast<uint4 *>(dY)[i] = d;
+  }
 }
 
 __global__ void avgpool2_kernel(const bf16 *X, bf16 *Y, int N, int H, int W, int C) {
-  const int Ho = H / 2, Wo = W / 2;
-  const size_t n = (size_t)N * Ho * Wo * C;
+  const int Ho = H / 2, Wo = W / 2, G = C / 8;
+  const size_t n = (size_t)N * Ho * Wo * G;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    size_t r = i / C;
+    const int g = (int)(i % G);
+    size_t r = i / G;
     const int x = (int)(r % Wo);
     r /= Wo;
     const int y = (int)(r % Ho);
     const int b = (int)(r / Ho);
-    const size_t base = (((size_t)b * H + 2 * y) * W + 2 * x) * C + c;
-    const float s = __bfloat162float(X[base]) + __bfloat162float(X[base + C]) + __bfloat162float(X[base + (size_t)W * C]) +
-                    __bfloat162float(X[base + (size_t)W * C + C]);
-    Y[i] = __float2bfloat16(0.25f * s);
+    const uint4 *src = reinterpret_cast<const uint4 *>(X);
+    const size_t base = (((size_t)b * H + 2 * y) * W + 2 * x) * G + g;
+    float a[8], t[8];
+    unpack8(src[base], a);
+    unpack8(src[base + G], t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] += t[j];
+    unpack8(src[base + (size_t)W * G], t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] += t[j];
+    unpack8(src[base + (size_t)W * G + G], t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = 0.25f * (a[j] + t[j]);
+    reinterpret_cast<uint4 *>(Y)[i] = pack8(a);
   }
 }
 
 // dX[2y+i][2x+j] = dX[..] + dY[y][x] / 4 (accumulates into the skip's gradient)
 __global__ void avgpool2_bwd_add_kernel(const bf16 *dY, bf16 *dX, int N, int H, int W, int C) {
-  const size_t n = (size_t)N * H * W * C;
+  const int G = C / 8;
+  const size_t n = (size_t)N * H * W * G;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    size_t r = i / C;
+    const int g = (int)(i % G);
+    size_t r = i / G;
     const int x = (int)(r % W);
     r /= W;
     const int y = (int)(r % H);
     const int b = (int)(r / H);
-    const float g = __bfloat162float(dY[(((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]);
-    dX[i] = __float2bfloat16(__bfloat162float(dX[i]) + 0.25f * g);
+    float a[8], t[8];
+    unpack8(reinterpret_cast<const uint4 *>(dY)[(((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * G + g], t);
+    unpack8(reinterpret_cast<uint4 *>(dX)[i], a);
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = a[j] + 0.25f * t[j];
+    reinterpret_cast<uint4 *>(dX)[i] = pack8(a);
   }
 }
 
 // out[y][x] = concat(coarse[y/2][x/2] (Cu channels), skip[y][x] (Cs channels))
 __global__ void up2_concat_kernel(const bf16 *coarse, const bf16 *skip, bf16 *out, int N, int H, int W, int Cu, int Cs) {
-  const int C = Cu + Cs;
-  const size_t n = (size_t)N * H * W * C;
+  const int Gu = Cu / 8, Gs = Cs / 8, G = Gu + Gs;
+  const size_t n = (size_t)N * H * W * G;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const size_t pix = i / C;
+    const int g = (int)(i % G);
+    const size_t pix = i / G;
     const int x = (int)(pix % W);
-    size_t r = pix / W;
+    const size_t r = pix / W;
     const int y = (int)(r % H);
     const int b = (int)(r / H);
-    out[i] = c < Cu ? coarse[(((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * Cu + c] : skip[pix * Cs + (c - Cu)];
+    reinterpret_cast<uint4 *>(out)[i] =
+        g < Gu ? reinterpret_cast<const uint4 *>(coarse)[(((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * Gu + g]
+               : reinterpret_cast<const uint4 *>(skip)[pix * Gs + (g - Gu)];
   }
 }
 
@@ -283,27 +332,37 @@ __global__ void up2_concat_kernel(const bf16 *coarse, const bf16 *skip, bf16 *ou
 // dSkip = dOut[.., Cu:]
 __global__ void up2_concat_bwd_kernel(const bf16 *dOut, bf16 *dCoarse, bf16 *dSkip, int N, int H, int W, int Cu,
                                       int Cs) {
-  const int C = Cu + Cs;
+  const int Gu = Cu / 8, Gs = Cs / 8, G = Gu + Gs;
   const int Hc = H / 2, Wc = W / 2;
-  const size_t nc = (size_t)N * Hc * Wc * Cu;
-  const size_t ns = (size_t)N * H * W * Cs;
+  const size_t nc = (size_t)N * Hc * Wc * Gu;
+  const size_t ns = (size_t)N * H * W * Gs;
+  const uint4 *src = reinterpret_cast<const uint4 *>(dOut);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc + ns; i += (size_t)gridDim.x * blockDim.x) {
     if (i < nc) {
-      const int c = (int)(i % Cu);
-      size_t r = i / Cu;
+      const int g = (int)(i % Gu);
+      size_t r = i / Gu;
       const int x = (int)(r % Wc);
       r /= Wc;
       const int y = (int)(r % Hc);
       const int b = (int)(r / Hc);
-      const size_t base = (((size_t)b * H + 2 * y) * W + 2 * x) * C + c;
-      const float s = __bfloat162float(dOut[base]) + __bfloat162float(dOut[base + C]) +
-                      __bfloat162float(dOut[base + (size_t)W * C]) + __bfloat162float(dOut[base + (size_t)W * C + C]);
-      dCoarse[i] = __float2bfloat16(s);
+      const size_t base = (((size_t)b * H + 2 * y) * W + 2 * x) * G + g;
+      float a[8], t[8];
+      unpack8(src[base], a);
+      unpack8(src[base + G], t);
+#pragma unroll
+      for (int j = 0; j < 8; j++) a[j] += t[j];
+      unpack8(src[base + (size_t)W * G], t);
+#pragma unroll
+      for (int j = 0; j < 8; j++) a[j] += t[j];
+      unpack8(src[base + (size_t)W * G + G], t);
+#pragma unroll
+      for (int j = 0; j < 8; j++) a[j] += t[j];
+      reinterpret_cast<uint4 *>(dCoarse)[i] = pack8(a);
     } else {
       const size_t j = i - nc;
-      const int c = (int)(j % Cs);
-      const size_t pix = j / Cs;
-      dSkip[j] = dOut[pix * C + Cu + c];
+      const int g = (int)(j % Gs);
+      const size_t pix = j / Gs;
+      reinterpret_cast<uint4 *>(dSkip)[j] = src[pix * G + Gu + g];
     }
   }
 }
@@ -320,17 +379,29 @@ __global__ void bias_grad_kernel(const bf16 *dY, float *db, size_t P, int C) {
 }
 
 // Feature packing: fp32 [N][H][W][16] (tracker features) -> bf16 network input
-// [N][Hp][Wp][16], zero outside H x W.
+// [N][Hp][Wp][16], zero outside H x W; one pixel per thread.
 __global__ void pack_features_kernel(const float *F, bf16 *X, int N, int H, int W, int Hp, int Wp) {
-  const size_t n = (size_t)N * Hp * Wp * 16;
+  const size_t n = (size_t)N * Hp * Wp;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i & 15);
-    size_t r = i >> 4;
-    const int x = (int)(r % Wp);
-    r /= Wp;
+    const int x = (int)(i % Wp);
+    const size_t r = i / Wp;
     const int y = (int)(r % Hp);
     const int b = (int)(r / Hp);
-    X[i] = __float2bfloat16(y < H && x < W ? F[(((size_t)b * H + y) * W + x) * 16 + c] : 0.f);
+    float f[16];
+    if (y < H && x < W) {
+      const float4 *src = reinterpret_cast<const float4 *>(F) + (((size_t)b * H + y) * W + x) * 4;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const float4 v = src[j];
+        f[4 * j] = v.x; f[4 * j + 1] = v.y; f[4 * j + 2] = v.z; f[4 * j + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; j++) f[j] = 0.f;
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(X) + 2 * i;
+    dst[0] = pack8(f);
+    dst[1] = pack8(f + 8);
   }
 }
 
@@ -440,32 +511,37 @@ int conv3x3_wgrad(const void *X, const void *dY, float *dW, int N, int H, int W,
 }
 
 int relu_bwd(void *dY, const void *Y, size_t n, int numSMs, void *stream) {
-  relu_bwd_kernel<<<grid_for(n, numSMs), 256, 0, (cudaStream_t)stream>>>((bf16 *)dY, (const bf16 *)Y, n);
+  if (n % 8) return (int)cudaErrorInvalidValue;
+  relu_bwd_kernel<<<grid_for(n / 8, numSMs), 256, 0, (cudaStream_t)stream>>>((bf16 *)dY, (const bf16 *)Y, n / 8);
   return (int)cudaGetLastError();
 }
 
 int avgpool2(const void *X, void *Y, int N, int H, int W, int C, int numSMs, void *stream) {
-  avgpool2_kernel<<<grid_for((size_t)N * H * W * C / 4, numSMs), 256, 0, (cudaStream_t)stream>>>((const bf16 *)X,
-                                                                                                  (bf16 *)Y, N, H, W, C);
+  if (C % 8) return (int)cudaErrorInvalidValue;
+  avgpool2_kernel<<<grid_for((size_t)N * (H / 2) * (W / 2) * (C / 8), numSMs), 256, 0, (cudaStream_t)stream>>>(
+      (const bf16 *)X, (bf16 *)Y, N, H, W, C);
   return (int)cudaGetLastError();
 }
 
 int avgpool2_bwd_add(const void *dY, void *dX, int N, int H, int W, int C, int numSMs, void *stream) {
-  avgpool2_bwd_add_kernel<<<grid_for((size_t)N * H * W * C, numSMs), 256, 0, (cudaStream_t)stream>>>(
+  if (C % 8) return (int)cudaErrorInvalidValue;
+  avgpool2_bwd_add_kernel<<<grid_for((size_t)N * H * W * (C / 8), numSMs), 256, 0, (cudaStream_t)stream>>>(
       (const bf16 *)dY, (bf16 *)dX, N, H, W, C);
   return (int)cudaGetLastError();
 }
 
 int up2_concat(const void *coarse, const void *skip, void *out, int N, int H, int W, int Cu, int Cs, int numSMs,
                void *stream) {
-  up2_concat_kernel<<<grid_for((size_t)N * H * W * (Cu + Cs), numSMs), 256, 0, (cudaStream_t)stream>>>(
+  if (Cu % 8 || Cs % 8) return (int)cudaErrorInvalidValue;
+  up2_concat_kernel<<<grid_for((size_t)N * H * W * ((Cu + Cs) / 8), numSMs), 256, 0, (cudaStream_t)stream>>>(
       (const bf16 *)coarse, (const bf16 *)skip, (bf16 *)out, N, H, W, Cu, Cs);
   return (int)cudaGetLastError();
 }
 
 int up2_concat_bwd(const void *dOut, void *dCoarse, void *dSkip, int N, int H, int W, int Cu, int Cs, int numSMs,
                    void *stream) {
-  const size_t n = (size_t)N * (H / 2) * (W / 2) * Cu + (size_t)N * H * W * Cs;
+  if (Cu % 8 || Cs % 8) return (int)cudaErrorInvalidValue;
+  const size_t n = (size_t)N * (H / 2) * (W / 2) * (Cu / 8) + (size_t)N * H * W * (Cs / 8);
   up2_concat_bwd_kernel<<<grid_for(n, numSMs), 256, 0, (cudaStream_t)stream>>>((const bf16 *)dOut, (bf16 *)dCoarse,
                                                                                (bf16 *)dSkip, N, H, W, Cu, Cs);
   return (int)cudaGetLastError();
@@ -478,8 +554,8 @@ int bias_grad(const void *dY, float *db, size_t P, int C, int numSMs, void *stre
 }
 
 int pack_features(const float *F, void *X, int N, int H, int W, int Hp, int Wp, int numSMs, void *stream) {
-  pack_features_kernel<<<grid_for((size_t)N * Hp * Wp * 16, numSMs), 256, 0, (cudaStream_t)stream>>>(F, (bf16 *)X, N, H,
-                                                                                                     W, Hp, Wp);
+  pack_features_kernel<<<grid_for((size_t)N * Hp * Wp, numSMs), 256, 0, (cudaStream_t)stream>>>(F, (bf16 *)X, N, H, W,
+                                                                                                Hp, Wp);
   return (int)cudaGetLastError();
 }
 

@@ -37,5 +37,12 @@ int adam(float *Wm, float *mW, float *vW, const float *gW, void *Wf, void *Wd, i
          float *vb, const float *gb, float lr, float b1, float b2, float eps, int step, int numSMs, void *stream);
 int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int numSMs, void *stream);
 
+// tcgen05 path (mdwt_nn_tc.cu): the same convolution with the weights in the operand
+// layout Wu[tap][ci / 8][co][8] (umma_weights); *err is set when a bounded wait gave up.
+bool conv3x3_tc_supported(int Cin, int Cout);
+int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream);
+int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
+               int relu, int outF32, int *err, void *stream);
+
 }  // namespace nn
 }  // namespace mdwt

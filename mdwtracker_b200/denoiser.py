@@ -54,6 +54,14 @@ class Denoiser:
         except Exception:
             pass
 
+    def setTensorCores(self, on: bool) -> None:
+        """tcgen05 convolutions (default) or the mma.sync kernels."""
+        self._call("set_tensor_cores", C.c_int(1 if on else 0))
+
+    def check(self) -> None:
+        """Synchronise; raises when a tensor-core kernel's bounded wait gave up."""
+        self._call("check")
+
     def params(self) -> np.ndarray:
         out = np.empty(self.numParams(self._lib), np.float32)
         self._call("get_params", out.ctypes.data_as(C.POINTER(C.c_float)))

@@ -115,3 +115,26 @@ def test_gpu_training_fits_a_fixed_batch():
     for _ in range(150):
         last = d.trainStep(Ft, Tt, n, h, w, 1e-3)
     assert math.isfinite(last) and last < 0.1 * first, (first, last)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,h,w", [(1, 7, 20), (2, 16, 130), (1, 12, 256)])
+def test_tensor_core_and_mma_paths_agree(n, h, w):
+    """The tcgen05 convolutions (TMA-staged operands, TMEM accumulator) against the
+    mma.sync ones: the same BF16 operands and FP32 accumulation in another order."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(n * 1000 + h * 10 + w)
+    d = Denoiser(0, seed=2)
+    d.setParams(R.init_params(13))
+    F = torch.from_numpy(_features(rng, n, h, w)).cuda()
+    outs = []
+    for tc in (False, True):
+        d.setTensorCores(tc)
+        o = torch.empty((n, h, w, 4), dtype=torch.float32, device="cuda")
+        d.infer(F, o, n, h, w)
+        d.check()
+        outs.append(o.cpu().numpy()[..., :3])
+    ref = outs[0] - F.cpu().numpy()[..., :3]
+    rel = np.linalg.norm(outs[1] - outs[0]) / max(np.linalg.norm(ref), 1e-30)
+    assert rel < 1e-2, rel
