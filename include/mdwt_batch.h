@@ -1,0 +1,68 @@
+/* mdwt_batch.h -- batched rendering of many requests and the autotuner (libmdwt.so).
+ *
+ * No counterpart in the reference renderer, which renders one scene per Renderer and
+ * launch (renderer.cpp:944-973).  A request is a fully set-up render context (its own
+ * channels, transfer functions, camera, resolution, spp, mode); a batch renders one frame
+ * of every request with one persistent trace launch (and one resolve launch) per kernel
+ * variant -- requests with the same mode, voxel storage (uint8 / float32), statistics and
+ * shading flags share a launch -- instead of one launch sequence per request.  The
+ * per-request results are the ones mdwt_render gives, bit for bit (frame and accumulation
+ * ids advance per request as in mdwt_render).  Each request's frame must fit one sample
+ * batch of path records (MDWT_ERR_UNSUPPORTED otherwise) and render all rows.
+ *
+ * Launch structure: warps take work units (a request's run of `unit_items` consecutive
+ * (8x4-tile, sample) work items) from a counter and run the tracker loop with that
+ * request's parameters.  With graphs on, the launch sequence (parameter uploads from
+ * pinned memory, counter resets, kernels) is captured once into a CUDA graph and replayed
+ * while the batch's structure (variants, request and unit counts, pixel totals) stays the
+ * same.
+ */
+#ifndef MDWT_BATCH_H
+#define MDWT_BATCH_H
+
+#include <stdint.h>
+
+#include "mdwt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mdwt_batch mdwt_batch;
+
+mdwt_status mdwt_batch_create(mdwt_batch **out, int device);
+mdwt_status mdwt_batch_destroy(mdwt_batch *b);
+const char *mdwt_batch_last_error(const mdwt_batch *b);
+/* Add a request (an initialised context on the batch's device; the batch does not own it). */
+mdwt_status mdwt_batch_add(mdwt_batch *b, mdwt_ctx *request);
+mdwt_status mdwt_batch_clear(mdwt_batch *b);
+/* One frame of every request, asynchronous on `stream` (NULL: the batch's own stream). */
+mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream);
+mdwt_status mdwt_batch_sync(mdwt_batch *b);
+/* Schedule knobs (0 keeps the current value): work-unit size in items (a multiple of 32),
+ * regeneration pool and phase-1 trips for every request of the batch. */
+mdwt_status mdwt_batch_set_schedule(mdwt_batch *b, int unit_items, int pool, int trips);
+mdwt_status mdwt_batch_set_graph(mdwt_batch *b, int enable);
+/* Device time (ms) of the last mdwt_batch_render, from events on its stream; synchronous. */
+mdwt_status mdwt_batch_last_ms(mdwt_batch *b, float *ms);
+/* out[0] kernels launched so far, [1] kernel-variant groups of the last frame, [2] work
+ * units, [3] graph replays, [4] graph captures, [5] unit items, [6] pool, [7] trips. */
+mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]);
+/* Autotuner: coordinate descent over the work-unit size {512..8192}, the regeneration
+ * pool {4, 8, 16, 32} and trips {1, 2, 3, 4}, each candidate timed over `frames` batch
+ * frames after one warm-up frame; keeps the fastest.  Results do not depend on these
+ * knobs; the requests' frame ids are restored and their accumulation reset afterwards.
+ * best[3] (optional) = unit items, pool, trips. */
+mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]);
+
+/* Macrocell autotuner for one context: for each candidate edge length (voxels per
+ * macrocell side; cells per side = ceil(dims / edge)) rebuild the value ranges and
+ * majorants (transfer functions kept), time `frames` frames, keep the fastest.  Frame ids
+ * are restored and the accumulation reset afterwards.  *best_edge (optional). */
+mdwt_status mdwt_autotune_macrocells(mdwt_ctx *ctx, const int *edges, int n_edges, int frames, int *best_edge);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

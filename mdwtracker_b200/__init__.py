@@ -9,5 +9,6 @@ benchmark and the tests.
 from .renderer import (FORMATS, LIB_PATH, MDWT_HOST_ONLY, MdwtError, Renderer,  # noqa: F401
                        load_library)
 from .denoiser import Denoiser  # noqa: F401
+from .batch import Batch  # noqa: F401
 
-__all__ = ["Renderer", "Denoiser", "MdwtError", "load_library", "LIB_PATH", "MDWT_HOST_ONLY", "FORMATS"]
+__all__ = ["Renderer", "Denoiser", "Batch", "MdwtError", "load_library", "LIB_PATH", "MDWT_HOST_ONLY", "FORMATS"]

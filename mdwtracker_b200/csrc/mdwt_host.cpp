@@ -23,6 +23,7 @@
 
 #include "../../include/mdwt.h"
 #include "../../include/mdwt_denoiser.h"
+#include "../../include/mdwt_batch.h"
 #include "mdwt_internal.h"
 
 using namespace mdwt;
@@ -706,10 +707,12 @@ mdwt_status mdwt_get_channel_info(const mdwt_ctx *c, int chn, int64_t dims[3], f
   return MDWT_OK;
 }
 
+static mdwt_status regrid(mdwt_ctx *c);
+
 mdwt_status mdwt_set_macrocells(mdwt_ctx *c, const uint32_t d[3]) {
   if (!c || !d) return MDWT_ERR_BAD_ARG;
-  if (c->inited) return fail(c, MDWT_ERR_STATE, "macrocells before mdwt_init");
   for (int a = 0; a < 3; a++) c->mcReq[a] = d[a];
+  if (c->inited) return regrid(c);   // after init: new grid, same transfer functions
   return MDWT_OK;
 }
 
@@ -996,12 +999,9 @@ static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   p.lightDir = f3(c->lightDir);
 }
 
-mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
-  if (!c) return MDWT_ERR_BAD_ARG;
-  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
-  CK(cudaSetDevice(c->device), "cudaSetDevice");
-  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-  TrackParams p;
+// Everything a frame's kernels need: parameters, the traced rectangle, record buffers
+// (grown as needed); *batchOut = samples per record batch.
+static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   fill_scene(c, p);
   p.accum = c->dAccum;
   p.fb = c->dFb;
@@ -1035,6 +1035,7 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   if (c->batchCap > 0) batch = std::min(batch, c->batchCap);
   const bool stats = c->statsOn;
   mdwt_status s = MDWT_OK;
+  (void)s;
   if (nrect > 0) {
     if ((s = grow(c, (void **)&c->dRec, c->recCap, (size_t)batch * nrect * 4, "records")) != MDWT_OK) return s;
     if (stats && (s = grow(c, (void **)&c->dRecStats, c->recStatsCap, (size_t)batch * nrect * 4, "record stats")) != MDWT_OK) return s;
@@ -1059,6 +1060,19 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   }
   p.partial = c->dPartial;
   p.partialStats = stats ? c->dPartialStats : nullptr;
+  *batchOut = batch;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  TrackParams p;
+  int batch = 0;
+  mdwt_status s = prepare_frame(c, p, &batch);
+  if (s) return s;
   // kernel timing: events around the trace and the resolve pass of a one-batch frame
   const bool timeIt = c->timing && batch >= c->spp;
   c->timed = false;
@@ -1188,6 +1202,422 @@ mdwt_status mdwt_image_rmse(mdwt_ctx *c, const float *img, double *rmse) {
   CK(cudaMemcpyAsync(&sum, c->dSqSum, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "rmse copy");
   CK(cudaStreamSynchronize(c->stream), "rmse sync");
   *rmse = std::sqrt(sum / (3.0 * (double)npix));
+  return MDWT_OK;
+}
+
+// ------------------------------------------------------------------ macrocell regrid
+// The value ranges and majorants of a new macrocell grid, transfer functions kept;
+// resets the accumulation like a transfer-function change.
+static mdwt_status regrid(mdwt_ctx *c) {
+  uint32_t mc[3];
+  resolve_mc(c, mc);
+  if (mc[0] == 0 || mc[1] == 0 || mc[2] == 0) return fail(c, MDWT_ERR_BAD_ARG, "zero macrocell dims");
+  if ((uint64_t)mc[0] * mc[1] * mc[2] > (1ull << 30)) return fail(c, MDWT_ERR_BAD_ARG, "macrocell grid above 2^30 cells");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(c->stream), "regrid");
+  if (c->dRanges) cudaFree(c->dRanges);
+  if (c->dMaj) cudaFree(c->dMaj);
+  if (c->dMask) cudaFree(c->dMask);
+  c->dRanges = nullptr; c->dMaj = nullptr; c->dMask = nullptr;
+  for (int a = 0; a < 3; a++) c->mc[a] = mc[a];
+  c->M = (size_t)mc[0] * mc[1] * mc[2];
+  const int C = (int)c->ch.size();
+  CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
+  CK(cudaMalloc(&c->dMaj, c->M * (c->mode == 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
+  mdwt_status s = build_ranges(c);
+  if (s) return s;
+  s = recalc(c);
+  if (s) return s;
+  reset_accum_ids(c);
+  CK(cudaStreamSynchronize(c->stream), "regrid");
+  return MDWT_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batches
+struct mdwt_batch {
+  int device = 0, numSMs = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<mdwt_ctx *> reqs;
+  int unitItems = 2048, pool = 0, trips = 0;
+  bool useGraph = true;
+  // pinned host staging and device copies: params, units, pixel offsets, unit counters
+  TrackParams *hParams = nullptr, *dParams = nullptr;
+  BatchUnit *hUnits = nullptr, *dUnits = nullptr;
+  unsigned long long *hPix = nullptr, *dPix = nullptr;
+  unsigned *dCounters = nullptr;
+  size_t capParams = 0, capUnits = 0, capPix = 0, capCounters = 0;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<long long> graphSig;
+  cudaStream_t graphStream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int64_t launches = 0, replays = 0, captures = 0, lastUnitsLaunch = 0;
+  int lastGroups = 0, lastUnits = 0;
+  std::string err;
+};
+
+namespace {
+
+mdwt_status bfail(mdwt_batch *b, mdwt_status s, const std::string &m) {
+  if (b) b->err = m;
+  return s;
+}
+#define BCK(call, what)                                                                         \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return bfail(b, MDWT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+mdwt_status grow_pair(mdwt_batch *b, T **h, T **d, size_t &cap, size_t n) {
+  if (n <= cap && *d) return MDWT_OK;
+  if (*h) cudaFreeHost(*h);
+  if (*d) cudaFree(*d);
+  *h = nullptr; *d = nullptr; cap = 0;
+  const size_t m = n < 16 ? 16 : n;
+  BCK(cudaMallocHost((void **)h, m * sizeof(T)), "pinned staging");
+  BCK(cudaMalloc((void **)d, m * sizeof(T)), "batch buffers");
+  cap = m;
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; b->graphSig.clear(); }   // pointers baked
+  return MDWT_OK;
+}
+
+struct GroupPlan {
+  int mode, store;
+  bool stats, ext, shade;
+  int first, count;           // request slots [first, first + count) of the params array
+  int unitFirst, unitCount;
+  int pixFirst;               // offset of the group's nReq + 1 pixel offsets
+  unsigned long long totalPix;
+};
+
+long long variant_key(const TrackParams &p, int store, bool stats) {
+  const bool ext = p.shadows || p.recT;
+  const bool shade = p.shadows || p.gradient;
+  return (long long)p.mode * 16 + store * 8 + (stats ? 4 : 0) + (ext ? 2 : 0) + (shade ? 1 : 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+mdwt_status mdwt_batch_create(mdwt_batch **out, int device) {
+  if (!out) return MDWT_ERR_BAD_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return MDWT_ERR_CUDA;
+  if (device < 0 || device >= count) return MDWT_ERR_BAD_ARG;
+  mdwt_batch *b = new mdwt_batch();
+  b->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+    delete b;
+    return MDWT_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&b->numSMs, cudaDevAttrMultiProcessorCount, device);
+  *out = b;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_destroy(mdwt_batch *b) {
+  if (!b) return MDWT_ERR_BAD_ARG;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->hParams) cudaFreeHost(b->hParams);
+  if (b->dParams) cudaFree(b->dParams);
+  if (b->hUnits) cudaFreeHost(b->hUnits);
+  if (b->dUnits) cudaFree(b->dUnits);
+  if (b->hPix) cudaFreeHost(b->hPix);
+  if (b->dPix) cudaFree(b->dPix);
+  if (b->dCounters) cudaFree(b->dCounters);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return MDWT_OK;
+}
+
+const char *mdwt_batch_last_error(const mdwt_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+mdwt_status mdwt_batch_add(mdwt_batch *b, mdwt_ctx *c) {
+  if (!b || !c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return bfail(b, MDWT_ERR_STATE, "request not initialised");
+  if (c->device != b->device) return bfail(b, MDWT_ERR_BAD_ARG, "request on another device");
+  b->reqs.push_back(c);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_clear(mdwt_batch *b) {
+  if (!b) return MDWT_ERR_BAD_ARG;
+  b->reqs.clear();
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_set_schedule(mdwt_batch *b, int unitItems, int pool, int trips) {
+  if (!b || unitItems < 0 || (unitItems % 32) || pool < 0 || pool > 32 || trips < 0 || trips > 64)
+    return MDWT_ERR_BAD_ARG;
+  if (unitItems) b->unitItems = unitItems;
+  if (pool) b->pool = pool;
+  if (trips) b->trips = trips;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_set_graph(mdwt_batch *b, int enable) {
+  if (!b) return MDWT_ERR_BAD_ARG;
+  b->useGraph = enable != 0;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
+  if (!b) return MDWT_ERR_BAD_ARG;
+  if (b->reqs.empty()) return bfail(b, MDWT_ERR_STATE, "empty batch");
+  BCK(cudaSetDevice(b->device), "cudaSetDevice");
+  const int n = (int)b->reqs.size();
+  // per-request frame parameters, in variant order
+  std::vector<TrackParams> ps(n);
+  std::vector<long long> keys(n);
+  for (int i = 0; i < n; i++) {
+    mdwt_ctx *c = b->reqs[i];
+    int batch = 0;
+    if (c->rowHi > c->rowLo) return bfail(b, MDWT_ERR_UNSUPPORTED, "batched requests render all rows");
+    mdwt_status s = prepare_frame(c, ps[i], &batch);
+    if (s) return bfail(b, s, std::string("request ") + std::to_string(i) + ": " + c->err);
+    if (batch < c->spp) return bfail(b, MDWT_ERR_UNSUPPORTED, "a batched request's frame exceeds one record batch");
+    ps[i].sBase = 0;          // the whole frame is one sample batch
+    ps[i].sCount = c->spp;
+    if (b->pool) ps[i].pool = b->pool;
+    if (b->trips) ps[i].trips = b->trips;
+    keys[i] = variant_key(ps[i], c->store, c->statsOn);
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return keys[a] < keys[c]; });
+  // groups, units, pixel offsets
+  std::vector<GroupPlan> groups;
+  std::vector<BatchUnit> units;
+  std::vector<unsigned long long> pix;
+  const unsigned U = (unsigned)b->unitItems;
+  for (int k = 0; k < n;) {
+    int e = k;
+    while (e < n && keys[order[e]] == keys[order[k]]) e++;
+    const TrackParams &p0 = ps[order[k]];
+    GroupPlan g;
+    g.mode = p0.mode; g.store = b->reqs[order[k]]->store; g.stats = b->reqs[order[k]]->statsOn;
+    g.ext = p0.shadows || p0.recT; g.shade = p0.shadows || p0.gradient;
+    g.first = k; g.count = e - k;
+    g.unitFirst = (int)units.size();
+    g.pixFirst = (int)pix.size();
+    unsigned long long acc = 0;
+    for (int j = k; j < e; j++) {
+      const TrackParams &p = ps[order[j]];
+      pix.push_back(acc);
+      acc += (unsigned long long)p.W * p.H;
+      const unsigned items = (unsigned)p.numTiles * 32u * (unsigned)p.spp;
+      for (unsigned a = 0; a < items; a += U) units.push_back(BatchUnit{j - k, a, std::min(items, a + U)});
+    }
+    pix.push_back(acc);
+    g.totalPix = acc;
+    g.unitCount = (int)units.size() - g.unitFirst;
+    groups.push_back(g);
+    k = e;
+  }
+  mdwt_status s;
+  if ((s = grow_pair(b, &b->hParams, &b->dParams, b->capParams, (size_t)n))) return s;
+  if ((s = grow_pair(b, &b->hUnits, &b->dUnits, b->capUnits, units.size()))) return s;
+  if ((s = grow_pair(b, &b->hPix, &b->dPix, b->capPix, pix.size()))) return s;
+  if (b->capCounters < groups.size()) {
+    if (b->dCounters) cudaFree(b->dCounters);
+    b->dCounters = nullptr;
+    BCK(cudaMalloc((void **)&b->dCounters, std::max<size_t>(16, groups.size()) * sizeof(unsigned)), "counters");
+    b->capCounters = std::max<size_t>(16, groups.size());
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; b->graphSig.clear(); }
+  }
+  for (int j = 0; j < n; j++) b->hParams[j] = ps[order[j]];
+  std::copy(units.begin(), units.end(), b->hUnits);
+  std::copy(pix.begin(), pix.end(), b->hPix);
+  // structure signature: what a captured graph bakes in
+  std::vector<long long> sig = {n, (long long)units.size(), (long long)pix.size(), (long long)b->numSMs};
+  for (auto &g : groups) {
+    sig.push_back(keys[order[g.first]]);
+    sig.push_back(g.count);
+    sig.push_back(g.unitCount);
+    sig.push_back((long long)g.totalPix);
+  }
+  cudaStream_t user = stream ? (cudaStream_t)stream : b->stream;
+  auto enqueue = [&](cudaStream_t st) -> mdwt_status {
+    BCK(cudaMemcpyAsync(b->dParams, b->hParams, (size_t)n * sizeof(TrackParams), cudaMemcpyHostToDevice, st), "params");
+    BCK(cudaMemcpyAsync(b->dUnits, b->hUnits, units.size() * sizeof(BatchUnit), cudaMemcpyHostToDevice, st), "units");
+    BCK(cudaMemcpyAsync(b->dPix, b->hPix, pix.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, st), "pix");
+    BCK(cudaMemsetAsync(b->dCounters, 0, groups.size() * sizeof(unsigned), st), "counters");
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+      const GroupPlan &g = groups[gi];
+      BatchGroup bg;
+      bg.mode = g.mode; bg.storeKind = g.store; bg.stats = g.stats; bg.ext = g.ext; bg.shade = g.shade;
+      bg.reqs = b->dParams + g.first;
+      bg.nReq = g.count;
+      bg.units = b->dUnits + g.unitFirst;
+      bg.numUnits = g.unitCount;
+      bg.unitCounter = b->dCounters + gi;
+      bg.pixOfs = b->dPix + g.pixFirst;
+      bg.totalPix = g.totalPix;
+      int launches = 0, grid = 0;
+      const int rc = launch_track_batch(bg, st, b->numSMs, &launches, &grid);
+      if (rc) return bfail(b, MDWT_ERR_CUDA, std::string("batched tracker: ") + cudaGetErrorString((cudaError_t)rc));
+      b->launches += launches;
+    }
+    return MDWT_OK;
+  };
+  BCK(cudaEventRecord(b->ev0, user), "event");
+  if (b->useGraph) {
+    if (!b->graph || b->graphSig != sig) {
+      if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+      cudaStream_t cs = b->stream;
+      if (cs == user) {   // capture on a private stream, replay on the caller's
+        if (!b->graphStream) BCK(cudaStreamCreateWithFlags(&b->graphStream, cudaStreamNonBlocking), "stream");
+        cs = b->graphStream;
+      }
+      BCK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+      const int64_t l0 = b->launches;
+      s = enqueue(cs);
+      cudaGraph_t gr = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(cs, &gr);
+      if (s) { if (gr) cudaGraphDestroy(gr); return s; }
+      if (ec != cudaSuccess) return bfail(b, MDWT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ec));
+      const cudaError_t ei = cudaGraphInstantiate(&b->graph, gr, 0);
+      cudaGraphDestroy(gr);
+      if (ei != cudaSuccess) { b->graph = nullptr; return bfail(b, MDWT_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ei)); }
+      b->graphSig = sig;
+      b->captures++;
+      b->lastUnitsLaunch = b->launches - l0;
+      b->launches = l0;
+    }
+    BCK(cudaGraphLaunch(b->graph, user), "graph launch");
+    b->launches += b->lastUnitsLaunch;
+    b->replays++;
+  } else {
+    if ((s = enqueue(user))) return s;
+  }
+  BCK(cudaEventRecord(b->ev1, user), "event");
+  for (auto *c : b->reqs) {   // Renderer::Render id increments (renderer.cpp:957-958)
+    c->accumParam = c->accumID++;
+    c->frameParam = c->frameID++;
+  }
+  b->lastGroups = (int)groups.size();
+  b->lastUnits = (int)units.size();
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_sync(mdwt_batch *b) {
+  if (!b) return MDWT_ERR_BAD_ARG;
+  BCK(cudaSetDevice(b->device), "cudaSetDevice");
+  BCK(cudaDeviceSynchronize(), "sync");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_last_ms(mdwt_batch *b, float *ms) {
+  if (!b || !ms) return MDWT_ERR_BAD_ARG;
+  BCK(cudaEventSynchronize(b->ev1), "event");
+  BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1), "elapsed");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]) {
+  if (!b || !out) return MDWT_ERR_BAD_ARG;
+  out[0] = b->launches; out[1] = b->lastGroups; out[2] = b->lastUnits; out[3] = b->replays; out[4] = b->captures;
+  out[5] = b->unitItems; out[6] = b->pool; out[7] = b->trips;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]) {
+  if (!b || frames <= 0) return MDWT_ERR_BAD_ARG;
+  if (b->reqs.empty()) return bfail(b, MDWT_ERR_STATE, "empty batch");
+  struct Ids { int f, a, fp, ap; };
+  std::vector<Ids> saved;
+  for (auto *c : b->reqs) saved.push_back({c->frameID, c->accumID, c->frameParam, c->accumParam});
+  auto trial = [&](double *ms) -> mdwt_status {
+    mdwt_status s = mdwt_batch_render(b, nullptr);   // warm-up (and capture)
+    if (s) return s;
+    double tot = 0.0;
+    for (int f = 0; f < frames; f++) {
+      if ((s = mdwt_batch_render(b, nullptr))) return s;
+      float m = 0.f;
+      if ((s = mdwt_batch_last_ms(b, &m))) return s;
+      tot += m;
+    }
+    *ms = tot / frames;
+    return MDWT_OK;
+  };
+  if (!b->pool) b->pool = b->reqs[0]->pool;
+  if (!b->trips) b->trips = b->reqs[0]->trips;
+  const int unitsC[] = {512, 1024, 2048, 4096, 8192};
+  const int poolsC[] = {4, 8, 16, 32};
+  const int tripsC[] = {1, 2, 3, 4};
+  mdwt_status s = MDWT_OK;
+  double bestMs = 1e300;
+  auto tune = [&](int *knob, const int *cand, int nc) -> mdwt_status {
+    int bestV = *knob;
+    for (int i = 0; i < nc; i++) {
+      *knob = cand[i];
+      double ms = 0.0;
+      mdwt_status st = trial(&ms);
+      if (st) return st;
+      if (ms < bestMs) { bestMs = ms; bestV = cand[i]; }
+    }
+    *knob = bestV;
+    return MDWT_OK;
+  };
+  if (!(s = tune(&b->unitItems, unitsC, 5)) && !(s = tune(&b->pool, poolsC, 4))) s = tune(&b->trips, tripsC, 4);
+  for (size_t i = 0; i < b->reqs.size(); i++) {
+    mdwt_ctx *c = b->reqs[i];
+    c->frameID = saved[i].f; c->accumID = saved[i].a; c->frameParam = saved[i].fp; c->accumParam = saved[i].ap;
+    reset_accum_ids(c);
+  }
+  if (s) return s;
+  if (best) { best[0] = b->unitItems; best[1] = b->pool; best[2] = b->trips; }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_autotune_macrocells(mdwt_ctx *c, const int *edges, int n, int frames, int *bestEdge) {
+  if (!c || !edges || n <= 0 || frames <= 0) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  for (int i = 0; i < n; i++)
+    if (edges[i] <= 0) return fail(c, MDWT_ERR_BAD_ARG, "macrocell edge must be positive");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  const int f0 = c->frameID, a0 = c->accumID, fp0 = c->frameParam, ap0 = c->accumParam;
+  int64_t dims[3] = {0, 0, 0};
+  for (auto &h : c->ch)
+    for (int a = 0; a < 3; a++) dims[a] = std::max<int64_t>(dims[a], h.dims[a]);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0), "event");
+  CK(cudaEventCreate(&e1), "event");
+  double bestMs = 1e300;
+  int best = edges[0];
+  mdwt_status s = MDWT_OK;
+  for (int i = 0; i < n && !s; i++) {
+    uint32_t mc[3];
+    for (int a = 0; a < 3; a++) mc[a] = (uint32_t)((dims[a] + edges[i] - 1) / edges[i]);
+    if ((s = mdwt_set_macrocells(c, mc))) break;
+    if ((s = mdwt_render(c, nullptr))) break;   // warm-up
+    cudaEventRecord(e0, c->stream);
+    for (int f = 0; f < frames && !s; f++) s = mdwt_render(c, nullptr);
+    cudaEventRecord(e1, c->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (!s && ms < bestMs) { bestMs = ms; best = edges[i]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s) return s;
+  uint32_t mc[3];
+  for (int a = 0; a < 3; a++) mc[a] = (uint32_t)((dims[a] + best - 1) / best);
+  if ((s = mdwt_set_macrocells(c, mc))) return s;
+  c->frameID = f0; c->accumID = a0; c->frameParam = fp0; c->accumParam = ap0;
+  reset_accum_ids(c);
+  if (bestEdge) *bestEdge = best;
   return MDWT_OK;
 }
 

@@ -87,6 +87,26 @@ struct TrackParams {
   uint32_t *partialStats;        // uint4 per rect pixel between batches (stats only)
 };
 
+// A work unit of the batched tracker: items [begin, end) of request `req`.
+struct BatchUnit {
+  int req;
+  unsigned begin, end;
+};
+
+// A group of batched requests sharing one kernel variant (device arrays).
+struct BatchGroup {
+  int mode, storeKind;
+  bool stats, ext, shade;                // per-pixel stats; extended trace; shaded resolve
+  const TrackParams *reqs;               // the group's requests
+  int nReq;
+  const BatchUnit *units;                // req indexes into `reqs`
+  int numUnits;
+  unsigned *unitCounter;                 // zeroed before the launch
+  const unsigned long long *pixOfs;      // nReq + 1 prefix offsets of W*H
+  unsigned long long totalPix;
+};
+int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launches, int *grid);
+
 constexpr int kMaxTexels = 16384;          // TF texels addressable by a path record
 constexpr size_t kRecordBudget = size_t(1) << 28;   // records per batch (1 GiB)
 

@@ -203,34 +203,33 @@ __device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, in
 enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_SAMPLE = 3, S_DONE = 4 };
 enum : int { A_CHAN = 0, A_ADVANCE = 1, A_NEWDDA = 2 };
 
-// SH: extended variant -- shadow rays (when P.shadows) and the hit distance of every path
-// (when P.recT: gradient shading, denoiser features).
+__device__ __forceinline__ ChanSm chan_params(const TrackParams &P, int c) {
+  ChanSm cs;
+  cs.vol = P.vol[c];
+  cs.tfAlpha = P.tfAlpha[c];
+  cs.X = P.dims[c][0]; cs.Y = P.dims[c][1]; cs.Z = P.dims[c][2];
+  cs.n = P.tfN[c];
+  cs.vd0 = P.vd[c][0]; cs.vd1 = P.vd[c][1];
+  cs.xd0 = P.xd[c][0]; cs.xd1 = P.xd[c][1];
+  cs.os = P.os[c];
+  return cs;
+}
+
+// The warp's tracking loop over work items [qBegin, limit) of one request: with a
+// dispenser, the warp takes `chunk` items at a time from it (qBegin = limit = the
+// request's item count); without, the warp owns the whole range.  Event counts are
+// added to tot[0..4] (samples, rejections, cells, paths, capped).
 template <int MODE, int SK, bool STATS, bool SH>
-__global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_constant__ TrackParams P) {
+__device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *sch, unsigned qBegin, unsigned limit,
+                                            unsigned *dispenser, unsigned chunk, uint32_t (&tot)[5]) {
   const int C = P.C;
   const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned total = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
   const int rw = P.cullX1 - P.cullX0 + 1;
   const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
-  uint32_t totSamp = 0, totRej = 0, totCell = 0, totPaths = 0, totCap = 0;
+  uint32_t &totSamp = tot[0], &totRej = tot[1], &totCell = tot[2], &totPaths = tot[3], &totCap = tot[4];
 
-  __shared__ ChanSm sch[kMaxChannels];
-  if (threadIdx.x < (unsigned)C) {
-    const int c = threadIdx.x;
-    ChanSm cs;
-    cs.vol = P.vol[c];
-    cs.tfAlpha = P.tfAlpha[c];
-    cs.X = P.dims[c][0]; cs.Y = P.dims[c][1]; cs.Z = P.dims[c][2];
-    cs.n = P.tfN[c];
-    cs.vd0 = P.vd[c][0]; cs.vd1 = P.vd[c][1];
-    cs.xd0 = P.xd[c][0]; cs.xd1 = P.xd[c][1];
-    cs.os = P.os[c];
-    sch[c] = cs;
-  }
-  __syncthreads();
-
-  unsigned qNext = 0, qEnd = 0;                // this warp's share of the item dispenser
+  unsigned qNext = dispenser ? 0u : qBegin, qEnd = dispenser ? 0u : limit;   // the warp's items in hand
   int st = S_NEED, act = A_CHAN;
   size_t recIdx = 0;
   uint32_t pSamp = 0, pRej = 0;                // per-path event counts (STATS)
@@ -342,14 +341,14 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
       const unsigned rank = __popc(need & ((1u << lane) - 1u));
       unsigned avail = qEnd - qNext, base = 0;
       if (avail < n) {
-        if (lane == 0) base = atomicAdd(P.workCounter, (unsigned)P.chunk);
+        if (lane == 0) base = dispenser ? atomicAdd(dispenser, chunk) : limit;
         base = __shfl_sync(kFull, base, 0);
       }
       unsigned item = rank < avail ? qNext + rank : base + (rank - avail);
-      if (avail < n) { qNext = base + (n - avail); qEnd = base + (unsigned)P.chunk; }
+      if (avail < n) { qNext = base + (n - avail); qEnd = base + chunk; }
       else qNext += n;
       if (st == S_NEED) {
-        if (item >= total) {
+        if (item >= limit) {
           st = S_DONE;
         } else {
           const unsigned tile = item / (32u * (unsigned)P.sCount);
@@ -566,18 +565,59 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
     }
     __syncwarp();
   }
+}
 
-  // ---------------- counters: warp reduction, one atomic per warp and counter
-  unsigned long long v[5] = {totSamp, totRej, totCell, totPaths, totCap};
+// counters: warp reduction, one atomic per warp and counter
+__device__ __forceinline__ void flush_counters(unsigned long long *counters, const uint32_t (&tot)[5]) {
+  unsigned long long v[5] = {tot[0], tot[1], tot[2], tot[3], tot[4]};
 #pragma unroll
   for (int k = 0; k < 5; k++) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(kFull, v[k], o);
   }
-  if (lane == 0) {
+  if ((threadIdx.x & 31u) == 0) {
 #pragma unroll
     for (int k = 0; k < 5; k++)
-      if (v[k]) atomicAdd(P.counters + k, v[k]);
+      if (v[k]) atomicAdd(counters + k, v[k]);
+  }
+}
+
+// SH: extended variant -- shadow rays (when P.shadows) and the hit distance of every path
+// (when P.recT: gradient shading, denoiser features).
+template <int MODE, int SK, bool STATS, bool SH>
+__global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_constant__ TrackParams P) {
+  __shared__ ChanSm sch[kMaxChannels];
+  if (threadIdx.x < (unsigned)P.C) sch[threadIdx.x] = chan_params(P, threadIdx.x);
+  __syncthreads();
+  const unsigned total = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
+  uint32_t tot[5] = {0, 0, 0, 0, 0};
+  trace_items<MODE, SK, STATS, SH>(P, sch, total, total, P.workCounter, (unsigned)P.chunk, tot);
+  flush_counters(P.counters, tot);
+}
+
+// Batched variant: many requests (render contexts) in one persistent launch.  Each warp
+// takes work units (request, item range) from a global counter and runs the same
+// tracking loop with that request's parameters (global memory) and channel table
+// (staged per warp in shared memory); the counters go to the unit's request.
+template <int MODE, int SK, bool STATS, bool SH>
+__global__ void __launch_bounds__(kTPB, kMinBlocks)
+    trace_batch_kernel(const TrackParams *__restrict__ reqs, const BatchUnit *__restrict__ units, int numUnits,
+                       unsigned *unitCounter) {
+  __shared__ ChanSm sch[kTPB / 32][kMaxChannels];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  while (true) {
+    unsigned u = 0;
+    if (lane == 0) u = atomicAdd(unitCounter, 1u);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= (unsigned)numUnits) break;
+    const BatchUnit U = units[u];
+    const TrackParams &P = reqs[U.req];
+    if (lane < (unsigned)P.C) sch[warp][lane] = chan_params(P, (int)lane);
+    __syncwarp();
+    uint32_t tot[5] = {0, 0, 0, 0, 0};
+    trace_items<MODE, SK, STATS, SH>(P, sch[warp], U.begin, U.end, nullptr, 0u, tot);
+    flush_counters(P.counters, tot);
+    __syncwarp();
   }
 }
 
@@ -704,25 +744,24 @@ __device__ void gradient_shading(const TrackParams &P, int ch, float tHit, float
   }
 }
 
+// One pixel of the resolve pass; returns the path-samples it accounts for without
+// tracing (culled pixels).
 template <bool STATS, bool SHADE, int SK>
-__global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ TrackParams P) {
-  const unsigned npix = (unsigned)P.W * (unsigned)(P.rowHi - P.rowLo);   // the rendered row band
+__device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, int py) {
   const int rw = P.cullX1 - P.cullX0 + 1;
   const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
   const bool last = P.sBase + P.sCount == P.spp;
   const float kd0 = (1.0f * 1.0f) * P.lightIntensity;   // diffuse * shadow * lightIntensity (unshaded)
   const float ks0 = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
-  uint32_t culledPaths = 0;
   const bool feat = P.feat != nullptr;   // denoiser features (one batch per frame)
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
-    const int px = (int)(i % (unsigned)P.W), py = P.rowLo + (int)(i / (unsigned)P.W);
+  {
     if (px < P.cullX0 || px > P.cullX1 || py < P.cullY0 || py > P.cullY1) {
       if (last) {
         write_pixel<STATS>(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], P.bgFin[3], make_uint4(0u, 0u, 0u, 0u));
         if (feat) write_features(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], 0u, 0.f, make_uint4(0u, 0u, 0u, 0u));
-        culledPaths += (uint32_t)P.spp;
+        return (uint32_t)P.spp;
       }
-      continue;
+      return 0u;
     }
     uint32_t hits = 0;
     uint4 cnt = make_uint4(0u, 0u, 0u, 0u);   // hits of channels 0..7, 16 bits each
@@ -798,10 +837,39 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Tr
       if (STATS) reinterpret_cast<uint4 *>(P.partialStats)[q] = sv;
     }
   }
+  return 0u;
+}
+
+template <bool STATS, bool SHADE, int SK>
+__global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ TrackParams P) {
+  const unsigned npix = (unsigned)P.W * (unsigned)(P.rowHi - P.rowLo);   // the rendered row band
+  uint32_t culledPaths = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x)
+    culledPaths += resolve_pixel<STATS, SHADE, SK>(P, (int)(i % (unsigned)P.W), P.rowLo + (int)(i / (unsigned)P.W));
   unsigned long long cp = culledPaths;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cp += __shfl_down_sync(kFull, cp, o);
   if ((threadIdx.x & 31) == 0 && cp) atomicAdd(P.counters + 3, cp);
+}
+
+// Batched resolve: the pixels of every request of a group, request r owning global
+// pixel indices [pixOfs[r], pixOfs[r + 1]).
+template <bool STATS, bool SHADE, int SK>
+__global__ void __launch_bounds__(256) resolve_batch_kernel(const TrackParams *__restrict__ reqs,
+                                                            const unsigned long long *__restrict__ pixOfs, int nReq) {
+  const unsigned long long total = pixOfs[nReq];
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < total;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nReq - 1;   // the request owning pixel i
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pixOfs[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    const TrackParams &P = reqs[lo];
+    const unsigned j = (unsigned)(i - pixOfs[lo]);
+    const uint32_t c = resolve_pixel<STATS, SHADE, SK>(P, (int)(j % (unsigned)P.W), (int)(j / (unsigned)P.W));
+    if (c) atomicAdd(P.counters + 3, (unsigned long long)c);
+  }
 }
 
 template <int MODE, int SK, bool STATS, bool SH>
@@ -836,7 +904,49 @@ int launch_s(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void 
   return p.stats ? launch_t<MODE, SK, true, false>(p, st, numSMs, grid, evMid) : launch_t<MODE, SK, false, false>(p, st, numSMs, grid, evMid);
 }
 
+template <int MODE, int SK, bool STATS, bool SH>
+int launch_tb(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
+  int bps = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_kernel<MODE, SK, STATS, SH>, kTPB, 0);
+  if (e != cudaSuccess) return (int)e;
+  if (bps < 1) bps = 1;
+  *grid = numSMs * bps;
+  if (g.numUnits > 0)
+    trace_batch_kernel<MODE, SK, STATS, SH><<<*grid, kTPB, 0, st>>>(g.reqs, g.units, g.numUnits, g.unitCounter);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  size_t rg = (size_t)((g.totalPix + 255) / 256);
+  if (rg > (size_t)numSMs * 8) rg = (size_t)numSMs * 8;
+  if (rg == 0) return (int)cudaSuccess;
+  if (g.shade) resolve_batch_kernel<STATS, true, SK><<<(unsigned)rg, 256, 0, st>>>(g.reqs, g.pixOfs, g.nReq);
+  else resolve_batch_kernel<STATS, false, SK><<<(unsigned)rg, 256, 0, st>>>(g.reqs, g.pixOfs, g.nReq);
+  return (int)cudaGetLastError();
+}
+
+template <int MODE, int SK>
+int launch_tbs(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
+  if (g.ext) return g.stats ? launch_tb<MODE, SK, true, true>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, true>(g, st, numSMs, grid);
+  return g.stats ? launch_tb<MODE, SK, true, false>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, false>(g, st, numSMs, grid);
+}
+
 }  // namespace
+
+// One group of a batch: every request with the same kernel variant, in one persistent
+// trace launch and one resolve launch.
+int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launches, int *grid) {
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool u8 = g.storeKind == kStoreU8;
+  int rc;
+  switch (g.mode) {
+    case 0: rc = u8 ? launch_tbs<0, kStoreU8>(g, st, numSMs, grid) : launch_tbs<0, kStoreF32>(g, st, numSMs, grid); break;
+    case 1: rc = u8 ? launch_tbs<1, kStoreU8>(g, st, numSMs, grid) : launch_tbs<1, kStoreF32>(g, st, numSMs, grid); break;
+    case 2: rc = u8 ? launch_tbs<2, kStoreU8>(g, st, numSMs, grid) : launch_tbs<2, kStoreF32>(g, st, numSMs, grid); break;
+    case 3: rc = u8 ? launch_tbs<3, kStoreU8>(g, st, numSMs, grid) : launch_tbs<3, kStoreF32>(g, st, numSMs, grid); break;
+    default: return (int)cudaErrorInvalidValue;
+  }
+  if (launches) *launches += (g.numUnits > 0 ? 1 : 0) + (g.totalPix > 0 ? 1 : 0);
+  return rc;
+}
 
 // One batch of samples [sBase, sBase + sCount): trace + resolve on `stream`.
 int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, int *launches, int *grid, int *block,

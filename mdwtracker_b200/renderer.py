@@ -233,6 +233,12 @@ class Renderer:
     def ResetAccumulation(self):
         self._call("reset_accumulation")
 
+    def autotuneMacrocells(self, edges=(4, 8, 16, 32), frames: int = 2) -> int:
+        """Time frames for each macrocell edge length (voxels per side), keep the fastest
+        grid; frame ids are restored and the accumulation reset."""
+        from .batch import autotune_macrocells
+        return autotune_macrocells(self, edges, frames)
+
     def setFrameId(self, frame_id: int):
         """The next frame renders with frame id `frame_id` (the reference's public frameID)."""
         self._call("set_frame_id", C.c_int(frame_id))

@@ -1194,6 +1194,17 @@ int orc_get_channel_info(Oracle *o, int c, int64_t dims[3], float b8[8]) {
 
 int orc_set_macrocells(Oracle *o, const uint32_t d[3]) {
   for (int a = 0; a < 3; a++) o->mcReq[a] = d[a];
+  if (o->inited) {   // after init: a new grid with the same transfer functions
+    uint32_t acc[3] = {0, 0, 0};
+    for (auto &h : o->ch)
+      for (int a = 0; a < 3; a++) acc[a] += (uint32_t)((float)(uint32_t)h.dims[a] / 4.0f);
+    for (int a = 0; a < 3; a++) acc[a] = (uint32_t)((float)acc[a] / (float)o->ch.size());
+    for (int a = 0; a < 3; a++) o->mc[a] = o->mcReq[a] ? o->mcReq[a] : acc[a];
+    if (o->mc[0] == 0 || o->mc[1] == 0 || o->mc[2] == 0) { o->err = "zero macrocell dims"; return ORC_BAD; }
+    build_ranges(*o);
+    recalc_majorants(*o);
+    o->accumID = 0; o->accumParam = 0;
+  }
   return ORC_OK;
 }
 

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_symbols():
     syms = set()
-    for h in ("mdwt.h", "mdwt_denoiser.h"):
+    for h in ("mdwt.h", "mdwt_denoiser.h", "mdwt_batch.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         syms |= set(re.findall(r"\b(mdwt_[a-z0-9_]+)\s*\(", text))
@@ -33,7 +33,8 @@ def test_header_declares_the_renderer_surface():
 def test_library_exports_every_declared_symbol(mdwt_lib):
     syms = header_symbols()
     for must in ["mdwt_denoiser_create", "mdwt_denoiser_train_step", "mdwt_denoiser_infer", "mdwt_denoise",
-                 "mdwt_render_expected", "mdwt_accum_rmse", "mdwt_set_features"]:
+                 "mdwt_render_expected", "mdwt_accum_rmse", "mdwt_set_features", "mdwt_batch_render",
+                 "mdwt_batch_autotune", "mdwt_autotune_macrocells"]:
         assert must in syms
     missing = [s for s in syms if not hasattr(mdwt_lib, s)]
     assert not missing, missing
