@@ -23,6 +23,11 @@ the estimator (libmdwt's mdwt_render_expected) -- and how long one low-spp frame
 learned denoiser (weights in mdwtracker_b200/weights, trained by
 mdwtracker_b200/train_denoiser.py) takes to get there.
 
+batch (--no-batch skips it): 64 render requests of mixed resolution, channel count,
+voxel format, method, camera and spp rendered per frame through the batch API (one
+persistent launch per kernel variant, CUDA-graph replay, autotuned schedule) against the
+same requests rendered one after the other.
+
 --impl reference times the reference's path restated on the CPU (the OpenMP oracle,
 the reference itself cannot be built: no OptiX/OWL) on the same scene, on all host
 cores, each step a band of image rows; rank 0 only.
@@ -54,6 +59,8 @@ def parse_args():
     ap.add_argument("--res", type=int, nargs=2, default=None, help="override the resolution (smaller profiling cases)")
     ap.add_argument("--spp", type=int, default=None, help="override samples per pixel")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-RMSE measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-request measurement")
+    ap.add_argument("--batch-requests", type=int, default=64)
     ap.add_argument("--ttr-config", default="c3", choices=["c1", "c2", "c3", "c3ndda"])
     ap.add_argument("--ttr-target", type=float, default=0.01)
     return ap.parse_args()
@@ -248,6 +255,63 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
                   "path_samples": frames * w * h, "trace": trace},
         "denoised": denoised,
     }
+
+
+def batch_throughput(device_index, n_requests, frames=3, small=False):
+    """The batched workload (64 requests of mixed resolution, channel count, format,
+    method, camera and spp): one batch frame = one frame of every request through
+    libmdwt's batch API (one persistent launch per kernel variant, CUDA-graph replay,
+    autotuned schedule), against the same requests rendered one after the other with
+    mdwt_render.  Device time from CUDA events."""
+    import torch
+    from mdwtracker_b200 import Batch, Renderer
+    from mdwtracker_b200 import synthetic as syn
+    t0 = time.perf_counter()
+    scenes = (syn.scenes_c4(n=n_requests, resolutions=((256, 256),), max_spp=4) if small
+              else syn.scenes_c4(n=n_requests))
+    reqs = [sc.setup(Renderer(device_index)) for sc in scenes]
+    setup_s = time.perf_counter() - t0
+    paths = sum(sc.resolution[0] * sc.resolution[1] * sc.spp for sc in scenes)
+    st = torch.cuda.Stream(torch.device("cuda", device_index))
+    # one after the other
+    for r in reqs:
+        r.Render(st.cuda_stream)
+    torch.cuda.synchronize()
+    a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seq = []
+    for _ in range(frames):
+        a.record(st)
+        for r in reqs:
+            r.Render(st.cuda_stream)
+        b2.record(st)
+        torch.cuda.synchronize()
+        seq.append(a.elapsed_time(b2))
+    # batched, autotuned
+    b = Batch(device_index)
+    for r in reqs:
+        b.add(r)
+    t0 = time.perf_counter()
+    best = b.autotune(frames=1)
+    tune_s = time.perf_counter() - t0
+    b.render(st.cuda_stream)
+    torch.cuda.synchronize()
+    bat = []
+    for _ in range(frames):
+        b.render(st.cuda_stream)
+        bat.append(b.lastMs())
+    info = b.info()
+    b.close()
+    for r in reqs:
+        r.close()
+    ms_seq, ms_bat = min(seq), min(bat)
+    return {"workload": f"c4_{n_requests}req_{'256x256_1-4spp' if small else 'mixed'}", "requests": n_requests,
+            "path_samples_per_frame": paths,
+            "batched": {"ms_per_frame": ms_bat, "Gpath_samples_per_s": paths / ms_bat / 1e6,
+                        "kernel_variant_groups": info["groups"], "work_units": info["units"],
+                        "graph_replays": info["graph_replays"], "autotuned": {"unit_items": best[0], "pool": best[1],
+                                                                              "trips": best[2], "seconds": tune_s}},
+            "one_by_one": {"ms_per_frame": ms_seq, "Gpath_samples_per_s": paths / ms_seq / 1e6},
+            "speedup": ms_seq / ms_bat, "setup_s": setup_s}
 
 
 DENOISER_WEIGHTS = os.path.join(ROOT, "mdwtracker_b200", "weights", "denoiser_c3_syncdda.npy")
@@ -468,6 +532,14 @@ def main():
         except Exception as ex:  # reported beside the throughput line, never required
             ttr = {"error": str(ex)}
 
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        try:
+            batch = {"mixed": batch_throughput(local, args.batch_requests),
+                     "small": batch_throughput(local, args.batch_requests, small=True)}
+        except Exception as ex:  # reported beside the throughput line, never required
+            batch = {"error": str(ex)}
+
     l2note = f"flushed between timed steps ({args.flush_mib} MiB write, outside the timed events)"
     line = {
         "metric": "Gpath-samples/s",
@@ -491,6 +563,7 @@ def main():
         "e2e": {"value": world * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": w * h * 4, "ms_per_step": e2e},
         "time_to_rmse": ttr,
+        "batch": batch,
         "gpu_launches": int(launches),
         "clocks": clk,
         "counters": {"density_samples": int(cnt[0]), "rejections": int(cnt[1]), "cells": int(cnt[2]),

@@ -200,3 +200,37 @@ def scene_c3(seed: int = 3, n: int = 512, channels: int = 6, edge: int = 16, mod
     mc = max(1, n // edge)
     return Scene(f"c3_{'syncdda' if mode == 2 else 'ndda'}_{channels}x{n}f32_e{edge}", vols, tfs, mode=mode,
                  macrocells=(mc, mc, mc), resolution=(1920, 1080), spp=256)
+
+
+def scenes_c4(seed: int = 4, n: int = 64, resolutions=((256, 256), (512, 512), (1024, 1024), (1920, 1080)),
+              max_spp: int = 64) -> List[Scene]:
+    """Batched workload: `n` render requests with resolutions drawn from {256^2, 512^2,
+    1024^2, 1920x1080}, 1-8 channels drawn from the 64^3 blob and 256^3 sparse-noise
+    generators (all uint8 or all float32 per request), -m 0 or -m 2, macrocells of 8 / 16
+    voxels, 1-64 spp, a random camera on the bounding sphere (distance 2.5, fovy 45) and
+    random transfer functions.  Volumes come from a small seeded pool shared by the
+    requests."""
+    rng = np.random.default_rng(seed)
+    pool_u8 = [blobs(64, 16, 100 + i) for i in range(3)] + [value_noise_sparse(256, occ, 200 + i)
+                                                          for i, occ in enumerate([0.1, 0.2, 0.3])]
+    pool_f32 = [(v.astype(np.float32) / 255.0) for v in pool_u8]
+    out = []
+    for i in range(n):
+        use_f32 = bool(rng.integers(0, 2))
+        pool = pool_f32 if use_f32 else pool_u8
+        nch = int(rng.integers(1, 9))
+        idx = rng.integers(0, len(pool), nch)
+        vols = [pool[j] for j in idx]
+        big = any(v.shape[0] == 256 for v in vols)
+        mc = 16 if big else 8
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        eye = tuple(float(x) for x in (0.5 + 2.5 * d))
+        up = (0.0, 1.0, 0.0) if abs(d[1]) < 0.95 else (1.0, 0.0, 0.0)
+        tfs = [ramp_tf(tuple(float(x) for x in rng.uniform(0.2, 1.0, 3)), alpha_max=float(rng.uniform(0.5, 1.0)))
+               for _ in range(nch)]
+        out.append(Scene(f"c4_req{i}", vols, tfs, mode=int(rng.choice([0, 2])), macrocells=(mc, mc, mc),
+                         resolution=tuple(resolutions[int(rng.integers(0, len(resolutions)))]),
+                         spp=int(rng.integers(1, max_spp + 1)),
+                         camera=(eye, (0.5, 0.5, 0.5), up, 45.0)))
+    return out
