@@ -720,8 +720,8 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   if (!c) return MDWT_ERR_BAD_ARG;
   if (c->inited) return fail(c, MDWT_ERR_STATE, "already initialised");
   if (c->ch.empty()) return fail(c, MDWT_ERR_STATE, "No data source specified (renderer.cpp:326-330)");
-  if (mode < MDWT_MODE_NDDA || mode > MDWT_MODE_CUMULATIVE)
-    return fail(c, MDWT_ERR_UNSUPPORTED, "mode not supported (0..3 are; 4..9 are the blending modes and ray marchers)");
+  if (mode < MDWT_MODE_NDDA || mode > MDWT_MODE_MIX)
+    return fail(c, MDWT_ERR_UNSUPPORTED, "mode not supported (0..5 are; 6..9 are the ray marchers)");
   if (c->device == MDWT_HOST_ONLY) return fail(c, MDWT_ERR_STATE, "host-only context: no device to initialise");
   CK(cudaSetDevice(c->device), "cudaSetDevice");
   c->mode = mode;
@@ -756,7 +756,7 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   }
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
-  CK(cudaMalloc(&c->dMaj, c->M * (mode == 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  CK(cudaMalloc(&c->dMaj, c->M * (mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
   CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
   c->inited = true;
   mdwt_status s = build_ranges(c);
@@ -1039,7 +1039,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   if (nrect > 0) {
     if ((s = grow(c, (void **)&c->dRec, c->recCap, (size_t)batch * nrect * 4, "records")) != MDWT_OK) return s;
     if (stats && (s = grow(c, (void **)&c->dRecStats, c->recStatsCap, (size_t)batch * nrect * 4, "record stats")) != MDWT_OK) return s;
-    if ((c->gradient || c->featOn) &&
+    if ((c->gradient || c->featOn || c->mode >= MDWT_MODE_MAX) &&
         (s = grow(c, (void **)&c->dRecT, c->recTCap, (size_t)batch * nrect * 4, "hit distances")) != MDWT_OK)
       return s;
     if (batch < c->spp) {
@@ -1049,7 +1049,9 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   }
   p.records = c->dRec;
   p.recStats = stats ? c->dRecStats : nullptr;
-  p.recT = (c->gradient || c->featOn) ? c->dRecT : nullptr;
+  // hit distances: gradient shading, features, and the blending modes (the resolve pass
+  // recomputes the blended colour at the hit)
+  p.recT = (c->gradient || c->featOn || c->mode >= MDWT_MODE_MAX) ? c->dRecT : nullptr;
   if (c->featOn) {
     if (batch < c->spp || c->spp > 65535)
       return fail(c, MDWT_ERR_UNSUPPORTED, "denoiser features need the frame in one sample batch and spp < 65536");
@@ -1223,7 +1225,7 @@ static mdwt_status regrid(mdwt_ctx *c) {
   c->M = (size_t)mc[0] * mc[1] * mc[2];
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
-  CK(cudaMalloc(&c->dMaj, c->M * (c->mode == 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  CK(cudaMalloc(&c->dMaj, c->M * (c->mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
   CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
   mdwt_status s = build_ranges(c);
   if (s) return s;
@@ -1784,7 +1786,7 @@ mdwt_status mdwt_get_majorants(mdwt_ctx *c, float *out) {
   if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
   CK(cudaSetDevice(c->device), "cudaSetDevice");
   CK(cudaDeviceSynchronize(), "sync");
-  const size_t n = c->M * (c->mode == 3 ? 1 : c->ch.size());
+  const size_t n = c->M * (c->mode >= 3 ? 1 : c->ch.size());
   CK(cudaMemcpy(out, c->dMaj, n * 4, cudaMemcpyDeviceToHost), "copy majorants");
   return MDWT_OK;
 }

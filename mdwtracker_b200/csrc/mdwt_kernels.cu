@@ -110,7 +110,7 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
   const int C = p.C;
   for (size_t cell = (size_t)blockIdx.x * blockDim.x + threadIdx.x; cell < p.M; cell += (size_t)gridDim.x * blockDim.x) {
     const float2 *r = reinterpret_cast<const float2 *>(p.ranges) + cell * C;
-    if (p.mode == 3) {
+    if (p.mode >= 3) {   // summed majorant: -m 3 and the blending modes -m 4/5 (renderer.cu:250-257)
       float sum = 0.f;
       for (int c = 0; c < C; c++) {
         const float2 rc = r[c];

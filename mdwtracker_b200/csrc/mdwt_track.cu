@@ -432,7 +432,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
               enter_cell();
               act = A_CHAN;
             }
-            if constexpr (MODE == 3) {  // summed majorant (deviceCode.cu:541-548)
+            if constexpr (MODE >= 3) {  // summed majorant (deviceCode.cu:541-548, 1003-1007)
               if (cmask & 1u) {
                 maj = __ldg(P.majorants + cellID);
                 t = ct0;
@@ -490,7 +490,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             if (tW >= t1w) {  // world exit
               if (STATS) pRej++;
               totRej++;
-              if ((MODE == 2 && ch == C - 1) || MODE == 1 || MODE == 3) finish();
+              if ((MODE == 2 && ch == C - 1) || MODE == 1 || MODE >= 3) finish();
               else { ch++; act = MODE == 2 ? A_CHAN : A_NEWDDA; st = S_TRANS; }
             } else {
               st = S_SAMPLE;
@@ -507,7 +507,29 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
       const float ys = fmaf(tW, wdy, SH ? loy : P.camOrg.y) * P.w2u.y;
       const float zs = fmaf(tW, wdz, SH ? loz : P.camOrg.z) * P.w2u.z;
       st = S_STEP;
-      if constexpr (MODE == 3) {  // one threshold walked down through the channels (deviceCode.cu:590-613)
+      if constexpr (MODE == 4) {  // blended sample, -m 4 and -m 5 (deviceCode.cu:165-241, 1031-1058)
+        // both blends have the maximum channel opacity as their opacity; the colour is
+        // recomputed from the hit position by the resolve pass
+        float w = 0.f;
+        if (!(xs < 0.0f || xs > 1.0f || ys < 0.0f || ys > 1.0f || zs < 0.0f || zs > 1.0f)) {
+          for (int c = 0; c < C; c++) {
+            const ChanSm &cs = sch[c];
+            Axis tax;
+            const float a = tf_alpha(cs, sample_volume<SK>(P, cs, xs, ys, zs), tax);
+            if (a > w) w = a;
+          }
+        }
+        if (STATS) pSamp++;
+        totSamp++;
+        if (w > 0.0f && rng_next(rng) * maj < w) {   // the draw only when w > 0 (deviceCode.cu:1049)
+          record = 0x80000000u;
+          if constexpr (SH) tHitW = tW;
+          finish();
+        } else {
+          if (STATS) pRej++;
+          totRej++;
+        }
+      } else if constexpr (MODE == 3) {  // one threshold walked down through the channels (deviceCode.cu:590-613)
         float thr = rng_next(rng) * maj;
         bool hitNow = false;
         for (int c = 0; c < C; c++) {
@@ -744,6 +766,57 @@ __device__ void gradient_shading(const TrackParams &P, int ch, float tHit, float
   }
 }
 
+// transferFunction (deviceCode.cu:27-42) with its colour: alpha * opacityScale, rgb;
+// (1, 0, 1) and alpha 0 outside the volume domain.
+__device__ __forceinline__ float tf_sample(const TrackParams &P, const ChanSm &cs, int c, float f, float &r, float &g,
+                                           float &b) {
+  r = 1.f; g = 0.f; b = 1.f;
+  if (cs.n <= 0 || f < cs.vd0 || f > cs.vd1) return 0.f;
+  const float r1 = (f - cs.vd0) / (cs.vd1 - cs.vd0);
+  const float r2 = (r1 - cs.xd0) / (cs.xd1 - cs.xd0);
+  const Axis ax = axis(r2, cs.n);
+  const float *R = P.tfRgba[c];
+  r = lerpf(ax.a, __ldg(R + 4 * ax.i0 + 0), __ldg(R + 4 * ax.i1 + 0));
+  g = lerpf(ax.a, __ldg(R + 4 * ax.i0 + 1), __ldg(R + 4 * ax.i1 + 1));
+  b = lerpf(ax.a, __ldg(R + 4 * ax.i0 + 2), __ldg(R + 4 * ax.i1 + 2));
+  return lerpf(ax.a, __ldg(cs.tfAlpha + ax.i0), __ldg(cs.tfAlpha + ax.i1)) * cs.os;
+}
+
+// Colour of a blended hit (-m 4 maxOpacityBlend, -m 5 mixBlend; deviceCode.cu:165-200)
+// recomputed at the hit: the primary ray of (px, py, sample s), world t = tHit.
+template <int SK>
+__device__ void blend_colour(const TrackParams &P, int px, int py, int s, float tHit, float &r, float &g, float &b) {
+  float dx, dy, dz;
+  primary_ray(P, px, py, s, dx, dy, dz);
+  const float x = fmaf(tHit, dx, P.camOrg.x) * P.w2u.x;
+  const float y = fmaf(tHit, dy, P.camOrg.y) * P.w2u.y;
+  const float z = fmaf(tHit, dz, P.camOrg.z) * P.w2u.z;
+  r = g = b = 0.f;
+  if (x < 0.0f || x > 1.0f || y < 0.0f || y > 1.0f || z < 0.0f || z > 1.0f) return;
+  if (P.mode == 4) {   // the sample of the most opaque channel
+    float best = 0.f;
+    for (int c = 0; c < P.C; c++) {
+      const ChanSm cs = chan_params(P, c);
+      float cr, cg, cb;
+      const float a = tf_sample(P, cs, c, sample_volume<SK>(P, cs, x, y, z), cr, cg, cb);
+      if (a > best) { best = a; r = cr; g = cg; b = cb; }
+    }
+  } else {             // opacity-weighted colours over the maximum opacity
+    float sr = 0.f, sg = 0.f, sb = 0.f, mo = 0.f;
+    for (int c = 0; c < P.C; c++) {
+      const ChanSm cs = chan_params(P, c);
+      float cr, cg, cb;
+      const float a = tf_sample(P, cs, c, sample_volume<SK>(P, cs, x, y, z), cr, cg, cb);
+      sr = fmaf(cr, a, sr);
+      sg = fmaf(cg, a, sg);
+      sb = fmaf(cb, a, sb);
+      if (a > mo) mo = a;
+    }
+    if (mo <= 0.0f) return;
+    r = sr / mo; g = sg / mo; b = sb / mo;
+  }
+}
+
 // One pixel of the resolve pass; returns the path-samples it accounts for without
 // tracing (culled pixels).
 template <bool STATS, bool SHADE, int SK>
@@ -778,13 +851,18 @@ __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, 
       float cr = 0.f, cg = 0.f, cb = 0.f, ca = 0.f;
       if (r) {
         const int ch = (int)((r >> 27) & 15u);
-        const int i0 = (int)((r >> 13) & 0x3fffu);
-        const int i1 = ((r >> 12) & 1u) ? i0 : i0 + 1;
-        const float a = (float)(r & 0x1ffu) * (1.0f / 256.0f);
-        const float *R = P.tfRgba[ch];
-        const float ar = lerpf(a, __ldg(R + 4 * i0 + 0), __ldg(R + 4 * i1 + 0));
-        const float ag = lerpf(a, __ldg(R + 4 * i0 + 1), __ldg(R + 4 * i1 + 1));
-        const float ab = lerpf(a, __ldg(R + 4 * i0 + 2), __ldg(R + 4 * i1 + 2));
+        float ar, ag, ab;
+        if (P.mode >= 4) {
+          blend_colour<SK>(P, px, py, P.sBase + k, P.recT[(size_t)k * nrect + q], ar, ag, ab);
+        } else {
+          const int i0 = (int)((r >> 13) & 0x3fffu);
+          const int i1 = ((r >> 12) & 1u) ? i0 : i0 + 1;
+          const float a = (float)(r & 0x1ffu) * (1.0f / 256.0f);
+          const float *R = P.tfRgba[ch];
+          ar = lerpf(a, __ldg(R + 4 * i0 + 0), __ldg(R + 4 * i1 + 0));
+          ag = lerpf(a, __ldg(R + 4 * i0 + 1), __ldg(R + 4 * i1 + 1));
+          ab = lerpf(a, __ldg(R + 4 * i0 + 2), __ldg(R + 4 * i1 + 2));
+        }
         float kd = kd0, ks = ks0;
         if constexpr (SHADE) {
           float diffuse = 1.0f, specular = 0.0f, shadow = 1.0f;
@@ -942,6 +1020,8 @@ int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launc
     case 1: rc = u8 ? launch_tbs<1, kStoreU8>(g, st, numSMs, grid) : launch_tbs<1, kStoreF32>(g, st, numSMs, grid); break;
     case 2: rc = u8 ? launch_tbs<2, kStoreU8>(g, st, numSMs, grid) : launch_tbs<2, kStoreF32>(g, st, numSMs, grid); break;
     case 3: rc = u8 ? launch_tbs<3, kStoreU8>(g, st, numSMs, grid) : launch_tbs<3, kStoreF32>(g, st, numSMs, grid); break;
+    case 4:
+    case 5: rc = u8 ? launch_tbs<4, kStoreU8>(g, st, numSMs, grid) : launch_tbs<4, kStoreF32>(g, st, numSMs, grid); break;
     default: return (int)cudaErrorInvalidValue;
   }
   if (launches) *launches += (g.numUnits > 0 ? 1 : 0) + (g.totalPix > 0 ? 1 : 0);
@@ -959,6 +1039,8 @@ int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, 
     case 1: rc = u8 ? launch_s<1, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<1, kStoreF32>(p, st, numSMs, grid, evMid); break;
     case 2: rc = u8 ? launch_s<2, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<2, kStoreF32>(p, st, numSMs, grid, evMid); break;
     case 3: rc = u8 ? launch_s<3, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<3, kStoreF32>(p, st, numSMs, grid, evMid); break;
+    case 4:
+    case 5: rc = u8 ? launch_s<4, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<4, kStoreF32>(p, st, numSMs, grid, evMid); break;
     default: return (int)cudaErrorInvalidValue;
   }
   *block = kTPB;

@@ -283,7 +283,7 @@ class Renderer:
         return int(d[0]) * int(d[1]) * int(d[2])
 
     def majorants(self) -> np.ndarray:
-        n = self._num_cells() * (1 if self.mode == 3 else self.numChannels)
+        n = self._num_cells() * (1 if self.mode >= 3 else self.numChannels)
         out = np.empty(n, dtype=np.float32)
         self._call("get_majorants", out.ctypes.data_as(C.POINTER(C.c_float)))
         return out

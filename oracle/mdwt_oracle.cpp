@@ -476,8 +476,9 @@ static float channel_majorant(const TFData &t, float mn, float mx) {
 static void recalc_majorants(Oracle &o) {
   const int C = (int)o.ch.size();
   const size_t M = (size_t)o.mc[0] * o.mc[1] * o.mc[2];
-  if (o.mode == 3) {
-    // _recalculateDensityRanges(float2*) renderer.cu:111-157: sum over channels
+  if (o.mode >= 3) {
+    // _recalculateDensityRanges(float2*) renderer.cu:111-157: sum over channels (-m 3, and
+    // the blending modes -m 4/5, renderer.cu:255-258)
     o.majorants.assign(M, 0.f);
     for (size_t cell = 0; cell < M; cell++) {
       float s = 0.f;
@@ -828,6 +829,66 @@ static void track_cumulative(const Oracle &o, TrackCtx &tc, RayPayload &prd) {
   dda3(tc.org, tc.dir, 1e20f, mc, lam);
 }
 
+// blendChannels (deviceCode.cu:165-241): opacity of the blended sample, its colour.
+static float blend_sample(const Oracle &o, V3 x, float rgb[3]) {
+  rgb[0] = rgb[1] = rgb[2] = 0.f;
+  if (x.x < 0.0f || x.x > 1.0f || x.y < 0.0f || x.y > 1.0f || x.z < 0.0f || x.z > 1.0f) return 0.f;
+  const int C = (int)o.ch.size();
+  if (o.mode == 4) {   // maxOpacityBlend
+    float best = 0.f;
+    for (int c = 0; c < C; c++) {
+      float crgb[3];
+      const float a = tf_eval(o.tf[c], sample_volume(o, c, x), crgb);
+      if (a > best) { best = a; rgb[0] = crgb[0]; rgb[1] = crgb[1]; rgb[2] = crgb[2]; }
+    }
+    return best;
+  }
+  float col[3] = {0.f, 0.f, 0.f}, mo = 0.f;   // mixBlend
+  for (int c = 0; c < C; c++) {
+    float crgb[3];
+    const float a = tf_eval(o.tf[c], sample_volume(o, c, x), crgb);
+    for (int k = 0; k < 3; k++) col[k] = std::fma(crgb[k], a, col[k]);
+    if (a > mo) mo = a;
+  }
+  if (mo <= 0.0f) return 0.f;
+  for (int k = 0; k < 3; k++) rgb[k] = col[k] / mo;
+  return mo;
+}
+
+// blendDTCH, -m 4 / -m 5 (deviceCode.cu:972-1065)
+static void track_blend(const Oracle &o, TrackCtx &tc, RayPayload &prd) {
+  const float *M = o.majorants.data();
+  const uint32_t *mc = o.mc;
+  auto lam = [&](const int cell[3], float t0, float t1) -> bool {
+    prd.cells++;
+    const int cellID = cell[0] + cell[1] * (int)mc[0] + cell[2] * (int)mc[0] * (int)mc[1];
+    const float majorant = M[cellID];
+    if (majorant == 0.00f) return true;
+    float t = t0;
+    while (true) {
+      if (!count_step(prd)) return false;
+      t = woodcock_step(t, prd.rng.next(), majorant, o.dt, tc.w2g);
+      if (t >= t1) break;
+      const float tWorld = t * tc.g2w;
+      const V3 x = tex_pos(tc, tWorld);
+      if (tWorld >= prd.t1) { prd.rejections++; return false; }
+      float rgb[3];
+      const float w = blend_sample(o, x, rgb);
+      prd.samples++;
+      if (w > 0.0f && prd.rng.next() * majorant < w) {   // the draw only when w > 0
+        prd.tHit = tWorld;
+        prd.rgb[0] = rgb[0]; prd.rgb[1] = rgb[1]; prd.rgb[2] = rgb[2];
+        prd.missed = false;
+        prd.channelID = 0;   // blendDTCH leaves the payload's channel at its initial 0
+        return false;
+      }
+      prd.rejections++;
+    }
+    return true;
+  };
+  dda3(tc.org, tc.dir, 1e20f, mc, lam);
+}
+
 static void trace_volume(const Oracle &o, V3 worldOrg, V3 worldDir, RayPayload &prd) {
   prd.missed = true;
   prd.rgb[0] = prd.rgb[1] = prd.rgb[2] = 0.f;
@@ -853,6 +914,8 @@ static void trace_volume(const Oracle &o, V3 worldOrg, V3 worldDir, RayPayload &
     case 1: track_multi(o, tc, prd); break;
     case 2: track_syncdda(o, tc, prd); break;
     case 3: track_cumulative(o, tc, prd); break;
+    case 4:
+    case 5: track_blend(o, tc, prd); break;
   }
 }
 
@@ -1224,7 +1287,7 @@ static void reset_dt(Oracle *o) {
 
 int orc_init(Oracle *o, int mode, int autoCam) {
   if (o->ch.empty()) { o->err = "no channels"; return ORC_STATE; }
-  if (mode < 0 || mode > 3) { o->err = "mode"; return ORC_UNSUP; }
+  if (mode < 0 || mode > 5) { o->err = "mode"; return ORC_UNSUP; }
   o->mode = mode;
   // CalculateMCGridDims(4) (renderer.cpp:1342-1355)
   if (o->mcReq[0] == 0 || o->mcReq[1] == 0 || o->mcReq[2] == 0) {

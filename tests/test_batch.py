@@ -22,6 +22,8 @@ def _requests():
         dict(vols=u8[1:], mode=2, res=(24, 70), spp=1, mc=(6, 6, 6), stats=False),
         dict(vols=f32[:1], mode=3, res=(40, 40), spp=5, mc=(3, 3, 3), stats=True, xf=(0.0, 0.05)),
         dict(vols=u8[:1], mode=1, res=(50, 30), spp=2, mc=(4, 4, 4), stats=False),
+        dict(vols=u8, mode=5, res=(36, 44), spp=3, mc=(5, 5, 5), stats=True),
+        dict(vols=f32, mode=4, res=(30, 30), spp=2, mc=(4, 4, 4), stats=False, xf=(0.0, 0.05)),
     ]
     return specs
 

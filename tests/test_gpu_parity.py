@@ -88,7 +88,7 @@ def test_c1_like_ndda(oracle):
     assert c[0] > 0 and c[3] == 96 * 80 * 5
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
 def test_c2_like_three_channels(oracle, mode):
     vols = [noise_u8(48, occ, 10 + i) for i, occ in enumerate([0.1, 0.2, 0.3])]
     tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(3)]
@@ -97,7 +97,7 @@ def test_c2_like_three_channels(oracle, mode):
     run_frames(p, o, 2)
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
 def test_float32_lognormal(oracle, mode):
     vols = [syn.lognormal(40, 5 + i, octaves=4) for i in range(2)]
     tfs = [syn.ramp_tf(syn.HUES[i], alpha_max=0.7) for i in range(2)]
@@ -113,7 +113,7 @@ def test_mixed_formats_and_ragged_dims(oracle):
     b = (syn.value_noise(24, 3, 4) * 40.0).astype(np.float32)[:, :20, :]  # dims (24, 20, 24)
     c = rng.integers(-20, 60, (17, 23, 29)).astype(np.int8)          # dims (29, 23, 17)
     tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(3)]
-    for mode in (0, 1, 2, 3):
+    for mode in (0, 1, 2, 3, 4, 5):
         p, o = make_pair(oracle, [a, b, c], tfs, mode, (7, 5, 3), (45, 37), 3, opacity=[1.0, 0.6, 2.0])
         assert_same_grid(p, o)
         run_frames(p, o, 2)
@@ -251,7 +251,7 @@ def _shade(r, shadows, gradient, light, nch):
                       gradientStep=(0.01, 0.2, 0.05)[i % 3], specularColor=(1.0, 0.9 - 0.2 * i, 0.8))
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("shadows,gradient", [(True, False), (False, True), (True, True)])
 def test_shadows_and_gradient_shading(oracle, mode, shadows, gradient):
     """Shadow rays traced by the same tracker from the hit point towards -lightDir
@@ -277,7 +277,7 @@ def test_shading_float_channels_and_batches(oracle, mode):
     run_frames(p, o, 2)
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
 def test_denoiser_features(oracle, mode):
     """Per-pixel denoiser features (radiance, depth, transmittance, channel hit fractions),
     bit for bit, and the accumulation unchanged by turning them on."""
