@@ -52,7 +52,9 @@ mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *d_features, 
                                      int h, int w, float lr, double *loss, void *stream);
 
 /* Convolution path: 1 (default) = tcgen05 tensor-core kernels (TMA operand loads, TMEM
- * accumulator) wherever the layer shapes allow, 0 = the mma.sync kernels everywhere. */
+ * accumulator) wherever the layer shapes allow, tiled for two CTAs per SM where possible;
+ * 2 = the same kernels with the most output rows per CTA (one CTA per SM); 0 = the
+ * mma.sync kernels everywhere.  The tiling is process-wide. */
 mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode);
 /* Wait for the denoiser's work; MDWT_ERR_TIMEOUT when a tensor-core kernel's bounded
  * wait for its operands gave up (its output is then invalid). */

@@ -404,12 +404,13 @@ mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *F, const flo
 }
 
 mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode) {
-  if (!d || mode < 0 || mode > 1) return MDWT_ERR_BAD_ARG;
+  if (!d || mode < 0 || mode > 2) return MDWT_ERR_BAD_ARG;
+  if (mode >= 1) mdwt::nn::conv3x3_tc_policy(mode == 1 ? 1 : 0);
   if (mode && !d->useTC) {   // operand copies may be stale after mma.sync-path training
     d->useTC = 1;
     return refresh_copies(d);
   }
-  d->useTC = mode;
+  d->useTC = mode ? 1 : 0;
   return MDWT_OK;
 }
 

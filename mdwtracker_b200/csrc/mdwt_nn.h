@@ -40,6 +40,8 @@ int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int nu
 // tcgen05 path (mdwt_nn_tc.cu): the same convolution with the weights in the operand
 // layout Wu[tap][ci / 8][co][8] (umma_weights); *err is set when a bounded wait gave up.
 bool conv3x3_tc_supported(int Cin, int Cout);
+// Tiling policy: 0 = most output rows per CTA, 1 = two CTAs per SM where possible.
+void conv3x3_tc_policy(int policy);
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream);
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
                int relu, int outF32, int *err, void *stream);

@@ -101,6 +101,7 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
+constexpr int kMaxStages = 4;     // weight ring depth (runtime NS <= kMaxStages)
 constexpr uint32_t kSlot = 2176;   // smem slot of one A box (8 channels x 130 pixels = 2080 B), 128-B aligned
 constexpr int kHalo = kTM + 2;     // input pixels per row segment (one-pixel halo each side)
 
@@ -110,9 +111,9 @@ constexpr int kHalo = kTM + 2;     // input pixels per row segment (one-pixel ha
 __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap mapX, const bf16 *Wu,
                                                          const float *bias, void *Y, int N, int H, int W, int Cin,
                                                          int Cout, int relu, int outF32, int tmemCols, int R, int KC,
-                                                         int *err) {
+                                                         int NS, int *err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t full[2], empty[2], fullA, freeA, done;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], fullA, freeA, done;
   __shared__ uint32_t tmemBase;
   uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -126,14 +127,14 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
   const uint32_t aBytes = (uint32_t)(R + 2) * aRowBytes;  // A buffer
   const uint32_t wBytes = (uint32_t)KC * Cout * 2;        // one tap's weights of a chunk
   uint8_t *bufA = smem;
-  uint8_t *stW[2] = {smem + aBytes, smem + aBytes + wBytes};
+  uint8_t *wBase = smem + aBytes;          // NS weight stages of wBytes each
   const int chunks = Cin / KC, Q = chunks * 9, Gtot = Cin / 8;
 
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
+    for (int i = 0; i < NS; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
     mbar_init(&fullA, 1);
     mbar_init(&freeA, 1);
     mbar_init(&done, 1);
@@ -159,22 +160,21 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
           tma_load_4d(bufA + r * aRowBytes + g * kSlot, &mapX, kc * KC + g * 8, x0 - 1, y0 - 1 + r, n, &fullA);
     };
     auto loadW = [&](int q) {
-      const int kc = q / 9, tap = q % 9, st = q & 1;
+      const int kc = q / 9, tap = q % 9, st = q % NS;
       mbar_expect_tx(&full[st], wBytes);
-      bulk_load(stW[st], Wu + ((size_t)tap * Gtot + (size_t)kc * G) * Cout * 8, wBytes, &full[st]);
+      bulk_load(wBase + (size_t)st * wBytes, Wu + ((size_t)tap * Gtot + (size_t)kc * G) * Cout * 8, wBytes, &full[st]);
     };
     loadA(0);
-    loadW(0);
-    if (Q > 1) loadW(1);
+    for (int q = 0; q < NS && q < Q; q++) loadW(q);   // fill the weight ring
     const uint32_t lboB = (uint32_t)Cout * 16;
     for (int q = 0; q < Q && ok; q++) {
-      const int kc = q / 9, t = q % 9, st = q & 1;
-      const uint32_t ph = (uint32_t)(q >> 1) & 1u;
+      const int kc = q / 9, t = q % 9, st = q % NS;
+      const uint32_t ph = (uint32_t)(q / NS) & 1u;
       if (t == 0 && !mbar_wait(&fullA, (uint32_t)kc & 1u)) { ok = false; break; }
       if (!mbar_wait(&full[st], ph)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;\n");
       const int dy = t / 3 - 1, dx = t % 3 - 1;
-      const uint32_t aBase = smem_u32(bufA) + (uint32_t)(dx + 1) * 16, bBase = smem_u32(stW[st]);
+      const uint32_t aBase = smem_u32(bufA) + (uint32_t)(dx + 1) * 16, bBase = smem_u32(wBase + (size_t)st * wBytes);
       for (int r = 0; r < R; r++) {
         const uint32_t rowBase = aBase + (uint32_t)(r + dy + 1) * aRowBytes;
         for (int k = 0; k < KC / 16; k++) {
@@ -185,9 +185,12 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
       }
       umma_commit(&empty[st]);
       if (t == 8) umma_commit(&freeA);
-      if (q + 2 < Q) {
-        if (!mbar_wait(&empty[st], ph)) { ok = false; break; }
-        loadW(q + 2);
+      // refill the stage of step q - 1 (its MMAs were issued before this step's, which
+      // are queued behind them) with step q - 1 + NS
+      if (q >= 1 && q - 1 + NS < Q) {
+        const int sp = (q - 1) % NS;
+        if (!mbar_wait(&empty[sp], (uint32_t)((q - 1) / NS) & 1u)) { ok = false; break; }
+        loadW(q - 1 + NS);
       }
       if (t == 8 && kc + 1 < chunks) {
         if (!mbar_wait(&freeA, (uint32_t)kc & 1u)) { ok = false; break; }
@@ -295,29 +298,43 @@ int tmem_cols_for(int cols) {
 }
 
 struct TcTiling {
-  int R = 0, KC = 0;
+  int R = 0, KC = 0, NS = 0;
   size_t smem = 0;
 };
 constexpr size_t kSmemBudget = 200 * 1024;
+constexpr size_t kSmemTwoCtas = 112 * 1024;   // two CTAs per SM
 
-size_t tc_smem(int R, int KC, int Cout) { return (size_t)(R + 2) * (KC / 8) * kSlot + (size_t)2 * KC * Cout * 2; }
+size_t tc_smem(int R, int KC, int Cout, int NS) {
+  return (size_t)(R + 2) * (KC / 8) * kSlot + (size_t)NS * KC * Cout * 2;
+}
 
-// Rows per CTA (<= 8, R * Cout <= 512 TMEM columns) and input-channel chunk (the largest
-// divisor of Cin, a multiple of 16, whose buffers fit the shared-memory budget).
+int g_tcPolicy = 1;   // 1: two CTAs per SM where possible (measured faster); 0: most rows per CTA
+
+// Rows per CTA R (<= 8), input-channel chunk KC (a divisor of Cin, multiple of 16) and
+// weight stages NS (3, else 2) whose buffers fit the shared-memory budget, R * Cout
+// TMEM columns.  Policy 1 first looks for a tiling that fits two CTAs per SM (R >= 2,
+// R * Cout <= 256, <= 112 KB).
 TcTiling tc_tiling(int Cin, int Cout, int H) {
   TcTiling t;
-  int rmax = 512 / Cout;
-  if (rmax > 8) rmax = 8;
-  if (rmax > H) rmax = H;
-  for (int R = rmax; R >= 1; R--)
-    for (int KC = Cin; KC >= 16; KC -= 16) {
-      if (Cin % KC) continue;
-      const size_t sm = tc_smem(R, KC, Cout);
-      if (sm <= kSmemBudget) {
-        t.R = R; t.KC = KC; t.smem = sm;
-        return t;
+  auto search = [&](size_t budget, int colsMax, int rmin) {
+    int rmax = colsMax / Cout;
+    if (rmax > 8) rmax = 8;
+    if (rmax > H) rmax = H;
+    for (int R = rmax; R >= rmin; R--)
+      for (int KC = Cin; KC >= 16; KC -= 16) {
+        if (Cin % KC) continue;
+        for (int NS = 3; NS >= 2; NS--) {
+          const size_t sm = tc_smem(R, KC, Cout, NS);
+          if (sm <= budget) {
+            t.R = R; t.KC = KC; t.NS = NS; t.smem = sm;
+            return true;
+          }
+        }
       }
-    }
+    return false;
+  };
+  if (g_tcPolicy == 1 && search(kSmemTwoCtas, 256, H >= 2 ? 2 : 1)) return t;
+  search(kSmemBudget, 512, 1);
   return t;
 }
 
@@ -327,6 +344,8 @@ bool conv3x3_tc_supported(int Cin, int Cout) {
   return Cin % 16 == 0 && Cin >= 16 && Cout % 16 == 0 && Cout >= 16 && Cout <= 256 && tc_tiling(Cin, Cout, 1).R > 0 &&
          encode_fn() != nullptr;
 }
+
+void conv3x3_tc_policy(int policy) { g_tcPolicy = policy == 1 ? 1 : 0; }
 
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream) {
   const size_t n = (size_t)9 * Cin * Cout;
@@ -357,7 +376,8 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   if (e != cudaSuccess) return (int)e;
   const int tilesX = (W + kTM - 1) / kTM, tilesY = (H + tl.R - 1) / tl.R;
   conv3x3_tc_kernel<<<(unsigned)(N * tilesY * tilesX), 128, smem, (cudaStream_t)stream>>>(
-      map, (const bf16 *)Wu, bias, Y, N, H, W, Cin, Cout, relu, outF32, tmem_cols_for(tl.R * Cout), tl.R, tl.KC, err);
+      map, (const bf16 *)Wu, bias, Y, N, H, W, Cin, Cout, relu, outF32, tmem_cols_for(tl.R * Cout), tl.R, tl.KC, tl.NS,
+      err);
   return (int)cudaGetLastError();
 }
 

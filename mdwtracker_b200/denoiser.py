@@ -54,9 +54,10 @@ class Denoiser:
         except Exception:
             pass
 
-    def setTensorCores(self, on: bool) -> None:
-        """tcgen05 convolutions (default) or the mma.sync kernels."""
-        self._call("set_tensor_cores", C.c_int(1 if on else 0))
+    def setTensorCores(self, on, two_ctas: bool = True) -> None:
+        """tcgen05 convolutions (default, tiled for two CTAs per SM; `two_ctas=False`:
+        the most output rows per CTA) or the mma.sync kernels."""
+        self._call("set_tensor_cores", C.c_int((1 if two_ctas else 2) if on else 0))
 
     def check(self) -> None:
         """Synchronise; raises when a tensor-core kernel's bounded wait gave up."""

@@ -68,6 +68,7 @@ def test_gpu_forward_matches_the_reference():
     ref = ref[:, :h, :w]
     rel = np.linalg.norm(got - ref) / np.linalg.norm(ref - F[..., :3])
     assert rel < 1e-2, rel
+    d.setTensorCores(True)
     assert np.all(out.cpu().numpy()[..., 3] == 1.0)
 
 
@@ -118,8 +119,9 @@ def test_gpu_training_fits_a_fixed_batch():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("two_ctas", [False, True])
 @pytest.mark.parametrize("n,h,w", [(1, 7, 20), (2, 16, 130), (1, 12, 256)])
-def test_tensor_core_and_mma_paths_agree(n, h, w):
+def test_tensor_core_and_mma_paths_agree(n, h, w, two_ctas):
     """The tcgen05 convolutions (TMA-staged operands, TMEM accumulator) against the
     mma.sync ones: the same BF16 operands and FP32 accumulation in another order."""
     import torch
@@ -130,7 +132,7 @@ def test_tensor_core_and_mma_paths_agree(n, h, w):
     F = torch.from_numpy(_features(rng, n, h, w)).cuda()
     outs = []
     for tc in (False, True):
-        d.setTensorCores(tc)
+        d.setTensorCores(tc, two_ctas)
         o = torch.empty((n, h, w, 4), dtype=torch.float32, device="cuda")
         d.infer(F, o, n, h, w)
         d.check()
@@ -138,3 +140,4 @@ def test_tensor_core_and_mma_paths_agree(n, h, w):
     ref = outs[0] - F.cpu().numpy()[..., :3]
     rel = np.linalg.norm(outs[1] - outs[0]) / max(np.linalg.norm(ref), 1e-30)
     assert rel < 1e-2, rel
+    d.setTensorCores(True)
