@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c3ndda"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c3ndda", "c3b", "c3bndda"])
     ap.add_argument("--impl", default="mdwt", choices=["mdwt", "reference"])
     ap.add_argument("--flush-mib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
@@ -76,6 +76,10 @@ def make_scene(name, res=None, spp=None):
         sc = syn.scene_c3(mode=2)
     elif name == "c3ndda":
         sc = syn.scene_c3(mode=0)
+    elif name == "c3b":
+        sc = syn.scene_c3b(mode=2)
+    elif name == "c3bndda":
+        sc = syn.scene_c3b(mode=0)
     else:
         raise ValueError(name)
     if res is not None:

@@ -202,6 +202,16 @@ def scene_c3(seed: int = 3, n: int = 512, channels: int = 6, edge: int = 16, mod
                  macrocells=(mc, mc, mc), resolution=(1920, 1080), spp=256)
 
 
+def scene_c3b(seed: int = 5, n: int = 1024, channels: int = 3, edge: int = 16, mode: int = 2) -> Scene:
+    """The HBM-bound variant of the 1080p scene: `channels` x n^3 float32 log-normal fields
+    (3 x 1024^3 = 12 GB), otherwise as scene_c3."""
+    vols = [lognormal_log10(n, seed * 31 + i) for i in range(channels)]
+    tfs = [ramp_tf(HUES[i % len(HUES)], alpha_max=0.25, start=0.5) for i in range(channels)]
+    mc = max(1, n // edge)
+    return Scene(f"c3b_{'syncdda' if mode == 2 else 'ndda'}_{channels}x{n}f32_e{edge}", vols, tfs, mode=mode,
+                 macrocells=(mc, mc, mc), resolution=(1920, 1080), spp=256)
+
+
 def scenes_c4(seed: int = 4, n: int = 64, resolutions=((256, 256), (512, 512), (1024, 1024), (1920, 1080)),
               max_spp: int = 64) -> List[Scene]:
     """Batched workload: `n` render requests with resolutions drawn from {256^2, 512^2,
