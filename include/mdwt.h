@@ -161,6 +161,11 @@ mdwt_status mdwt_set_mirror(mdwt_ctx *ctx, int enable);
  * frame/accumulation ids; afterwards they advance exactly like the reference
  * (owlParamsSet1i(.., accumID++) after the launch). */
 mdwt_status mdwt_render(mdwt_ctx *ctx, void *cuda_stream);
+/* n successive frames (n Renderer::Render calls) with their paths traced in one launch
+ * when their path records fit the record budget together (no counterpart in the
+ * reference): the same frames, ids, accumulation and counters as n mdwt_render calls,
+ * bit for bit; the framebuffer, statistics and features are the last frame's. */
+mdwt_status mdwt_render_frames(mdwt_ctx *ctx, int n, void *cuda_stream);
 /* No reference counterpart: render only the rows [row0, row1) of the frame (other rows
  * keep their contents; row1 <= row0 = all rows).  Frame and accumulation ids advance
  * as for a full frame, so N contexts rendering disjoint bands of the same frame

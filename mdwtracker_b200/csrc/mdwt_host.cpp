@@ -1062,8 +1062,18 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   }
   p.partial = c->dPartial;
   p.partialStats = stats ? c->dPartialStats : nullptr;
+  p.nFrames = 1;
   *batchOut = batch;
   return MDWT_OK;
+}
+
+// Frames traced per launch by mdwt_render_frames: their path records fit the budget.
+static int frames_per_launch(const TrackParams &p, int spp, int n) {
+  const int rw = p.cullX1 - p.cullX0 + 1, rh = p.cullY1 - p.cullY0 + 1;
+  const size_t nrect = p.numTiles > 0 ? (size_t)rw * (size_t)rh : 0;
+  if (nrect == 0) return n;
+  const size_t g = kRecordBudget / (nrect * (size_t)spp);
+  return (int)std::min<size_t>((size_t)n, g);
 }
 
 mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
@@ -1620,6 +1630,55 @@ mdwt_status mdwt_autotune_macrocells(mdwt_ctx *c, const int *edges, int n, int f
   c->frameID = f0; c->accumID = a0; c->frameParam = fp0; c->accumParam = ap0;
   reset_accum_ids(c);
   if (bestEdge) *bestEdge = best;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_render_frames(mdwt_ctx *c, int n, void *stream) {
+  if (!c || n <= 0) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  if (n == 1) return mdwt_render(c, stream);
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  while (n > 0) {
+    TrackParams p;
+    int batch = 0;
+    mdwt_status s = prepare_frame(c, p, &batch);
+    if (s) return s;
+    const int g = batch >= c->spp ? frames_per_launch(p, c->spp, n) : 1;
+    if (g < 2) {   // a frame alone fills the record budget: one launch sequence per frame
+      if ((s = mdwt_render(c, stream))) return s;
+      n--;
+      continue;
+    }
+    const int rw = p.cullX1 - p.cullX0 + 1, rh = p.cullY1 - p.cullY0 + 1;
+    const size_t nrect = p.numTiles > 0 ? (size_t)rw * (size_t)rh : 0;
+    const size_t samples = (size_t)g * c->spp;
+    if (nrect > 0) {
+      if ((s = grow(c, (void **)&c->dRec, c->recCap, samples * nrect * 4, "records")) != MDWT_OK) return s;
+      if (c->statsOn &&
+          (s = grow(c, (void **)&c->dRecStats, c->recStatsCap, samples * nrect * 4, "record stats")) != MDWT_OK)
+        return s;
+      if ((c->gradient || c->featOn || c->mode >= MDWT_MODE_MAX) &&
+          (s = grow(c, (void **)&c->dRecT, c->recTCap, samples * nrect * 4, "hit distances")) != MDWT_OK)
+        return s;
+      p.records = c->dRec;
+      p.recStats = c->statsOn ? c->dRecStats : nullptr;
+      p.recT = (c->gradient || c->featOn || c->mode >= MDWT_MODE_MAX) ? c->dRecT : nullptr;
+    }
+    // the ids g successive Render calls hand their frames (renderer.cpp:957-958)
+    p.nFrames = g;
+    p.frameParam1 = (uint32_t)c->frameID;
+    p.accumParam1 = (uint32_t)c->accumID;
+    p.sBase = 0;
+    p.sCount = (int)samples;
+    CK(cudaMemsetAsync(c->dWork, 0, sizeof(unsigned int), st), "reset work counter");
+    CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock, nullptr), "tracker kernels");
+    for (int k = 0; k < g; k++) {
+      c->accumParam = c->accumID++;
+      c->frameParam = c->frameID++;
+    }
+    n -= g;
+  }
   return MDWT_OK;
 }
 

@@ -23,6 +23,11 @@ struct TrackParams {
   // frame
   int W, H, spp;
   uint32_t frameParam, accumParam;  // LaunchParams::frameID / accumID as the frame sees them
+  // frames traced in one launch: frame k >= 1 sees frameParam1 + k - 1, accumParam1 + k - 1
+  // (the ids n successive Render calls hand their frames); sample j of the launch is
+  // sample j % spp of frame j / spp
+  int nFrames;
+  uint32_t frameParam1, accumParam1;
   int accumulate, mirror;
   F3 bg;
   // camera basis (LaunchParams::camera)

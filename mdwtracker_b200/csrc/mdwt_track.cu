@@ -181,9 +181,9 @@ __device__ __forceinline__ void grid_dir(const TrackParams &P, float wdx, float 
 
 // Seeding, jitter and generateRay of one path-sample (deviceCode.cu:293-298, 61-76):
 // the normalised world direction; returns the generator state after the jitter draw.
-__device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, int py, int s, float &wdx, float &wdy,
-                                                float &wdz) {
-  const uint32_t seed = (uint32_t)P.W * (uint32_t)P.H * (P.frameParam + 1u) * (uint32_t)(s + 1);
+__device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, int py, uint32_t frame, int s, float &wdx,
+                                                float &wdy, float &wdz) {
+  const uint32_t seed = (uint32_t)P.W * (uint32_t)P.H * (frame + 1u) * (uint32_t)(s + 1);
   uint32_t rng = tea4((uint32_t)px + seed, (uint32_t)py + seed);
   const float jit = rng_next(rng);
   const float sxf = ((float)px + jit) / (float)P.W;
@@ -198,6 +198,17 @@ __device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, in
   const float inv = 1.0f / sqrtf(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
   wdx = dx * inv; wdy = dy * inv; wdz = dz * inv;
   return rng;
+}
+
+// Frame id and sample of sample j of the launch.
+__device__ __forceinline__ uint32_t sample_frame(const TrackParams &P, int j, int &s) {
+  if (P.nFrames <= 1) { s = j; return P.frameParam; }
+  const int k = j / P.spp;
+  s = j - k * P.spp;
+  return k == 0 ? P.frameParam : P.frameParam1 + (uint32_t)(k - 1);
+}
+__device__ __forceinline__ uint32_t frame_accum(const TrackParams &P, int k) {
+  return k == 0 ? P.accumParam : P.accumParam1 + (uint32_t)(k - 1);
 }
 
 enum : int { S_NEED = 0, S_TRANS = 1, S_STEP = 2, S_SAMPLE = 3, S_DONE = 4 };
@@ -249,6 +260,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
   int leg = 0;                                  // 0 primary, 1 shadow ray (SH)
   uint32_t primRec = 0, pxy = 0;
   float primT = 0.f;
+  uint32_t pathFrame = 0;                       // frame id of the current path (shadow seed)
 
   auto enter_cell = [&]() {  // cell_t0 / cell_t1 of the DDA lambda call (dda.h:164-170)
     const float tc = fminf(fminf(d.tnx, d.tny), d.tnz);
@@ -305,7 +317,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
         lox = fmaf(tHitW, wdx, P.camOrg.x);
         loy = fmaf(tHitW, wdy, P.camOrg.y);
         loz = fmaf(tHitW, wdz, P.camOrg.z);
-        const uint32_t sseed = (uint32_t)P.W * (uint32_t)P.H * P.frameParam;
+        const uint32_t sseed = (uint32_t)P.W * (uint32_t)P.H * pathFrame;
         rng = tea4((pxy & 0xffffu) + sseed + 1u, (pxy >> 16) + sseed + 1u);
         if (start_leg(-P.lightDir.x, -P.lightDir.y, -P.lightDir.z)) return;
         record = 0u;
@@ -358,7 +370,9 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
           const int ly = (int)(tile / (unsigned)P.tilesX) * 4 + (w >> 3);
           const int px = P.cullX0 + lx, py = P.cullY0 + ly;
           if (px <= P.cullX1 && py <= P.cullY1) {
-            const int s = P.sBase + k;
+            int s;
+            const uint32_t fr = sample_frame(P, P.sBase + k, s);
+            if constexpr (SH) pathFrame = fr;
             recIdx = (size_t)k * nrect + (size_t)ly * rw + lx;
             pxy = (uint32_t)px | ((uint32_t)py << 16);
             record = 0;
@@ -367,7 +381,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             tHitW = 0.f;
             pSamp = pRej = 0;
             float dx, dy, dz;
-            rng = primary_ray(P, px, py, s, dx, dy, dz);
+            rng = primary_ray(P, px, py, fr, s, dx, dy, dz);
             if (!start_leg(dx, dy, dz)) finish();
           }
         }
@@ -663,12 +677,12 @@ __device__ __forceinline__ void write_features(const TrackParams &P, int px, int
 
 template <bool STATS>
 __device__ __forceinline__ void write_pixel(const TrackParams &P, int px, int py, float o0, float o1, float o2, float o3,
-                                            uint4 st) {
+                                            uint4 st, uint32_t accumId) {
   const size_t pix = (size_t)px + (size_t)P.W * (size_t)py;
   if (P.accumulate) {
     float4 *ap = reinterpret_cast<float4 *>(P.accum) + pix;
     const float4 prev = *ap;
-    const float k = (float)P.accumParam, k1 = (float)(P.accumParam + 1u);
+    const float k = (float)accumId, k1 = (float)(accumId + 1u);
     o0 = fmaf(k, prev.x, o0) / k1;
     o1 = fmaf(k, prev.y, o1) / k1;
     o2 = fmaf(k, prev.z, o2) / k1;
@@ -785,9 +799,10 @@ __device__ __forceinline__ float tf_sample(const TrackParams &P, const ChanSm &c
 // Colour of a blended hit (-m 4 maxOpacityBlend, -m 5 mixBlend; deviceCode.cu:165-200)
 // recomputed at the hit: the primary ray of (px, py, sample s), world t = tHit.
 template <int SK>
-__device__ void blend_colour(const TrackParams &P, int px, int py, int s, float tHit, float &r, float &g, float &b) {
+__device__ void blend_colour(const TrackParams &P, int px, int py, uint32_t frame, int s, float tHit, float &r, float &g,
+                             float &b) {
   float dx, dy, dz;
-  primary_ray(P, px, py, s, dx, dy, dz);
+  primary_ray(P, px, py, frame, s, dx, dy, dz);
   const float x = fmaf(tHit, dx, P.camOrg.x) * P.w2u.x;
   const float y = fmaf(tHit, dy, P.camOrg.y) * P.w2u.y;
   const float z = fmaf(tHit, dz, P.camOrg.z) * P.w2u.z;
@@ -823,16 +838,19 @@ template <bool STATS, bool SHADE, int SK>
 __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, int py) {
   const int rw = P.cullX1 - P.cullX0 + 1;
   const size_t nrect = (size_t)rw * (size_t)(P.cullY1 - P.cullY0 + 1);
-  const bool last = P.sBase + P.sCount == P.spp;
+  const bool last = P.nFrames > 1 || P.sBase + P.sCount == P.spp;   // multi-frame launches are one batch
   const float kd0 = (1.0f * 1.0f) * P.lightIntensity;   // diffuse * shadow * lightIntensity (unshaded)
   const float ks0 = (0.0f * 1.0f) * P.lightIntensity;   // specular * shadow * lightIntensity
   const bool feat = P.feat != nullptr;   // denoiser features (one batch per frame)
   {
+    const int nF = P.nFrames > 1 ? P.nFrames : 1;
     if (px < P.cullX0 || px > P.cullX1 || py < P.cullY0 || py > P.cullY1) {
       if (last) {
-        write_pixel<STATS>(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], P.bgFin[3], make_uint4(0u, 0u, 0u, 0u));
+        for (int fi = 0; fi < nF; fi++)
+          write_pixel<STATS>(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], P.bgFin[3], make_uint4(0u, 0u, 0u, 0u),
+                             frame_accum(P, fi));
         if (feat) write_features(P, px, py, P.bgFin[0], P.bgFin[1], P.bgFin[2], 0u, 0.f, make_uint4(0u, 0u, 0u, 0u));
-        return (uint32_t)P.spp;
+        return (uint32_t)P.spp * (uint32_t)nF;
       }
       return 0u;
     }
@@ -847,13 +865,15 @@ __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, 
       if (STATS) sv = reinterpret_cast<const uint4 *>(P.partialStats)[q];
     }
     for (int k = 0; k < P.sCount; k++) {
+      int s;   // this record's frame and sample
+      const uint32_t fr = sample_frame(P, P.sBase + k, s);
       const uint32_t r = P.records[(size_t)k * nrect + q];
       float cr = 0.f, cg = 0.f, cb = 0.f, ca = 0.f;
       if (r) {
         const int ch = (int)((r >> 27) & 15u);
         float ar, ag, ab;
         if (P.mode >= 4) {
-          blend_colour<SK>(P, px, py, P.sBase + k, P.recT[(size_t)k * nrect + q], ar, ag, ab);
+          blend_colour<SK>(P, px, py, fr, s, P.recT[(size_t)k * nrect + q], ar, ag, ab);
         } else {
           const int i0 = (int)((r >> 13) & 0x3fffu);
           const int i1 = ((r >> 12) & 1u) ? i0 : i0 + 1;
@@ -868,7 +888,7 @@ __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, 
           float diffuse = 1.0f, specular = 0.0f, shadow = 1.0f;
           if (P.gradient && sqrtf(fmaf(ab, ab, fmaf(ag, ag, ar * ar))) > 0.001f) {
             float dx, dy, dz;
-            primary_ray(P, px, py, P.sBase + k, dx, dy, dz);
+            primary_ray(P, px, py, fr, s, dx, dy, dz);
             gradient_shading<SK>(P, ch, P.recT[(size_t)k * nrect + q], dx, dy, dz, diffuse, specular);
           }
           if (P.shadows) shadow = (1.f - P.ambient) * (1.f - (((r >> 9) & 1u) ? 1.0f : 0.0f));
@@ -883,7 +903,7 @@ __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, 
         cg = fmaf(P.ambient, mg, fmaf(ks, mg, kd * ag));
         cb = fmaf(P.ambient, mb, fmaf(ks, mb, kd * ab));
         ca = 1.0f;
-        if (STATS) { sv.z++; sv.w ^= (uint32_t)(ch + 1) << ((P.sBase + k) & 15); }
+        if (STATS) { sv.z++; sv.w ^= (uint32_t)(ch + 1) << (s & 15); }
         if (feat) {
           hits++;
           sT += P.recT[(size_t)k * nrect + q];
@@ -905,10 +925,22 @@ __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, 
       f.y += fmaf(P.bg.y * 1.0f, oma, cg);
       f.z += fmaf(P.bg.z * 1.0f, oma, cb);
       f.w += fmaf(oma, 1.0f, ca);
+      if (nF > 1 && s == P.spp - 1) {   // end of one of the launch's frames
+        const float fs = (float)P.spp;
+        const int fi = (P.sBase + k) / P.spp;
+        write_pixel<STATS>(P, px, py, f.x / fs, f.y / fs, f.z / fs, f.w / fs, sv, frame_accum(P, fi));
+        if (feat && fi == nF - 1) write_features(P, px, py, f.x / fs, f.y / fs, f.z / fs, hits, sT, cnt);
+        f = make_float4(0.f, 0.f, 0.f, 1.f);
+        sv = make_uint4(0u, 0u, 0u, 0u);
+        hits = 0;
+        cnt = make_uint4(0u, 0u, 0u, 0u);
+        sT = 0.f;
+      }
     }
-    if (last) {
+    if (nF > 1) {
+    } else if (last) {
       const float fs = (float)P.spp;
-      write_pixel<STATS>(P, px, py, f.x / fs, f.y / fs, f.z / fs, f.w / fs, sv);
+      write_pixel<STATS>(P, px, py, f.x / fs, f.y / fs, f.z / fs, f.w / fs, sv, P.accumParam);
       if (feat) write_features(P, px, py, f.x / fs, f.y / fs, f.z / fs, hits, sT, cnt);
     } else {
       reinterpret_cast<float4 *>(P.partial)[q] = f;

@@ -239,6 +239,10 @@ class Renderer:
         from .batch import autotune_macrocells
         return autotune_macrocells(self, edges, frames)
 
+    def RenderFrames(self, n: int, stream: Optional[int] = None):
+        """n successive frames (as n Render calls), traced in one launch where they fit."""
+        self._call("render_frames", C.c_int(n), C.c_void_p(stream) if stream else None)
+
     def setFrameId(self, frame_id: int):
         """The next frame renders with frame id `frame_id` (the reference's public frameID)."""
         self._call("set_frame_id", C.c_int(frame_id))

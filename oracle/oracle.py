@@ -81,6 +81,10 @@ class OracleRenderer(Renderer):
     def Render(self, stream=None):
         self.renderRows(*self._band)
 
+    def RenderFrames(self, n: int, stream=None):
+        for _ in range(n):
+            self.Render()
+
     _expected = None
 
     def renderExpected(self, jitter: int = 4, stepVoxels: float = 0.5, stream=None):

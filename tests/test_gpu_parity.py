@@ -294,3 +294,33 @@ def test_denoiser_features(oracle, mode):
         np.testing.assert_array_equal(fp.view(np.uint32), fo.view(np.uint32))
     st = p.pixelStats()
     np.testing.assert_allclose(fp[..., 4] * 6 + st[..., 2], 6, atol=1e-5)
+
+
+@pytest.mark.parametrize("mode,extra", [(0, "stats"), (2, "stats"), (1, ""), (3, "features"), (4, "shade"),
+                                        (5, "stats"), (2, "shade")])
+def test_render_frames_equals_successive_renders(oracle, mode, extra):
+    """mdwt_render_frames(n): n frames traced in one launch give exactly the frames, ids,
+    accumulation and counters of n Render calls -- from a fresh context (the reference's
+    post-increment ids: frames 0 and 1 share seeds), after a reset, and with
+    accumulation off."""
+    vols = [noise_u8(40, occ, 60 + i) for i, occ in enumerate([0.2, 0.3])]
+    tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(2)]
+    p, o = make_pair(oracle, vols, tfs, mode, (5, 5, 5), (41, 35), 2)
+    for r in (p, o):
+        if extra == "features":
+            r.setFeatures(True)
+        if extra == "shade":
+            _shade(r, True, True, (0.35, -0.8, 0.25), 2)
+    for n in (3, 1, 5):
+        p.RenderFrames(n)
+        o.RenderFrames(n)
+        assert_same_frame(p, o, f"{n} frames")
+        if extra == "features":
+            np.testing.assert_array_equal(p.features().view(np.uint32), o.features().view(np.uint32))
+    for r in (p, o):
+        r.ResetAccumulation()
+        r.setAccumulation(False)
+    p.RenderFrames(4)
+    o.RenderFrames(4)
+    assert_same_frame(p, o, "no accumulation")
+    np.testing.assert_array_equal(p.counters(), o.counters())
