@@ -91,7 +91,8 @@ def make_scene(name, res=None, spp=None):
 
 def workload_name(sc):
     w, h = sc.resolution
-    return f"{sc.name}_mc{sc.macrocells[0]}_{w}x{h}_{sc.spp}spp"
+    frames = f"x{sc.frames}frames" if sc.frames > 1 else ""
+    return f"{sc.name}_mc{sc.macrocells[0]}_{w}x{h}_{sc.spp}spp{frames}"
 
 
 def scene_config(sc, l2note, parallelism):
@@ -441,9 +442,17 @@ def main():
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream
     flush = torch.empty(args.flush_mib << 20, dtype=torch.uint8, device=dev)
+    # one step = the workload's frames (several successive frames in one launch through
+    # mdwt_render_frames when the configuration renders more than one)
+    def step():
+        if sc.frames > 1:
+            r.RenderFrames(sc.frames, sptr)
+        else:
+            r.Render(sptr)
+
     # distinct frame seeds per rank: rank r starts r*(warmup+steps) frames later
     for _ in range(rank * (args.warmup + args.steps)):
-        r.Render(sptr)
+        step()
     torch.cuda.synchronize(dev)
 
     def barrier():
@@ -453,7 +462,7 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             flush.fill_(1)
-            r.Render(sptr)
+            step()
     torch.cuda.synchronize(dev)
     r.resetCounters()
     timed = True
@@ -472,9 +481,9 @@ def main():
         for k in range(args.steps):
             flush.fill_(k & 0xff)
             ev[k][0].record(stream)
-            r.Render(sptr)
+            step()
             ev[k][1].record(stream)
-            if timed:
+            if timed and sc.frames == 1:
                 trace_ms.append(r.kernelTimes()[0])  # trace kernel, CUDA events on the render stream
     torch.cuda.synchronize(dev)
     barrier()
@@ -487,7 +496,7 @@ def main():
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    paths = w * h * sc.spp
+    paths = w * h * sc.spp * sc.frames
     value = world * paths / (ms / 1e3) / 1e9
 
     # algorithmic bytes of the dominant kernel (trace_kernel) per launch: 8*bpv per
@@ -511,7 +520,7 @@ def main():
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         r.setCamera(*cam)
-        r.Render(sptr)
+        step()
         r._call("get_framebuffer", C.cast(C.c_void_p(pinned.data_ptr()), C.POINTER(C.c_uint32)))
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     barrier()
