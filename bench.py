@@ -212,6 +212,8 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     sc = make_scene(name)
     r = sc.setup(Renderer(device_index))
     w, h = sc.resolution
+    r.setSpp(1)
+    tuned = r.autotuneSchedule(frames=2)   # the tracker schedule for this scene (plain and denoised)
     t0 = time.perf_counter()
     coarse = r.expectedImage(4, 0.5)
     ref = r.expectedImage(8, 0.25)          # stays on the device for accumRmse
@@ -252,6 +254,7 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     return {
         "target": target, "metric": "RMSE of linear RGB (accumulation buffer) vs the FP64 expected image",
         "workload": workload_name(sc).replace(f"_{sc.spp}spp", ""), "resolution": [w, h], "mode": sc.mode,
+        "schedule": {"pool": tuned[0], "trips": tuned[1], "by": "mdwt_autotune_schedule"},
         "reference": {"kind": "FP64 expected image of the estimator (mdwt_render_expected)",
                       "jitter_points": 8, "step_voxels": 0.25, "seconds": t_ref,
                       "rmse_vs_4_jitter_0.5_voxel": quad},
@@ -439,6 +442,9 @@ def main():
     sc = make_scene(args.config, args.res, args.spp)
     r = sc.setup(Renderer(local))
     w, h = sc.resolution
+    schedule = None
+    if args.config.startswith("c3"):   # traversal-heavy scenes: tune the tracker schedule first
+        schedule = r.autotuneSchedule(frames=1)
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream
     flush = torch.empty(args.flush_mib << 20, dtype=torch.uint8, device=dev)
@@ -567,7 +573,9 @@ def main():
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded generators in mdwtracker_b200/synthetic.py)",
-        "config": scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
+        "config": dict(scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
+                       schedule={"pool": schedule[0], "trips": schedule[1], "by": "mdwt_autotune_schedule"}
+                       if schedule else {"pool": 8, "trips": 2, "by": "default"}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profiled_traffic(workload_name(sc)),
                      "peak_source": peak_kind, "kernel": "trace_kernel",

@@ -55,6 +55,13 @@ mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]);
  * best[3] (optional) = unit items, pool, trips. */
 mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]);
 
+/* Schedule autotuner for one context: coordinate descent over the phase-1 trips
+ * {1, 2, 3, 4, 6, 8} and the regeneration pool {4, 8, 16, 32}, each candidate timed over
+ * `frames` frames after a warm-up frame; keeps the fastest (results do not depend on
+ * them).  Frame ids are restored and the accumulation reset.  best[2] (optional) =
+ * pool, trips. */
+mdwt_status mdwt_autotune_schedule(mdwt_ctx *ctx, int frames, int best[2]);
+
 /* Macrocell autotuner for one context: for each candidate edge length (voxels per
  * macrocell side; cells per side = ceil(dims / edge)) rebuild the value ranges and
  * majorants (transfer functions kept), time `frames` frames, keep the fastest.  Frame ids

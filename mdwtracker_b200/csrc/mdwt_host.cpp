@@ -1592,6 +1592,52 @@ mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]) {
   return MDWT_OK;
 }
 
+mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
+  if (!c || frames <= 0) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  const int f0 = c->frameID, a0 = c->accumID, fp0 = c->frameParam, ap0 = c->accumParam;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0), "event");
+  CK(cudaEventCreate(&e1), "event");
+  mdwt_status s = MDWT_OK;
+  double bestMs = 1e300;
+  auto trial = [&](double *ms) -> mdwt_status {
+    mdwt_status st = mdwt_render(c, nullptr);   // warm-up
+    if (st) return st;
+    cudaEventRecord(e0, c->stream);
+    for (int f = 0; f < frames && !st; f++) st = mdwt_render(c, nullptr);
+    cudaEventRecord(e1, c->stream);
+    cudaEventSynchronize(e1);
+    float m = 0.f;
+    cudaEventElapsedTime(&m, e0, e1);
+    *ms = m / frames;
+    return st;
+  };
+  auto tune = [&](int *knob, const int *cand, int nc) -> mdwt_status {
+    int bestV = *knob;
+    for (int i = 0; i < nc; i++) {
+      *knob = cand[i];
+      double ms = 0.0;
+      mdwt_status st = trial(&ms);
+      if (st) return st;
+      if (ms < bestMs) { bestMs = ms; bestV = cand[i]; }
+    }
+    *knob = bestV;
+    return MDWT_OK;
+  };
+  const int tripsC[] = {1, 2, 3, 4, 6, 8};
+  const int poolsC[] = {4, 8, 16, 32};
+  if (!(s = tune(&c->trips, tripsC, 6))) s = tune(&c->pool, poolsC, 4);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->frameID = f0; c->accumID = a0; c->frameParam = fp0; c->accumParam = ap0;
+  reset_accum_ids(c);
+  if (s) return s;
+  if (best) { best[0] = c->pool; best[1] = c->trips; }
+  return MDWT_OK;
+}
+
 mdwt_status mdwt_autotune_macrocells(mdwt_ctx *c, const int *edges, int n, int frames, int *bestEdge) {
   if (!c || !edges || n <= 0 || frames <= 0) return MDWT_ERR_BAD_ARG;
   if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");

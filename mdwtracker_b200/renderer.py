@@ -233,6 +233,13 @@ class Renderer:
     def ResetAccumulation(self):
         self._call("reset_accumulation")
 
+    def autotuneSchedule(self, frames: int = 2):
+        """Time frames for each (trips, pool) candidate, keep the fastest; frame ids are
+        restored and the accumulation reset.  Returns (pool, trips)."""
+        best = (C.c_int * 2)()
+        self._call("autotune_schedule", C.c_int(frames), best)
+        return tuple(best)
+
     def autotuneMacrocells(self, edges=(4, 8, 16, 32), frames: int = 2) -> int:
         """Time frames for each macrocell edge length (voxels per side), keep the fastest
         grid; frame ids are restored and the accumulation reset."""

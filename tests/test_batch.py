@@ -135,3 +135,17 @@ def test_macrocell_autotuner_picks_a_candidate(oracle):
     assert r.frameIds()[0] == ids[0]
     n = -(-40 // best)
     assert r.macrocellDims == (n, n, n)
+
+
+def test_schedule_autotuner_keeps_results(oracle):
+    spec = _requests()[2]
+    r, twin = _setup(spec), _setup(spec)
+    r.Render()
+    twin.Render()
+    pool, trips = r.autotuneSchedule(frames=1)
+    assert pool in (4, 8, 16, 32) and trips in (1, 2, 3, 4, 6, 8)
+    twin.ResetAccumulation()
+    for _ in range(2):
+        r.Render()
+        twin.Render()
+    _same(r, twin, spec["stats"])
