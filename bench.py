@@ -315,8 +315,8 @@ def batch_throughput(device_index, n_requests, frames=3, small=False):
     return {"workload": f"c4_{n_requests}req_{'256x256_1-4spp' if small else 'mixed'}", "requests": n_requests,
             "path_samples_per_frame": paths,
             "batched": {"ms_per_frame": ms_bat, "Gpath_samples_per_s": paths / ms_bat / 1e6,
-                        "kernel_variant_groups": info["groups"], "work_units": info["units"],
-                        "graph_replays": info["graph_replays"], "autotuned": {"unit_items": best[0], "pool": best[1],
+                        "kernel_variant_groups": info["groups"],
+                        "graph_replays": info["graph_replays"], "autotuned": {"chunk_items": best[0] or "per request", "pool": best[1],
                                                                               "trips": best[2], "seconds": tune_s}},
             "one_by_one": {"ms_per_frame": ms_seq, "Gpath_samples_per_s": paths / ms_seq / 1e6},
             "speedup": ms_seq / ms_bat, "setup_s": setup_s}

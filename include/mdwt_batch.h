@@ -10,12 +10,12 @@
  * ids advance per request as in mdwt_render).  Each request's frame must fit one sample
  * batch of path records (MDWT_ERR_UNSUPPORTED otherwise) and render all rows.
  *
- * Launch structure: warps take work units (a request's run of `unit_items` consecutive
- * (8x4-tile, sample) work items) from a counter and run the tracker loop with that
- * request's parameters.  With graphs on, the launch sequence (parameter uploads from
- * pinned memory, counter resets, kernels) is captured once into a CUDA graph and replayed
- * while the batch's structure (variants, request and unit counts, pixel totals) stays the
- * same.
+ * Launch structure: every request has a work dispenser of (8x4-tile, sample) items; a
+ * warp starts at one request, takes chunks of its items until they run out, then moves
+ * to the next request with items left (draining its lanes only at a change of request).
+ * With graphs on, the launch sequence (parameter uploads from pinned memory, dispenser
+ * resets, kernels) is captured once into a CUDA graph and replayed while the batch's
+ * structure (variants, request counts, pixel totals) stays the same.
  */
 #ifndef MDWT_BATCH_H
 #define MDWT_BATCH_H
@@ -39,20 +39,22 @@ mdwt_status mdwt_batch_clear(mdwt_batch *b);
 /* One frame of every request, asynchronous on `stream` (NULL: the batch's own stream). */
 mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream);
 mdwt_status mdwt_batch_sync(mdwt_batch *b);
-/* Schedule knobs (0 keeps the current value): work-unit size in items (a multiple of 32),
- * regeneration pool and phase-1 trips for every request of the batch. */
+/* Schedule knobs (0 keeps the current value): dispenser chunk in items (a multiple of 32;
+ * by default sized per request like a single-request launch), regeneration pool and
+ * phase-1 trips for every request of the batch. */
 mdwt_status mdwt_batch_set_schedule(mdwt_batch *b, int unit_items, int pool, int trips);
 mdwt_status mdwt_batch_set_graph(mdwt_batch *b, int enable);
 /* Device time (ms) of the last mdwt_batch_render, from events on its stream; synchronous. */
 mdwt_status mdwt_batch_last_ms(mdwt_batch *b, float *ms);
-/* out[0] kernels launched so far, [1] kernel-variant groups of the last frame, [2] work
- * units, [3] graph replays, [4] graph captures, [5] unit items, [6] pool, [7] trips. */
+/* out[0] kernels launched so far, [1] kernel-variant groups of the last frame, [2]
+ * requests, [3] graph replays, [4] graph captures, [5] chunk items (0 = per request),
+ * [6] pool, [7] trips. */
 mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]);
-/* Autotuner: coordinate descent over the work-unit size {512..8192}, the regeneration
- * pool {4, 8, 16, 32} and trips {1, 2, 3, 4}, each candidate timed over `frames` batch
- * frames after one warm-up frame; keeps the fastest.  Results do not depend on these
- * knobs; the requests' frame ids are restored and their accumulation reset afterwards.
- * best[3] (optional) = unit items, pool, trips. */
+/* Autotuner: coordinate descent over the phase-1 trips {1, 2, 3, 4, 6, 8}, the
+ * regeneration pool {4, 8, 16, 32} and the dispenser chunk {per request, 32..256}, each
+ * candidate timed over `frames` batch frames after one warm-up frame; keeps the fastest.
+ * Results do not depend on these knobs; the requests' frame ids are restored and their
+ * accumulation reset afterwards.  best[3] (optional) = chunk items, pool, trips. */
 mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]);
 
 /* Schedule autotuner for one context: coordinate descent over the phase-1 trips

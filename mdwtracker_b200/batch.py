@@ -64,7 +64,7 @@ class Batch:
     def info(self) -> dict:
         out = (C.c_int64 * 8)()
         self._call("info", out)
-        keys = ["launches", "groups", "units", "graph_replays", "graph_captures", "unit_items", "pool", "trips"]
+        keys = ["launches", "groups", "requests", "graph_replays", "graph_captures", "chunk_items", "pool", "trips"]
         return dict(zip(keys, [int(x) for x in out]))
 
     def autotune(self, frames: int = 2):

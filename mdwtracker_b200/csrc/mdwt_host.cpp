@@ -1253,14 +1253,13 @@ struct mdwt_batch {
   int device = 0, numSMs = 0;
   cudaStream_t stream = nullptr;
   std::vector<mdwt_ctx *> reqs;
-  int unitItems = 2048, pool = 0, trips = 0;
+  int unitItems = 0, pool = 0, trips = 0;   // unitItems: dispenser chunk (0 = sized per request)
   bool useGraph = true;
   // pinned host staging and device copies: params, units, pixel offsets, unit counters
   TrackParams *hParams = nullptr, *dParams = nullptr;
-  BatchUnit *hUnits = nullptr, *dUnits = nullptr;
   unsigned long long *hPix = nullptr, *dPix = nullptr;
-  unsigned *dCounters = nullptr;
-  size_t capParams = 0, capUnits = 0, capPix = 0, capCounters = 0;
+  unsigned *dDisp = nullptr;                 // one work dispenser per request
+  size_t capParams = 0, capPix = 0, capDisp = 0;
   cudaGraphExec_t graph = nullptr;
   std::vector<long long> graphSig;
   cudaStream_t graphStream = nullptr;
@@ -1300,9 +1299,8 @@ struct GroupPlan {
   int mode, store;
   bool stats, ext, shade;
   int first, count;           // request slots [first, first + count) of the params array
-  int unitFirst, unitCount;
   int pixFirst;               // offset of the group's nReq + 1 pixel offsets
-  unsigned long long totalPix;
+  unsigned long long totalItems, totalPix;
 };
 
 long long variant_key(const TrackParams &p, int store, bool stats) {
@@ -1340,11 +1338,9 @@ mdwt_status mdwt_batch_destroy(mdwt_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->hParams) cudaFreeHost(b->hParams);
   if (b->dParams) cudaFree(b->dParams);
-  if (b->hUnits) cudaFreeHost(b->hUnits);
-  if (b->dUnits) cudaFree(b->dUnits);
   if (b->hPix) cudaFreeHost(b->hPix);
   if (b->dPix) cudaFree(b->dPix);
-  if (b->dCounters) cudaFree(b->dCounters);
+  if (b->dDisp) cudaFree(b->dDisp);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1371,7 +1367,7 @@ mdwt_status mdwt_batch_clear(mdwt_batch *b) {
 mdwt_status mdwt_batch_set_schedule(mdwt_batch *b, int unitItems, int pool, int trips) {
   if (!b || unitItems < 0 || (unitItems % 32) || pool < 0 || pool > 32 || trips < 0 || trips > 64)
     return MDWT_ERR_BAD_ARG;
-  if (unitItems) b->unitItems = unitItems;
+  if (unitItems) b->unitItems = unitItems;   // dispenser chunk for every request
   if (pool) b->pool = pool;
   if (trips) b->trips = trips;
   return MDWT_OK;
@@ -1407,11 +1403,9 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
   std::vector<int> order(n);
   for (int i = 0; i < n; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return keys[a] < keys[c]; });
-  // groups, units, pixel offsets
+  // groups, dispenser chunks, pixel offsets
   std::vector<GroupPlan> groups;
-  std::vector<BatchUnit> units;
   std::vector<unsigned long long> pix;
-  const unsigned U = (unsigned)b->unitItems;
   for (int k = 0; k < n;) {
     int e = k;
     while (e < n && keys[order[e]] == keys[order[k]]) e++;
@@ -1420,59 +1414,59 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
     g.mode = p0.mode; g.store = b->reqs[order[k]]->store; g.stats = b->reqs[order[k]]->statsOn;
     g.ext = p0.shadows || p0.recT; g.shade = p0.shadows || p0.gradient;
     g.first = k; g.count = e - k;
-    g.unitFirst = (int)units.size();
     g.pixFirst = (int)pix.size();
-    unsigned long long acc = 0;
+    // the group's persistent grid: chunks sized like the single-request launch
+    const size_t warps = (size_t)b->numSMs * batch_trace_occupancy(g.mode, g.store, g.stats, g.ext) * 4;
+    unsigned long long acc = 0, items = 0;
     for (int j = k; j < e; j++) {
-      const TrackParams &p = ps[order[j]];
+      TrackParams &p = ps[order[j]];
       pix.push_back(acc);
       acc += (unsigned long long)p.W * p.H;
-      const unsigned items = (unsigned)p.numTiles * 32u * (unsigned)p.spp;
-      for (unsigned a = 0; a < items; a += U) units.push_back(BatchUnit{j - k, a, std::min(items, a + U)});
+      const size_t it = (size_t)p.numTiles * 32u * (size_t)p.spp;
+      items += it;
+      size_t chunk = b->unitItems > 0 ? (size_t)b->unitItems : it / (warps * 8);
+      chunk = chunk < 32 ? 32 : (chunk > 256 && b->unitItems <= 0 ? 256 : chunk & ~(size_t)31);
+      p.chunk = (int)chunk;
     }
     pix.push_back(acc);
     g.totalPix = acc;
-    g.unitCount = (int)units.size() - g.unitFirst;
+    g.totalItems = items;
     groups.push_back(g);
     k = e;
   }
   mdwt_status s;
   if ((s = grow_pair(b, &b->hParams, &b->dParams, b->capParams, (size_t)n))) return s;
-  if ((s = grow_pair(b, &b->hUnits, &b->dUnits, b->capUnits, units.size()))) return s;
   if ((s = grow_pair(b, &b->hPix, &b->dPix, b->capPix, pix.size()))) return s;
-  if (b->capCounters < groups.size()) {
-    if (b->dCounters) cudaFree(b->dCounters);
-    b->dCounters = nullptr;
-    BCK(cudaMalloc((void **)&b->dCounters, std::max<size_t>(16, groups.size()) * sizeof(unsigned)), "counters");
-    b->capCounters = std::max<size_t>(16, groups.size());
+  if (b->capDisp < (size_t)n) {
+    if (b->dDisp) cudaFree(b->dDisp);
+    b->dDisp = nullptr;
+    BCK(cudaMalloc((void **)&b->dDisp, std::max<size_t>(64, n) * sizeof(unsigned)), "dispensers");
+    b->capDisp = std::max<size_t>(64, n);
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; b->graphSig.clear(); }
   }
   for (int j = 0; j < n; j++) b->hParams[j] = ps[order[j]];
-  std::copy(units.begin(), units.end(), b->hUnits);
   std::copy(pix.begin(), pix.end(), b->hPix);
   // structure signature: what a captured graph bakes in
-  std::vector<long long> sig = {n, (long long)units.size(), (long long)pix.size(), (long long)b->numSMs};
+  std::vector<long long> sig = {n, (long long)pix.size(), (long long)b->numSMs};
   for (auto &g : groups) {
     sig.push_back(keys[order[g.first]]);
     sig.push_back(g.count);
-    sig.push_back(g.unitCount);
+    sig.push_back((long long)(g.totalItems > 0));
     sig.push_back((long long)g.totalPix);
   }
   cudaStream_t user = stream ? (cudaStream_t)stream : b->stream;
   auto enqueue = [&](cudaStream_t st) -> mdwt_status {
     BCK(cudaMemcpyAsync(b->dParams, b->hParams, (size_t)n * sizeof(TrackParams), cudaMemcpyHostToDevice, st), "params");
-    BCK(cudaMemcpyAsync(b->dUnits, b->hUnits, units.size() * sizeof(BatchUnit), cudaMemcpyHostToDevice, st), "units");
     BCK(cudaMemcpyAsync(b->dPix, b->hPix, pix.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, st), "pix");
-    BCK(cudaMemsetAsync(b->dCounters, 0, groups.size() * sizeof(unsigned), st), "counters");
+    BCK(cudaMemsetAsync(b->dDisp, 0, (size_t)n * sizeof(unsigned), st), "dispensers");
     for (size_t gi = 0; gi < groups.size(); gi++) {
       const GroupPlan &g = groups[gi];
       BatchGroup bg;
       bg.mode = g.mode; bg.storeKind = g.store; bg.stats = g.stats; bg.ext = g.ext; bg.shade = g.shade;
       bg.reqs = b->dParams + g.first;
       bg.nReq = g.count;
-      bg.units = b->dUnits + g.unitFirst;
-      bg.numUnits = g.unitCount;
-      bg.unitCounter = b->dCounters + gi;
+      bg.dispensers = b->dDisp + g.first;
+      bg.totalItems = g.totalItems;
       bg.pixOfs = b->dPix + g.pixFirst;
       bg.totalPix = g.totalPix;
       int launches = 0, grid = 0;
@@ -1518,7 +1512,7 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
     c->frameParam = c->frameID++;
   }
   b->lastGroups = (int)groups.size();
-  b->lastUnits = (int)units.size();
+  b->lastUnits = n;
   return MDWT_OK;
 }
 
@@ -1564,9 +1558,9 @@ mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]) {
   };
   if (!b->pool) b->pool = b->reqs[0]->pool;
   if (!b->trips) b->trips = b->reqs[0]->trips;
-  const int unitsC[] = {512, 1024, 2048, 4096, 8192};
+  const int unitsC[] = {0, 32, 64, 128, 256};   // dispenser chunk (0 = sized per request)
   const int poolsC[] = {4, 8, 16, 32};
-  const int tripsC[] = {1, 2, 3, 4};
+  const int tripsC[] = {1, 2, 3, 4, 6, 8};
   mdwt_status s = MDWT_OK;
   double bestMs = 1e300;
   auto tune = [&](int *knob, const int *cand, int nc) -> mdwt_status {
@@ -1581,7 +1575,7 @@ mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]) {
     *knob = bestV;
     return MDWT_OK;
   };
-  if (!(s = tune(&b->unitItems, unitsC, 5)) && !(s = tune(&b->pool, poolsC, 4))) s = tune(&b->trips, tripsC, 4);
+  if (!(s = tune(&b->trips, tripsC, 6)) && !(s = tune(&b->pool, poolsC, 4))) s = tune(&b->unitItems, unitsC, 5);
   for (size_t i = 0; i < b->reqs.size(); i++) {
     mdwt_ctx *c = b->reqs[i];
     c->frameID = saved[i].f; c->accumID = saved[i].a; c->frameParam = saved[i].fp; c->accumParam = saved[i].ap;

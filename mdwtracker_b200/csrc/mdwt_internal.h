@@ -92,24 +92,19 @@ struct TrackParams {
   uint32_t *partialStats;        // uint4 per rect pixel between batches (stats only)
 };
 
-// A work unit of the batched tracker: items [begin, end) of request `req`.
-struct BatchUnit {
-  int req;
-  unsigned begin, end;
-};
-
 // A group of batched requests sharing one kernel variant (device arrays).
 struct BatchGroup {
   int mode, storeKind;
   bool stats, ext, shade;                // per-pixel stats; extended trace; shaded resolve
-  const TrackParams *reqs;               // the group's requests
+  const TrackParams *reqs;               // the group's requests (chunk = dispenser chunk)
   int nReq;
-  const BatchUnit *units;                // req indexes into `reqs`
-  int numUnits;
-  unsigned *unitCounter;                 // zeroed before the launch
+  unsigned *dispensers;                  // one work counter per request, zeroed before the launch
+  unsigned long long totalItems;         // work items of the group
   const unsigned long long *pixOfs;      // nReq + 1 prefix offsets of W*H
   unsigned long long totalPix;
 };
+// Blocks per SM of the batched trace kernel of a variant (for chunk sizing).
+int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext);
 int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launches, int *grid);
 
 constexpr int kMaxTexels = 16384;          // TF texels addressable by a path record

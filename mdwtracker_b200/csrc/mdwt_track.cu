@@ -631,27 +631,30 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
   flush_counters(P.counters, tot);
 }
 
-// Batched variant: many requests (render contexts) in one persistent launch.  Each warp
-// takes work units (request, item range) from a global counter and runs the same
-// tracking loop with that request's parameters (global memory) and channel table
-// (staged per warp in shared memory); the counters go to the unit's request.
+// Batched variant: many requests (render contexts) in one persistent launch.  Every
+// request has its own work dispenser; a warp starts at request (global warp id mod nReq),
+// takes chunks of that request's items until they run out, then moves on to the next
+// request with items left, so it drains its lanes only when it changes request.  The
+// request's channel table is staged per warp in shared memory; the counters go to the
+// request.
 template <int MODE, int SK, bool STATS, bool SH>
 __global__ void __launch_bounds__(kTPB, kMinBlocks)
-    trace_batch_kernel(const TrackParams *__restrict__ reqs, const BatchUnit *__restrict__ units, int numUnits,
-                       unsigned *unitCounter) {
+    trace_batch_kernel(const TrackParams *__restrict__ reqs, int nReq, unsigned *dispensers) {
   __shared__ ChanSm sch[kTPB / 32][kMaxChannels];
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  while (true) {
-    unsigned u = 0;
-    if (lane == 0) u = atomicAdd(unitCounter, 1u);
-    u = __shfl_sync(kFull, u, 0);
-    if (u >= (unsigned)numUnits) break;
-    const BatchUnit U = units[u];
-    const TrackParams &P = reqs[U.req];
+  const unsigned gw = blockIdx.x * (kTPB / 32) + warp;
+  for (int i = 0; i < nReq; i++) {
+    const int r = (int)((gw + (unsigned)i) % (unsigned)nReq);
+    const TrackParams &P = reqs[r];
+    const unsigned total = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
+    unsigned peek = 0;
+    if (lane == 0) peek = *(volatile unsigned *)(dispensers + r);
+    peek = __shfl_sync(kFull, peek, 0);
+    if (peek >= total) continue;   // nothing left of this request
     if (lane < (unsigned)P.C) sch[warp][lane] = chan_params(P, (int)lane);
     __syncwarp();
     uint32_t tot[5] = {0, 0, 0, 0, 0};
-    trace_items<MODE, SK, STATS, SH>(P, sch[warp], U.begin, U.end, nullptr, 0u, tot);
+    trace_items<MODE, SK, STATS, SH>(P, sch[warp], total, total, dispensers + r, (unsigned)P.chunk, tot);
     flush_counters(P.counters, tot);
     __syncwarp();
   }
@@ -1021,8 +1024,7 @@ int launch_tb(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
   if (e != cudaSuccess) return (int)e;
   if (bps < 1) bps = 1;
   *grid = numSMs * bps;
-  if (g.numUnits > 0)
-    trace_batch_kernel<MODE, SK, STATS, SH><<<*grid, kTPB, 0, st>>>(g.reqs, g.units, g.numUnits, g.unitCounter);
+  if (g.totalItems > 0) trace_batch_kernel<MODE, SK, STATS, SH><<<*grid, kTPB, 0, st>>>(g.reqs, g.nReq, g.dispensers);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   size_t rg = (size_t)((g.totalPix + 255) / 256);
@@ -1039,7 +1041,29 @@ int launch_tbs(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
   return g.stats ? launch_tb<MODE, SK, true, false>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, false>(g, st, numSMs, grid);
 }
 
+template <int MODE, int SK>
+int occ_tbs(bool stats, bool ext) {
+  int bps = 0;
+  cudaError_t e;
+  if (ext) e = stats ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_kernel<MODE, SK, true, true>, kTPB, 0)
+                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_kernel<MODE, SK, false, true>, kTPB, 0);
+  else e = stats ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_kernel<MODE, SK, true, false>, kTPB, 0)
+                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_kernel<MODE, SK, false, false>, kTPB, 0);
+  return (e == cudaSuccess && bps > 0) ? bps : 1;
+}
+
 }  // namespace
+
+int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext) {
+  const bool u8 = storeKind == kStoreU8;
+  switch (mode) {
+    case 0: return u8 ? occ_tbs<0, kStoreU8>(stats, ext) : occ_tbs<0, kStoreF32>(stats, ext);
+    case 1: return u8 ? occ_tbs<1, kStoreU8>(stats, ext) : occ_tbs<1, kStoreF32>(stats, ext);
+    case 2: return u8 ? occ_tbs<2, kStoreU8>(stats, ext) : occ_tbs<2, kStoreF32>(stats, ext);
+    case 3: return u8 ? occ_tbs<3, kStoreU8>(stats, ext) : occ_tbs<3, kStoreF32>(stats, ext);
+    default: return u8 ? occ_tbs<4, kStoreU8>(stats, ext) : occ_tbs<4, kStoreF32>(stats, ext);
+  }
+}
 
 // One group of a batch: every request with the same kernel variant, in one persistent
 // trace launch and one resolve launch.
@@ -1056,7 +1080,7 @@ int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launc
     case 5: rc = u8 ? launch_tbs<4, kStoreU8>(g, st, numSMs, grid) : launch_tbs<4, kStoreF32>(g, st, numSMs, grid); break;
     default: return (int)cudaErrorInvalidValue;
   }
-  if (launches) *launches += (g.numUnits > 0 ? 1 : 0) + (g.totalPix > 0 ? 1 : 0);
+  if (launches) *launches += (g.totalItems > 0 ? 1 : 0) + (g.totalPix > 0 ? 1 : 0);
   return rc;
 }
 
