@@ -204,9 +204,10 @@ def cpu_baseline(sc, budget_s, full=False):
 def time_to_rmse(name, target, device_index, max_frames=20000):
     """Plain accumulation until the accumulation buffer's RGB is within `target` RMSE of
     the FP64 expected image: one sample per frame (frame f draws with seed factor f+1, so
-    no two samples of the run share a seed), the RMSE checked on the device after every
-    frame (first 16) and every 8th frame after that.  Time = device time of the frames
-    (CUDA events on the render stream) up to the first frame that meets the target."""
+    no two samples of the run share a seed); the first 16 frames one by one, then blocks
+    of 8 frames per launch (mdwt_render_frames), the RMSE checked on the device after
+    each.  Time = device time of the frames (CUDA events on the render stream) up to the
+    first check that meets the target."""
     import torch
     from mdwtracker_b200 import Renderer
     sc = make_scene(name)
@@ -227,19 +228,21 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     torch.cuda.synchronize()
     tw = time.perf_counter()
     while frames < max_frames:
+        # the first 16 frames one by one, then blocks of 8 frames in one launch
+        # (mdwt_render_frames: the same frames as 8 Render calls), checked after each
+        n = 1 if frames < 16 else 8
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        r.Render(stream.cuda_stream)
+        r.RenderFrames(n, stream.cuda_stream)
         b.record(stream)
         evs.append((a, b))
-        frames += 1
-        if frames <= 16 or frames % 8 == 0:
-            torch.cuda.synchronize()
-            rmse = r.accumRmse()
-            if frames in (1, 4, 16, 64) or frames % 256 == 0:
-                trace.append([frames, rmse])
-            if rmse <= target:
-                break
+        frames += n
+        torch.cuda.synchronize()
+        rmse = r.accumRmse()
+        if frames in (1, 4, 16, 64) or frames % 256 == 0:
+            trace.append([frames, rmse])
+        if rmse <= target:
+            break
     torch.cuda.synchronize()
     wall = time.perf_counter() - tw
     dev_ms = sum(a.elapsed_time(b) for a, b in evs)
