@@ -578,7 +578,7 @@ def main():
         "data": "synthetic (seeded generators in mdwtracker_b200/synthetic.py)",
         "config": dict(scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
                        schedule={"pool": schedule[0], "trips": schedule[1], "by": "mdwt_autotune_schedule"}
-                       if schedule else {"pool": 8, "trips": 2, "by": "default"}),
+                       if schedule else {"pool": 8, "trips": 4, "quorum": 16, "by": "default"}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profiled_traffic(workload_name(sc)),
                      "peak_source": peak_kind, "kernel": "trace_kernel",

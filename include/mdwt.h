@@ -208,8 +208,10 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * MDWT_TUNE_BATCH: at most `value` samples per pixel per trace pass (0 = as many as the
  * 1 GiB path-record budget allows); the per-pixel sums still run in sample order.
  * MDWT_TUNE_TRIPS: transition/free-flight trips (1..64) a warp takes per round before
- * it evaluates its pending density samples together. */
-enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2 };
+ * it evaluates its pending density samples together.
+ * MDWT_TUNE_QUORUM: a round's trips also end once `value` (1..33; 33 = never) of the
+ * warp's lanes hold a pending density sample. */
+enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2, MDWT_TUNE_QUORUM = 3 };
 mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
 
 /* No reference counterpart: CUDA events on the render stream around the trace kernel

@@ -58,7 +58,8 @@ mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]);
 mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]);
 
 /* Schedule autotuner for one context: coordinate descent over the phase-1 trips
- * {1, 2, 3, 4, 6, 8} and the regeneration pool {4, 8, 16, 32}, each candidate timed over
+ * {1, 2, 3, 4, 6, 8}, the regeneration pool {4, 8, 16, 32} and the sample quorum
+ * {8, 16, 24, never} (MDWT_TUNE_*), each candidate timed over
  * `frames` frames after a warm-up frame; keeps the fastest (results do not depend on
  * them).  Frame ids are restored and the accumulation reset.  best[2] (optional) =
  * pool, trips. */

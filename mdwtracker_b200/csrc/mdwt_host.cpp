@@ -163,7 +163,8 @@ struct mdwt_ctx {
   int lastGrid = 0, lastBlock = 0;
   int pool = 8;       // regeneration pool of the tracker (MDWT_TUNE_POOL)
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
-  int trips = 2;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
+  int trips = 4;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
+  int quorum = 16;    // end a round's trips early once this many lanes wait to sample (33: never)
   int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
   bool timing = false;        // CUDA events around the trace and resolve kernels
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -1024,6 +1025,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   p.gOrg = {p.gScale.x * (c->cOrg.x - p.gLo.x), p.gScale.y * (c->cOrg.y - p.gLo.y), p.gScale.z * (c->cOrg.z - p.gLo.z)};
   p.pool = c->pool;
   p.trips = c->trips;
+  p.quorum = c->quorum;
   p.vol32 = 1;
   for (auto &h : c->ch)
     if ((uint64_t)h.dims[0] * h.dims[1] * h.dims[2] >= (1ull << 32)) p.vol32 = 0;
@@ -1622,7 +1624,8 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
   };
   const int tripsC[] = {1, 2, 3, 4, 6, 8};
   const int poolsC[] = {4, 8, 16, 32};
-  if (!(s = tune(&c->trips, tripsC, 6))) s = tune(&c->pool, poolsC, 4);
+  const int quorumC[] = {8, 16, 24, 33};
+  if (!(s = tune(&c->trips, tripsC, 6)) && !(s = tune(&c->pool, poolsC, 4))) s = tune(&c->quorum, quorumC, 4);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->frameID = f0; c->accumID = a0; c->frameParam = fp0; c->accumParam = ap0;
@@ -1861,6 +1864,11 @@ mdwt_status mdwt_set_tuning(mdwt_ctx *c, int key, int value) {
   if (key == MDWT_TUNE_TRIPS) {
     if (value < 1 || value > 64) return fail(c, MDWT_ERR_BAD_ARG, "trips must be in 1..64");
     c->trips = value;
+    return MDWT_OK;
+  }
+  if (key == MDWT_TUNE_QUORUM) {
+    if (value < 1 || value > 33) return fail(c, MDWT_ERR_BAD_ARG, "quorum must be in 1..33");
+    c->quorum = value;
     return MDWT_OK;
   }
   if (key == MDWT_TUNE_BATCH) {

@@ -393,6 +393,8 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
     // a few trips per round, the lanes that are ready wait
     for (int trip = 0; trip < P.trips; trip++) {
       if (!__any_sync(kFull, st == S_TRANS || st == S_STEP)) break;
+      // enough lanes hold a pending density sample: sample them together now
+      if (trip > 0 && __popc(__ballot_sync(kFull, st == S_SAMPLE)) >= P.quorum) break;
       // transitions: walk channels / cells to the next non-zero majorant
       if (st == S_TRANS) {
         bool stepping = false;
