@@ -2,7 +2,8 @@
 
   python -m mdwtracker_b200.train_denoiser [--pairs 2000] [--steps 3000] [--out weights.npy]
 
-Data: the 6 x 512^3 float32 log-normal scene (syncDDA), random cameras around the volume
+Data: the 6 x 512^3 float32 log-normal scene and the 3 x 256^3 uint8 sparse-noise scene
+(syncDDA; half the pairs each by default), random cameras around the volume
 looking at random points inside it with the pixel footprint of the 1920x1080 view (so the
 crops have the noise and detail scale of the full frame), random per-channel transfer
 functions (hue, opacity maximum, ramp start).  Per pair: a low-spp frame with the
@@ -161,7 +162,9 @@ def main(argv=None):
     ap.add_argument("--out", default="")
     ap.add_argument("--init", default="", help="start from these weights (.npy)")
     ap.add_argument("--eval", action="store_true")
-    ap.add_argument("--eval-spp", type=int, nargs="+", default=[4, 8, 16, 32, 64])
+    ap.add_argument("--eval-spp", type=int, nargs="+", default=[1, 2, 4, 8, 16])
+    ap.add_argument("--scenes", nargs="+", default=["c3", "c2"], choices=["c2", "c3"],
+                    help="volumes of the training pairs (half the pairs each)")
     a = ap.parse_args(argv)
     import torch
     from . import Denoiser, Renderer
@@ -173,8 +176,13 @@ def main(argv=None):
     rng = np.random.default_rng(a.seed)
     t0 = time.perf_counter()
     sc = syn.scene_c3(mode=2)
-    r = sc.setup(Renderer(0))
-    log(f"scene ready in {time.perf_counter() - t0:.1f} s")
+    scenes = [sc]
+    if "c2" in a.scenes:
+        scenes.append(syn.scene_c2())
+    if "c3" not in a.scenes:
+        scenes = scenes[1:]
+    renderers = [s.setup(Renderer(0)) for s in scenes]
+    log(f"scenes ready in {time.perf_counter() - t0:.1f} s")
     den = Denoiser(0, seed=a.seed)
     if a.init:
         den.load(a.init)
@@ -182,8 +190,13 @@ def main(argv=None):
               "batch": a.batch, "lr": a.lr}
     if a.steps > 0:
         t0 = time.perf_counter()
-        F, T = render_pairs(r, a.pairs, a.res, a.spp, a.target_spp, rng, log)
+        import torch as _t
+        parts = [render_pairs(rr, a.pairs // len(renderers), a.res, a.spp, a.target_spp, rng, log) for rr in renderers]
+        F = _t.cat([p[0] for p in parts]) if len(parts) > 1 else parts[0][0]
+        T = _t.cat([p[1] for p in parts]) if len(parts) > 1 else parts[0][1]
+        del parts
         report["data_s"] = time.perf_counter() - t0
+        report["scenes"] = [s.name for s in scenes]
         t0 = time.perf_counter()
         losses = train(den, F, T, a.steps, a.batch, a.lr, rng, log)
         torch.cuda.synchronize()
@@ -198,7 +211,8 @@ def main(argv=None):
         report["eval"] = evaluate(r2, den, a.eval_spp)
         r2.close()
     print(json.dumps(report))
-    r.close()
+    for rr in renderers:
+        rr.close()
     return 0
 
 
