@@ -342,6 +342,10 @@ def denoised_time_to_rmse(r, target, stream, spps=(1, 2, 4, 8, 16, 32, 64), reps
     w, h = r.fbSize
     out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
     r.setFeatures(True)
+    r.setSpp(1)
+    r.Render(stream.cuda_stream)
+    torch.cuda.synchronize()
+    den.autotune(r.deviceFeatures(), 1, h, w)   # tensor-core tilings for this frame size
     tried = []
     found = None
     frame = 5_000_000

@@ -56,6 +56,12 @@ mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *d_features, 
  * 2 = the same kernels with the most output rows per CTA (one CTA per SM); 0 = the
  * mma.sync kernels everywhere.  The tiling is process-wide. */
 mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode);
+/* Autotuner of the tensor-core convolutions for one input shape: every layer's candidate
+ * tilings (output rows per CTA, input-channel chunk, weight stages) are timed on the real
+ * operands of a forward pass on d_features [n][h][w][16] (and, with backward != 0, the
+ * data gradients); the fastest are used for that shape until another is tuned.
+ * Synchronous; results do not depend on the tiling beyond FP32 summation order. */
+mdwt_status mdwt_denoiser_autotune(mdwt_denoiser *d, const float *d_features, int n, int h, int w, int backward);
 /* Wait for the denoiser's work; MDWT_ERR_TIMEOUT when a tensor-core kernel's bounded
  * wait for its operands gave up (its output is then invalid). */
 mdwt_status mdwt_denoiser_check(mdwt_denoiser *d);

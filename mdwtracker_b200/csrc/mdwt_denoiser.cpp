@@ -60,6 +60,9 @@ struct mdwt_denoiser {
   Acts A;
   int step = 0;
   int useTC = 1;          // tcgen05 convolutions where the shapes allow
+  // autotuned tcgen05 tilings per layer (forward, data gradient) for one activation shape
+  mdwt::nn::TcTiling tileF[kLayers], tileD[kLayers];
+  int tunedN = 0, tunedH = 0, tunedW = 0;
   int *dErr = nullptr;    // set by a tensor-core kernel whose bounded wait gave up
   std::string err;
 };
@@ -129,9 +132,15 @@ mdwt_status ensure_acts(mdwt_denoiser *d, int N, int Hp, int Wp) {
   return MDWT_OK;
 }
 
+bool tuned_for(const mdwt_denoiser *d) {
+  return d->tunedN == d->A.N && d->tunedH == d->A.Hp && d->tunedW == d->A.Wp && d->tunedN > 0;
+}
+
 mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st) {
+  const int li = (int)(&l - d->L);
   if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout))
-    DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st),
+    DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st,
+                              tuned_for(d) ? &d->tileF[li] : nullptr),
          "conv forward (tcgen05)");
   else
     DCKI(mdwt::nn::conv3x3_fwd(x, l.Wf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, st), "conv forward");
@@ -176,8 +185,10 @@ mdwt_status layer_bwd(mdwt_denoiser *d, const Layer &l, const void *x, const voi
   DCKI(mdwt::nn::conv3x3_wgrad(x, dy, l.gW, N, H, W, l.cin, l.cout, st), "weight gradient");
   DCKI(mdwt::nn::bias_grad(dy, l.gb, (size_t)N * H * W, l.cout, d->numSMs, st), "bias gradient");
   if (dx) {
+    const int li = (int)(&l - d->L);
     if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cout, l.cin))
-      DCKI(mdwt::nn::conv3x3_tc(dy, l.Wud, nullptr, dx, N, H, W, l.cout, l.cin, 0, 0, d->dErr, st),
+      DCKI(mdwt::nn::conv3x3_tc(dy, l.Wud, nullptr, dx, N, H, W, l.cout, l.cin, 0, 0, d->dErr, st,
+                                tuned_for(d) ? &d->tileD[li] : nullptr),
            "data gradient (tcgen05)");
     else
       DCKI(mdwt::nn::conv3x3_fwd(dy, l.Wd, nullptr, dx, N, H, W, l.cout, l.cin, 0, 0, st), "data gradient");
@@ -412,6 +423,70 @@ mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode) {
   }
   d->useTC = mode ? 1 : 0;
   return MDWT_OK;
+}
+
+// Time every candidate tiling of one convolution on its real operands; keep the fastest.
+static mdwt_status tune_one(mdwt_denoiser *d, int cin, int cout, const void *x, const void *w, const float *bias, void *y,
+                            int N, int H, int W, int relu, int f32, mdwt::nn::TcTiling *best, cudaStream_t st) {
+  mdwt::nn::TcTiling cand[32];
+  const int nc = mdwt::nn::conv3x3_tc_candidates(cin, cout, H, cand, 32);
+  cudaEvent_t e0, e1;
+  DCK(cudaEventCreate(&e0), "event");
+  DCK(cudaEventCreate(&e1), "event");
+  float bestMs = 1e30f;
+  *best = mdwt::nn::TcTiling();
+  for (int i = 0; i < nc; i++) {
+    float ms = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+      cudaEventRecord(e0, st);
+      const int rc = mdwt::nn::conv3x3_tc(x, w, bias, y, N, H, W, cin, cout, relu, f32, d->dErr, st, &cand[i]);
+      cudaEventRecord(e1, st);
+      if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(d, MDWT_ERR_CUDA, "tuning launch"); }
+      cudaEventSynchronize(e1);
+      float m = 0.f;
+      cudaEventElapsedTime(&m, e0, e1);
+      if (rep > 0 && m < ms) ms = m;
+    }
+    if (ms < bestMs) { bestMs = ms; *best = cand[i]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoiser_autotune(mdwt_denoiser *d, const float *F, int n, int h, int w, int backward) {
+  if (!d || !F || !dims_ok(n, h, w)) return MDWT_ERR_BAD_ARG;
+  if (!d->useTC) return MDWT_OK;
+  DCK(cudaSetDevice(d->device), "cudaSetDevice");
+  cudaStream_t st = nullptr;
+  d->tunedN = 0;
+  mdwt_status s = forward(d, F, n, h, w, st);   // activations of this shape
+  if (s) return s;
+  DCK(cudaStreamSynchronize(st), "sync");
+  Acts &A = d->A;
+  const int Hp = A.Hp, Wp = A.Wp, H1 = Hp / 2, W1 = Wp / 2, H2 = Hp / 4, W2 = Wp / 4;
+  const void *in[kLayers] = {A.x0, A.a1, A.p0, A.a2, A.p1, A.a3, A.u1, A.a4, A.u0, A.a5};
+  void *out[kLayers] = {A.a1, A.s0, A.a2, A.s1, A.a3, A.b2, A.a4, A.b1, A.a5, A.o};
+  const int hh[kLayers] = {Hp, Hp, H1, H1, H2, H2, H1, H1, Hp, Hp};
+  const int ww[kLayers] = {Wp, Wp, W1, W1, W2, W2, W1, W1, Wp, Wp};
+  for (int i = 0; i < kLayers; i++) {
+    const Layer &l = d->L[i];
+    if (!mdwt::nn::conv3x3_tc_supported(l.cin, l.cout)) continue;
+    if ((s = tune_one(d, l.cin, l.cout, in[i], l.Wuf, l.b, out[i], n, hh[i], ww[i], l.relu, i == kLayers - 1, &d->tileF[i],
+                      st)))
+      return s;
+  }
+  // data gradients: dy -> dx buffers of the backward pass (contents do not matter for timing)
+  void *dyb[kLayers] = {nullptr, A.d_s0, A.d_a2, A.d_s1, A.d_a3, A.d_b2, A.d_a4, A.d_b1, A.d_a5, A.d_o};
+  void *dxb[kLayers] = {nullptr, A.d_a1, A.d_p0, A.d_a2, A.d_p1, A.d_a3, A.d_u1, A.d_a4, A.d_u0, A.d_a5};
+  for (int i = 1; backward && i < kLayers; i++) {
+    const Layer &l = d->L[i];
+    if (!mdwt::nn::conv3x3_tc_supported(l.cout, l.cin)) continue;
+    if ((s = tune_one(d, l.cout, l.cin, dyb[i], l.Wud, nullptr, dxb[i], n, hh[i], ww[i], 0, 0, &d->tileD[i], st)))
+      return s;
+  }
+  d->tunedN = n; d->tunedH = Hp; d->tunedW = Wp;
+  return mdwt_denoiser_check(d);
 }
 
 mdwt_status mdwt_denoiser_check(mdwt_denoiser *d) {

@@ -101,7 +101,7 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
-constexpr int kMaxStages = 4;     // weight ring depth (runtime NS <= kMaxStages)
+constexpr int kMaxStages = 9;     // weight ring depth (runtime NS <= kMaxStages; 9 = a whole chunk's taps)
 constexpr uint32_t kSlot = 2176;   // smem slot of one A box (8 channels x 130 pixels = 2080 B), 128-B aligned
 constexpr int kHalo = kTM + 2;     // input pixels per row segment (one-pixel halo each side)
 
@@ -297,10 +297,6 @@ int tmem_cols_for(int cols) {
   return c;
 }
 
-struct TcTiling {
-  int R = 0, KC = 0, NS = 0;
-  size_t smem = 0;
-};
 constexpr size_t kSmemBudget = 200 * 1024;
 constexpr size_t kSmemTwoCtas = 112 * 1024;   // two CTAs per SM
 
@@ -316,6 +312,7 @@ int g_tcPolicy = 1;   // 1: two CTAs per SM where possible (measured faster); 0:
 // R * Cout <= 256, <= 112 KB).
 TcTiling tc_tiling(int Cin, int Cout, int H) {
   TcTiling t;
+  t.R = 0;
   auto search = [&](size_t budget, int colsMax, int rmin) {
     int rmax = colsMax / Cout;
     if (rmax > 8) rmax = 8;
@@ -326,7 +323,7 @@ TcTiling tc_tiling(int Cin, int Cout, int H) {
         for (int NS = 3; NS >= 2; NS--) {
           const size_t sm = tc_smem(R, KC, Cout, NS);
           if (sm <= budget) {
-            t.R = R; t.KC = KC; t.NS = NS; t.smem = sm;
+            t.R = R; t.KC = KC; t.NS = NS;
             return true;
           }
         }
@@ -339,6 +336,34 @@ TcTiling tc_tiling(int Cin, int Cout, int H) {
 }
 
 }  // namespace
+
+bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t) {
+  return t.R >= 1 && t.R <= 8 && t.R * Cout <= 512 && t.R <= (H > 0 ? H : 1) && t.KC >= 16 && t.KC % 16 == 0 &&
+         Cin % t.KC == 0 && t.NS >= 2 && t.NS <= kMaxStages && tc_smem(t.R, t.KC, Cout, t.NS) <= kSmemBudget;
+}
+
+// Candidate tilings for the autotuner: for each rows-per-CTA R, the largest channel chunk
+// that fits with a 3-stage ring, and with a ring of all of the chunk's 9 taps.
+int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut) {
+  int n = 0;
+  for (int R = 1; R <= 8 && n < maxOut; R++) {
+    if (R * Cout > 512 || R > H) break;
+    for (int NS : {3, 9}) {
+      for (int KC = Cin; KC >= 16; KC -= 16) {
+        if (Cin % KC) continue;
+        TcTiling t;
+        t.R = R; t.KC = KC; t.NS = NS;
+        if (tc_smem(R, KC, Cout, NS) <= kSmemBudget) {
+          bool dup = false;
+          for (int i = 0; i < n; i++) dup = dup || (out[i].R == R && out[i].KC == KC && out[i].NS == NS);
+          if (!dup && n < maxOut) out[n++] = t;
+          break;
+        }
+      }
+    }
+  }
+  return n;
+}
 
 bool conv3x3_tc_supported(int Cin, int Cout) {
   return Cin % 16 == 0 && Cin >= 16 && Cout % 16 == 0 && Cout >= 16 && Cout <= 256 && tc_tiling(Cin, Cout, 1).R > 0 &&
@@ -356,10 +381,14 @@ int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *
 }
 
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
-               int relu, int outF32, int *err, void *stream) {
+               int relu, int outF32, int *err, void *stream, const TcTiling *tiling) {
   if (!conv3x3_tc_supported(Cin, Cout) || N <= 0 || H <= 0 || W <= 0) return (int)cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(Wu) & 15)) return (int)cudaErrorInvalidValue;
-  const TcTiling tl = tc_tiling(Cin, Cout, H);
+  TcTiling tl = tc_tiling(Cin, Cout, H);
+  if (tiling && tiling->R > 0) {
+    if (!conv3x3_tc_valid(Cin, Cout, H, *tiling)) return (int)cudaErrorInvalidValue;
+    tl = *tiling;
+  }
   if (tl.R == 0) return (int)cudaErrorInvalidValue;
   CUtensorMap map;
   const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
@@ -370,7 +399,7 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
                                   es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return (int)cudaErrorInvalidValue;
-  const size_t smem = tl.smem + 1024;
+  const size_t smem = tc_smem(tl.R, tl.KC, Cout, tl.NS) + 1024;
   cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSmemBudget + 1024));
   if (e != cudaSuccess) return (int)e;

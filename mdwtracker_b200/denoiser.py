@@ -59,6 +59,10 @@ class Denoiser:
         the most output rows per CTA) or the mma.sync kernels."""
         self._call("set_tensor_cores", C.c_int((1 if two_ctas else 2) if on else 0))
 
+    def autotune(self, features, n: int, h: int, w: int, backward: bool = False) -> None:
+        """Time the candidate tensor-core tilings of every layer for this input shape."""
+        self._call("autotune", _ptr(features), C.c_int(n), C.c_int(h), C.c_int(w), C.c_int(1 if backward else 0))
+
     def check(self) -> None:
         """Synchronise; raises when a tensor-core kernel's bounded wait gave up."""
         self._call("check")
@@ -101,29 +105,3 @@ class Denoiser:
     def load(self, path: str) -> None:
         self.setParams(np.load(path))
 
-
-def _main(argv=None) -> int:
-    """python -m mdwtracker_b200.denoiser H W [runs]: inference on random features (a
-    profiling target); prints the device time per run."""
-    import sys
-    import torch
-    a = list(argv if argv is not None else sys.argv[1:])
-    h, w = int(a[0]), int(a[1])
-    runs = int(a[2]) if len(a) > 2 else 2
-    d = Denoiser(0, seed=1)
-    F = torch.rand((1, h, w, 16), device="cuda")
-    O = torch.empty((1, h, w, 4), device="cuda")
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    d.infer(F, O, 1, h, w)
-    e0.record()
-    for _ in range(runs):
-        d.infer(F, O, 1, h, w)
-    e1.record()
-    d.check()
-    torch.cuda.synchronize()
-    print(f"{h}x{w}: {e0.elapsed_time(e1) / runs:.3f} ms per inference")
-    return 0
-
-
-if __name__ == "__main__":
-    raise SystemExit(_main())

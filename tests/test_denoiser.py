@@ -141,3 +141,30 @@ def test_tensor_core_and_mma_paths_agree(n, h, w, two_ctas):
     rel = np.linalg.norm(outs[1] - outs[0]) / max(np.linalg.norm(ref), 1e-30)
     assert rel < 1e-2, rel
     d.setTensorCores(True)
+
+
+@pytest.mark.gpu
+def test_autotuned_tilings_agree_with_mma_path():
+    """After the tiling autotuner (forward and data gradients), inference and gradients
+    still agree with the mma.sync path."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(21)
+    n, h, w = 2, 36, 140
+    d = Denoiser(0, seed=4)
+    d.setParams(R.init_params(17))
+    F = torch.from_numpy(_features(rng, n, h, w)).cuda()
+    T = torch.from_numpy(rng.random((n, h, w, 4)).astype(np.float32)).cuda()
+    d.autotune(F, n, h, w, backward=True)
+    outs, grads = [], []
+    for tc in (True, False):
+        d.setTensorCores(tc)
+        o = torch.empty((n, h, w, 4), dtype=torch.float32, device="cuda")
+        d.infer(F, o, n, h, w)
+        d.check()
+        outs.append(o.cpu().numpy()[..., :3])
+        d.backward(F, T, n, h, w)
+        grads.append(d.grads())
+    ref = outs[1] - F.cpu().numpy()[..., :3]
+    assert np.linalg.norm(outs[0] - outs[1]) < 1e-2 * np.linalg.norm(ref)
+    assert np.linalg.norm(grads[0] - grads[1]) < 3e-2 * np.linalg.norm(grads[1])
