@@ -1345,6 +1345,7 @@ mdwt_status mdwt_batch_destroy(mdwt_batch *b) {
   if (b->dDisp) cudaFree(b->dDisp);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->graphStream) cudaStreamDestroy(b->graphStream);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return MDWT_OK;
