@@ -34,8 +34,8 @@ mdwt_status mdwt_batch_create(mdwt_batch **out, int device);
 mdwt_status mdwt_batch_destroy(mdwt_batch *b);
 const char *mdwt_batch_last_error(const mdwt_batch *b);
 /* Add a request (an initialised context on the batch's device; the batch does not own it:
- * the context must stay alive while the batch renders it, and a request added twice is
- * rendered twice per frame). */
+ * the context must stay alive while the batch renders it; adding it twice is
+ * MDWT_ERR_BAD_ARG). */
 mdwt_status mdwt_batch_add(mdwt_batch *b, mdwt_ctx *request);
 mdwt_status mdwt_batch_clear(mdwt_batch *b);
 /* One frame of every request, asynchronous on `stream` (NULL: the batch's own stream). */

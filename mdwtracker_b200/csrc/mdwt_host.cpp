@@ -1357,6 +1357,8 @@ mdwt_status mdwt_batch_add(mdwt_batch *b, mdwt_ctx *c) {
   if (!b || !c) return MDWT_ERR_BAD_ARG;
   if (!c->inited) return bfail(b, MDWT_ERR_STATE, "request not initialised");
   if (c->device != b->device) return bfail(b, MDWT_ERR_BAD_ARG, "request on another device");
+  for (auto *r : b->reqs)   // one frame per request and batch frame: its buffers are per context
+    if (r == c) return bfail(b, MDWT_ERR_BAD_ARG, "request already in the batch");
   b->reqs.push_back(c);
   return MDWT_OK;
 }

@@ -149,3 +149,14 @@ def test_schedule_autotuner_keeps_results(oracle):
         r.Render()
         twin.Render()
     _same(r, twin, spec["stats"])
+
+
+def test_batch_rejects_duplicates_and_foreign_state():
+    from mdwtracker_b200 import MdwtError
+    r = _setup(_requests()[0])
+    b = Batch(0)
+    b.add(r)
+    with pytest.raises(MdwtError):
+        b.add(r)
+    with pytest.raises(MdwtError):
+        Batch(0).render()            # empty batch
