@@ -78,23 +78,30 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 
 // K-major, no-swizzle shared-memory matrix descriptor (tcgen05 format: start >> 4 in
 // bits 0-13, leading (K-direction) byte offset >> 4 in bits 16-29, stride (M/N-direction)
-// byte offset >> 4 in bits 32-45, descriptor version 1 in bits 46-47, layout 0).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo & 0x3FFFFu) >> 4) << 16) |
-         ((uint64_t)((sbo & 0x3FFFFu) >> 4) << 32) | (1ull << 46);
+// byte offset >> 4 in bits 32-45, descriptor version 1 in bits 46-47, layout 0), as its
+// low and high 32-bit words.  Shared-memory addresses are below 256 KB, so adding a byte
+// offset >> 4 to the low word moves the start within its 14-bit field without a carry.
+__device__ __forceinline__ uint32_t smem_desc_lo(uint32_t addr, uint32_t lbo) {
+  return ((addr & 0x3FFFFu) >> 4) | (((lbo & 0x3FFFFu) >> 4) << 16);
 }
+__device__ __forceinline__ uint32_t smem_desc_hi(uint32_t sbo) { return ((sbo & 0x3FFFFu) >> 4) | (1u << 14); }
 // Instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12
 // = 1), both K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28.
 __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int acc) {
+// One MMA; the descriptors are given as low words plus one shared high word (the same
+// stride and version for A and B), so the issuing loop only adds offsets.
+__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint32_t alo, uint32_t blo, uint32_t hi, uint32_t idesc,
+                                         uint32_t acc) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+      "{\n\t.reg .pred p;\n\t.reg .b64 a, b;\n\t"
+      "setp.ne.b32 p, %5, 0;\n\t"
+      "mov.b64 a, {%1, %3};\n\t"
+      "mov.b64 b, {%2, %3};\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], a, b, %4, p;\n\t}\n" ::"r"(dtmem),
+      "r"(alo), "r"(blo), "r"(hi), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
@@ -167,6 +174,12 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
     loadA(0);
     for (int q = 0; q < NS && q < Q; q++) loadW(q);   // fill the weight ring
     const uint32_t lboB = (uint32_t)Cout * 16;
+    // descriptor words: start offsets in 16-byte units are added to the low words
+    const uint32_t hi = smem_desc_hi(128);
+    const uint32_t aLo0 = smem_desc_lo(smem_u32(bufA), kSlot), bLo0 = smem_desc_lo(smem_u32(wBase), lboB);
+    const uint32_t aRowStep = aRowBytes >> 4, aKStep = (2 * kSlot) >> 4, bKStep = (2 * lboB) >> 4;
+    const uint32_t wStep = wBytes >> 4;
+    const int nk = KC / 16;
     for (int q = 0; q < Q && ok; q++) {
       const int kc = q / 9, t = q % 9, st = q % NS;
       const uint32_t ph = (uint32_t)(q / NS) & 1u;
@@ -174,13 +187,16 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
       if (!mbar_wait(&full[st], ph)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;\n");
       const int dy = t / 3 - 1, dx = t % 3 - 1;
-      const uint32_t aBase = smem_u32(bufA) + (uint32_t)(dx + 1) * 16, bBase = smem_u32(wBase + (size_t)st * wBytes);
-      for (int r = 0; r < R; r++) {
-        const uint32_t rowBase = aBase + (uint32_t)(r + dy + 1) * aRowBytes;
-        for (int k = 0; k < KC / 16; k++) {
-          const uint64_t ad = smem_desc(rowBase + 2 * k * kSlot, kSlot, 128);
-          const uint64_t bd = smem_desc(bBase + 2 * k * lboB, lboB, 128);
-          umma_f16(tmem + (uint32_t)(r * Cout), ad, bd, idesc, (q > 0 || k > 0) ? 1 : 0);
+      const uint32_t bStep = bLo0 + (uint32_t)st * wStep;
+      uint32_t aRow = aLo0 + (uint32_t)(dx + 1) + (uint32_t)(dy + 1) * aRowStep;
+      uint32_t d = tmem;
+      for (int r = 0; r < R; r++, aRow += aRowStep, d += (uint32_t)Cout) {
+        uint32_t a = aRow, b = bStep;
+        umma_f16(d, a, b, hi, idesc, q > 0 ? 1u : 0u);
+        for (int k = 1; k < nk; k++) {
+          a += aKStep;
+          b += bKStep;
+          umma_f16(d, a, b, hi, idesc, 1u);
         }
       }
       umma_commit(&empty[st]);
