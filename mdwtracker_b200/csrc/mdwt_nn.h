@@ -39,15 +39,17 @@ int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int nu
 
 // tcgen05 path (mdwt_nn_tc.cu): the same convolution with the weights in the operand
 // layout Wu[tap][ci / 8][co][8] (umma_weights); *err is set when a bounded wait gave up.
-// A tcgen05 convolution tiling: R output rows per CTA, input channels in chunks of KC,
-// NS weight stages (NS >= 9 x chunks preloads every tap).
+// A tcgen05 convolution tiling: R output rows per tile (x 128 pixels), input channels in
+// chunks of KC, SA input stages, AB accumulators in tensor memory (2: the epilogue of one
+// tile overlaps the MMAs of the next), NS weight stages (NS >= 9 x chunks keeps all the
+// weights resident for the launch).
 struct TcTiling {
-  int R = 0, KC = 0, NS = 0;
+  int R = 0, KC = 0, NS = 0, SA = 0, AB = 0;
 };
 bool conv3x3_tc_supported(int Cin, int Cout);
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t);
 int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut);
-// Tiling policy: 0 = most output rows per CTA, 1 = two CTAs per SM where possible.
+// Tiling policy: 1 = two accumulators (default), 0 = one accumulator with the most rows.
 void conv3x3_tc_policy(int policy);
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream);
 // tiling: null or R == 0 = the default policy's tiling

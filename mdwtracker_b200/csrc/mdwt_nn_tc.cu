@@ -1,26 +1,22 @@
 // mdwt_nn_tc.cu -- the denoiser's 3x3 convolution on the 5th-generation tensor cores.
 //
-// Implicit GEMM per CTA: D[128 pixels of one image row][Cout] = sum over the 9 taps of
-// A_tap[128 pixels][Cin] x B_tap[Cin][Cout].  Per tap:
-//   * A: the 128 input pixels (y + dy, x0 + dx .. x0 + dx + 127) x Cin channels, one TMA
-//     tile load per group of 8 channels (box 8 channels x 128 pixels from the NHWC tensor
-//     map; out-of-image pixels -- padding, row ends -- are zero-filled by the TMA unit);
-//   * B: the tap's weights, pre-arranged on the device in the operand layout
-//     [ci / 8][co][8], one bulk copy.
-// Both land in shared memory in the K-major, no-swizzle core-matrix layout (8 rows x 16
-// bytes per core matrix; 8-row groups 128 B apart, K groups LBO apart).  One thread
-// issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in tensor memory, M = 128,
-// N = Cout, K = 16 per instruction) and tcgen05.commit to an mbarrier; two stages, the
-// loads of tap t + 2 wait for the MMAs of tap t.  Epilogue: each warp reads its 32 TMEM
-// lanes (= pixels) with tcgen05.ld, adds the bias, applies ReLU and stores BF16 or FP32.
-// Every mbarrier wait is bounded; a wait that gives up sets *err and the CTA skips to
-// freeing its tensor memory.
-#include <cuda.h>
+// Implicit GEMM: D[128 pixels of one image row][Cout] = sum over the 9 taps of
+// A_tap[128 pixels][Cin] x B_tap[Cin][Cout].
+//   * A: the input rows y - 1 .. y + R of a tile, pixels x0 - 1 .. x0 + 128, staged by
+//     coalesced 16-byte cp.async copies of the NHWC rows (out-of-image pixels -- padding,
+//     row ends -- zero-filled); tap (dy, dx) of output row r reads input row r + dy from
+//     pixel dx on;
+//   * B: the weights, pre-arranged on the device in the operand layout [tap][ci / 8][co][8]
+//     and bulk-copied (once per launch when they fit, else per chunk and tap).
+// Both sit in shared memory in the K-major, no-swizzle core-matrix layout (8 rows x 16
+// bytes per core matrix; 8-row groups 128 B apart, K groups LBO apart).  tcgen05.mma
+// kind::f16: BF16 inputs, FP32 accumulator in tensor memory, M = 128, N = Cout, K = 16.
+// The kernel is persistent and warp-specialised (producer, MMA issuer, epilogue warps; see
+// conv3x3_tc_kernel).  Every mbarrier wait is bounded; a wait that gives up sets *err.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <mutex>
 
 #include "mdwt_nn.h"
 
@@ -31,7 +27,7 @@ namespace {
 typedef __nv_bfloat16 bf16;
 
 constexpr int kTM = 128;                 // pixels per CTA (MMA M)
-constexpr uint32_t kSpinLimit = 1u << 22;   // bounded mbarrier waits (with nanosleep back-off)
+constexpr long long kWaitClocks = 1ll << 31;   // bounded mbarrier waits: give up after ~1 s of SM clocks
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -52,23 +48,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: false when it gave up
+// bounded wait: false when it gave up (after kWaitClocks SM clocks)
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kSpinLimit; i++) {
+  const long long t0 = clock64();
+  for (uint32_t i = 0;; i++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 15u) == 15u && clock64() - t0 > kWaitClocks) return false;
     if (i > 64) __nanosleep(64);
   }
-  return false;
 }
 
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
-                                            uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];\n" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-      : "memory");
-}
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                    smem_u32(dst)),
@@ -91,16 +80,18 @@ __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// One MMA; the descriptors are given as low words plus one shared high word (the same
-// stride and version for A and B), so the issuing loop only adds offsets.
+// One MMA, issued by one elected lane of a converged warp (all lanes call it); the
+// descriptors are given as low words plus one shared high word (the same stride and
+// version for A and B), so the issuing loop only adds offsets.
 __device__ __forceinline__ void umma_f16(uint32_t dtmem, uint32_t alo, uint32_t blo, uint32_t hi, uint32_t idesc,
                                          uint32_t acc) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\t.reg .b64 a, b;\n\t"
+      "{\n\t.reg .pred p, e;\n\t.reg .b64 a, b;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
       "setp.ne.b32 p, %5, 0;\n\t"
       "mov.b64 a, {%1, %3};\n\t"
       "mov.b64 b, {%2, %3};\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], a, b, %4, p;\n\t}\n" ::"r"(dtmem),
+      "@e tcgen05.mma.cta_group::1.kind::f16 [%0], a, b, %4, p;\n\t}\n" ::"r"(dtmem),
       "r"(alo), "r"(blo), "r"(hi), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -108,173 +99,332 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
-constexpr int kMaxStages = 9;     // weight ring depth (runtime NS <= kMaxStages; 9 = a whole chunk's taps)
-constexpr uint32_t kSlot = 2176;   // smem slot of one A box (8 channels x 130 pixels = 2080 B), 128-B aligned
-constexpr int kHalo = kTM + 2;     // input pixels per row segment (one-pixel halo each side)
+constexpr int kMaxAStages = 4;            // input (A) ring depth
+constexpr int kMaxWStages = 16;           // weight stages (one input-channel chunk x 9 taps each)
+constexpr int kLoadWarps = 4;             // input producers
+constexpr int kEpiWarps = 8;              // epilogue warps (two per TMEM lane quarter)
+constexpr int kWarpW = kLoadWarps;        // weight producer and TMEM allocator
+constexpr int kWarpMma = kLoadWarps + 1;  // MMA issuer
+constexpr int kWarpEpi = kLoadWarps + 2;  // first epilogue warp
+constexpr int kThreads = 32 * (kLoadWarps + 2 + kEpiWarps);
+constexpr int kHalo = kTM + 2;            // input pixels per row segment (one-pixel halo each side)
+constexpr uint32_t kRowBytes = kHalo * 16;   // one row segment of 8 channels: 2080 B
 
-// CTA: R output rows x 128 pixels, all Cout channels.  Input channels in chunks of KC;
-// per chunk the R + 2 input rows (with a one-pixel halo) are loaded once; the horizontal
-// taps are the same rows read from a descriptor start 16 B (one pixel) further.
-__global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap mapX, const bf16 *Wu,
-                                                         const float *bias, void *Y, int N, int H, int W, int Cin,
-                                                         int Cout, int relu, int outF32, int tmemCols, int R, int KC,
-                                                         int NS, int *err) {
+// Shared-memory slot of one channel group of a stage (R + 2 rows x 130 pixels x 8
+// channels), 128-B aligned.
+__host__ __device__ inline uint32_t a_slot(int R) { return ((uint32_t)(R + 2) * kRowBytes + 127u) & ~127u; }
+
+struct ConvArgs {
+  const bf16 *X;
+  const bf16 *Wu;
+  const float *bias;
+  void *Y;
+  int *err;
+  int N, H, W, Cin, Cout, relu, outF32;
+  int R, KC, NS, SA, AB, resident, tmemCols, tilesX, tilesY, tiles;
+};
+
+// bounded wait that also gives up once another role of the CTA has aborted
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abortFlag) {
+  const long long t0 = clock64();
+  for (uint32_t i = 0;; i++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 15u) == 15u && (*abortFlag || clock64() - t0 > kWaitClocks)) return false;
+    if (i > 64) __nanosleep(32);
+  }
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent, warp-specialised implicit-GEMM convolution.  A tile is R output rows x 128
+// pixels of one image, all Cout channels; CTA b takes tiles b, b + grid, ...  Per tile and
+// input-channel chunk (KC channels) the R + 2 input rows with a one-pixel halo are staged
+// once; the horizontal taps read the same rows from a descriptor start one pixel (16 B)
+// further, the vertical taps from the neighbouring rows.
+//   warps 0-3: input producers -- 16-byte cp.async of the NHWC rows into the core-matrix
+//     layout, each thread one channel group (zero stores outside the image), a ring of SA
+//     stages; each thread waits for its own copies, fences them to the async proxy and
+//     arrives on the stage's barrier;
+//   warp 4, lane 0: weights -- by bulk copies into stages of one input-channel chunk x 9
+//     taps, once for the whole launch (resident) or per tile and chunk through a ring of
+//     NS stages;
+//   warp 5: MMA issuer -- the warp runs the loops, lane 0 issues: per chunk and output
+//     row, 9 taps x KC / 16 tcgen05.mma (M = 128 pixels, N = Cout, K = 16) into that
+//     row's accumulator back to back; AB accumulators of R x Cout TMEM columns alternate
+//     between tiles, so the epilogue of one tile overlaps the MMAs of the next;
+//   warps 6-13: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
+//     BF16 or FP32 stores; the two warps of a quarter take alternate rows.
+// Every wait is bounded; a role that gives up sets *err and the CTA abort flag, the others
+// leave their loops, every producer waits for its copies in flight and the MMA issuer for
+// its MMAs before the tensor memory is freed.
+__global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], fullA, freeA, done;
+  __shared__ __align__(8) uint64_t aFull[kMaxAStages], aEmpty[kMaxAStages], wFull[kMaxWStages], wEmpty[kMaxWStages];
+  __shared__ __align__(8) uint64_t wRes, accFull[2], accEmpty[2], mmaDone;
   __shared__ uint32_t tmemBase;
+  __shared__ volatile int abortFlag;
   uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tilesX = (W + kTM - 1) / kTM, tilesY = (H + R - 1) / R;
-  const int bx = blockIdx.x;
-  const int x0 = (bx % tilesX) * kTM;
-  const int y0 = ((bx / tilesX) % tilesY) * R;
-  const int n = bx / (tilesX * tilesY);
-  const int G = KC / 8;                                   // A boxes per row and chunk
-  const uint32_t aRowBytes = (uint32_t)G * kSlot;
-  const uint32_t aBytes = (uint32_t)(R + 2) * aRowBytes;  // A buffer
-  const uint32_t wBytes = (uint32_t)KC * Cout * 2;        // one tap's weights of a chunk
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int R = a.R, Cout = a.Cout, G = a.KC / 8, chunks = a.Cin / a.KC, Gtot = a.Cin / 8;
+  const uint32_t slot = a_slot(R), stageA = (uint32_t)G * slot;
+  const uint32_t tapChunkBytes = (uint32_t)G * Cout * 16;   // one tap's weights of a chunk
+  const uint32_t wStageBytes = 9 * tapChunkBytes;
+  const int wStages = a.resident ? chunks : a.NS;
   uint8_t *bufA = smem;
-  uint8_t *wBase = smem + aBytes;          // NS weight stages of wBytes each
-  const int chunks = Cin / KC, Q = chunks * 9, Gtot = Cin / 8;
+  uint8_t *bufW = smem + (size_t)a.SA * stageA;
 
-  if (tid == 0) {
-    for (int i = 0; i < NS; i++) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], 1);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < a.SA; i++) {
+      mbar_init(&aFull[i], 32 * kLoadWarps);
+      mbar_init(&aEmpty[i], 1);
     }
-    mbar_init(&fullA, 1);
-    mbar_init(&freeA, 1);
-    mbar_init(&done, 1);
+    for (int i = 0; i < kMaxWStages; i++) {
+      mbar_init(&wFull[i], 1);
+      mbar_init(&wEmpty[i], 1);
+    }
+    mbar_init(&wRes, 1);
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&accFull[i], 1);
+      mbar_init(&accEmpty[i], kEpiWarps);
+    }
+    mbar_init(&mmaDone, 1);
+    abortFlag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == kWarpW) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmemBase)),
-                 "r"(tmemCols));
+                 "r"(a.tmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n");
   const uint32_t tmem = tmemBase;
+  auto fail = [&]() {
+    abortFlag = 1;
+    atomicExch(a.err, 1);
+  };
 
-  if (tid == 0) {
+  if (warp < kLoadWarps) {
+    // ------------------------------------------------------------------ input producers
+    // thread p copies channel group g = p % G of pixels p / G, p / G + 128 / G, ... of every
+    // row (G divides 128); out-of-image pixels are zero stores
+    const int p = threadIdx.x;   // 0 .. 32 * kLoadWarps - 1
+    const int g = p % G, pxStep = (32 * kLoadWarps) / G;
+    const int px0 = p / G;
+    bool ok = true;
+    uint32_t gA = 0;
+    int pending = -1;   // stage whose copies are issued but not yet signalled
+    for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
+      const int tx = t % a.tilesX, ty = (t / a.tilesX) % a.tilesY, n = t / (a.tilesX * a.tilesY);
+      const int x0 = tx * kTM, y0 = ty * R;
+      for (int kc = 0; kc < chunks; kc++) {
+        const uint32_t s = gA % (uint32_t)a.SA, use = gA / (uint32_t)a.SA;
+        int go = 1;
+        if (lane == 0) go = abortFlag ? 0 : ((use == 0 || mbar_wait_ab(&aEmpty[s], (use - 1) & 1u, &abortFlag)) ? 1 : 2);
+        go = __shfl_sync(0xffffffffu, go, 0);
+        if (go != 1) {
+          if (go == 2 && lane == 0) fail();
+          ok = false;
+          break;
+        }
+        const uint32_t dst0 = smem_u32(bufA) + s * stageA + (uint32_t)g * slot;
+        const bf16 *src0 = a.X + (size_t)n * a.H * a.W * a.Cin + (size_t)kc * a.KC + g * 8;
+        for (int r = 0; r < R + 2; r++) {
+          const int gy = y0 - 1 + r;
+          const bool rowIn = gy >= 0 && gy < a.H;
+          const bf16 *rowSrc = src0 + (size_t)(rowIn ? gy : 0) * a.W * a.Cin;
+          const uint32_t rowDst = dst0 + (uint32_t)r * kRowBytes;
+          for (int px = px0; px < kHalo; px += pxStep) {
+            const int gx = x0 - 1 + px;
+            const uint32_t dst = rowDst + (uint32_t)px * 16;
+            if (rowIn && gx >= 0 && gx < a.W)
+              asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(rowSrc + (size_t)gx * a.Cin)
+                           : "memory");
+            else
+              asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};\n" ::"r"(dst), "r"(0u) : "memory");
+          }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        if (pending >= 0) {   // the previous stage: its copies done, visible to the tensor cores
+          asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          mbar_arrive(&aFull[pending]);
+        }
+        pending = (int)s;
+        gA++;
+      }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (pending >= 0) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_arrive(&aFull[pending]);
+    }
+  } else if (warp == kWarpW) {
+    if (lane == 0) {
+      // ---------------------------------------------------------------- weights
+      // stage = one input-channel chunk, all 9 taps: [tap][G][Cout][8]; resident weights
+      // fill one stage per chunk once, streamed weights cycle NS stages per tile and chunk
+      bool ok = true;
+      uint32_t gW = 0;
+      auto loadChunk = [&](uint32_t st, int kc) {
+        mbar_expect_tx(&wFull[st], wStageBytes);
+        for (int tap = 0; tap < 9; tap++)
+          bulk_load(bufW + (size_t)st * wStageBytes + (size_t)tap * tapChunkBytes,
+                    a.Wu + ((size_t)tap * Gtot + (size_t)kc * G) * Cout * 8, tapChunkBytes, &wFull[st]);
+      };
+      if (a.resident) {
+        for (int kc = 0; kc < chunks; kc++) loadChunk((uint32_t)kc, kc);
+        gW = (uint32_t)chunks;
+      } else {
+        for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
+          if (abortFlag) break;
+          for (int kc = 0; kc < chunks; kc++) {
+            const uint32_t sw = gW % (uint32_t)wStages, uw = gW / (uint32_t)wStages;
+            if (uw > 0 && !mbar_wait_ab(&wEmpty[sw], (uw - 1) & 1u, &abortFlag)) { ok = false; break; }
+            loadChunk(sw, kc);
+            gW++;
+          }
+        }
+      }
+      if (!ok) fail();
+      // wait for every copy issued (the last one into each stage may still be in flight)
+      for (uint32_t st = 0; st < (uint32_t)wStages; st++)
+        if (gW > st && !mbar_wait(&wFull[st], ((gW - 1 - st) / (uint32_t)wStages) & 1u)) fail();
+    }
+    __syncwarp();
+  } else if (warp == kWarpMma) {
+    // ------------------------------------------------------------------ MMA issuer
+    // The whole warp runs the (uniform) loops; one elected lane issues.  Per chunk and
+    // output row the KC / 16 x 9 taps MMAs go to that row's accumulator back to back.
+    auto warpWait = [&](uint64_t *bar, uint32_t parity) -> bool {
+      int okw = 0;
+      if (lane == 0) okw = mbar_wait_ab(bar, parity, &abortFlag) ? 1 : 0;
+      return __shfl_sync(0xffffffffu, okw, 0) != 0;
+    };
     bool ok = true;
     const uint32_t idesc = instr_desc(kTM, Cout);
-    auto loadA = [&](int kc) {
-      mbar_expect_tx(&fullA, (uint32_t)(R + 2) * G * (kHalo * 16));
-      for (int r = 0; r < R + 2; r++)
-        for (int g = 0; g < G; g++)
-          tma_load_4d(bufA + r * aRowBytes + g * kSlot, &mapX, kc * KC + g * 8, x0 - 1, y0 - 1 + r, n, &fullA);
-    };
-    auto loadW = [&](int q) {
-      const int kc = q / 9, tap = q % 9, st = q % NS;
-      mbar_expect_tx(&full[st], wBytes);
-      bulk_load(wBase + (size_t)st * wBytes, Wu + ((size_t)tap * Gtot + (size_t)kc * G) * Cout * 8, wBytes, &full[st]);
-    };
-    loadA(0);
-    for (int q = 0; q < NS && q < Q; q++) loadW(q);   // fill the weight ring
-    const uint32_t lboB = (uint32_t)Cout * 16;
-    // descriptor words: start offsets in 16-byte units are added to the low words
     const uint32_t hi = smem_desc_hi(128);
-    const uint32_t aLo0 = smem_desc_lo(smem_u32(bufA), kSlot), bLo0 = smem_desc_lo(smem_u32(wBase), lboB);
-    const uint32_t aRowStep = aRowBytes >> 4, aKStep = (2 * kSlot) >> 4, bKStep = (2 * lboB) >> 4;
-    const uint32_t wStep = wBytes >> 4;
-    const int nk = KC / 16;
-    for (int q = 0; q < Q && ok; q++) {
-      const int kc = q / 9, t = q % 9, st = q % NS;
-      const uint32_t ph = (uint32_t)(q / NS) & 1u;
-      if (t == 0 && !mbar_wait(&fullA, (uint32_t)kc & 1u)) { ok = false; break; }
-      if (!mbar_wait(&full[st], ph)) { ok = false; break; }
+    // descriptor low words; offsets in 16-byte units are added to them
+    const uint32_t aLo0 = smem_desc_lo(smem_u32(bufA), slot);
+    const uint32_t bLo0 = smem_desc_lo(smem_u32(bufW), (uint32_t)Cout * 16);
+    const uint32_t rowStep = kRowBytes >> 4, aKStep = (2 * slot) >> 4, bKStep = 2u * Cout;
+    const uint32_t stageAU = stageA >> 4, wStageU = wStageBytes >> 4, tapU = tapChunkBytes >> 4;
+    const int nk = a.KC / 16;
+    uint32_t gA = 0, gW = 0;
+    int it = 0;
+    for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x, it++) {
+      const uint32_t ab = (uint32_t)(it % a.AB), use = (uint32_t)(it / a.AB);
+      if (use > 0 && !warpWait(&accEmpty[ab], (use - 1) & 1u)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;\n");
-      const int dy = t / 3 - 1, dx = t % 3 - 1;
-      const uint32_t bStep = bLo0 + (uint32_t)st * wStep;
-      uint32_t aRow = aLo0 + (uint32_t)(dx + 1) + (uint32_t)(dy + 1) * aRowStep;
-      uint32_t d = tmem;
-      for (int r = 0; r < R; r++, aRow += aRowStep, d += (uint32_t)Cout) {
-        uint32_t a = aRow, b = bStep;
-        umma_f16(d, a, b, hi, idesc, q > 0 ? 1u : 0u);
-        for (int k = 1; k < nk; k++) {
-          a += aKStep;
-          b += bKStep;
-          umma_f16(d, a, b, hi, idesc, 1u);
-        }
-      }
-      umma_commit(&empty[st]);
-      if (t == 8) umma_commit(&freeA);
-      // refill the stage of step q - 1 (its MMAs were issued before this step's, which
-      // are queued behind them) with step q - 1 + NS
-      if (q >= 1 && q - 1 + NS < Q) {
-        const int sp = (q - 1) % NS;
-        if (!mbar_wait(&empty[sp], (uint32_t)((q - 1) / NS) & 1u)) { ok = false; break; }
-        loadW(q - 1 + NS);
-      }
-      if (t == 8 && kc + 1 < chunks) {
-        if (!mbar_wait(&freeA, (uint32_t)kc & 1u)) { ok = false; break; }
-        loadA(kc + 1);
-      }
-    }
-    if (ok) {
-      umma_commit(&done);
-      if (!mbar_wait(&done, 0)) ok = false;
-    }
-    if (!ok) atomicExch(err, 1);
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;\n");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n");
-  const bool good = *(volatile int *)err == 0;
-
-  if (good) {
-    // epilogue: warp w owns TMEM lanes 32w .. 32w + 31 = pixels x0 + 32w + lane
-    const int px = x0 + warp * 32 + lane;
-    const bool validX = px < W;
-    for (int r = 0; r < R; r++) {
-      const int y = y0 + r;
-      const bool valid = validX && y < H;
-      const size_t pix = (((size_t)n * H + (y < H ? y : 0)) * W + (validX ? px : 0));
-      for (int c0 = 0; c0 < Cout; c0 += 16) {
-        uint32_t v32[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * Cout + c0);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-            : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
-              "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]),
-              "=r"(v32[14]), "=r"(v32[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-        if (!valid) continue;
-        float v[16];
+      const uint32_t dBase = tmem + ab * (uint32_t)(R * Cout);
+      for (int kc = 0; kc < chunks; kc++) {
+        const uint32_t s = gA % (uint32_t)a.SA;
+        const uint32_t sw = a.resident ? (uint32_t)kc : gW % (uint32_t)wStages;
+        const uint32_t pw = a.resident ? 0u : (gW / (uint32_t)wStages) & 1u;
+        if (!warpWait(&aFull[s], (gA / (uint32_t)a.SA) & 1u) || !warpWait(&wFull[sw], pw)) { ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;\n");
+        const uint32_t aSt = aLo0 + s * stageAU, wSt = bLo0 + sw * wStageU;
+        uint32_t d = dBase, aRow = aSt;
+        for (int r = 0; r < R; r++, d += (uint32_t)Cout, aRow += rowStep) {
+          uint32_t aK = aRow, bK = wSt;
+          for (int k = 0; k < nk; k++, aK += aKStep, bK += bKStep) {
+            umma_f16(d, aK, bK, hi, idesc, (kc > 0 || k > 0) ? 1u : 0u);
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          float f = __uint_as_float(v32[j]);
-          if (bias) f += bias[c0 + j];
-          if (relu) f = fmaxf(f, 0.f);
-          v[j] = f;
-        }
-        if (outF32) {
-          float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(Y) + pix * Cout + c0);
-#pragma unroll
-          for (int j = 0; j < 4; j++) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-        } else {
-          uint4 w[2];
-          uint32_t *wp = reinterpret_cast<uint32_t *>(w);
-#pragma unroll
-          for (int j = 0; j < 8; j++) {
-            __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-            wp[j] = *reinterpret_cast<uint32_t *>(&b2);
+            for (int tap = 1; tap < 9; tap++)
+              umma_f16(d, aK + (uint32_t)(tap / 3) * rowStep + (uint32_t)(tap % 3), bK + (uint32_t)tap * tapU, hi,
+                       idesc, 1u);
           }
-          uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(Y) + pix * Cout + c0);
-          o[0] = w[0];
-          o[1] = w[1];
+        }
+        if (lane == 0) {
+          umma_commit(&aEmpty[s]);
+          if (!a.resident) umma_commit(&wEmpty[sw]);
+        }
+        __syncwarp();
+        gA++;
+        if (!a.resident) gW++;
+      }
+      if (!ok) break;
+      if (lane == 0) umma_commit(&accFull[ab]);
+      __syncwarp();
+    }
+    if (lane == 0) {
+      if (!ok) fail();
+      umma_commit(&mmaDone);   // all MMAs issued by this warp have completed
+      if (!mbar_wait(&mmaDone, 0)) fail();
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------------ epilogue
+    const int qd = warp & 3, half = (warp - kWarpEpi) >> 2;
+    bool ok = true;
+    int it = 0;
+    for (int t = blockIdx.x; t < a.tiles; t += gridDim.x, it++) {
+      int go = 1;
+      const uint32_t ab = (uint32_t)(it % a.AB), use = (uint32_t)(it / a.AB);
+      if (lane == 0) go = abortFlag ? 0 : (mbar_wait_ab(&accFull[ab], use & 1u, &abortFlag) ? 1 : 2);
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (go != 1) {
+        ok = go == 0;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n");
+      const int tx = t % a.tilesX, ty = (t / a.tilesX) % a.tilesY, n = t / (a.tilesX * a.tilesY);
+      const int px = tx * kTM + qd * 32 + lane;
+      const bool validX = px < a.W;
+      const uint32_t tBase = tmem + ((uint32_t)(qd * 32) << 16) + ab * (uint32_t)(R * Cout);
+      for (int r = half; r < R; r += 2) {
+        const int y = ty * R + r;
+        const bool valid = validX && y < a.H;
+        const size_t pix = (((size_t)n * a.H + (y < a.H ? y : 0)) * a.W + (validX ? px : 0));
+        for (int c0 = 0; c0 < Cout; c0 += 16) {
+          uint32_t v32[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+              : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
+                "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]),
+                "=r"(v32[14]), "=r"(v32[15])
+              : "r"(tBase + (uint32_t)(r * Cout + c0)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          if (!valid) continue;
+          float v[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            float f = __uint_as_float(v32[j]);
+            if (a.bias) f += a.bias[c0 + j];
+            if (a.relu) f = fmaxf(f, 0.f);
+            v[j] = f;
+          }
+          if (a.outF32) {
+            float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(a.Y) + pix * Cout + c0);
+#pragma unroll
+            for (int j = 0; j < 4; j++) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+          } else {
+            uint4 w[2];
+            uint32_t *wp = reinterpret_cast<uint32_t *>(w);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+              wp[j] = *reinterpret_cast<uint32_t *>(&b2);
+            }
+            uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(a.Y) + pix * Cout + c0);
+            o[0] = w[0];
+            o[1] = w[1];
+          }
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;\n");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accEmpty[ab]);
     }
+    if (!ok && lane == 0) fail();
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n");
   __syncthreads();
-  if (warp == 0) {
+  if (warp == kWarpW) {
     asm volatile("tcgen05.fence::after_thread_sync;\n");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmemCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(a.tmemCols));
   }
 }
 
@@ -290,100 +440,124 @@ __global__ void umma_weights_kernel(const bf16 *Wf, bf16 *Wu, int Cin, int Cout)
   }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  });
-  return fn;
-}
-
 int tmem_cols_for(int cols) {
   int c = 32;
   while (c < cols) c <<= 1;
   return c;
 }
 
-constexpr size_t kSmemBudget = 200 * 1024;
-constexpr size_t kSmemTwoCtas = 112 * 1024;   // two CTAs per SM
+constexpr size_t kSmemBudget = 224 * 1024;     // dynamic shared memory of one CTA (one per SM)
+constexpr size_t kSmemFloor = 120 * 1024;      // requested at least: keeps a second CTA off the SM
+constexpr size_t kResidentMax = 112 * 1024;    // weights kept resident up to this size
 
-size_t tc_smem(int R, int KC, int Cout, int NS) {
-  return (size_t)(R + 2) * (KC / 8) * kSlot + (size_t)NS * KC * Cout * 2;
+int chunks_of(int Cin, const TcTiling &t) { return t.KC > 0 ? Cin / t.KC : 0; }
+// weight stages hold one input-channel chunk (all 9 taps); NS >= chunks keeps them resident
+bool resident_of(int Cin, const TcTiling &t) { return t.NS >= chunks_of(Cin, t); }
+
+size_t tc_smem(int Cin, int Cout, const TcTiling &t) {
+  const int stages = resident_of(Cin, t) ? chunks_of(Cin, t) : t.NS;
+  return (size_t)t.SA * (t.KC / 8) * a_slot(t.R) + (size_t)stages * 18 * t.KC * Cout;
 }
 
-int g_tcPolicy = 1;   // 1: two CTAs per SM where possible (measured faster); 0: most rows per CTA
+int g_tcPolicy = 1;   // 1: one accumulator, most input stages (measured fastest); 0: two accumulators
 
-// Rows per CTA R (<= 8), input-channel chunk KC (a divisor of Cin, multiple of 16) and
-// weight stages NS (3, else 2) whose buffers fit the shared-memory budget, R * Cout
-// TMEM columns.  Policy 1 first looks for a tiling that fits two CTAs per SM (R >= 2,
-// R * Cout <= 256, <= 112 KB).
+// Largest input-channel chunk (a divisor of Cin, multiple of 16) that fits the budget with
+// SA input stages and the given weight staging (NS = 0: resident); 0 when none does.
+int fit_kc(int Cin, int Cout, int R, int SA, int NS, int AB) {
+  for (int KC = Cin; KC >= 16; KC -= 16) {
+    if (Cin % KC || ((KC / 8) & (KC / 8 - 1))) continue;
+    TcTiling t;
+    t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
+    t.NS = NS > 0 ? NS : Cin / KC;
+    if (Cin / KC > kMaxWStages && NS == 0) continue;
+    if (tc_smem(Cin, Cout, t) <= kSmemBudget) return KC;
+  }
+  return 0;
+}
+
+int rows_max(int Cout, int AB, int H) {
+  int r = (512 / AB) / Cout;
+  if (r > 8) r = 8;
+  if (r > H) r = H;
+  return r;
+}
+
+// Default tiling: the most rows that AB accumulators allow, resident weights when they
+// fit kResidentMax (else a ring of 2 chunk stages), the most input stages (4 .. 2) that fit
+// with the largest chunk.  Policy 1 uses one accumulator (the MMAs of a tile start after
+// the previous epilogue), policy 0 two.
 TcTiling tc_tiling(int Cin, int Cout, int H) {
   TcTiling t;
-  t.R = 0;
-  auto search = [&](size_t budget, int colsMax, int rmin) {
-    int rmax = colsMax / Cout;
-    if (rmax > 8) rmax = 8;
-    if (rmax > H) rmax = H;
-    for (int R = rmax; R >= rmin; R--)
-      for (int KC = Cin; KC >= 16; KC -= 16) {
-        if (Cin % KC) continue;
-        for (int NS = 3; NS >= 2; NS--) {
-          const size_t sm = tc_smem(R, KC, Cout, NS);
-          if (sm <= budget) {
-            t.R = R; t.KC = KC; t.NS = NS;
-            return true;
-          }
-        }
-      }
-    return false;
-  };
-  if (g_tcPolicy == 1 && search(kSmemTwoCtas, 256, H >= 2 ? 2 : 1)) return t;
-  search(kSmemBudget, 512, 1);
+  const int AB = g_tcPolicy == 1 ? 1 : 2;
+  const int R = rows_max(Cout, AB, H > 0 ? H : 1);
+  if (R < 1) return t;
+  const bool res = (size_t)18 * Cin * Cout <= kResidentMax;
+  for (int SA = kMaxAStages; SA >= 2; SA--) {
+    const int KC = fit_kc(Cin, Cout, R, SA, res ? 0 : 2, AB);
+    if (KC) {
+      t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
+      t.NS = res ? Cin / KC : 2;
+      return t;
+    }
+  }
   return t;
+}
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = n > 0 ? n : 148;
+  }
+  return cached[dev];
 }
 
 }  // namespace
 
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t) {
-  return t.R >= 1 && t.R <= 8 && t.R * Cout <= 512 && t.R <= (H > 0 ? H : 1) && t.KC >= 16 && t.KC % 16 == 0 &&
-         Cin % t.KC == 0 && t.NS >= 2 && t.NS <= kMaxStages && tc_smem(t.R, t.KC, Cout, t.NS) <= kSmemBudget;
+  if (t.R < 1 || t.R > 8 || t.R > (H > 0 ? H : 1) || (t.AB != 1 && t.AB != 2) || t.AB * t.R * Cout > 512) return false;
+  if (t.KC < 16 || t.KC % 16 || Cin % t.KC || ((t.KC / 8) & (t.KC / 8 - 1)) || t.KC > 128 || t.SA < 2 ||
+      t.SA > kMaxAStages)
+    return false;
+  if (resident_of(Cin, t) ? chunks_of(Cin, t) > kMaxWStages : (t.NS < 2 || t.NS > kMaxWStages)) return false;
+  return tc_smem(Cin, Cout, t) <= kSmemBudget;
 }
 
-// Candidate tilings for the autotuner: for each rows-per-CTA R, the largest channel chunk
-// that fits with a 3-stage ring, and with a ring of all of the chunk's 9 taps.
+// Candidate tilings for the autotuner: rows per tile (the most, half of it; one or two
+// accumulators), input stages 2..4, weights resident or in a ring of 2 or 3 chunk stages,
+// each with the largest chunk that fits.
 int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut) {
   int n = 0;
-  for (int R = 1; R <= 8 && n < maxOut; R++) {
-    if (R * Cout > 512 || R > H) break;
-    for (int NS : {3, 9}) {
-      for (int KC = Cin; KC >= 16; KC -= 16) {
-        if (Cin % KC) continue;
-        TcTiling t;
-        t.R = R; t.KC = KC; t.NS = NS;
-        if (tc_smem(R, KC, Cout, NS) <= kSmemBudget) {
-          bool dup = false;
-          for (int i = 0; i < n; i++) dup = dup || (out[i].R == R && out[i].KC == KC && out[i].NS == NS);
-          if (!dup && n < maxOut) out[n++] = t;
-          break;
-        }
+  auto add = [&](int R, int AB, int SA, int NS) {
+    if (R < 1 || n >= maxOut) return;
+    const int KC = fit_kc(Cin, Cout, R, SA, NS, AB);
+    if (!KC) return;
+    TcTiling t;
+    t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
+    t.NS = NS > 0 ? NS : Cin / KC;
+    if (!conv3x3_tc_valid(Cin, Cout, H, t)) return;
+    for (int i = 0; i < n; i++)
+      if (out[i].R == t.R && out[i].KC == t.KC && out[i].SA == t.SA && out[i].AB == t.AB && out[i].NS == t.NS) return;
+    out[n++] = t;
+  };
+  const int h = H > 0 ? H : 1;
+  for (int AB = 2; AB >= 1; AB--) {
+    const int Rm = rows_max(Cout, AB, h);
+    for (int R : {Rm, Rm / 2})
+      for (int SA = 2; SA <= kMaxAStages; SA++) {
+        if ((size_t)18 * Cin * Cout <= kSmemBudget) add(R, AB, SA, 0);
+        add(R, AB, SA, 2);
+        add(R, AB, SA, 3);
       }
-    }
   }
   return n;
 }
 
 bool conv3x3_tc_supported(int Cin, int Cout) {
-  return Cin % 16 == 0 && Cin >= 16 && Cout % 16 == 0 && Cout >= 16 && Cout <= 256 && tc_tiling(Cin, Cout, 1).R > 0 &&
-         encode_fn() != nullptr;
+  return Cin % 16 == 0 && Cin >= 16 && Cout % 16 == 0 && Cout >= 16 && Cout <= 256 && tc_tiling(Cin, Cout, 1).R > 0;
 }
 
 void conv3x3_tc_policy(int policy) { g_tcPolicy = policy == 1 ? 1 : 0; }
@@ -401,28 +575,25 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   if (!conv3x3_tc_supported(Cin, Cout) || N <= 0 || H <= 0 || W <= 0) return (int)cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(Wu) & 15)) return (int)cudaErrorInvalidValue;
   TcTiling tl = tc_tiling(Cin, Cout, H);
-  if (tiling && tiling->R > 0) {
-    if (!conv3x3_tc_valid(Cin, Cout, H, *tiling)) return (int)cudaErrorInvalidValue;
-    tl = *tiling;
-  }
-  if (tl.R == 0) return (int)cudaErrorInvalidValue;
-  CUtensorMap map;
-  const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
-  const cuuint64_t strides[3] = {(cuuint64_t)Cin * 2, (cuuint64_t)W * Cin * 2, (cuuint64_t)H * W * Cin * 2};
-  const cuuint32_t box[4] = {8, (cuuint32_t)kHalo, 1, 1};
-  const cuuint32_t es[4] = {1, 1, 1, 1};
-  const CUresult cr = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(X), dims, strides, box,
-                                  es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (cr != CUDA_SUCCESS) return (int)cudaErrorInvalidValue;
-  const size_t smem = tc_smem(tl.R, tl.KC, Cout, tl.NS) + 1024;
+  if (tiling && tiling->R > 0) tl = *tiling;
+  if (!conv3x3_tc_valid(Cin, Cout, H, tl)) return (int)cudaErrorInvalidValue;
+  ConvArgs a;
+  a.X = (const bf16 *)X; a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
+  a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout; a.relu = relu; a.outF32 = outF32;
+  a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB;
+  a.resident = resident_of(Cin, tl) ? 1 : 0;
+  a.tmemCols = tmem_cols_for(tl.AB * tl.R * Cout);
+  a.tilesX = (W + kTM - 1) / kTM;
+  a.tilesY = (H + tl.R - 1) / tl.R;
+  a.tiles = N * a.tilesX * a.tilesY;
+  size_t smem = tc_smem(Cin, Cout, tl) + 1024;
+  if (smem < kSmemFloor) smem = kSmemFloor;
   cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSmemBudget + 1024));
   if (e != cudaSuccess) return (int)e;
-  const int tilesX = (W + kTM - 1) / kTM, tilesY = (H + tl.R - 1) / tl.R;
-  conv3x3_tc_kernel<<<(unsigned)(N * tilesY * tilesX), 128, smem, (cudaStream_t)stream>>>(
-      map, (const bf16 *)Wu, bias, Y, N, H, W, Cin, Cout, relu, outF32, tmem_cols_for(tl.R * Cout), tl.R, tl.KC, tl.NS,
-      err);
+  int grid = num_sms();
+  if (grid > a.tiles) grid = a.tiles;
+  conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(a);
   return (int)cudaGetLastError();
 }
 
