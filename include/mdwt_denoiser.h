@@ -52,9 +52,9 @@ mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *d_features, 
                                      int h, int w, float lr, double *loss, void *stream);
 
 /* Convolution path: 1 (default) = tcgen05 tensor-core kernels (persistent, warp-specialised;
- * one TMEM accumulator per tile, the most input stages that fit) wherever the layer shapes
- * allow; 2 = the same kernels with two accumulators, so a tile's epilogue overlaps the
- * next tile's MMAs; 0 = the mma.sync kernels everywhere.  The tiling is process-wide. */
+ * two TMEM accumulators, so a tile's epilogue overlaps the next tile's MMAs) wherever the
+ * layer shapes allow; 2 = the same kernels with one accumulator and the most rows per tile;
+ * 0 = the mma.sync kernels everywhere.  The tiling is process-wide. */
 mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode);
 /* Autotuner of the tensor-core convolutions for one input shape: every layer's candidate
  * tilings (output rows per CTA, input-channel chunk, weight stages) are timed on the real

@@ -2,10 +2,10 @@
 //
 // Implicit GEMM: D[128 pixels of one image row][Cout] = sum over the 9 taps of
 // A_tap[128 pixels][Cin] x B_tap[Cin][Cout].
-//   * A: the input rows y - 1 .. y + R of a tile, pixels x0 - 1 .. x0 + 128, staged by
-//     coalesced 16-byte cp.async copies of the NHWC rows (out-of-image pixels -- padding,
-//     row ends -- zero-filled); tap (dy, dx) of output row r reads input row r + dy from
-//     pixel dx on;
+//   * A: the input rows y - 1 .. y + R of a tile, pixels x0 - 1 .. x0 + 128, one TMA load
+//     per group of 8 channels (a box of 8 channels x 130 pixels x R + 2 rows of the NHWC
+//     tensor map; out-of-image pixels -- padding, row ends -- are zero-filled by the TMA
+//     unit); tap (dy, dx) of output row r reads input row r + dy from pixel dx on;
 //   * B: the weights, pre-arranged on the device in the operand layout [tap][ci / 8][co][8]
 //     and bulk-copied (once per launch when they fit, else per chunk and tap).
 // Both sit in shared memory in the K-major, no-swizzle core-matrix layout (8 rows x 16
@@ -13,9 +13,12 @@
 // kind::f16: BF16 inputs, FP32 accumulator in tensor memory, M = 128, N = Cout, K = 16.
 // The kernel is persistent and warp-specialised (producer, MMA issuer, epilogue warps; see
 // conv3x3_tc_kernel).  Every mbarrier wait is bounded; a wait that gives up sets *err.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <mutex>
 
 
 #include "mdwt_nn.h"
@@ -58,6 +61,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   }
 }
 
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                    smem_u32(dst)),
@@ -101,12 +112,12 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
 
 constexpr int kMaxAStages = 4;            // input (A) ring depth
 constexpr int kMaxWStages = 16;           // weight stages (one input-channel chunk x 9 taps each)
-constexpr int kLoadWarps = 4;             // input producers
 constexpr int kEpiWarps = 8;              // epilogue warps (two per TMEM lane quarter)
-constexpr int kWarpW = kLoadWarps;        // weight producer and TMEM allocator
-constexpr int kWarpMma = kLoadWarps + 1;  // MMA issuer
-constexpr int kWarpEpi = kLoadWarps + 2;  // first epilogue warp
-constexpr int kThreads = 32 * (kLoadWarps + 2 + kEpiWarps);
+constexpr int kWarpA = 0;                 // input producer (TMA)
+constexpr int kWarpW = 1;                 // weight producer and TMEM allocator
+constexpr int kWarpMma = 2;               // MMA issuer
+constexpr int kWarpEpi = 3;               // first epilogue warp
+constexpr int kThreads = 32 * (3 + kEpiWarps);
 constexpr int kHalo = kTM + 2;            // input pixels per row segment (one-pixel halo each side)
 constexpr uint32_t kRowBytes = kHalo * 16;   // one row segment of 8 channels: 2080 B
 
@@ -115,7 +126,6 @@ constexpr uint32_t kRowBytes = kHalo * 16;   // one row segment of 8 channels: 2
 __host__ __device__ inline uint32_t a_slot(int R) { return ((uint32_t)(R + 2) * kRowBytes + 127u) & ~127u; }
 
 struct ConvArgs {
-  const bf16 *X;
   const bf16 *Wu;
   const float *bias;
   void *Y;
@@ -142,23 +152,23 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // input-channel chunk (KC channels) the R + 2 input rows with a one-pixel halo are staged
 // once; the horizontal taps read the same rows from a descriptor start one pixel (16 B)
 // further, the vertical taps from the neighbouring rows.
-//   warps 0-3: input producers -- 16-byte cp.async of the NHWC rows into the core-matrix
-//     layout, each thread one channel group (zero stores outside the image), a ring of SA
-//     stages; each thread waits for its own copies, fences them to the async proxy and
-//     arrives on the stage's barrier;
-//   warp 4, lane 0: weights -- by bulk copies into stages of one input-channel chunk x 9
+//   warp 0, lane 0: input producer -- per tile and chunk one TMA load per 8-channel group
+//     (a box of 8 channels x 130 pixels x R + 2 rows of the NHWC tensor map, zero-filled
+//     outside the image) into a ring of SA stages;
+//   warp 1, lane 0: weights -- by bulk copies into stages of one input-channel chunk x 9
 //     taps, once for the whole launch (resident) or per tile and chunk through a ring of
 //     NS stages;
-//   warp 5: MMA issuer -- the warp runs the loops, lane 0 issues: per chunk and output
+//   warp 2: MMA issuer -- the warp runs the loops, lane 0 issues: per chunk and output
 //     row, 9 taps x KC / 16 tcgen05.mma (M = 128 pixels, N = Cout, K = 16) into that
 //     row's accumulator back to back; AB accumulators of R x Cout TMEM columns alternate
 //     between tiles, so the epilogue of one tile overlaps the MMAs of the next;
-//   warps 6-13: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
+//   warps 3-10: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
 //     BF16 or FP32 stores; the two warps of a quarter take alternate rows.
 // Every wait is bounded; a role that gives up sets *err and the CTA abort flag, the others
-// leave their loops, every producer waits for its copies in flight and the MMA issuer for
+// leave their loops, the producers wait for their copies in flight and the MMA issuer for
 // its MMAs before the tensor memory is freed.
-__global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const ConvArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap mapX,
+                                                                  const ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t aFull[kMaxAStages], aEmpty[kMaxAStages], wFull[kMaxWStages], wEmpty[kMaxWStages];
   __shared__ __align__(8) uint64_t wRes, accFull[2], accEmpty[2], mmaDone;
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const ConvArgs 
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < a.SA; i++) {
-      mbar_init(&aFull[i], 32 * kLoadWarps);
+      mbar_init(&aFull[i], 1);
       mbar_init(&aEmpty[i], 1);
     }
     for (int i = 0; i < kMaxWStages; i++) {
@@ -206,61 +216,32 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const ConvArgs 
     atomicExch(a.err, 1);
   };
 
-  if (warp < kLoadWarps) {
-    // ------------------------------------------------------------------ input producers
-    // thread p copies channel group g = p % G of pixels p / G, p / G + 128 / G, ... of every
-    // row (G divides 128); out-of-image pixels are zero stores
-    const int p = threadIdx.x;   // 0 .. 32 * kLoadWarps - 1
-    const int g = p % G, pxStep = (32 * kLoadWarps) / G;
-    const int px0 = p / G;
-    bool ok = true;
-    uint32_t gA = 0;
-    int pending = -1;   // stage whose copies are issued but not yet signalled
-    for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
-      const int tx = t % a.tilesX, ty = (t / a.tilesX) % a.tilesY, n = t / (a.tilesX * a.tilesY);
-      const int x0 = tx * kTM, y0 = ty * R;
-      for (int kc = 0; kc < chunks; kc++) {
-        const uint32_t s = gA % (uint32_t)a.SA, use = gA / (uint32_t)a.SA;
-        int go = 1;
-        if (lane == 0) go = abortFlag ? 0 : ((use == 0 || mbar_wait_ab(&aEmpty[s], (use - 1) & 1u, &abortFlag)) ? 1 : 2);
-        go = __shfl_sync(0xffffffffu, go, 0);
-        if (go != 1) {
-          if (go == 2 && lane == 0) fail();
-          ok = false;
-          break;
+  if (warp == kWarpA) {
+    if (lane == 0) {
+      // ---------------------------------------------------------------- input producer
+      // per tile and chunk, one TMA load per 8-channel group: a box of 8 channels x 130
+      // pixels x R + 2 rows (zero-filled outside the image) into the group's slot
+      bool ok = true;
+      uint32_t gA = 0;
+      for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
+        if (abortFlag) break;
+        const int tx = t % a.tilesX, ty = (t / a.tilesX) % a.tilesY, n = t / (a.tilesX * a.tilesY);
+        const int x0 = tx * kTM, y0 = ty * R;
+        for (int kc = 0; kc < chunks; kc++) {
+          const uint32_t s = gA % (uint32_t)a.SA, use = gA / (uint32_t)a.SA;
+          if (use > 0 && !mbar_wait_ab(&aEmpty[s], (use - 1) & 1u, &abortFlag)) { ok = false; break; }
+          mbar_expect_tx(&aFull[s], (uint32_t)G * (R + 2) * kRowBytes);
+          for (int g = 0; g < G; g++)
+            tma_load_4d(bufA + s * stageA + g * slot, &mapX, kc * a.KC + g * 8, x0 - 1, y0 - 1, n, &aFull[s]);
+          gA++;
         }
-        const uint32_t dst0 = smem_u32(bufA) + s * stageA + (uint32_t)g * slot;
-        const bf16 *src0 = a.X + (size_t)n * a.H * a.W * a.Cin + (size_t)kc * a.KC + g * 8;
-        for (int r = 0; r < R + 2; r++) {
-          const int gy = y0 - 1 + r;
-          const bool rowIn = gy >= 0 && gy < a.H;
-          const bf16 *rowSrc = src0 + (size_t)(rowIn ? gy : 0) * a.W * a.Cin;
-          const uint32_t rowDst = dst0 + (uint32_t)r * kRowBytes;
-          for (int px = px0; px < kHalo; px += pxStep) {
-            const int gx = x0 - 1 + px;
-            const uint32_t dst = rowDst + (uint32_t)px * 16;
-            if (rowIn && gx >= 0 && gx < a.W)
-              asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(rowSrc + (size_t)gx * a.Cin)
-                           : "memory");
-            else
-              asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};\n" ::"r"(dst), "r"(0u) : "memory");
-          }
-        }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        if (pending >= 0) {   // the previous stage: its copies done, visible to the tensor cores
-          asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-          mbar_arrive(&aFull[pending]);
-        }
-        pending = (int)s;
-        gA++;
       }
+      if (!ok) fail();
+      // wait for every load issued (the last one into each stage may still be in flight)
+      for (uint32_t st = 0; st < (uint32_t)a.SA; st++)
+        if (gA > st && !mbar_wait(&aFull[st], ((gA - 1 - st) / (uint32_t)a.SA) & 1u)) fail();
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    if (pending >= 0) {
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      mbar_arrive(&aFull[pending]);
-    }
+    __syncwarp();
   } else if (warp == kWarpW) {
     if (lane == 0) {
       // ---------------------------------------------------------------- weights
@@ -440,6 +421,23 @@ __global__ void umma_weights_kernel(const bf16 *Wf, bf16 *Wu, int Cin, int Cout)
   }
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  });
+  return fn;
+}
+
 int tmem_cols_for(int cols) {
   int c = 32;
   while (c < cols) c <<= 1;
@@ -459,13 +457,13 @@ size_t tc_smem(int Cin, int Cout, const TcTiling &t) {
   return (size_t)t.SA * (t.KC / 8) * a_slot(t.R) + (size_t)stages * 18 * t.KC * Cout;
 }
 
-int g_tcPolicy = 1;   // 1: one accumulator, most input stages (measured fastest); 0: two accumulators
+int g_tcPolicy = 1;   // 1: two accumulators (the epilogue overlaps the next tile); 0: one
 
 // Largest input-channel chunk (a divisor of Cin, multiple of 16) that fits the budget with
 // SA input stages and the given weight staging (NS = 0: resident); 0 when none does.
 int fit_kc(int Cin, int Cout, int R, int SA, int NS, int AB) {
   for (int KC = Cin; KC >= 16; KC -= 16) {
-    if (Cin % KC || ((KC / 8) & (KC / 8 - 1))) continue;
+    if (Cin % KC) continue;
     TcTiling t;
     t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
     t.NS = NS > 0 ? NS : Cin / KC;
@@ -484,11 +482,11 @@ int rows_max(int Cout, int AB, int H) {
 
 // Default tiling: the most rows that AB accumulators allow, resident weights when they
 // fit kResidentMax (else a ring of 2 chunk stages), the most input stages (4 .. 2) that fit
-// with the largest chunk.  Policy 1 uses one accumulator (the MMAs of a tile start after
-// the previous epilogue), policy 0 two.
+// with the largest chunk.  Policy 1 uses two accumulators (the epilogue of a tile overlaps
+// the MMAs of the next), policy 0 one.
 TcTiling tc_tiling(int Cin, int Cout, int H) {
   TcTiling t;
-  const int AB = g_tcPolicy == 1 ? 1 : 2;
+  const int AB = g_tcPolicy == 1 ? 2 : 1;
   const int R = rows_max(Cout, AB, H > 0 ? H : 1);
   if (R < 1) return t;
   const bool res = (size_t)18 * Cin * Cout <= kResidentMax;
@@ -519,9 +517,7 @@ int num_sms() {
 
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t) {
   if (t.R < 1 || t.R > 8 || t.R > (H > 0 ? H : 1) || (t.AB != 1 && t.AB != 2) || t.AB * t.R * Cout > 512) return false;
-  if (t.KC < 16 || t.KC % 16 || Cin % t.KC || ((t.KC / 8) & (t.KC / 8 - 1)) || t.KC > 128 || t.SA < 2 ||
-      t.SA > kMaxAStages)
-    return false;
+  if (t.KC < 16 || t.KC % 16 || Cin % t.KC || t.SA < 2 || t.SA > kMaxAStages) return false;
   if (resident_of(Cin, t) ? chunks_of(Cin, t) > kMaxWStages : (t.NS < 2 || t.NS > kMaxWStages)) return false;
   return tc_smem(Cin, Cout, t) <= kSmemBudget;
 }
@@ -557,7 +553,8 @@ int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut) {
 }
 
 bool conv3x3_tc_supported(int Cin, int Cout) {
-  return Cin % 16 == 0 && Cin >= 16 && Cout % 16 == 0 && Cout >= 16 && Cout <= 256 && tc_tiling(Cin, Cout, 1).R > 0;
+  return Cin % 16 == 0 && Cin >= 16 && Cout % 16 == 0 && Cout >= 16 && Cout <= 256 && tc_tiling(Cin, Cout, 1).R > 0 &&
+         encode_fn() != nullptr;
 }
 
 void conv3x3_tc_policy(int policy) { g_tcPolicy = policy == 1 ? 1 : 0; }
@@ -577,8 +574,17 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   TcTiling tl = tc_tiling(Cin, Cout, H);
   if (tiling && tiling->R > 0) tl = *tiling;
   if (!conv3x3_tc_valid(Cin, Cout, H, tl)) return (int)cudaErrorInvalidValue;
+  CUtensorMap map;
+  const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+  const cuuint64_t strides[3] = {(cuuint64_t)Cin * 2, (cuuint64_t)W * Cin * 2, (cuuint64_t)H * W * Cin * 2};
+  const cuuint32_t box[4] = {8, (cuuint32_t)kHalo, (cuuint32_t)(tl.R + 2), 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const CUresult cr = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(X), dims, strides, box,
+                                  es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return (int)cudaErrorInvalidValue;
   ConvArgs a;
-  a.X = (const bf16 *)X; a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
+  a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
   a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout; a.relu = relu; a.outF32 = outF32;
   a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB;
   a.resident = resident_of(Cin, tl) ? 1 : 0;
@@ -593,7 +599,7 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   if (e != cudaSuccess) return (int)e;
   int grid = num_sms();
   if (grid > a.tiles) grid = a.tiles;
-  conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(a);
+  conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(map, a);
   return (int)cudaGetLastError();
 }
 
