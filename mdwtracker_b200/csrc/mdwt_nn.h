@@ -38,7 +38,7 @@ int adam(float *Wm, float *mW, float *vW, const float *gW, void *Wf, void *Wd, i
 int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int numSMs, void *stream);
 
 // tcgen05 path (mdwt_nn_tc.cu): the same convolution with the weights in the operand
-// layout Wu[tap][ci / 8][co][8] (umma_weights); *err is set when a bounded wait gave up.
+// layout Wu[dx][ci / 8][dy][co][8] (umma_weights); *err is set when a bounded wait gave up.
 // A tcgen05 convolution tiling: R output rows per tile (x 128 pixels), input channels in
 // chunks of KC, SA input stages, AB accumulators in tensor memory (2: the epilogue of one
 // tile overlaps the MMAs of the next), NS weight stages (NS >= 9 x chunks keeps all the

@@ -6,8 +6,9 @@
 //     per group of 8 channels (a box of 8 channels x 130 pixels x R + 2 rows of the NHWC
 //     tensor map; out-of-image pixels -- padding, row ends -- are zero-filled by the TMA
 //     unit); tap (dy, dx) of output row r reads input row r + dy from pixel dx on;
-//   * B: the weights, pre-arranged on the device in the operand layout [tap][ci / 8][co][8]
-//     and bulk-copied (once per launch when they fit, else per chunk and tap).
+//   * B: the weights, pre-arranged on the device in the operand layout
+//     [dx][ci / 8][dy][co][8] and bulk-copied (once per launch when they fit, else per
+//     tile and chunk).
 // Both sit in shared memory in the K-major, no-swizzle core-matrix layout (8 rows x 16
 // bytes per core matrix; 8-row groups 128 B apart, K groups LBO apart).  tcgen05.mma
 // kind::f16: BF16 inputs, FP32 accumulator in tensor memory, M = 128, N = Cout, K = 16.
@@ -110,6 +111,15 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
+// store 16 zero columns of this warp's 32 TMEM lanes
+__device__ __forceinline__ void tmem_zero16(uint32_t taddr) {
+  const uint32_t z = 0;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};\n" ::"r"(taddr),
+      "r"(z)
+      : "memory");
+}
+
 constexpr int kMaxAStages = 4;            // input (A) ring depth
 constexpr int kMaxWStages = 16;           // weight stages (one input-channel chunk x 9 taps each)
 constexpr int kEpiWarps = 8;              // epilogue warps (two per TMEM lane quarter)
@@ -158,12 +168,15 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 //   warp 1, lane 0: weights -- by bulk copies into stages of one input-channel chunk x 9
 //     taps, once for the whole launch (resident) or per tile and chunk through a ring of
 //     NS stages;
-//   warp 2: MMA issuer -- the warp runs the loops, lane 0 issues: per chunk and output
-//     row, 9 taps x KC / 16 tcgen05.mma (M = 128 pixels, N = Cout, K = 16) into that
-//     row's accumulator back to back; AB accumulators of R x Cout TMEM columns alternate
-//     between tiles, so the epilogue of one tile overlaps the MMAs of the next;
+//   warp 2: MMA issuer -- the warp runs the loops, one elected lane issues tcgen05.mma
+//     (M = 128 pixels, K = 16): for Cout <= 85 one MMA per staged input row, horizontal
+//     tap and K step covers the three vertical taps (N = 3 Cout, the three output rows'
+//     accumulators being adjacent in TMEM), else one MMA per tap (N = Cout); AB
+//     accumulators of R x Cout TMEM columns alternate between tiles, so the epilogue of
+//     one tile overlaps the MMAs of the next;
 //   warps 3-10: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
-//     BF16 or FP32 stores; the two warps of a quarter take alternate rows.
+//     BF16 or FP32 stores, then zero the columns read (the MMAs only accumulate); the two
+//     warps of a quarter take alternate rows.
 // Every wait is bounded; a role that gives up sets *err and the CTA abort flag, the others
 // leave their loops, the producers wait for their copies in flight and the MMA issuer for
 // its MMAs before the tensor memory is freed.
@@ -245,15 +258,15 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
   } else if (warp == kWarpW) {
     if (lane == 0) {
       // ---------------------------------------------------------------- weights
-      // stage = one input-channel chunk, all 9 taps: [tap][G][Cout][8]; resident weights
+      // stage = one input-channel chunk, all 9 taps: [dx][G][dy][Cout][8]; resident weights
       // fill one stage per chunk once, streamed weights cycle NS stages per tile and chunk
       bool ok = true;
       uint32_t gW = 0;
       auto loadChunk = [&](uint32_t st, int kc) {
         mbar_expect_tx(&wFull[st], wStageBytes);
-        for (int tap = 0; tap < 9; tap++)
-          bulk_load(bufW + (size_t)st * wStageBytes + (size_t)tap * tapChunkBytes,
-                    a.Wu + ((size_t)tap * Gtot + (size_t)kc * G) * Cout * 8, tapChunkBytes, &wFull[st]);
+        for (int dx = 0; dx < 3; dx++)
+          bulk_load(bufW + (size_t)st * wStageBytes + (size_t)dx * 3 * tapChunkBytes,
+                    a.Wu + ((size_t)dx * Gtot + (size_t)kc * G) * 3 * Cout * 8, 3 * tapChunkBytes, &wFull[st]);
       };
       if (a.resident) {
         for (int kc = 0; kc < chunks; kc++) loadChunk((uint32_t)kc, kc);
@@ -285,19 +298,29 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
       return __shfl_sync(0xffffffffu, okw, 0) != 0;
     };
     bool ok = true;
-    const uint32_t idesc = instr_desc(kTM, Cout);
+    // Accumulator of output row r: TMEM columns c(r) = (R - 1 - r) Cout of the tile's buffer
+    // (descending), zeroed by the epilogue; every MMA accumulates.  Stacked (3 Cout <= 256):
+    // staged input row j, horizontal tap dx and K step k feed output rows j - dy for the
+    // valid vertical taps dy in [d0, d1] with ONE MMA: B = the weights of (dx, dy = d0..d1)
+    // (contiguous rows), N = (d1 - d0 + 1) Cout, D at c(j - d0).  Otherwise one MMA per
+    // tap (N = Cout) into c(r).
+    const bool stacked = 3 * Cout <= 256;
+    const uint32_t idesc1 = instr_desc(kTM, Cout), idesc2 = stacked ? instr_desc(kTM, 2 * Cout) : 0u,
+                   idesc3 = stacked ? instr_desc(kTM, 3 * Cout) : 0u;
     const uint32_t hi = smem_desc_hi(128);
     // descriptor low words; offsets in 16-byte units are added to them
     const uint32_t aLo0 = smem_desc_lo(smem_u32(bufA), slot);
-    const uint32_t bLo0 = smem_desc_lo(smem_u32(bufW), (uint32_t)Cout * 16);
-    const uint32_t rowStep = kRowBytes >> 4, aKStep = (2 * slot) >> 4, bKStep = 2u * Cout;
-    const uint32_t stageAU = stageA >> 4, wStageU = wStageBytes >> 4, tapU = tapChunkBytes >> 4;
+    const uint32_t bLo0 = smem_desc_lo(smem_u32(bufW), (uint32_t)Cout * 48);   // K groups of [dy][Cout][8]
+    const uint32_t rowStep = kRowBytes >> 4, aKStep = (2 * slot) >> 4, bKStep = 6u * Cout;
+    const uint32_t stageAU = stageA >> 4, wStageU = wStageBytes >> 4, dxU = (3 * tapChunkBytes) >> 4;
+    const uint32_t dyU = (uint32_t)Cout;   // one vertical tap's Cout rows, 16-byte units
     const int nk = a.KC / 16;
     uint32_t gA = 0, gW = 0;
     int it = 0;
     for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x, it++) {
       const uint32_t ab = (uint32_t)(it % a.AB), use = (uint32_t)(it / a.AB);
-      if (use > 0 && !warpWait(&accEmpty[ab], (use - 1) & 1u)) { ok = false; break; }
+      // the epilogue has read and zeroed this accumulator (phase 0: the initial zeroing)
+      if (!warpWait(&accEmpty[ab], use & 1u)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;\n");
       const uint32_t dBase = tmem + ab * (uint32_t)(R * Cout);
       for (int kc = 0; kc < chunks; kc++) {
@@ -307,15 +330,27 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
         if (!warpWait(&aFull[s], (gA / (uint32_t)a.SA) & 1u) || !warpWait(&wFull[sw], pw)) { ok = false; break; }
         asm volatile("tcgen05.fence::after_thread_sync;\n");
         const uint32_t aSt = aLo0 + s * stageAU, wSt = bLo0 + sw * wStageU;
-        uint32_t d = dBase, aRow = aSt;
-        for (int r = 0; r < R; r++, d += (uint32_t)Cout, aRow += rowStep) {
-          uint32_t aK = aRow, bK = wSt;
-          for (int k = 0; k < nk; k++, aK += aKStep, bK += bKStep) {
-            umma_f16(d, aK, bK, hi, idesc, (kc > 0 || k > 0) ? 1u : 0u);
+        if (stacked) {
+          for (int j = 0; j < R + 2; j++) {
+            const int d0 = j - R + 1 > 0 ? j - R + 1 : 0, d1 = j < 2 ? j : 2;
+            const uint32_t id = d1 == d0 ? idesc1 : (d1 - d0 == 1 ? idesc2 : idesc3);
+            const uint32_t d = dBase + (uint32_t)((R - 1 - (j - d0)) * Cout);
+            uint32_t aK = aSt + (uint32_t)j * rowStep, bK = wSt + (uint32_t)d0 * dyU;
+            for (int k = 0; k < nk; k++, aK += aKStep, bK += bKStep) {
 #pragma unroll
-            for (int tap = 1; tap < 9; tap++)
-              umma_f16(d, aK + (uint32_t)(tap / 3) * rowStep + (uint32_t)(tap % 3), bK + (uint32_t)tap * tapU, hi,
-                       idesc, 1u);
+              for (int dx = 0; dx < 3; dx++) umma_f16(d, aK + (uint32_t)dx, bK + (uint32_t)dx * dxU, hi, id, 1u);
+            }
+          }
+        } else {
+          uint32_t d = dBase + (uint32_t)((R - 1) * Cout), aRow = aSt;
+          for (int r = 0; r < R; r++, d -= (uint32_t)Cout, aRow += rowStep) {
+            uint32_t aK = aRow, bK = wSt;
+            for (int k = 0; k < nk; k++, aK += aKStep, bK += bKStep) {
+#pragma unroll
+              for (int tap = 0; tap < 9; tap++)
+                umma_f16(d, aK + (uint32_t)(tap / 3) * rowStep + (uint32_t)(tap % 3),
+                         bK + (uint32_t)(tap % 3) * dxU + (uint32_t)(tap / 3) * dyU, hi, idesc1, 1u);
+            }
           }
         }
         if (lane == 0) {
@@ -341,6 +376,16 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     const int qd = warp & 3, half = (warp - kWarpEpi) >> 2;
     bool ok = true;
     int it = 0;
+    // zero this warp's rows of every accumulator buffer once, then hand them to the MMA warp
+    for (int ab = 0; ab < a.AB; ab++) {
+      const uint32_t zBase = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(ab * R * Cout);
+      for (int r = half; r < R; r += 2)
+        for (int c0 = 0; c0 < Cout; c0 += 16) tmem_zero16(zBase + (uint32_t)(r * Cout + c0));
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;\n");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accEmpty[ab]);
+    }
     for (int t = blockIdx.x; t < a.tiles; t += gridDim.x, it++) {
       int go = 1;
       const uint32_t ab = (uint32_t)(it % a.AB), use = (uint32_t)(it / a.AB);
@@ -366,8 +411,9 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
               : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
                 "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]),
                 "=r"(v32[14]), "=r"(v32[15])
-              : "r"(tBase + (uint32_t)(r * Cout + c0)));
+              : "r"(tBase + (uint32_t)((R - 1 - r) * Cout + c0)));
           asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          tmem_zero16(tBase + (uint32_t)((R - 1 - r) * Cout + c0));   // ready for the next tile
           if (!valid) continue;
           float v[16];
 #pragma unroll
@@ -395,6 +441,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
           }
         }
       }
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;\n");
       __syncwarp();
       if (lane == 0) mbar_arrive(&accEmpty[ab]);
@@ -409,7 +456,9 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
   }
 }
 
-// weights [tap][co][ci] (forward layout) -> operand layout [tap][ci / 8][co][8]
+// weights [tap][co][ci] (forward layout, tap = 3 dy + dx) -> operand layout
+// [dx][ci / 8][dy][co][8]: for one horizontal tap and 8 input channels the three vertical
+// taps' Cout rows are contiguous, so one MMA can take all three (N = 3 Cout)
 __global__ void umma_weights_kernel(const bf16 *Wf, bf16 *Wu, int Cin, int Cout) {
   const size_t n = (size_t)9 * Cin * Cout;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -417,7 +466,8 @@ __global__ void umma_weights_kernel(const bf16 *Wf, bf16 *Wu, int Cin, int Cout)
     const size_t r = i / Cin;
     const int co = (int)(r % Cout);
     const int tap = (int)(r / Cout);
-    Wu[(((size_t)tap * (Cin / 8) + ci / 8) * Cout + co) * 8 + (ci & 7)] = Wf[i];
+    const int dy = tap / 3, dx = tap % 3;
+    Wu[((((size_t)dx * (Cin / 8) + ci / 8) * 3 + dy) * Cout + co) * 8 + (ci & 7)] = Wf[i];
   }
 }
 
