@@ -145,17 +145,40 @@ class ClockSampler:
         self.proc = None
         self.path = os.path.join("/tmp", f"mdwt_clocks_{os.getpid()}.csv")
 
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return f.read().splitlines()
+        except OSError:
+            return []
+
     def start(self):
+        """Start sampling every 20 ms and return once the first sample is written; samples
+        before mark() are not counted."""
+        self.mark_at = 0
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_id), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.perf_counter()
+        while not self._lines() and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.mark()
+
+    def mark(self):
+        """The timed region starts: later samples are the ones counted."""
+        self.mark_at = len(self._lines())
 
     def stop(self):
         if self.proc is None:
             return None
+        # the sample that covers the end of the timed region (at most one interval later)
+        t0 = time.perf_counter()
+        while len(self._lines()) <= self.mark_at and time.perf_counter() - t0 < 0.5 and self.proc.poll() is None:
+            time.sleep(0.005)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -163,7 +186,7 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in self._lines()[self.mark_at:]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -214,7 +237,9 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     r = sc.setup(Renderer(device_index))
     w, h = sc.resolution
     r.setSpp(1)
-    tuned = r.autotuneSchedule(frames=2)   # the tracker schedule for this scene (plain and denoised)
+    # the tracker schedule for this scene, tuned on the 8-frame launches that make up the
+    # plain accumulation (the denoised path's single frame is insensitive to it)
+    tuned = r.autotuneSchedule(frames=8)
     t0 = time.perf_counter()
     coarse = r.expectedImage(4, 0.5)
     ref = r.expectedImage(8, 0.25)          # stays on the device for accumRmse
@@ -472,6 +497,10 @@ def main():
         if world > 1:
             dist.barrier()
 
+    # clock sampler: started before the warm-up (its start-up then lies outside the timed
+    # region); only the samples written after mark() are counted
+    clocks = ClockSampler(torch.cuda.get_device_properties(dev).uuid and f"GPU-{torch.cuda.get_device_properties(dev).uuid}")
+    clocks.start()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             flush.fill_(1)
@@ -484,11 +513,10 @@ def main():
     except Exception:
         timed = False
     launches0 = r.renderInfo()[0]
-    clocks = ClockSampler(torch.cuda.get_device_properties(dev).uuid and f"GPU-{torch.cuda.get_device_properties(dev).uuid}")
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize(dev)
-    clocks.start()
+    clocks.mark()
     trace_ms = []
     with torch.cuda.stream(stream):
         for k in range(args.steps):

@@ -1601,11 +1601,13 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
   CK(cudaEventCreate(&e1), "event");
   mdwt_status s = MDWT_OK;
   double bestMs = 1e300;
+  // a candidate renders `frames` frames as one multi-frame launch sequence (the shape
+  // of an accumulation loop), after a warm-up of the same
   auto trial = [&](double *ms) -> mdwt_status {
-    mdwt_status st = mdwt_render(c, nullptr);   // warm-up
+    mdwt_status st = mdwt_render_frames(c, frames, nullptr);   // warm-up
     if (st) return st;
     cudaEventRecord(e0, c->stream);
-    for (int f = 0; f < frames && !st; f++) st = mdwt_render(c, nullptr);
+    st = mdwt_render_frames(c, frames, nullptr);
     cudaEventRecord(e1, c->stream);
     cudaEventSynchronize(e1);
     float m = 0.f;

@@ -151,11 +151,11 @@ def evaluate(r, den, spps, frame_base=3_000_000):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--pairs", type=int, default=4000)
     ap.add_argument("--res", type=int, default=128)
-    ap.add_argument("--spp", type=int, nargs="+", default=[4, 8, 16, 32, 64])
+    ap.add_argument("--spp", type=int, nargs="+", default=[1, 2, 4, 8, 16, 32])
     ap.add_argument("--target-spp", type=int, default=1024)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=16000)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=7)
