@@ -264,30 +264,31 @@ __global__ void relu_bwd_kernel(bf16 *dY, const bf16 *Y, size_t n8) {
   }
 }
 
-__global__ void avgpool2_kernel(const bf16 *X, bf16 *Y, int N, int H, int W, int C) {
-  const int Ho = H / 2, Wo = W / 2, G = C / 8;
-  const size_t n = (size_t)N * Ho * Wo * G;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int g = (int)(i % G);
-    size_t r = i / G;
-    const int x = (int)(r % Wo);
-    r /= Wo;
-    const int y = (int)(r % Ho);
-    const int b = (int)(r / Ho);
-    const uint4 *src = reinterpret_cast<const uint4 *>(X);
-    const size_t base = (((size_t)b * H + 2 * y) * W + 2 * x) * G + g;
-    float a[8], t[8];
-    unpack8(src[base], a);
-    unpack8(src[base + G], t);
+// rows of the output (N x Ho) along grid y, a row's elements (Wo x G uint4) along grid x;
+// e / G by a multiply-high with the reciprocal `mg` (exact for e * G < 2^32)
+__global__ void avgpool2_kernel(const bf16 *X, bf16 *Y, int N, int H, int W, int C, unsigned mg) {
+  const unsigned G = (unsigned)C / 8, Ho = (unsigned)H / 2, Wo = (unsigned)W / 2, perRow = Wo * G;
+  const uint4 *src = reinterpret_cast<const uint4 *>(X);
+  for (unsigned row = blockIdx.y; row < (unsigned)N * Ho; row += gridDim.y) {
+    const unsigned b = row / Ho, yo = row - b * Ho;
+    const uint4 *in = src + (size_t)(b * (unsigned)H + 2 * yo) * (unsigned)W * G;
+    uint4 *out = reinterpret_cast<uint4 *>(Y) + (size_t)row * perRow;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < perRow; e += gridDim.x * blockDim.x) {
+      const unsigned xo = G == 1 ? e : __umulhi(e, mg), g = e - xo * G;
+      const size_t base = (size_t)(2 * xo) * G + g;
+      float a[8], t[8];
+      unpack8(in[base], a);
+      unpack8(in[base + G], t);
 #pragma unroll
-    for (int j = 0; j < 8; j++) a[j] += t[j];
-    unpack8(src[base + (size_t)W * G], t);
+      for (int j = 0; j < 8; j++) a[j] += t[j];
+      unpack8(in[base + (size_t)W * G], t);
 #pragma unroll
-    for (int j = 0; j < 8; j++) a[j] += t[j];
-    unpack8(src[base + (size_t)W * G + G], t);
+      for (int j = 0; j < 8; j++) a[j] += t[j];
+      unpack8(in[base + (size_t)W * G + G], t);
 #pragma unroll
-    for (int j = 0; j < 8; j++) a[j] = 0.25f * (a[j] + t[j]);
-    reinterpret_cast<uint4 *>(Y)[i] = pack8(a);
+      for (int j = 0; j < 8; j++) a[j] = 0.25f * (a[j] + t[j]);
+      out[e] = pack8(a);
+    }
   }
 }
 
@@ -312,19 +313,21 @@ __global__ void avgpool2_bwd_add_kernel(const bf16 *dY, bf16 *dX, int N, int H, 
 }
 
 // out[y][x] = concat(coarse[y/2][x/2] (Cu channels), skip[y][x] (Cs channels))
-__global__ void up2_concat_kernel(const bf16 *coarse, const bf16 *skip, bf16 *out, int N, int H, int W, int Cu, int Cs) {
-  const int Gu = Cu / 8, Gs = Cs / 8, G = Gu + Gs;
-  const size_t n = (size_t)N * H * W * G;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int g = (int)(i % G);
-    const size_t pix = i / G;
-    const int x = (int)(pix % W);
-    const size_t r = pix / W;
-    const int y = (int)(r % H);
-    const int b = (int)(r / H);
-    reinterpret_cast<uint4 *>(out)[i] =
-        g < Gu ? reinterpret_cast<const uint4 *>(coarse)[(((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * Gu + g]
-               : reinterpret_cast<const uint4 *>(skip)[pix * Gs + (g - Gu)];
+// rows of the output (N x H) along grid y, a row's elements (W x (Gu + Gs) uint4) along
+// grid x; e / G by a multiply-high with the reciprocal `mg`
+__global__ void up2_concat_kernel(const bf16 *coarse, const bf16 *skip, bf16 *out, int N, int H, int W, int Cu, int Cs,
+                                  unsigned mg) {
+  const unsigned Gu = (unsigned)Cu / 8, Gs = (unsigned)Cs / 8, G = Gu + Gs, perRow = (unsigned)W * G;
+  const unsigned Hc = (unsigned)H / 2, Wc = (unsigned)W / 2;
+  for (unsigned row = blockIdx.y; row < (unsigned)N * (unsigned)H; row += gridDim.y) {
+    const unsigned b = row / (unsigned)H, y = row - b * (unsigned)H;
+    const uint4 *crow = reinterpret_cast<const uint4 *>(coarse) + (size_t)(b * Hc + y / 2) * Wc * Gu;
+    const uint4 *srow = reinterpret_cast<const uint4 *>(skip) + (size_t)row * (unsigned)W * Gs;
+    uint4 *orow = reinterpret_cast<uint4 *>(out) + (size_t)row * perRow;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < perRow; e += gridDim.x * blockDim.x) {
+      const unsigned x = G == 1 ? e : __umulhi(e, mg), g = e - x * G;
+      orow[e] = g < Gu ? crow[(x >> 1) * Gu + g] : srow[x * Gs + (g - Gu)];
+    }
   }
 }
 
@@ -381,27 +384,26 @@ __global__ void bias_grad_kernel(const bf16 *dY, float *db, size_t P, int C) {
 // Feature packing: fp32 [N][H][W][16] (tracker features) -> bf16 network input
 // [N][Hp][Wp][16], zero outside H x W; one pixel per thread.
 __global__ void pack_features_kernel(const float *F, bf16 *X, int N, int H, int W, int Hp, int Wp) {
-  const size_t n = (size_t)N * Hp * Wp;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % Wp);
-    const size_t r = i / Wp;
-    const int y = (int)(r % Hp);
-    const int b = (int)(r / Hp);
-    float f[16];
-    if (y < H && x < W) {
-      const float4 *src = reinterpret_cast<const float4 *>(F) + (((size_t)b * H + y) * W + x) * 4;
+  for (unsigned row = blockIdx.y; row < (unsigned)N * (unsigned)Hp; row += gridDim.y) {
+    const unsigned b = row / (unsigned)Hp, y = row - b * (unsigned)Hp;
+    for (unsigned x = blockIdx.x * blockDim.x + threadIdx.x; x < (unsigned)Wp; x += gridDim.x * blockDim.x) {
+      const size_t i = (size_t)row * (unsigned)Wp + x;
+      float f[16];
+      if (y < (unsigned)H && x < (unsigned)W) {
+        const float4 *src = reinterpret_cast<const float4 *>(F) + ((size_t)(b * (unsigned)H + y) * (unsigned)W + x) * 4;
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const float4 v = src[j];
-        f[4 * j] = v.x; f[4 * j + 1] = v.y; f[4 * j + 2] = v.z; f[4 * j + 3] = v.w;
+        for (int j = 0; j < 4; j++) {
+          const float4 v = src[j];
+          f[4 * j] = v.x; f[4 * j + 1] = v.y; f[4 * j + 2] = v.z; f[4 * j + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++) f[j] = 0.f;
       }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 16; j++) f[j] = 0.f;
+      uint4 *dst = reinterpret_cast<uint4 *>(X) + 2 * i;
+      dst[0] = pack8(f);
+      dst[1] = pack8(f + 8);
     }
-    uint4 *dst = reinterpret_cast<uint4 *>(X) + 2 * i;
-    dst[0] = pack8(f);
-    dst[1] = pack8(f + 8);
   }
 }
 
@@ -411,21 +413,20 @@ __global__ void pack_features_kernel(const float *F, bf16 *X, int N, int H, int 
 __global__ void residual_out_kernel(const float *F, const float *O, int Co, float *out4, const float *target4,
                                     bf16 *dO, double *lossSum, int N, int H, int W, int Hp, int Wp, float invCount) {
   double s = 0.0;
-  const size_t P = (size_t)N * H * W;
-  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(p % W);
-    const size_t r = p / W;
-    const int y = (int)(r % H);
-    const int b = (int)(r / H);
-    const size_t q = ((size_t)b * Hp + y) * Wp + x;
-    float o[3];
-    for (int k = 0; k < 3; k++) o[k] = F[p * 16 + k] + O[q * Co + k];
-    if (out4) *reinterpret_cast<float4 *>(out4 + 4 * p) = make_float4(o[0], o[1], o[2], 1.f);
-    if (target4) {
-      for (int k = 0; k < 3; k++) {
-        const float d = o[k] - target4[4 * p + k];
-        s += (double)d * d;
-        dO[q * Co + k] = __float2bfloat16(2.f * d * invCount);
+  for (unsigned row = blockIdx.y; row < (unsigned)N * (unsigned)H; row += gridDim.y) {
+    const unsigned b = row / (unsigned)H, y = row - b * (unsigned)H;
+    for (unsigned x = blockIdx.x * blockDim.x + threadIdx.x; x < (unsigned)W; x += gridDim.x * blockDim.x) {
+      const size_t p = (size_t)row * (unsigned)W + x;
+      const size_t q = (size_t)(b * (unsigned)Hp + y) * (unsigned)Wp + x;
+      float o[3];
+      for (int k = 0; k < 3; k++) o[k] = F[p * 16 + k] + O[q * Co + k];
+      if (out4) *reinterpret_cast<float4 *>(out4 + 4 * p) = make_float4(o[0], o[1], o[2], 1.f);
+      if (target4) {
+        for (int k = 0; k < 3; k++) {
+          const float d = o[k] - target4[4 * p + k];
+          s += (double)d * d;
+          dO[q * Co + k] = __float2bfloat16(2.f * d * invCount);
+        }
       }
     }
   }
@@ -481,6 +482,17 @@ __global__ void weight_copies_kernel(const float *Wm, bf16 *Wf, bf16 *Wd, int Ci
   }
 }
 
+// grid of row kernels: blocks along x cover a row of perRow elements (256 threads each),
+// grid y takes rows (the kernels loop when there are more than 65535)
+inline dim3 row_grid(size_t rows, size_t perRow) {
+  size_t gx = (perRow + 255) / 256;
+  if (gx > 64) gx = 64;
+  size_t gy = rows < 65535 ? rows : 65535;
+  return dim3((unsigned)(gx ? gx : 1), (unsigned)(gy ? gy : 1));
+}
+// reciprocal for e / d as __umulhi(e, m), exact while e * d < 2^32 (d = 1 is handled apart)
+inline unsigned div_magic(unsigned d) { return d <= 1 ? 0u : (unsigned)(((1ull << 32) + d - 1) / d); }
+
 inline unsigned grid_for(size_t n, int numSMs) {
   size_t g = (n + 255) / 256;
   const size_t cap = (size_t)numSMs * 16;
@@ -517,9 +529,10 @@ int relu_bwd(void *dY, const void *Y, size_t n, int numSMs, void *stream) {
 }
 
 int avgpool2(const void *X, void *Y, int N, int H, int W, int C, int numSMs, void *stream) {
-  if (C % 8) return (int)cudaErrorInvalidValue;
-  avgpool2_kernel<<<grid_for((size_t)N * (H / 2) * (W / 2) * (C / 8), numSMs), 256, 0, (cudaStream_t)stream>>>(
-      (const bf16 *)X, (bf16 *)Y, N, H, W, C);
+  (void)numSMs;
+  if (C % 8 || (size_t)(W / 2) * (C / 8) * (C / 8) >= (1ull << 32)) return (int)cudaErrorInvalidValue;
+  avgpool2_kernel<<<row_grid((size_t)N * (H / 2), (size_t)(W / 2) * (C / 8)), 256, 0, (cudaStream_t)stream>>>(
+      (const bf16 *)X, (bf16 *)Y, N, H, W, C, div_magic((unsigned)C / 8));
   return (int)cudaGetLastError();
 }
 
@@ -532,9 +545,11 @@ int avgpool2_bwd_add(const void *dY, void *dX, int N, int H, int W, int C, int n
 
 int up2_concat(const void *coarse, const void *skip, void *out, int N, int H, int W, int Cu, int Cs, int numSMs,
                void *stream) {
-  if (Cu % 8 || Cs % 8) return (int)cudaErrorInvalidValue;
-  up2_concat_kernel<<<grid_for((size_t)N * H * W * ((Cu + Cs) / 8), numSMs), 256, 0, (cudaStream_t)stream>>>(
-      (const bf16 *)coarse, (const bf16 *)skip, (bf16 *)out, N, H, W, Cu, Cs);
+  (void)numSMs;
+  const size_t G = (size_t)(Cu + Cs) / 8;
+  if (Cu % 8 || Cs % 8 || (size_t)W * G * G >= (1ull << 32)) return (int)cudaErrorInvalidValue;
+  up2_concat_kernel<<<row_grid((size_t)N * H, (size_t)W * G), 256, 0, (cudaStream_t)stream>>>(
+      (const bf16 *)coarse, (const bf16 *)skip, (bf16 *)out, N, H, W, Cu, Cs, div_magic((unsigned)G));
   return (int)cudaGetLastError();
 }
 
@@ -554,14 +569,16 @@ int bias_grad(const void *dY, float *db, size_t P, int C, int numSMs, void *stre
 }
 
 int pack_features(const float *F, void *X, int N, int H, int W, int Hp, int Wp, int numSMs, void *stream) {
-  pack_features_kernel<<<grid_for((size_t)N * Hp * Wp, numSMs), 256, 0, (cudaStream_t)stream>>>(F, (bf16 *)X, N, H, W,
-                                                                                                Hp, Wp);
+  (void)numSMs;
+  pack_features_kernel<<<row_grid((size_t)N * Hp, (size_t)Wp), 256, 0, (cudaStream_t)stream>>>(F, (bf16 *)X, N, H, W, Hp,
+                                                                                               Wp);
   return (int)cudaGetLastError();
 }
 
 int residual_out(const float *F, const float *O, int Co, float *out4, const float *target4, void *dO, double *lossSum,
                  int N, int H, int W, int Hp, int Wp, float invCount, int numSMs, void *stream) {
-  residual_out_kernel<<<grid_for((size_t)N * H * W, numSMs), 256, 0, (cudaStream_t)stream>>>(
+  (void)numSMs;
+  residual_out_kernel<<<row_grid((size_t)N * H, (size_t)W), 256, 0, (cudaStream_t)stream>>>(
       F, O, Co, out4, target4, (bf16 *)dO, lossSum, N, H, W, Hp, Wp, invCount);
   return (int)cudaGetLastError();
 }
