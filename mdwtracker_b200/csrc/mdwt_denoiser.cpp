@@ -428,8 +428,8 @@ mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode) {
 // Time every candidate tiling of one convolution on its real operands; keep the fastest.
 static mdwt_status tune_one(mdwt_denoiser *d, int cin, int cout, const void *x, const void *w, const float *bias, void *y,
                             int N, int H, int W, int relu, int f32, mdwt::nn::TcTiling *best, cudaStream_t st) {
-  mdwt::nn::TcTiling cand[32];
-  const int nc = mdwt::nn::conv3x3_tc_candidates(cin, cout, H, cand, 32);
+  mdwt::nn::TcTiling cand[64];
+  const int nc = mdwt::nn::conv3x3_tc_candidates(cin, cout, H, cand, 64);
   cudaEvent_t e0, e1;
   DCK(cudaEventCreate(&e0), "event");
   DCK(cudaEventCreate(&e1), "event");

@@ -43,8 +43,9 @@ int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int nu
 // chunks of KC, SA input stages, AB accumulators in tensor memory (2: the epilogue of one
 // tile overlaps the MMAs of the next), NS weight stages (NS >= 9 x chunks keeps all the
 // weights resident for the launch).
+// ST = 1 stacks the three vertical taps into one MMA (N = 3 Cout; needs 3 Cout <= 256).
 struct TcTiling {
-  int R = 0, KC = 0, NS = 0, SA = 0, AB = 0;
+  int R = 0, KC = 0, NS = 0, SA = 0, AB = 0, ST = 0;
 };
 bool conv3x3_tc_supported(int Cin, int Cout);
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t);

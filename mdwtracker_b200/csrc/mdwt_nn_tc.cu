@@ -141,7 +141,7 @@ struct ConvArgs {
   void *Y;
   int *err;
   int N, H, W, Cin, Cout, relu, outF32;
-  int R, KC, NS, SA, AB, resident, tmemCols, tilesX, tilesY, tiles;
+  int R, KC, NS, SA, AB, ST, resident, tmemCols, tilesX, tilesY, tiles;
 };
 
 // bounded wait that also gives up once another role of the CTA has aborted
@@ -169,9 +169,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 //     taps, once for the whole launch (resident) or per tile and chunk through a ring of
 //     NS stages;
 //   warp 2: MMA issuer -- the warp runs the loops, one elected lane issues tcgen05.mma
-//     (M = 128 pixels, K = 16): for Cout <= 85 one MMA per staged input row, horizontal
-//     tap and K step covers the three vertical taps (N = 3 Cout, the three output rows'
-//     accumulators being adjacent in TMEM), else one MMA per tap (N = Cout); AB
+//     (M = 128 pixels, K = 16): stacked (ST, Cout <= 85), one MMA per staged input row,
+//     horizontal tap and K step covers the three vertical taps (N = 3 Cout, the three
+//     output rows' accumulators being adjacent in TMEM), else one MMA per tap (N = Cout); AB
 //     accumulators of R x Cout TMEM columns alternate between tiles, so the epilogue of
 //     one tile overlaps the MMAs of the next;
 //   warps 3-10: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     // valid vertical taps dy in [d0, d1] with ONE MMA: B = the weights of (dx, dy = d0..d1)
     // (contiguous rows), N = (d1 - d0 + 1) Cout, D at c(j - d0).  Otherwise one MMA per
     // tap (N = Cout) into c(r).
-    const bool stacked = 3 * Cout <= 256;
+    const bool stacked = a.ST != 0;
     const uint32_t idesc1 = instr_desc(kTM, Cout), idesc2 = stacked ? instr_desc(kTM, 2 * Cout) : 0u,
                    idesc3 = stacked ? instr_desc(kTM, 3 * Cout) : 0u;
     const uint32_t hi = smem_desc_hi(128);
@@ -545,6 +545,7 @@ TcTiling tc_tiling(int Cin, int Cout, int H) {
     if (KC) {
       t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
       t.NS = res ? Cin / KC : 2;
+      t.ST = 3 * Cout <= 256 ? 1 : 0;
       return t;
     }
   }
@@ -568,37 +569,41 @@ int num_sms() {
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t) {
   if (t.R < 1 || t.R > 8 || t.R > (H > 0 ? H : 1) || (t.AB != 1 && t.AB != 2) || t.AB * t.R * Cout > 512) return false;
   if (t.KC < 16 || t.KC % 16 || Cin % t.KC || t.SA < 2 || t.SA > kMaxAStages) return false;
+  if (t.ST && 3 * Cout > 256) return false;
   if (resident_of(Cin, t) ? chunks_of(Cin, t) > kMaxWStages : (t.NS < 2 || t.NS > kMaxWStages)) return false;
   return tc_smem(Cin, Cout, t) <= kSmemBudget;
 }
 
-// Candidate tilings for the autotuner: rows per tile (the most, half of it; one or two
-// accumulators), input stages 2..4, weights resident or in a ring of 2 or 3 chunk stages,
-// each with the largest chunk that fits.
+// Candidate tilings for the autotuner: stacked vertical taps or not, rows per tile (the
+// most, half of it; one or two accumulators), input stages 2..4, weights resident or in a
+// ring of 2 or 3 chunk stages, each with the largest chunk that fits.
 int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut) {
   int n = 0;
-  auto add = [&](int R, int AB, int SA, int NS) {
+  auto add = [&](int R, int AB, int SA, int NS, int ST) {
     if (R < 1 || n >= maxOut) return;
     const int KC = fit_kc(Cin, Cout, R, SA, NS, AB);
     if (!KC) return;
     TcTiling t;
-    t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
+    t.R = R; t.KC = KC; t.SA = SA; t.AB = AB; t.ST = ST;
     t.NS = NS > 0 ? NS : Cin / KC;
     if (!conv3x3_tc_valid(Cin, Cout, H, t)) return;
     for (int i = 0; i < n; i++)
-      if (out[i].R == t.R && out[i].KC == t.KC && out[i].SA == t.SA && out[i].AB == t.AB && out[i].NS == t.NS) return;
+      if (out[i].R == t.R && out[i].KC == t.KC && out[i].SA == t.SA && out[i].AB == t.AB && out[i].NS == t.NS &&
+          out[i].ST == t.ST)
+        return;
     out[n++] = t;
   };
   const int h = H > 0 ? H : 1;
-  for (int AB = 2; AB >= 1; AB--) {
-    const int Rm = rows_max(Cout, AB, h);
-    for (int R : {Rm, Rm / 2})
-      for (int SA = 2; SA <= kMaxAStages; SA++) {
-        if ((size_t)18 * Cin * Cout <= kSmemBudget) add(R, AB, SA, 0);
-        add(R, AB, SA, 2);
-        add(R, AB, SA, 3);
-      }
-  }
+  for (int ST = 3 * Cout <= 256 ? 1 : 0; ST >= 0; ST--)
+    for (int AB = 2; AB >= 1; AB--) {
+      const int Rm = rows_max(Cout, AB, h);
+      for (int R : {Rm, Rm / 2})
+        for (int SA = 2; SA <= kMaxAStages; SA++) {
+          if ((size_t)18 * Cin * Cout <= kSmemBudget) add(R, AB, SA, 0, ST);
+          add(R, AB, SA, 2, ST);
+          add(R, AB, SA, 3, ST);
+        }
+    }
   return n;
 }
 
@@ -636,7 +641,7 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   ConvArgs a;
   a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
   a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout; a.relu = relu; a.outF32 = outF32;
-  a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB;
+  a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB; a.ST = tl.ST;
   a.resident = resident_of(Cin, tl) ? 1 : 0;
   a.tmemCols = tmem_cols_for(tl.AB * tl.R * Cout);
   a.tilesX = (W + kTM - 1) / kTM;
