@@ -368,6 +368,9 @@ def denoised_time_to_rmse(r, target, stream, spps=(1, 2, 4, 8, 16, 32, 64), reps
     out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
     r.setFeatures(True)
     r.setSpp(1)
+    # this path renders one frame per measurement: the tracker schedule is tuned on single
+    # frames (the plain path's is tuned on its 8-frame launches)
+    single = r.autotuneSchedule(frames=1)
     r.Render(stream.cuda_stream)
     torch.cuda.synchronize()
     den.autotune(r.deviceFeatures(), 1, h, w)   # tensor-core tilings for this frame size
@@ -403,7 +406,8 @@ def denoised_time_to_rmse(r, target, stream, spps=(1, 2, 4, 8, 16, 32, 64), reps
     r.setFeatures(False)
     den.close()
     res = {"weights": os.path.relpath(DENOISER_WEIGHTS, ROOT), "tried": tried,
-           "reached": found is not None}
+           "reached": found is not None,
+           "schedule": {"pool": single[0], "trips": single[1], "by": "mdwt_autotune_schedule, single frames"}}
     if found:
         res.update({"spp": found["spp"], "rmse": found["rmse"], "device_ms": found["render_ms"] + found["denoise_ms"],
                     "render_ms": found["render_ms"], "denoise_ms": found["denoise_ms"]})
