@@ -54,10 +54,11 @@ class Denoiser:
         except Exception:
             pass
 
-    def setTensorCores(self, on, two_ctas: bool = True) -> None:
-        """tcgen05 convolutions (default, tiled for two CTAs per SM; `two_ctas=False`:
-        the most output rows per CTA) or the mma.sync kernels."""
-        self._call("set_tensor_cores", C.c_int((1 if two_ctas else 2) if on else 0))
+    def setTensorCores(self, on, overlap: bool = True) -> None:
+        """tcgen05 convolutions (default: two TMEM accumulators, a tile's epilogue
+        overlapping the next tile's MMAs; `overlap=False`: one accumulator with the most
+        rows per tile) or the mma.sync kernels."""
+        self._call("set_tensor_cores", C.c_int((1 if overlap else 2) if on else 0))
 
     def autotune(self, features, n: int, h: int, w: int, backward: bool = False) -> None:
         """Time the candidate tensor-core tilings of every layer for this input shape."""

@@ -119,9 +119,9 @@ def test_gpu_training_fits_a_fixed_batch():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("two_ctas", [False, True])
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("n,h,w", [(1, 7, 20), (2, 16, 130), (1, 12, 256)])
-def test_tensor_core_and_mma_paths_agree(n, h, w, two_ctas):
+def test_tensor_core_and_mma_paths_agree(n, h, w, overlap):
     """The tcgen05 convolutions (TMA-staged operands, TMEM accumulator) against the
     mma.sync ones: the same BF16 operands and FP32 accumulation in another order."""
     import torch
@@ -132,7 +132,7 @@ def test_tensor_core_and_mma_paths_agree(n, h, w, two_ctas):
     F = torch.from_numpy(_features(rng, n, h, w)).cuda()
     outs = []
     for tc in (False, True):
-        d.setTensorCores(tc, two_ctas)
+        d.setTensorCores(tc, overlap)
         o = torch.empty((n, h, w, 4), dtype=torch.float32, device="cuda")
         d.infer(F, o, n, h, w)
         d.check()
