@@ -136,13 +136,18 @@ bool tuned_for(const mdwt_denoiser *d) {
   return d->tunedN == d->A.N && d->tunedH == d->A.Hp && d->tunedW == d->A.Wp && d->tunedN > 0;
 }
 
-mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st) {
+// res (optional): fuse the residual output into the tensor-core epilogue; *fused tells
+// whether it was (the mma.sync path stores y and leaves the residual to the caller)
+mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st,
+                 const mdwt::nn::TcResidual *res = nullptr, bool *fused = nullptr) {
   const int li = (int)(&l - d->L);
-  if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout))
+  if (fused) *fused = false;
+  if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout)) {
     DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st,
-                              tuned_for(d) ? &d->tileF[li] : nullptr),
+                              tuned_for(d) ? &d->tileF[li] : nullptr, res),
          "conv forward (tcgen05)");
-  else
+    if (fused) *fused = res != nullptr;
+  } else
     DCKI(mdwt::nn::conv3x3_fwd(x, l.Wf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, st), "conv forward");
   return MDWT_OK;
 }
@@ -154,7 +159,10 @@ mdwt_status umma_copies(mdwt_denoiser *d, const Layer &l, void *st) {
   return MDWT_OK;
 }
 
-mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void *st) {
+// out4 (optional, inference): the denoised RGBA, fused into the last layer's epilogue when
+// the tensor-core path runs it (*fused then true)
+mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void *st, float *out4 = nullptr,
+                    bool *fused = nullptr) {
   const int Hp = (H + 3) & ~3, Wp = (W + 3) & ~3;
   mdwt_status s = ensure_acts(d, N, Hp, Wp);
   if (s) return s;
@@ -174,7 +182,9 @@ mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void 
   if ((s = conv(d, d->L[7], A.a4, A.b1, N, H1, W1, false, st))) return s;
   DCKI(mdwt::nn::up2_concat(A.b1, A.s0, A.u0, N, Hp, Wp, 64, 32, S, st), "up+concat");
   if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st))) return s;
-  if ((s = conv(d, d->L[9], A.a5, A.o, N, Hp, Wp, true, st))) return s;
+  mdwt::nn::TcResidual res;
+  res.F = F; res.out4 = out4; res.H = H; res.W = W;
+  if ((s = conv(d, d->L[9], A.a5, A.o, N, Hp, Wp, true, st, out4 ? &res : nullptr, fused))) return s;
   return MDWT_OK;
 }
 
@@ -375,11 +385,13 @@ mdwt_status mdwt_denoiser_get_grads(mdwt_denoiser *d, float *out) {
 mdwt_status mdwt_denoiser_infer(mdwt_denoiser *d, const float *F, float *out, int n, int h, int w, void *stream) {
   if (!d || !F || !out || !dims_ok(n, h, w)) return fail(d, MDWT_ERR_BAD_ARG, "bad denoiser arguments");
   DCK(cudaSetDevice(d->device), "cudaSetDevice");
-  mdwt_status s = forward(d, F, n, h, w, stream);
+  bool fused = false;
+  mdwt_status s = forward(d, F, n, h, w, stream, out, &fused);
   if (s) return s;
-  DCKI(mdwt::nn::residual_out(F, d->A.o, 16, out, nullptr, nullptr, nullptr, n, h, w, d->A.Hp, d->A.Wp, 0.f,
-                              d->numSMs, stream),
-       "output");
+  if (!fused)
+    DCKI(mdwt::nn::residual_out(F, d->A.o, 16, out, nullptr, nullptr, nullptr, n, h, w, d->A.Hp, d->A.Wp, 0.f,
+                                d->numSMs, stream),
+         "output");
   return MDWT_OK;
 }
 

@@ -53,9 +53,18 @@ int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut);
 // Tiling policy: 1 = two accumulators (default), 0 = one accumulator with the most rows.
 void conv3x3_tc_policy(int policy);
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream);
+// Residual output fused into the epilogue (the denoiser's last layer, inference): instead of
+// storing Y, out4[n][y][x] = (F[n][y][x][0..2] + conv[0..2], 1) for y < H, x < W (F has 16
+// floats per pixel; the convolution's H x W may be padded beyond them).
+struct TcResidual {
+  const float *F = nullptr;
+  float *out4 = nullptr;
+  int H = 0, W = 0;
+};
 // tiling: null or R == 0 = the default policy's tiling
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
-               int relu, int outF32, int *err, void *stream, const TcTiling *tiling = nullptr);
+               int relu, int outF32, int *err, void *stream, const TcTiling *tiling = nullptr,
+               const TcResidual *res = nullptr);
 
 }  // namespace nn
 }  // namespace mdwt

@@ -142,6 +142,9 @@ struct ConvArgs {
   int *err;
   int N, H, W, Cin, Cout, relu, outF32;
   int R, KC, NS, SA, AB, ST, resident, tmemCols, tilesX, tilesY, tiles;
+  const float *resF;   // residual output (TcResidual) when resOut != nullptr
+  float *resOut;
+  int resH, resW;
 };
 
 // bounded wait that also gives up once another role of the CTA has aborted
@@ -175,8 +178,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 //     accumulators of R x Cout TMEM columns alternate between tiles, so the epilogue of
 //     one tile overlaps the MMAs of the next;
 //   warps 3-10: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
-//     BF16 or FP32 stores, then zero the columns read (the MMAs only accumulate); the two
-//     warps of a quarter take alternate rows.
+//     BF16 or FP32 stores (or the fused residual output), then zero the columns read (the
+//     MMAs only accumulate); the two warps of a quarter take alternate rows.
 // Every wait is bounded; a role that gives up sets *err and the CTA abort flag, the others
 // leave their loops, the producers wait for their copies in flight and the MMA issuer for
 // its MMAs before the tensor memory is freed.
@@ -414,6 +417,21 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
               : "r"(tBase + (uint32_t)((R - 1 - r) * Cout + c0)));
           asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
           tmem_zero16(tBase + (uint32_t)((R - 1 - r) * Cout + c0));   // ready for the next tile
+          if (a.resOut) {   // fused residual output: channels 0..2 of the real image only
+            if (c0 == 0 && y < a.resH && px < a.resW) {
+              const size_t q = ((size_t)n * a.resH + y) * a.resW + px;
+              float o[3];
+#pragma unroll
+              for (int j = 0; j < 3; j++) {
+                float f = __uint_as_float(v32[j]);
+                if (a.bias) f += a.bias[j];
+                if (a.relu) f = fmaxf(f, 0.f);
+                o[j] = a.resF[q * 16 + j] + f;
+              }
+              reinterpret_cast<float4 *>(a.resOut)[q] = make_float4(o[0], o[1], o[2], 1.f);
+            }
+            continue;
+          }
           if (!valid) continue;
           float v[16];
 #pragma unroll
@@ -623,7 +641,7 @@ int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *
 }
 
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
-               int relu, int outF32, int *err, void *stream, const TcTiling *tiling) {
+               int relu, int outF32, int *err, void *stream, const TcTiling *tiling, const TcResidual *res) {
   if (!conv3x3_tc_supported(Cin, Cout) || N <= 0 || H <= 0 || W <= 0) return (int)cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(Wu) & 15)) return (int)cudaErrorInvalidValue;
   TcTiling tl = tc_tiling(Cin, Cout, H);
@@ -642,6 +660,11 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
   a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout; a.relu = relu; a.outF32 = outF32;
   a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB; a.ST = tl.ST;
+  a.resF = res ? res->F : nullptr;
+  a.resOut = res ? res->out4 : nullptr;
+  a.resH = res ? res->H : 0;
+  a.resW = res ? res->W : 0;
+  if (res && (!res->F || !res->out4 || res->H > H || res->W > W || Cout < 3)) return (int)cudaErrorInvalidValue;
   a.resident = resident_of(Cin, tl) ? 1 : 0;
   a.tmemCols = tmem_cols_for(tl.AB * tl.R * Cout);
   a.tilesX = (W + kTM - 1) / kTM;
