@@ -138,13 +138,17 @@ bool tuned_for(const mdwt_denoiser *d) {
 
 // res (optional): fuse the residual output into the tensor-core epilogue; *fused tells
 // whether it was (the mma.sync path stores y and leaves the residual to the caller)
+// pool (optional): also the 2x2 average pooling of y, fused into the tensor-core epilogue
+// when its tiling allows (*pooled tells; otherwise the caller pools)
 mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st,
-                 const mdwt::nn::TcResidual *res = nullptr, bool *fused = nullptr) {
+                 const mdwt::nn::TcResidual *res = nullptr, bool *fused = nullptr, void *pool = nullptr,
+                 bool *pooled = nullptr) {
   const int li = (int)(&l - d->L);
   if (fused) *fused = false;
+  if (pooled) *pooled = false;
   if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout)) {
     DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st,
-                              tuned_for(d) ? &d->tileF[li] : nullptr, res),
+                              tuned_for(d) ? &d->tileF[li] : nullptr, res, pool, pooled),
          "conv forward (tcgen05)");
     if (fused) *fused = res != nullptr;
   } else
@@ -170,11 +174,12 @@ mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void 
   const int H1 = Hp / 2, W1 = Wp / 2, H2 = Hp / 4, W2 = Wp / 4, S = d->numSMs;
   DCKI(mdwt::nn::pack_features(F, A.x0, N, H, W, Hp, Wp, S, st), "pack features");
   if ((s = conv(d, d->L[0], A.x0, A.a1, N, Hp, Wp, false, st))) return s;
-  if ((s = conv(d, d->L[1], A.a1, A.s0, N, Hp, Wp, false, st))) return s;
-  DCKI(mdwt::nn::avgpool2(A.s0, A.p0, N, Hp, Wp, 32, S, st), "pool");
+  bool pooled = false;
+  if ((s = conv(d, d->L[1], A.a1, A.s0, N, Hp, Wp, false, st, nullptr, nullptr, A.p0, &pooled))) return s;
+  if (!pooled) DCKI(mdwt::nn::avgpool2(A.s0, A.p0, N, Hp, Wp, 32, S, st), "pool");
   if ((s = conv(d, d->L[2], A.p0, A.a2, N, H1, W1, false, st))) return s;
-  if ((s = conv(d, d->L[3], A.a2, A.s1, N, H1, W1, false, st))) return s;
-  DCKI(mdwt::nn::avgpool2(A.s1, A.p1, N, H1, W1, 64, S, st), "pool");
+  if ((s = conv(d, d->L[3], A.a2, A.s1, N, H1, W1, false, st, nullptr, nullptr, A.p1, &pooled))) return s;
+  if (!pooled) DCKI(mdwt::nn::avgpool2(A.s1, A.p1, N, H1, W1, 64, S, st), "pool");
   if ((s = conv(d, d->L[4], A.p1, A.a3, N, H2, W2, false, st))) return s;
   if ((s = conv(d, d->L[5], A.a3, A.b2, N, H2, W2, false, st))) return s;
   DCKI(mdwt::nn::up2_concat(A.b2, A.s1, A.u1, N, H1, W1, 128, 64, S, st), "up+concat");

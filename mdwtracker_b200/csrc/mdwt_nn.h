@@ -61,10 +61,12 @@ struct TcResidual {
   float *out4 = nullptr;
   int H = 0, W = 0;
 };
-// tiling: null or R == 0 = the default policy's tiling
+// tiling: null or R == 0 = the default policy's tiling.  poolOut (optional, BF16 output
+// only): also write the 2x2 average pooling of Y there, as avgpool2 would, when the tiling
+// allows it (an even row count per tile); *pooled tells whether it did.
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
                int relu, int outF32, int *err, void *stream, const TcTiling *tiling = nullptr,
-               const TcResidual *res = nullptr);
+               const TcResidual *res = nullptr, void *poolOut = nullptr, bool *pooled = nullptr);
 
 }  // namespace nn
 }  // namespace mdwt

@@ -143,6 +143,7 @@ struct ConvArgs {
   int N, H, W, Cin, Cout, relu, outF32;
   int R, KC, NS, SA, AB, ST, resident, tmemCols, tilesX, tilesY, tiles;
   const float *resF;   // residual output (TcResidual) when resOut != nullptr
+  void *poolOut;       // fused 2x2 average pooling of Y (BF16) when non-null
   float *resOut;
   int resH, resW;
 };
@@ -178,8 +179,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 //     accumulators of R x Cout TMEM columns alternate between tiles, so the epilogue of
 //     one tile overlaps the MMAs of the next;
 //   warps 3-10: epilogue -- tcgen05.ld of their lane quarter (32 pixels), bias, ReLU,
-//     BF16 or FP32 stores (or the fused residual output), then zero the columns read (the
-//     MMAs only accumulate); the two warps of a quarter take alternate rows.
+//     BF16 or FP32 stores (or the fused residual output; or also the fused 2x2 average
+//     pooling, rows then taken in pairs), then zero the columns read (the MMAs only
+//     accumulate); the two warps of a quarter take alternate rows.
 // Every wait is bounded; a role that gives up sets *err and the CTA abort flag, the others
 // leave their loops, the producers wait for their copies in flight and the MMA issuer for
 // its MMAs before the tensor memory is freed.
@@ -403,7 +405,74 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
       const int px = tx * kTM + qd * 32 + lane;
       const bool validX = px < a.W;
       const uint32_t tBase = tmem + ((uint32_t)(qd * 32) << 16) + ab * (uint32_t)(R * Cout);
-      for (int r = half; r < R; r += 2) {
+      if (a.poolOut) {
+        // fused 2x2 average pooling (R even, H and W even): rows in pairs (2p, 2p + 1), pair p
+        // to warp half p % 2; lanes l and l ^ 1 hold horizontal neighbours.  The pooled value
+        // is formed from the BF16-rounded outputs in the order of the separate pooling kernel.
+        const int Hq = a.H / 2, Wq = a.W / 2;
+        for (int pr = half; pr < R / 2; pr += 2) {
+          const int y = ty * R + 2 * pr;
+          const bool validP = validX && y < a.H;
+          for (int c0 = 0; c0 < Cout; c0 += 16) {
+            float v[2][16];
+#pragma unroll
+            for (int h2 = 0; h2 < 2; h2++) {
+              const uint32_t col = tBase + (uint32_t)((R - 1 - (2 * pr + h2)) * Cout + c0);
+              uint32_t v32[16];
+              asm volatile(
+                  "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                  "[%16];\n"
+                  : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
+                    "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]),
+                    "=r"(v32[13]), "=r"(v32[14]), "=r"(v32[15])
+                  : "r"(col));
+              asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+              tmem_zero16(col);   // ready for the next tile
+              uint4 w[2];
+              uint32_t *wp = reinterpret_cast<uint32_t *>(w);
+#pragma unroll
+              for (int j = 0; j < 8; j++) {
+                float f0 = __uint_as_float(v32[2 * j]), f1 = __uint_as_float(v32[2 * j + 1]);
+                if (a.bias) { f0 += a.bias[c0 + 2 * j]; f1 += a.bias[c0 + 2 * j + 1]; }
+                if (a.relu) { f0 = fmaxf(f0, 0.f); f1 = fmaxf(f1, 0.f); }
+                __nv_bfloat162 b2 = __floats2bfloat162_rn(f0, f1);
+                wp[j] = *reinterpret_cast<uint32_t *>(&b2);
+                v[h2][2 * j] = __low2float(b2);
+                v[h2][2 * j + 1] = __high2float(b2);
+              }
+              if (validP) {   // rows y and y + 1 are both inside (H even)
+                uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(a.Y) +
+                                                     (((size_t)n * a.H + y + h2) * a.W + px) * Cout + c0);
+                o[0] = w[0];
+                o[1] = w[1];
+              }
+            }
+            float q[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+              const float x01 = __shfl_xor_sync(0xffffffffu, v[0][j], 1);
+              const float x11 = __shfl_xor_sync(0xffffffffu, v[1][j], 1);
+              float acc = v[0][j] + x01;
+              acc += v[1][j];
+              q[j] = 0.25f * (acc + x11);
+            }
+            if (validP && (lane & 1) == 0) {
+              uint4 w[2];
+              uint32_t *wp = reinterpret_cast<uint32_t *>(w);
+#pragma unroll
+              for (int j = 0; j < 8; j++) {
+                __nv_bfloat162 b2 = __floats2bfloat162_rn(q[2 * j], q[2 * j + 1]);
+                wp[j] = *reinterpret_cast<uint32_t *>(&b2);
+              }
+              uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(a.poolOut) +
+                                                   (((size_t)n * Hq + y / 2) * Wq + px / 2) * Cout + c0);
+              o[0] = w[0];
+              o[1] = w[1];
+            }
+          }
+        }
+      }
+      for (int r = half; r < R && !a.poolOut; r += 2) {
         const int y = ty * R + r;
         const bool valid = validX && y < a.H;
         const size_t pix = (((size_t)n * a.H + (y < a.H ? y : 0)) * a.W + (validX ? px : 0));
@@ -641,7 +710,9 @@ int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *
 }
 
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
-               int relu, int outF32, int *err, void *stream, const TcTiling *tiling, const TcResidual *res) {
+               int relu, int outF32, int *err, void *stream, const TcTiling *tiling, const TcResidual *res,
+               void *poolOut, bool *pooled) {
+  if (pooled) *pooled = false;
   if (!conv3x3_tc_supported(Cin, Cout) || N <= 0 || H <= 0 || W <= 0) return (int)cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(Wu) & 15)) return (int)cudaErrorInvalidValue;
   TcTiling tl = tc_tiling(Cin, Cout, H);
@@ -665,6 +736,8 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   a.resH = res ? res->H : 0;
   a.resW = res ? res->W : 0;
   if (res && (!res->F || !res->out4 || res->H > H || res->W > W || Cout < 3)) return (int)cudaErrorInvalidValue;
+  const bool fusePool = poolOut && !res && !outF32 && tl.R % 2 == 0 && H % 2 == 0 && W % 2 == 0;
+  a.poolOut = fusePool ? poolOut : nullptr;
   a.resident = resident_of(Cin, tl) ? 1 : 0;
   a.tmemCols = tmem_cols_for(tl.AB * tl.R * Cout);
   a.tilesX = (W + kTM - 1) / kTM;
@@ -678,7 +751,9 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   int grid = num_sms();
   if (grid > a.tiles) grid = a.tiles;
   conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(map, a);
-  return (int)cudaGetLastError();
+  const cudaError_t le = cudaGetLastError();
+  if (le == cudaSuccess && pooled) *pooled = fusePool;
+  return (int)le;
 }
 
 }  // namespace nn
