@@ -63,8 +63,14 @@ mdwt_status mdwt_denoiser_set_tensor_cores(mdwt_denoiser *d, int mode);
  * Synchronous; results do not depend on the tiling beyond FP32 summation order. */
 mdwt_status mdwt_denoiser_autotune(mdwt_denoiser *d, const float *d_features, int n, int h, int w, int backward);
 /* Wait for the denoiser's work; MDWT_ERR_TIMEOUT when a tensor-core kernel's bounded
- * wait for its operands gave up (its output is then invalid). */
+ * wait for its operands gave up (its output is then invalid).  The error is reported once
+ * (the flag is cleared). */
 mdwt_status mdwt_denoiser_check(mdwt_denoiser *d);
+/* Test hook of the failure path (process-wide): the next `launches` tensor-core
+ * convolutions issue no operand loads, so every CTA's bounded wait gives up after about a
+ * second of SM clocks, the kernel exits cleanly and mdwt_denoiser_check reports
+ * MDWT_ERR_TIMEOUT.  No GPU fault is involved.  0 cancels. */
+mdwt_status mdwt_denoiser_test_stall(mdwt_denoiser *d, int launches);
 
 /* Denoise the last frame of a render context (its features must be on) into
  * d_out_rgba [H][W][4] on the context's stream. */

@@ -512,7 +512,16 @@ mdwt_status mdwt_denoiser_check(mdwt_denoiser *d) {
   DCK(cudaDeviceSynchronize(), "sync");
   int e = 0;
   DCK(cudaMemcpy(&e, d->dErr, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-  if (e) return fail(d, MDWT_ERR_TIMEOUT, "a tensor-core convolution gave up waiting for its operands");
+  if (e) {
+    DCK(cudaMemset(d->dErr, 0, sizeof(int)), "error flag");   // reported once
+    return fail(d, MDWT_ERR_TIMEOUT, "a tensor-core convolution gave up waiting for its operands");
+  }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoiser_test_stall(mdwt_denoiser *d, int launches) {
+  if (!d || launches < 0) return MDWT_ERR_BAD_ARG;
+  mdwt::nn::conv3x3_tc_stall_test(launches);
   return MDWT_OK;
 }
 

@@ -52,6 +52,9 @@ bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t);
 int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut);
 // Tiling policy: 1 = two accumulators (default), 0 = one accumulator with the most rows.
 void conv3x3_tc_policy(int policy);
+// Test hook: the next `launches` tensor-core convolutions issue no input loads, so their
+// bounded waits give up and set *err (0 = off).
+void conv3x3_tc_stall_test(int launches);
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream);
 // Residual output fused into the epilogue (the denoiser's last layer, inference): instead of
 // storing Y, out4[n][y][x] = (F[n][y][x][0..2] + conv[0..2], 1) for y < H, x < W (F has 16

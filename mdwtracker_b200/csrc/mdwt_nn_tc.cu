@@ -142,6 +142,7 @@ struct ConvArgs {
   int *err;
   int N, H, W, Cin, Cout, relu, outF32;
   int R, KC, NS, SA, AB, ST, resident, tmemCols, tilesX, tilesY, tiles;
+  int stallTest;       // test hook: the input producer issues nothing (every wait then gives up)
   const float *resF;   // residual output (TcResidual) when resOut != nullptr
   void *poolOut;       // fused 2x2 average pooling of Y (BF16) when non-null
   float *resOut;
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
       // pixels x R + 2 rows (zero-filled outside the image) into the group's slot
       bool ok = true;
       uint32_t gA = 0;
-      for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
+      for (int t = blockIdx.x; t < a.tiles && ok && !a.stallTest; t += gridDim.x) {
         if (abortFlag) break;
         const int tx = t % a.tilesX, ty = (t / a.tilesX) % a.tilesY, n = t / (a.tilesX * a.tilesY);
         const int x0 = tx * kTM, y0 = ty * R;
@@ -594,6 +595,7 @@ size_t tc_smem(int Cin, int Cout, const TcTiling &t) {
   return (size_t)t.SA * (t.KC / 8) * a_slot(t.R) + (size_t)stages * 18 * t.KC * Cout;
 }
 
+int g_tcStall = 0;     // launches left that run with the stall test hook
 int g_tcPolicy = 1;   // 1: two accumulators (the epilogue overlaps the next tile); 0: one
 
 // Largest input-channel chunk (a divisor of Cin, multiple of 16) that fits the budget with
@@ -699,6 +701,8 @@ bool conv3x3_tc_supported(int Cin, int Cout) {
          encode_fn() != nullptr;
 }
 
+void conv3x3_tc_stall_test(int launches) { g_tcStall = launches > 0 ? launches : 0; }
+
 void conv3x3_tc_policy(int policy) { g_tcPolicy = policy == 1 ? 1 : 0; }
 
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream) {
@@ -731,6 +735,8 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
   a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout; a.relu = relu; a.outF32 = outF32;
   a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB; a.ST = tl.ST;
+  a.stallTest = g_tcStall > 0 ? 1 : 0;
+  if (g_tcStall > 0) g_tcStall--;
   a.resF = res ? res->F : nullptr;
   a.resOut = res ? res->out4 : nullptr;
   a.resH = res ? res->H : 0;

@@ -65,8 +65,14 @@ class Denoiser:
         self._call("autotune", _ptr(features), C.c_int(n), C.c_int(h), C.c_int(w), C.c_int(1 if backward else 0))
 
     def check(self) -> None:
-        """Synchronise; raises when a tensor-core kernel's bounded wait gave up."""
+        """Synchronise; raises when a tensor-core kernel's bounded wait gave up (reported
+        once)."""
         self._call("check")
+
+    def testStall(self, launches: int) -> None:
+        """Test hook: the next `launches` tensor-core convolutions issue no operand loads,
+        so their bounded waits give up and check() raises (no GPU fault involved)."""
+        self._call("test_stall", C.c_int(launches))
 
     def params(self) -> np.ndarray:
         out = np.empty(self.numParams(self._lib), np.float32)

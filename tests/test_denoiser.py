@@ -168,3 +168,34 @@ def test_autotuned_tilings_agree_with_mma_path():
     ref = outs[1] - F.cpu().numpy()[..., :3]
     assert np.linalg.norm(outs[0] - outs[1]) < 1e-2 * np.linalg.norm(ref)
     assert np.linalg.norm(grads[0] - grads[1]) < 3e-2 * np.linalg.norm(grads[1])
+
+
+@pytest.mark.gpu
+def test_bounded_wait_gives_up_and_recovers():
+    """The tensor-core convolutions' failure path, without a GPU fault: with the test hook the
+    next convolution issues no operand loads, so its bounded waits give up (about a second
+    of SM clocks), the kernel exits cleanly and check() reports MDWT_ERR_TIMEOUT once; the
+    next inference is exact again."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    from mdwtracker_b200.renderer import MdwtError
+    rng = np.random.default_rng(5)
+    d = Denoiser(0, seed=3)
+    d.setTensorCores(True)
+    n, h, w = 1, 24, 40
+    F = torch.from_numpy(_features(rng, n, h, w)).cuda()
+    ref = torch.empty((n, h, w, 4), dtype=torch.float32, device="cuda")
+    d.infer(F, ref, n, h, w)
+    d.check()
+    d.testStall(1)
+    bad = torch.empty_like(ref)
+    d.infer(F, bad, n, h, w)
+    with pytest.raises(MdwtError) as err:
+        d.check()
+    assert err.value.status == 8   # MDWT_ERR_TIMEOUT
+    d.check()                      # reported once
+    again = torch.empty_like(ref)
+    d.infer(F, again, n, h, w)
+    d.check()
+    assert torch.equal(again, ref)
+    d.close()
