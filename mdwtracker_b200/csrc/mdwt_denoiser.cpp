@@ -140,15 +140,17 @@ bool tuned_for(const mdwt_denoiser *d) {
 // whether it was (the mma.sync path stores y and leaves the residual to the caller)
 // pool (optional): also the 2x2 average pooling of y, fused into the tensor-core epilogue
 // when its tiling allows (*pooled tells; otherwise the caller pools)
+// x2 (optional, tensor-core path only): the input is the concatenation of x (c1 channels)
+// and x2 (the rest)
 mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st,
                  const mdwt::nn::TcResidual *res = nullptr, bool *fused = nullptr, void *pool = nullptr,
-                 bool *pooled = nullptr) {
+                 bool *pooled = nullptr, const void *x2 = nullptr, int c1 = 0) {
   const int li = (int)(&l - d->L);
   if (fused) *fused = false;
   if (pooled) *pooled = false;
   if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout)) {
     DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st,
-                              tuned_for(d) ? &d->tileF[li] : nullptr, res, pool, pooled),
+                              tuned_for(d) ? &d->tileF[li] : nullptr, res, pool, pooled, x2, c1),
          "conv forward (tcgen05)");
     if (fused) *fused = res != nullptr;
   } else
@@ -164,7 +166,10 @@ mdwt_status umma_copies(mdwt_denoiser *d, const Layer &l, void *st) {
 }
 
 // out4 (optional, inference): the denoised RGBA, fused into the last layer's epilogue when
-// the tensor-core path runs it (*fused then true)
+// the tensor-core path runs it (*fused then true).  Without out4 (training) the decoder
+// inputs u1, u0 are the full concatenations the weight gradients read; with it, where the
+// tensor-core path runs the decoder layer, only the upsampled channels are materialised
+// (in the same buffer) and the convolution reads the skip channels from the skip tensor.
 mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void *st, float *out4 = nullptr,
                     bool *fused = nullptr) {
   const int Hp = (H + 3) & ~3, Wp = (W + 3) & ~3;
@@ -182,11 +187,23 @@ mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void 
   if (!pooled) DCKI(mdwt::nn::avgpool2(A.s1, A.p1, N, H1, W1, 64, S, st), "pool");
   if ((s = conv(d, d->L[4], A.p1, A.a3, N, H2, W2, false, st))) return s;
   if ((s = conv(d, d->L[5], A.a3, A.b2, N, H2, W2, false, st))) return s;
-  DCKI(mdwt::nn::up2_concat(A.b2, A.s1, A.u1, N, H1, W1, 128, 64, S, st), "up+concat");
-  if ((s = conv(d, d->L[6], A.u1, A.a4, N, H1, W1, false, st))) return s;
+  const bool split6 = out4 && d->useTC && mdwt::nn::conv3x3_tc_supported(d->L[6].cin, d->L[6].cout);
+  if (split6) {
+    DCKI(mdwt::nn::up2_concat(A.b2, A.b2, A.u1, N, H1, W1, 128, 0, S, st), "upsample");
+    if ((s = conv(d, d->L[6], A.u1, A.a4, N, H1, W1, false, st, nullptr, nullptr, nullptr, nullptr, A.s1, 128))) return s;
+  } else {
+    DCKI(mdwt::nn::up2_concat(A.b2, A.s1, A.u1, N, H1, W1, 128, 64, S, st), "up+concat");
+    if ((s = conv(d, d->L[6], A.u1, A.a4, N, H1, W1, false, st))) return s;
+  }
   if ((s = conv(d, d->L[7], A.a4, A.b1, N, H1, W1, false, st))) return s;
-  DCKI(mdwt::nn::up2_concat(A.b1, A.s0, A.u0, N, Hp, Wp, 64, 32, S, st), "up+concat");
-  if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st))) return s;
+  const bool split8 = out4 && d->useTC && mdwt::nn::conv3x3_tc_supported(d->L[8].cin, d->L[8].cout);
+  if (split8) {
+    DCKI(mdwt::nn::up2_concat(A.b1, A.b1, A.u0, N, Hp, Wp, 64, 0, S, st), "upsample");
+    if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st, nullptr, nullptr, nullptr, nullptr, A.s0, 64))) return s;
+  } else {
+    DCKI(mdwt::nn::up2_concat(A.b1, A.s0, A.u0, N, Hp, Wp, 64, 32, S, st), "up+concat");
+    if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st))) return s;
+  }
   mdwt::nn::TcResidual res;
   res.F = F; res.out4 = out4; res.H = H; res.W = W;
   if ((s = conv(d, d->L[9], A.a5, A.o, N, Hp, Wp, true, st, out4 ? &res : nullptr, fused))) return s;

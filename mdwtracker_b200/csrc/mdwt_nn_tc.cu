@@ -143,6 +143,7 @@ struct ConvArgs {
   int N, H, W, Cin, Cout, relu, outF32;
   int R, KC, NS, SA, AB, ST, resident, tmemCols, tilesX, tilesY, tiles;
   int stallTest;       // test hook: the input producer issues nothing (every wait then gives up)
+  int C1;              // input channels [0, C1) from mapX, [C1, Cin) from mapX2 (C1 = Cin: one tensor)
   const float *resF;   // residual output (TcResidual) when resOut != nullptr
   void *poolOut;       // fused 2x2 average pooling of Y (BF16) when non-null
   float *resOut;
@@ -169,7 +170,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // further, the vertical taps from the neighbouring rows.
 //   warp 0, lane 0: input producer -- per tile and chunk one TMA load per 8-channel group
 //     (a box of 8 channels x 130 pixels x R + 2 rows of the NHWC tensor map, zero-filled
-//     outside the image) into a ring of SA stages;
+//     outside the image; channels from C1 on from a second tensor when the input is the
+//     concatenation of two) into a ring of SA stages;
 //   warp 1, lane 0: weights -- by bulk copies into stages of one input-channel chunk x 9
 //     taps, once for the whole launch (resident) or per tile and chunk through a ring of
 //     NS stages;
@@ -187,6 +189,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // leave their loops, the producers wait for their copies in flight and the MMA issuer for
 // its MMAs before the tensor memory is freed.
 __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap mapX,
+                                                                  const __grid_constant__ CUtensorMap mapX2,
                                                                   const ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t aFull[kMaxAStages], aEmpty[kMaxAStages], wFull[kMaxWStages], wEmpty[kMaxWStages];
@@ -251,7 +254,11 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
           if (use > 0 && !mbar_wait_ab(&aEmpty[s], (use - 1) & 1u, &abortFlag)) { ok = false; break; }
           mbar_expect_tx(&aFull[s], (uint32_t)G * (R + 2) * kRowBytes);
           for (int g = 0; g < G; g++)
-            tma_load_4d(bufA + s * stageA + g * slot, &mapX, kc * a.KC + g * 8, x0 - 1, y0 - 1, n, &aFull[s]);
+          {
+            const int c = kc * a.KC + g * 8;   // the first tensor's channels, then the second's
+            if (c < a.C1) tma_load_4d(bufA + s * stageA + g * slot, &mapX, c, x0 - 1, y0 - 1, n, &aFull[s]);
+            else tma_load_4d(bufA + s * stageA + g * slot, &mapX2, c - a.C1, x0 - 1, y0 - 1, n, &aFull[s]);
+          }
           gA++;
         }
       }
@@ -715,24 +722,34 @@ int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *
 
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
                int relu, int outF32, int *err, void *stream, const TcTiling *tiling, const TcResidual *res,
-               void *poolOut, bool *pooled) {
+               void *poolOut, bool *pooled, const void *X2, int C1) {
   if (pooled) *pooled = false;
+  if (!X2) C1 = Cin;
+  if (C1 <= 0 || C1 > Cin || C1 % 8 || (X2 && (reinterpret_cast<uintptr_t>(X2) & 15)))
+    return (int)cudaErrorInvalidValue;
   if (!conv3x3_tc_supported(Cin, Cout) || N <= 0 || H <= 0 || W <= 0) return (int)cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(Wu) & 15)) return (int)cudaErrorInvalidValue;
   TcTiling tl = tc_tiling(Cin, Cout, H);
   if (tiling && tiling->R > 0) tl = *tiling;
   if (!conv3x3_tc_valid(Cin, Cout, H, tl)) return (int)cudaErrorInvalidValue;
-  CUtensorMap map;
-  const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
-  const cuuint64_t strides[3] = {(cuuint64_t)Cin * 2, (cuuint64_t)W * Cin * 2, (cuuint64_t)H * W * Cin * 2};
-  const cuuint32_t box[4] = {8, (cuuint32_t)kHalo, (cuuint32_t)(tl.R + 2), 1};
-  const cuuint32_t es[4] = {1, 1, 1, 1};
-  const CUresult cr = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(X), dims, strides, box,
-                                  es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (cr != CUDA_SUCCESS) return (int)cudaErrorInvalidValue;
+  // NHWC tensor maps of the input (C1 channels) and, split inputs, of the second input
+  // (Cin - C1 channels); box 8 channels x 130 pixels x R + 2 rows
+  auto encode = [&](CUtensorMap *m, const void *base, int C) -> bool {
+    const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kHalo, (cuuint32_t)(tl.R + 2), 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  CUtensorMap map, map2;
+  if (!encode(&map, X, C1)) return (int)cudaErrorInvalidValue;
+  if (X2 ? !encode(&map2, X2, Cin - C1) : false) return (int)cudaErrorInvalidValue;
+  if (!X2) map2 = map;
   ConvArgs a;
   a.Wu = (const bf16 *)Wu; a.bias = bias; a.Y = Y; a.err = err;
+  a.C1 = C1;
   a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout; a.relu = relu; a.outF32 = outF32;
   a.R = tl.R; a.KC = tl.KC; a.NS = tl.NS; a.SA = tl.SA; a.AB = tl.AB; a.ST = tl.ST;
   a.stallTest = g_tcStall > 0 ? 1 : 0;
@@ -756,7 +773,7 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   if (e != cudaSuccess) return (int)e;
   int grid = num_sms();
   if (grid > a.tiles) grid = a.tiles;
-  conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(map, a);
+  conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(map, map2, a);
   const cudaError_t le = cudaGetLastError();
   if (le == cudaSuccess && pooled) *pooled = fusePool;
   return (int)le;
