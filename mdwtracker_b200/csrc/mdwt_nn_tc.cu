@@ -11,16 +11,17 @@
 //     tile and chunk).
 // Both sit in shared memory in the K-major, no-swizzle core-matrix layout (8 rows x 16
 // bytes per core matrix; 8-row groups 128 B apart, K groups LBO apart).  tcgen05.mma
-// kind::f16: BF16 inputs, FP32 accumulator in tensor memory, M = 128, N = Cout, K = 16.
-// The kernel is persistent and warp-specialised (producer, MMA issuer, epilogue warps; see
-// conv3x3_tc_kernel).  Every mbarrier wait is bounded; a wait that gives up sets *err.
+// kind::f16: BF16 inputs, FP32 accumulator in tensor memory, M = 128 pixels, K = 16, N =
+// Cout (or 3 Cout with the vertical taps stacked).  The kernel is persistent and
+// warp-specialised (producers, MMA issuer, epilogue warps; see conv3x3_tc_kernel); its
+// epilogue can also write the pooled output or the denoiser's residual output.  Every
+// mbarrier wait is bounded; a wait that gives up sets *err.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <mutex>
-
 
 #include "mdwt_nn.h"
 
