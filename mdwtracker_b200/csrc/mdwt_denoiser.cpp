@@ -144,13 +144,13 @@ bool tuned_for(const mdwt_denoiser *d) {
 // and x2 (the rest)
 mdwt_status conv(mdwt_denoiser *d, const Layer &l, const void *x, void *y, int N, int H, int W, bool f32, void *st,
                  const mdwt::nn::TcResidual *res = nullptr, bool *fused = nullptr, void *pool = nullptr,
-                 bool *pooled = nullptr, const void *x2 = nullptr, int c1 = 0) {
+                 bool *pooled = nullptr, const void *x2 = nullptr, int c1 = 0, int pdl = 0) {
   const int li = (int)(&l - d->L);
   if (fused) *fused = false;
   if (pooled) *pooled = false;
   if (d->useTC && mdwt::nn::conv3x3_tc_supported(l.cin, l.cout)) {
     DCKI(mdwt::nn::conv3x3_tc(x, l.Wuf, l.b, y, N, H, W, l.cin, l.cout, l.relu, f32 ? 1 : 0, d->dErr, st,
-                              tuned_for(d) ? &d->tileF[li] : nullptr, res, pool, pooled, x2, c1),
+                              tuned_for(d) ? &d->tileF[li] : nullptr, res, pool, pooled, x2, c1, pdl),
          "conv forward (tcgen05)");
     if (fused) *fused = res != nullptr;
   } else
@@ -178,35 +178,39 @@ mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void 
   Acts &A = d->A;
   const int H1 = Hp / 2, W1 = Wp / 2, H2 = Hp / 4, W2 = Wp / 4, S = d->numSMs;
   DCKI(mdwt::nn::pack_features(F, A.x0, N, H, W, Hp, Wp, S, st), "pack features");
-  if ((s = conv(d, d->L[0], A.x0, A.a1, N, Hp, Wp, false, st))) return s;
+  // inference: each convolution a programmatic dependent of the previous kernel (none writes
+  // what its predecessor reads)
+  const int pd = out4 ? 1 : 0;
+  if ((s = conv(d, d->L[0], A.x0, A.a1, N, Hp, Wp, false, st, nullptr, nullptr, nullptr, nullptr, nullptr, 0, pd))) return s;
   bool pooled = false;
-  if ((s = conv(d, d->L[1], A.a1, A.s0, N, Hp, Wp, false, st, nullptr, nullptr, A.p0, &pooled))) return s;
+  if ((s = conv(d, d->L[1], A.a1, A.s0, N, Hp, Wp, false, st, nullptr, nullptr, A.p0, &pooled, nullptr, 0, pd))) return s;
   if (!pooled) DCKI(mdwt::nn::avgpool2(A.s0, A.p0, N, Hp, Wp, 32, S, st), "pool");
-  if ((s = conv(d, d->L[2], A.p0, A.a2, N, H1, W1, false, st))) return s;
-  if ((s = conv(d, d->L[3], A.a2, A.s1, N, H1, W1, false, st, nullptr, nullptr, A.p1, &pooled))) return s;
+  if ((s = conv(d, d->L[2], A.p0, A.a2, N, H1, W1, false, st, nullptr, nullptr, nullptr, nullptr, nullptr, 0, pd))) return s;
+  if ((s = conv(d, d->L[3], A.a2, A.s1, N, H1, W1, false, st, nullptr, nullptr, A.p1, &pooled, nullptr, 0, pd))) return s;
   if (!pooled) DCKI(mdwt::nn::avgpool2(A.s1, A.p1, N, H1, W1, 64, S, st), "pool");
-  if ((s = conv(d, d->L[4], A.p1, A.a3, N, H2, W2, false, st))) return s;
-  if ((s = conv(d, d->L[5], A.a3, A.b2, N, H2, W2, false, st))) return s;
+  if ((s = conv(d, d->L[4], A.p1, A.a3, N, H2, W2, false, st, nullptr, nullptr, nullptr, nullptr, nullptr, 0, pd))) return s;
+  if ((s = conv(d, d->L[5], A.a3, A.b2, N, H2, W2, false, st, nullptr, nullptr, nullptr, nullptr, nullptr, 0, pd))) return s;
   const bool split6 = out4 && d->useTC && mdwt::nn::conv3x3_tc_supported(d->L[6].cin, d->L[6].cout);
   if (split6) {
     DCKI(mdwt::nn::up2_concat(A.b2, A.b2, A.u1, N, H1, W1, 128, 0, S, st), "upsample");
-    if ((s = conv(d, d->L[6], A.u1, A.a4, N, H1, W1, false, st, nullptr, nullptr, nullptr, nullptr, A.s1, 128))) return s;
+    if ((s = conv(d, d->L[6], A.u1, A.a4, N, H1, W1, false, st, nullptr, nullptr, nullptr, nullptr, A.s1, 128, pd))) return s;
   } else {
     DCKI(mdwt::nn::up2_concat(A.b2, A.s1, A.u1, N, H1, W1, 128, 64, S, st), "up+concat");
     if ((s = conv(d, d->L[6], A.u1, A.a4, N, H1, W1, false, st))) return s;
   }
-  if ((s = conv(d, d->L[7], A.a4, A.b1, N, H1, W1, false, st))) return s;
+  if ((s = conv(d, d->L[7], A.a4, A.b1, N, H1, W1, false, st, nullptr, nullptr, nullptr, nullptr, nullptr, 0, pd))) return s;
   const bool split8 = out4 && d->useTC && mdwt::nn::conv3x3_tc_supported(d->L[8].cin, d->L[8].cout);
   if (split8) {
     DCKI(mdwt::nn::up2_concat(A.b1, A.b1, A.u0, N, Hp, Wp, 64, 0, S, st), "upsample");
-    if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st, nullptr, nullptr, nullptr, nullptr, A.s0, 64))) return s;
+    if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st, nullptr, nullptr, nullptr, nullptr, A.s0, 64, pd))) return s;
   } else {
     DCKI(mdwt::nn::up2_concat(A.b1, A.s0, A.u0, N, Hp, Wp, 64, 32, S, st), "up+concat");
     if ((s = conv(d, d->L[8], A.u0, A.a5, N, Hp, Wp, false, st))) return s;
   }
   mdwt::nn::TcResidual res;
   res.F = F; res.out4 = out4; res.H = H; res.W = W;
-  if ((s = conv(d, d->L[9], A.a5, A.o, N, Hp, Wp, true, st, out4 ? &res : nullptr, fused))) return s;
+  if ((s = conv(d, d->L[9], A.a5, A.o, N, Hp, Wp, true, st, out4 ? &res : nullptr, fused, nullptr, nullptr, nullptr, 0, pd)))
+    return s;
   return MDWT_OK;
 }
 

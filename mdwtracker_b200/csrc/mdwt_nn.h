@@ -67,11 +67,13 @@ struct TcResidual {
 // tiling: null or R == 0 = the default policy's tiling.  poolOut (optional, BF16 output
 // only): also write the 2x2 average pooling of Y there, as avgpool2 would, when the tiling
 // allows it (an even row count per tile); *pooled tells whether it did.  X2 (optional): the input
-// is the channel concatenation of X (C1 channels, a multiple of 8) and X2 (Cin - C1).
+// is the channel concatenation of X (C1 channels, a multiple of 8) and X2 (Cin - C1).  pdl:
+// launch as a programmatic dependent of the previous kernel in the stream (its set-up
+// overlaps that kernel's tail; it must not write what that kernel reads).
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
                int relu, int outF32, int *err, void *stream, const TcTiling *tiling = nullptr,
                const TcResidual *res = nullptr, void *poolOut = nullptr, bool *pooled = nullptr,
-               const void *X2 = nullptr, int C1 = 0);
+               const void *X2 = nullptr, int C1 = 0, int pdl = 0);
 
 }  // namespace nn
 }  // namespace mdwt

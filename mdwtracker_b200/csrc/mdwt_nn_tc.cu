@@ -144,6 +144,7 @@ struct ConvArgs {
   int N, H, W, Cin, Cout, relu, outF32;
   int R, KC, NS, SA, AB, ST, resident, tmemCols, tilesX, tilesY, tiles;
   int stallTest;       // test hook: the input producer issues nothing (every wait then gives up)
+  int pdl;             // launched as a programmatic dependent of the previous kernel
   int C1;              // input channels [0, C1) from mapX, [C1, Cin) from mapX2 (C1 = Cin: one tensor)
   const float *resF;   // residual output (TcResidual) when resOut != nullptr
   void *poolOut;       // fused 2x2 average pooling of Y (BF16) when non-null
@@ -234,6 +235,10 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n");
   const uint32_t tmem = tmemBase;
+  // programmatic dependent launch: the next kernel's CTAs may be scheduled as SMs free up
+  // (their set-up overlaps this kernel's tail); only the reads of the previous kernel's
+  // output wait for it (griddepcontrol.wait in the input producer)
+  if (a.pdl) asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   auto fail = [&]() {
     abortFlag = 1;
     atomicExch(a.err, 1);
@@ -246,6 +251,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
       // pixels x R + 2 rows (zero-filled outside the image) into the group's slot
       bool ok = true;
       uint32_t gA = 0;
+      if (a.pdl) asm volatile("griddepcontrol.wait;\n" ::: "memory");   // the input is complete
       for (int t = blockIdx.x; t < a.tiles && ok && !a.stallTest; t += gridDim.x) {
         if (abortFlag) break;
         const int tx = t % a.tilesX, ty = (t / a.tilesX) % a.tilesY, n = t / (a.tilesX * a.tilesY);
@@ -723,7 +729,7 @@ int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *
 
 int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N, int H, int W, int Cin, int Cout,
                int relu, int outF32, int *err, void *stream, const TcTiling *tiling, const TcResidual *res,
-               void *poolOut, bool *pooled, const void *X2, int C1) {
+               void *poolOut, bool *pooled, const void *X2, int C1, int pdl) {
   if (pooled) *pooled = false;
   if (!X2) C1 = Cin;
   if (C1 <= 0 || C1 > Cin || C1 % 8 || (X2 && (reinterpret_cast<uintptr_t>(X2) & 15)))
@@ -762,6 +768,7 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   if (res && (!res->F || !res->out4 || res->H > H || res->W > W || Cout < 3)) return (int)cudaErrorInvalidValue;
   const bool fusePool = poolOut && !res && !outF32 && tl.R % 2 == 0 && H % 2 == 0 && W % 2 == 0;
   a.poolOut = fusePool ? poolOut : nullptr;
+  a.pdl = pdl ? 1 : 0;
   a.resident = resident_of(Cin, tl) ? 1 : 0;
   a.tmemCols = tmem_cols_for(tl.AB * tl.R * Cout);
   a.tilesX = (W + kTM - 1) / kTM;
@@ -774,8 +781,18 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   if (e != cudaSuccess) return (int)e;
   int grid = num_sms();
   if (grid > a.tiles) grid = a.tiles;
-  conv3x3_tc_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(map, map2, a);
-  const cudaError_t le = cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = (cudaStream_t)stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaError_t le = cudaLaunchKernelEx(&cfg, conv3x3_tc_kernel, map, map2, a);
+  if (le == cudaSuccess) le = cudaGetLastError();
   if (le == cudaSuccess && pooled) *pooled = fusePool;
   return (int)le;
 }
