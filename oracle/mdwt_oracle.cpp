@@ -20,11 +20,14 @@
 //   camera          camera.h:83-125, renderer.cpp:1058-1092
 //   dt / mc dims    renderer.cpp:1317-1361, 1363-1466
 //
-// PARITY UNPINNED: the reference cannot be built here (OptiX SDK and the OWL,
-// GLFW, ImGui, argparse and umesh submodules are absent) and it ships no tests or
-// golden vectors.  The oracle is pinned instead by analytic known-answer tests
-// (tests/test_oracle_known_answers.py): empty volume -> background, constant slab ->
-// Beer-Lambert transmittance, hand-checked majorants, zero-alpha TF -> zero majorant.
+// PARITY PARTLY PINNED: the reference renderer cannot be built here (OptiX SDK and the
+// OWL, GLFW, ImGui, argparse and umesh submodules are absent) and it ships no tests or
+// golden vectors.  Two parts compile on their own and pin this restatement bit for bit
+// (tests/test_ref_pins.py): the 3-D DDA (dda.h) and the raw loader (rawFile.cpp), built
+// where they lie with a stand-in for OWL's vector types (oracle/ref_shim, `make ref`).
+// The rest is pinned by analytic known-answer tests (tests/test_oracle_known_answers.py):
+// empty volume -> background, constant slab -> Beer-Lambert transmittance, hand-checked
+// majorants, zero-alpha TF -> zero majorant.
 //
 // Arithmetic specification shared with the CUDA kernels (both sides implement it
 // independently; bit-identical results are the parity bar):
@@ -1469,6 +1472,25 @@ int orc_get_pixel_stats(Oracle *o, uint32_t *out) {
 int orc_get_majorants(Oracle *o, float *out) { std::memcpy(out, o->majorants.data(), o->majorants.size() * 4); return ORC_OK; }
 int orc_get_ranges(Oracle *o, float *out) { std::memcpy(out, o->ranges.data(), o->ranges.size() * 4); return ORC_OK; }
 int orc_num_channels(Oracle *o, int *n) { *n = (int)o->ch.size(); return ORC_OK; }
+// The converted float values of channel c (RawR::getDataVector, rawFile.cpp:201-204).
+int orc_get_channel_data(Oracle *o, int c, float *out) {
+  if (c < 0 || c >= (int)o->ch.size()) return ORC_BAD;
+  std::memcpy(out, o->ch[c].data.data(), o->ch[c].data.size() * sizeof(float));
+  return ORC_OK;
+}
+// The oracle's dda3 over a grid of gs cells: the cells visited and their (t0, t1), at
+// most maxOut of them (the callback stops the walk there).  Returns the number written.
+int orc_dda_trace(const float org[3], const float dir[3], float tMax, const uint32_t gs[3], int maxOut,
+                  int32_t *cells, float *t0, float *t1) {
+  int n = 0;
+  if (maxOut <= 0) return 0;
+  dda3(v3(org[0], org[1], org[2]), v3(dir[0], dir[1], dir[2]), tMax, gs, [&](const int *c, float a, float b) {
+    cells[3 * n] = c[0]; cells[3 * n + 1] = c[1]; cells[3 * n + 2] = c[2];
+    t0[n] = a; t1[n] = b;
+    return ++n < maxOut;
+  });
+  return n;
+}
 
 // Test hooks: the primitives of the arithmetic specification.
 float orc_log(float x) { return mlog(x); }
