@@ -60,12 +60,12 @@ enum {
 
 /* Tracking methods, numbered like dtracker::Mode (renderer.h:24-36). */
 enum {
-  MDWT_MODE_NDDA = 0,        /* BASELINE: one DDA per channel   (deviceCode.cu:858-970) */
-  MDWT_MODE_MULTI = 1,       /* MULTI: min-of-channels free flight (deviceCode.cu:619-745) */
-  MDWT_MODE_SYNCDDA = 2,     /* MULTI_ALT: one DDA, per-channel samplers (deviceCode.cu:747-856) */
-  MDWT_MODE_CUMULATIVE = 3,  /* CUMMULATIVE: summed majorant (deviceCode.cu:513-617) */
-  MDWT_MODE_MAX = 4,         /* MAX: max-opacity blended sample, summed majorant (deviceCode.cu:165-180, 972-1065) */
-  MDWT_MODE_MIX = 5          /* MIX: opacity-weighted colour mix (deviceCode.cu:182-200, 972-1065) */
+  MDWT_MODE_NDDA = 0,        /* Mode::BASELINE: one DDA per channel (deviceCode.cu:858-970) */
+  MDWT_MODE_MULTI = 1,       /* Mode::MULTI: min-of-channels free flight (deviceCode.cu:619-745) */
+  MDWT_MODE_SYNCDDA = 2,     /* Mode::MULTI_ALT: one DDA, per-channel samplers (deviceCode.cu:747-856) */
+  MDWT_MODE_CUMULATIVE = 3,  /* Mode::CUMMULATIVE: summed majorant (deviceCode.cu:513-617) */
+  MDWT_MODE_MAX = 4,         /* Mode::MAX: max-opacity blended sample, summed majorant (deviceCode.cu:165-180, 972-1065) */
+  MDWT_MODE_MIX = 5          /* Mode::MIX: opacity-weighted colour mix (deviceCode.cu:182-200, 972-1065) */
 };
 
 /* ---- context ---------------------------------------------------------- */

@@ -4,8 +4,8 @@
  * (deviceCode.cu:463-471).  The denoiser maps one low-spp frame's per-pixel features
  * (mdwt_set_features: radiance, depth, transmittance, channel hit fractions; 16 floats per
  * pixel) to a denoised RGB image, so that an image reaches a given RMSE with far fewer
- * path samples than plain accumulation; the plain accumulation stays the fallback and
- * the judge of its error (mdwt_accum_rmse / mdwt_image_rmse).
+ * path samples than plain accumulation; the plain accumulation stays the fallback, and
+ * the error of both is measured the same way (mdwt_accum_rmse / mdwt_image_rmse).
  *
  * Network: a 3-level U-Net of 3x3 convolutions, 32/64/128 channels, ReLU, 2x2 average
  * pooling down, nearest 2x upsampling + skip concatenation up, a residual RGB output

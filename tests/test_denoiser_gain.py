@@ -1,5 +1,5 @@
 """What the learned denoiser gains over plain accumulation, measured against the FP64
-expected image of the estimator (the plain accumulation stays the judge of the error).
+expected image of the estimator (the same RMSE measure as for plain accumulation).
 
 * the committed network (mdwtracker_b200/weights, trained by train_denoiser.py on the
   6 x 512^3 log-normal scene with random views and transfer functions) on the scene's
