@@ -60,6 +60,10 @@ def parse_args():
     ap.add_argument("--spp", type=int, default=None, help="override samples per pixel")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-RMSE measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-request measurement")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default tracker schedule (regrouped tracker, trips 4) instead of tuning it")
+    ap.add_argument("--regroup", type=int, choices=[0, 1], default=None,
+                    help="force the -m 2 tracker after tuning: 1 regrouped, 0 warp-local")
     ap.add_argument("--batch-requests", type=int, default=64)
     ap.add_argument("--ttr-config", default="c3", choices=["c1", "c2", "c3", "c3ndda"])
     ap.add_argument("--ttr-target", type=float, default=0.01)
@@ -120,9 +124,9 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload):
+def profiled_traffic(kernel, workload):
     """DRAM bytes per tracker launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"trace_kernel_{workload}.md")
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -239,7 +243,8 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     r.setSpp(1)
     # the tracker schedule for this scene, tuned on the 8-frame launches that make up the
     # plain accumulation (the denoised path's single frame is insensitive to it)
-    tuned = r.autotuneSchedule(frames=8)
+    r.autotuneSchedule(frames=8)
+    plain_schedule = schedule_of(r, "mdwt_autotune_schedule")
     t0 = time.perf_counter()
     coarse = r.expectedImage(4, 0.5)
     ref = r.expectedImage(8, 0.25)          # stays on the device for accumRmse
@@ -282,7 +287,7 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     return {
         "target": target, "metric": "RMSE of linear RGB (accumulation buffer) vs the FP64 expected image",
         "workload": workload_name(sc).replace(f"_{sc.spp}spp", ""), "resolution": [w, h], "mode": sc.mode,
-        "schedule": {"pool": tuned[0], "trips": tuned[1], "by": "mdwt_autotune_schedule"},
+        "schedule": plain_schedule,
         "reference": {"kind": "FP64 expected image of the estimator (mdwt_render_expected)",
                       "jitter_points": 8, "step_voxels": 0.25, "seconds": t_ref,
                       "rmse_vs_4_jitter_0.5_voxel": quad},
@@ -407,7 +412,7 @@ def denoised_time_to_rmse(r, target, stream, spps=(1, 2, 4, 8, 16, 32, 64), reps
     den.close()
     res = {"weights": os.path.relpath(DENOISER_WEIGHTS, ROOT), "tried": tried,
            "reached": found is not None,
-           "schedule": {"pool": single[0], "trips": single[1], "by": "mdwt_autotune_schedule, single frames"}}
+           "schedule": schedule_of(r, "mdwt_autotune_schedule, single frames")}
     if found:
         res.update({"spp": found["spp"], "rmse": found["rmse"], "device_ms": found["render_ms"] + found["denoise_ms"],
                     "render_ms": found["render_ms"], "denoise_ms": found["denoise_ms"]})
@@ -455,6 +460,15 @@ def run_reference(args):
     return 0
 
 
+def schedule_of(r, by):
+    """The context's tracker schedule (MDWT_TUNE_*): which tracker, its trips, and the
+    warp-local tracker's pool and quorum."""
+    names = {4: "regroup", 2: "trips", 0: "pool", 3: "quorum"}
+    out = {v: r.getTuning(k) for k, v in names.items()}
+    out["by"] = by
+    return out
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -478,9 +492,14 @@ def main():
     sc = make_scene(args.config, args.res, args.spp)
     r = sc.setup(Renderer(local))
     w, h = sc.resolution
-    schedule = None
-    if args.config.startswith("c3"):   # traversal-heavy scenes: tune the tracker schedule first
-        schedule = r.autotuneSchedule(frames=1)
+    # the tracker schedule is tuned for the workload first (outside the timed region), on
+    # launches of the step's shape
+    if not args.no_autotune:
+        r.autotuneSchedule(frames=sc.frames)
+    if args.regroup is not None:
+        r.setTuning(4, args.regroup)
+    schedule = schedule_of(r, ("default" if args.no_autotune else "mdwt_autotune_schedule") +
+                           ("" if args.regroup is None else f", regroup forced to {args.regroup}"))
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream
     flush = torch.empty(args.flush_mib << 20, dtype=torch.uint8, device=dev)
@@ -517,6 +536,8 @@ def main():
     except Exception:
         timed = False
     launches0 = r.renderInfo()[0]
+    # the tracker kernel the frames run: the regrouped one launches 256-thread blocks
+    tracker = "trace_regroup_kernel" if r.renderInfo()[3] == 256 else "trace_kernel"
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize(dev)
@@ -613,11 +634,10 @@ def main():
         "dtype": "f32",
         "data": "synthetic (seeded generators in mdwtracker_b200/synthetic.py)",
         "config": dict(scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
-                       schedule={"pool": schedule[0], "trips": schedule[1], "by": "mdwt_autotune_schedule"}
-                       if schedule else {"pool": 8, "trips": 4, "quorum": 16, "by": "default"}),
+                       schedule=schedule),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": profiled_traffic(workload_name(sc)),
-                     "peak_source": peak_kind, "kernel": "trace_kernel",
+                     "frac": achieved / peak, "traffic": profiled_traffic(tracker, workload_name(sc)),
+                     "peak_source": peak_kind, "kernel": tracker,
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
         "cpu_baseline": cpu,
         "e2e": {"value": world * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",

@@ -210,9 +210,17 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * MDWT_TUNE_TRIPS: transition/free-flight trips (1..64) a warp takes per round before
  * it evaluates its pending density samples together.
  * MDWT_TUNE_QUORUM: a round's trips also end once `value` (1..33; 33 = never) of the
- * warp's lanes hold a pending density sample. */
-enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2, MDWT_TUNE_QUORUM = 3 };
+ * warp's lanes hold a pending density sample.
+ * MDWT_TUNE_REGROUP: 1 (default) = -m 2 frames without shadows, features or per-pixel
+ * statistics run the tracker that keeps 64 paths per warp and runs, at each step, the
+ * operation most of them need next (path start, walk, density sample), one path per
+ * lane; a walk takes at most TRIPS free-flight draws.  0 = the warp-local tracker (32
+ * paths per warp; POOL and QUORUM apply to it only). */
+enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2, MDWT_TUNE_QUORUM = 3, MDWT_TUNE_REGROUP = 4 };
 mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
+/* The current value of a tuning knob (defaults: pool 8, batch 0, trips 4, quorum 16,
+ * regroup 1). */
+mdwt_status mdwt_get_tuning(const mdwt_ctx *ctx, int key, int *value);
 
 /* No reference counterpart: CUDA events on the render stream around the trace kernel
  * (with the work-counter reset before it) and the resolve kernel of each frame whose

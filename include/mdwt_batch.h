@@ -59,12 +59,14 @@ mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]);
  * accumulation reset afterwards.  best[3] (optional) = chunk items, pool, trips. */
 mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]);
 
-/* Schedule autotuner for one context: coordinate descent over the phase-1 trips
- * {1, 2, 3, 4, 6, 8}, the regeneration pool {4, 8, 16, 32} and the sample quorum
+/* Schedule autotuner for one context: coordinate descent over, for -m 2, the tracker
+ * (MDWT_TUNE_REGROUP {1, 0}), then the trips {1, 2, 3, 4, 6, 8}, then -- for the
+ * warp-local tracker -- the regeneration pool {4, 8, 16, 32} and the sample quorum
  * {8, 16, 24, never} (MDWT_TUNE_*), each candidate timed on `frames` frames rendered by
  * mdwt_render_frames (after a warm-up of the same), so pass the frames per call of the
- * loop being tuned; keeps the fastest (results do not depend on them).  Frame ids are
- * restored and the accumulation reset.  best[2] (optional) = pool, trips. */
+ * loop being tuned; keeps the fastest (results do not depend on them).  Frame ids and the
+ * event counters are restored and the accumulation reset.  best[2] (optional) = pool,
+ * trips; mdwt_get_tuning reads every knob. */
 mdwt_status mdwt_autotune_schedule(mdwt_ctx *ctx, int frames, int best[2]);
 
 /* Macrocell autotuner for one context: for each candidate edge length (voxels per

@@ -165,6 +165,7 @@ struct mdwt_ctx {
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
   int trips = 4;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
   int quorum = 16;    // end a round's trips early once this many lanes wait to sample (33: never)
+  int regroup = 1;    // -m 2: the tracker that regroups each warp's paths by operation (MDWT_TUNE_REGROUP)
   int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
   bool timing = false;        // CUDA events around the trace and resolve kernels
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -1026,6 +1027,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   p.pool = c->pool;
   p.trips = c->trips;
   p.quorum = c->quorum;
+  p.regroup = c->regroup;
   p.vol32 = 1;
   for (auto &h : c->ch)
     if ((uint64_t)h.dims[0] * h.dims[1] * h.dims[2] >= (1ull << 32)) p.vol32 = 0;
@@ -1596,6 +1598,10 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
   if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
   CK(cudaSetDevice(c->device), "cudaSetDevice");
   const int f0 = c->frameID, a0 = c->accumID, fp0 = c->frameParam, ap0 = c->accumParam;
+  // the trial frames must not show in the context's event counters
+  unsigned long long counters0[8];
+  CK(cudaStreamSynchronize(c->stream), "sync");
+  CK(cudaMemcpy(counters0, c->dCounters, sizeof(counters0), cudaMemcpyDeviceToHost), "save counters");
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CK(cudaEventCreate(&e0), "event");
   CK(cudaEventCreate(&e1), "event");
@@ -1627,14 +1633,24 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
     *knob = bestV;
     return MDWT_OK;
   };
+  const int regroupC[] = {1, 0};
   const int tripsC[] = {1, 2, 3, 4, 6, 8};
   const int poolsC[] = {4, 8, 16, 32};
   const int quorumC[] = {8, 16, 24, 33};
-  if (!(s = tune(&c->trips, tripsC, 6)) && !(s = tune(&c->pool, poolsC, 4))) s = tune(&c->quorum, quorumC, 4);
+  // the regrouped tracker runs -m 2 frames without shadows, gradient shading, features or
+  // per-pixel statistics; other frames run the warp-local tracker whatever the knob says
+  const bool regroupable = c->mode == 2 && !c->shadows && !c->gradient && !c->featOn && !c->statsOn;
+  if (regroupable) s = tune(&c->regroup, regroupC, 2);
+  if (!s && !(s = tune(&c->trips, tripsC, 6)) && !(regroupable && c->regroup)) {
+    // the regeneration pool and the sample quorum belong to the warp-local tracker
+    if (!(s = tune(&c->pool, poolsC, 4))) s = tune(&c->quorum, quorumC, 4);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->frameID = f0; c->accumID = a0; c->frameParam = fp0; c->accumParam = ap0;
   reset_accum_ids(c);
+  CK(cudaStreamSynchronize(c->stream), "sync");
+  CK(cudaMemcpy(c->dCounters, counters0, sizeof(counters0), cudaMemcpyHostToDevice), "restore counters");
   if (s) return s;
   if (best) { best[0] = c->pool; best[1] = c->trips; }
   return MDWT_OK;
@@ -1876,12 +1892,29 @@ mdwt_status mdwt_set_tuning(mdwt_ctx *c, int key, int value) {
     c->quorum = value;
     return MDWT_OK;
   }
+  if (key == MDWT_TUNE_REGROUP) {
+    if (value < 0 || value > 1) return fail(c, MDWT_ERR_BAD_ARG, "regroup must be 0 or 1");
+    c->regroup = value;
+    return MDWT_OK;
+  }
   if (key == MDWT_TUNE_BATCH) {
     if (value < 0) return fail(c, MDWT_ERR_BAD_ARG, "batch must be >= 0");
     c->batchCap = value;
     return MDWT_OK;
   }
   return fail(c, MDWT_ERR_BAD_ARG, "unknown tuning key");
+}
+
+mdwt_status mdwt_get_tuning(const mdwt_ctx *c, int key, int *value) {
+  if (!c || !value) return MDWT_ERR_BAD_ARG;
+  switch (key) {
+    case MDWT_TUNE_POOL: *value = c->pool; return MDWT_OK;
+    case MDWT_TUNE_BATCH: *value = c->batchCap; return MDWT_OK;
+    case MDWT_TUNE_TRIPS: *value = c->trips; return MDWT_OK;
+    case MDWT_TUNE_QUORUM: *value = c->quorum; return MDWT_OK;
+    case MDWT_TUNE_REGROUP: *value = c->regroup; return MDWT_OK;
+    default: return MDWT_ERR_BAD_ARG;
+  }
 }
 
 mdwt_status mdwt_get_render_info(const mdwt_ctx *c, int64_t out[4]) {

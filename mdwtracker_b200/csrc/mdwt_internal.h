@@ -80,6 +80,7 @@ struct TrackParams {
   int chunk;                     // work items a warp takes from the dispenser at once
   int trips;                     // phase-1 transition/draw trips per warp round (at most)
   int quorum;                    // ... ending early once this many lanes hold a pending sample
+  int regroup;                   // -m 2: regroup paths across the block's warps (trace_regroup_kernel)
   int vol32;                     // every channel has < 2^32 voxels: 32-bit voxel offsets
   // sample batch [sBase, sBase + sCount) of the frame; one 4-byte record per traced
   // path, [k * nrect + rect-local pixel], nrect = pixels of the traced rectangle

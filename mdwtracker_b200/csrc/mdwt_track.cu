@@ -633,6 +633,278 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
   flush_counters(P.counters, tot);
 }
 
+// ------------------------------------------------------------------ regrouped tracker
+// trace_regroup_kernel: the syncDDA tracker (-m 2; no shadows, features or per-pixel
+// statistics) with each warp's paths regrouped by their next operation.  A warp keeps 64
+// path states in shared memory (structure of arrays), twice its lanes.  Each iteration it
+// counts its slots per stage -- start a path, walk (cell and channel transitions with
+// free-flight draws, at most `trips` draws), evaluate a pending density sample -- and runs
+// the most populated stage with lane i on the i-th slot of that stage, so at least 22 of
+// its 32 lanes work on the same operation.  Warps run independently (no block barrier).
+// Every path runs exactly the arithmetic of trace_items (the same helpers, in the same
+// order), so records and counters are identical; only which lane runs which path when
+// changes.  The loop ends when every slot has run out of work items; each path is
+// bounded by kMaxStepsPerSample draws and maxCells cells.
+namespace rg {
+constexpr int kTPB = 256;
+constexpr int kSPT = 2;                  // path slots per thread
+constexpr int kSlots = kTPB * kSPT;
+constexpr int kMinBlocks = 4;            // 64 registers, 32 warps per SM
+constexpr int kWalkCells = 1 << 20;      // cells a walk may enter before it yields the lane
+enum : uint32_t { NEED = 0, WALK = 1, SAMPLE = 2, DONE = 3 };
+// meta word: bits 0-1 stage, bit 2 a channel is selected (free flights pending), bit 3
+// the cell's channels are exhausted (advance the walk), bits 4-7 channel, bit 8 capped,
+// bits 9-20 the cell's non-zero-majorant channels, bits 21-31 cells entered
+constexpr uint32_t kDraw = 4u, kAdvance = 8u, kCapped = 256u;
+struct Slots {
+  uint32_t meta[kSlots], recIdx[kSlots], rng[kSlots], steps[kSlots], record[kSlots], cell[kSlots];
+  float wdx[kSlots], wdy[kSlots], wdz[kSlots], t1w[kSlots], w2g[kSlots], g2w[kSlots];
+  float tnx[kSlots], tny[kSlots], tnz[kSlots], tsx[kSlots], tsy[kSlots], tsz[kSlots];
+  float rt0[kSlots], ncb[kSlots], maj[kSlots], t[kSlots], lim[kSlots];
+};
+__device__ __forceinline__ uint32_t pack_meta(uint32_t stage, uint32_t flags, int ch, uint32_t cmask, uint32_t visits) {
+  return stage | flags | ((uint32_t)ch << 4) | ((cmask & 0xfffu) << 9) | (visits << 21);
+}
+__device__ __forceinline__ void load_dda(const Slots &S, unsigned s, DDA &d) {
+  d.tnx = S.tnx[s]; d.tny = S.tny[s]; d.tnz = S.tnz[s];
+  d.tsx = S.tsx[s]; d.tsy = S.tsy[s]; d.tsz = S.tsz[s];
+  const uint32_t c = S.cell[s];
+  d.cx = (int)(c & 1023u); d.cy = (int)((c >> 10) & 1023u); d.cz = (int)(c >> 20);
+  d.rt0 = S.rt0[s]; d.ncb = S.ncb[s];
+}
+// enter_cell of trace_items: the cell's exit distance, id and channel mask
+__device__ __forceinline__ int enter(const TrackParams &P, const DDA &d, float &ct1, uint32_t &cmask) {
+  const float tc = fminf(fminf(d.tnx, d.tny), d.tnz);
+  ct1 = d.rt0 + fminf(tc, 1e20f);
+  const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
+  cmask = __ldg(P.mask + cellID);
+  return cellID;
+}
+__device__ __forceinline__ void finish(const TrackParams &P, Slots &S, unsigned s, uint32_t record, bool capped,
+                                       uint32_t (&tot)[5]) {
+  P.records[S.recIdx[s]] = capped ? 0u : record;
+  tot[3]++;
+  if (capped) tot[4]++;
+  S.meta[s] = NEED;
+}
+
+// Start the path of work item `item` in slot s (the pooled start of trace_items).
+__device__ __forceinline__ void start(const TrackParams &P, Slots &S, unsigned s, unsigned item, unsigned limit,
+                                      uint32_t (&tot)[5]) {
+  if (item >= limit) { S.meta[s] = DONE; return; }
+  const int rw = P.cullX1 - P.cullX0 + 1;
+  const uint32_t nrect = (uint32_t)rw * (uint32_t)(P.cullY1 - P.cullY0 + 1);
+  const unsigned tile = item / (32u * (unsigned)P.sCount);
+  const unsigned rem = item - tile * 32u * (unsigned)P.sCount;
+  const int k = (int)(rem >> 5), w = (int)(rem & 31u);
+  const int lx = (int)(tile % (unsigned)P.tilesX) * 8 + (w & 7);
+  const int ly = (int)(tile / (unsigned)P.tilesX) * 4 + (w >> 3);
+  const int px = P.cullX0 + lx, py = P.cullY0 + ly;
+  if (px > P.cullX1 || py > P.cullY1) return;   // outside the traced rectangle: take another item
+  int smp;
+  const uint32_t fr = sample_frame(P, P.sBase + k, smp);
+  S.recIdx[s] = (uint32_t)k * nrect + (uint32_t)(ly * rw + lx);
+  float wdx, wdy, wdz;
+  const uint32_t rng = primary_ray(P, px, py, fr, smp, wdx, wdy, wdz);
+  // start_leg of trace_items (volumeIntersection, grid transform, DDA start)
+  const float frx = 1.0f / wdx, fry = 1.0f / wdy, frz = 1.0f / wdz;
+  const float t1 = (P.rootLo.x - P.camOrg.x) * frx, t2 = (P.rootHi.x - P.camOrg.x) * frx;
+  const float t3 = (P.rootLo.y - P.camOrg.y) * fry, t4 = (P.rootHi.y - P.camOrg.y) * fry;
+  const float t5 = (P.rootLo.z - P.camOrg.z) * frz, t6 = (P.rootHi.z - P.camOrg.z) * frz;
+  const float th0 = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
+  const float th1 = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
+  if (th1 < 0 || th0 >= th1) { finish(P, S, s, 0u, false, tot); return; }
+  float gx, gy, gz, w2g, g2w;
+  grid_dir(P, wdx, wdy, wdz, gx, gy, gz, w2g, g2w);
+  DDA d;
+  if (!dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) { finish(P, S, s, 0u, false, tot); return; }
+  float ct1;
+  uint32_t cmask;
+  enter(P, d, ct1, cmask);
+  tot[2]++;
+  S.rng[s] = rng; S.steps[s] = 0u; S.record[s] = 0u;
+  S.wdx[s] = wdx; S.wdy[s] = wdy; S.wdz[s] = wdz;
+  S.t1w[s] = fminf(1e20f, th1); S.w2g[s] = w2g; S.g2w[s] = g2w;
+  S.tnx[s] = d.tnx; S.tny[s] = d.tny; S.tnz[s] = d.tnz;
+  S.tsx[s] = d.tsx; S.tsy[s] = d.tsy; S.tsz[s] = d.tsz;
+  S.cell[s] = (uint32_t)d.cx | ((uint32_t)d.cy << 10) | ((uint32_t)d.cz << 20);
+  S.rt0[s] = d.rt0; S.ncb[s] = d.ncb;
+  S.lim[s] = ct1;
+  S.meta[s] = pack_meta(WALK, 0u, 0, cmask, 1u);
+}
+
+// Walk: transitions to the next channel with a non-zero majorant, then free-flight draws,
+// until a tentative collision (-> SAMPLE), the end of the path, or `trips` draws.
+__device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s, uint32_t maxCells,
+                                     uint32_t (&tot)[5]) {
+  const uint32_t m0 = S.meta[s];
+  bool drawing = (m0 & kDraw) != 0u, advance = (m0 & kAdvance) != 0u;
+  int ch = (int)((m0 >> 4) & 15u);
+  uint32_t cmask = (m0 >> 9) & 0xfffu, visits = m0 >> 21;
+  uint32_t record = S.record[s], steps = S.steps[s], rng = S.rng[s];
+  float maj = S.maj[s], t = S.t[s], lim = S.lim[s];
+  const float w2g = S.w2g[s];
+  const float wdx = S.wdx[s], wdy = S.wdy[s], wdz = S.wdz[s];
+  DDA d;
+  load_dda(S, s, d);
+  d.visits = visits;
+  bool moved = false, paused = false;
+  int cellsLeft = kWalkCells;
+  uint32_t stage = WALK;
+  for (int k = 0;;) {
+    if (!drawing) {
+      bool ended = false;
+      while (true) {
+        if (advance) {
+          if (cellsLeft == 0) { paused = true; break; }   // bounded walk: resume at this cell boundary
+          cellsLeft--;
+          if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ended = true; break; }
+          float ct1;
+          enter(P, d, ct1, cmask);
+          d.visits++;
+          tot[2]++;
+          moved = true;
+          lim = ct1;
+          ch = 0;
+          advance = false;
+        }
+        const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
+        if (rem == 0u) {   // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
+          if (record) { ended = true; break; }
+          advance = true;
+          continue;
+        }
+        ch += __ffs(rem) - 1;
+        const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
+        maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
+        t = d.rt0 + d.ncb;   // the cell's entry distance
+        break;
+      }
+      if (ended) { finish(P, S, s, record, false, tot); return; }
+      if (paused) break;
+      drawing = true;
+    }
+    // free-flight draw (deviceCode.cu:800-820)
+    if (++steps >= kMaxStepsPerSample) { finish(P, S, s, record, true, tot); return; }
+    const float u = rng_next(rng);
+    t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+    if (t >= lim) {
+      ch++;
+      drawing = false;
+    } else {
+      const float tW = t * S.g2w[s];
+      if (tW >= S.t1w[s]) {   // world exit
+        tot[1]++;
+        if (ch == P.C - 1) { finish(P, S, s, record, false, tot); return; }
+        ch++;
+        drawing = false;
+      } else {
+        stage = SAMPLE;
+        break;
+      }
+    }
+    if (++k >= P.trips) break;
+  }
+  S.meta[s] = pack_meta(stage, (drawing ? kDraw : 0u) | (advance ? kAdvance : 0u), ch, cmask, d.visits);
+  S.steps[s] = steps; S.rng[s] = rng; S.maj[s] = maj; S.t[s] = t; S.lim[s] = lim;
+  if (moved) {
+    S.tnx[s] = d.tnx; S.tny[s] = d.tny; S.tnz[s] = d.tnz;
+    S.cell[s] = (uint32_t)d.cx | ((uint32_t)d.cy << 10) | ((uint32_t)d.cz << 20);
+    S.ncb[s] = d.ncb;
+  }
+}
+
+// The pending density sample of slot s (phase 2 of trace_items, -m 2).
+template <int SK>
+__device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const ChanSm *sch, unsigned s,
+                                       uint32_t (&tot)[5]) {
+  const uint32_t m0 = S.meta[s];
+  const int ch = (int)((m0 >> 4) & 15u);
+  const float tW = S.t[s] * S.g2w[s];
+  const float xs = fmaf(tW, S.wdx[s], P.camOrg.x) * P.w2u.x;
+  const float ys = fmaf(tW, S.wdy[s], P.camOrg.y) * P.w2u.y;
+  const float zs = fmaf(tW, S.wdz[s], P.camOrg.z) * P.w2u.z;
+  uint32_t rng = S.rng[s];
+  const float thr = rng_next(rng) * S.maj[s];
+  const ChanSm &cs = sch[ch];
+  const float v = sample_volume<SK>(P, cs, xs, ys, zs);
+  tot[0]++;
+  if (v == v) {
+    Axis tax;
+    const float a = tf_alpha(cs, v, tax);
+    if (a > 0.0f && thr < a) {
+      S.record[s] = make_record(ch, tax);
+      S.lim[s] = fminf(S.t[s], S.lim[s]);
+    }
+  }
+  tot[1]++;   // -m 2 counts every sample as a rejection, hits included (deviceCode.cu:836-846)
+  S.rng[s] = rng;
+  S.meta[s] = (m0 & ~3u) | WALK | kDraw;
+}
+}  // namespace rg
+
+template <int SK>
+__global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel(const __grid_constant__ TrackParams P) {
+  extern __shared__ __align__(16) unsigned char rgSmem[];
+  rg::Slots &S = *reinterpret_cast<rg::Slots *>(rgSmem);
+  __shared__ ChanSm sch[kMaxChannels];
+  const unsigned tid = threadIdx.x, lane = tid & 31u;
+  const unsigned wbase = (tid >> 5) * (32u * rg::kSPT);   // the warp's slots: group g is wbase + 32 g + lane
+  if (tid < (unsigned)P.C) sch[tid] = chan_params(P, (int)tid);
+#pragma unroll
+  for (int g = 0; g < rg::kSPT; g++) S.meta[wbase + 32u * g + lane] = rg::NEED;
+  __syncthreads();   // the channel table
+  const unsigned limit = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
+  const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
+  uint32_t tot[5] = {0, 0, 0, 0, 0};
+  while (true) {
+    // the warp's slots by stage; the most populated stage runs, one slot per lane
+    unsigned ms[rg::kSPT][3];
+    int n[3] = {0, 0, 0};
+#pragma unroll
+    for (int g = 0; g < rg::kSPT; g++) {
+      const uint32_t st = S.meta[wbase + 32u * g + lane] & 3u;
+#pragma unroll
+      for (int X = 0; X < 3; X++) {
+        ms[g][X] = __ballot_sync(kFull, st == (uint32_t)X);
+        n[X] += __popc(ms[g][X]);
+      }
+    }
+    if (n[0] + n[1] + n[2] == 0) break;   // every slot is out of work items
+    int X = rg::SAMPLE, nX = n[rg::SAMPLE];
+    if (n[rg::WALK] > nX) { X = rg::WALK; nX = n[rg::WALK]; }
+    if (n[rg::NEED] > nX) { X = rg::NEED; nX = n[rg::NEED]; }
+    const int nx = nX < 32 ? nX : 32;
+    const bool mine = (int)lane < nx;
+    // lane i takes the i-th slot of stage X in slot order
+    unsigned s = 0;
+    int below = 0;
+    bool found = false;
+#pragma unroll
+    for (int g = 0; g < rg::kSPT; g++) {
+      const unsigned m = X == rg::SAMPLE ? ms[g][rg::SAMPLE] : (X == rg::WALK ? ms[g][rg::WALK] : ms[g][rg::NEED]);
+      const int c = __popc(m);
+      if (mine && !found && (int)lane < below + c) {
+        s = wbase + 32u * g + (unsigned)__fns(m, 0u, (int)lane - below + 1);
+        found = true;
+      }
+      below += c;
+    }
+    if (X == rg::SAMPLE) {
+      if (mine) rg::sample<SK>(P, S, sch, s, tot);
+    } else if (X == rg::WALK) {
+      if (mine) rg::walk(P, S, s, maxCells, tot);
+    } else {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(P.workCounter, (unsigned)nx);
+      base = __shfl_sync(kFull, base, 0);
+      if (mine) rg::start(P, S, s, base + lane, limit, tot);
+    }
+    __syncwarp();
+  }
+  flush_counters(P.counters, tot);
+}
+
 // Batched variant: many requests (render contexts) in one persistent launch.  Every
 // request has its own work dispenser; a warp starts at request (global warp id mod nReq),
 // takes chunks of that request's items until they run out, then moves on to the next
@@ -987,8 +1259,52 @@ __global__ void __launch_bounds__(256) resolve_batch_kernel(const TrackParams *_
   }
 }
 
+// The regrouped tracker's packed slot fields: cells < 1024 per axis, at most 2047 cells
+// entered, 32-bit record indices.
+bool regroup_fits(const TrackParams &p) {
+  const size_t nrect = (size_t)(p.cullX1 - p.cullX0 + 1) * (size_t)(p.cullY1 - p.cullY0 + 1);
+  return p.mode == 2 && p.regroup && p.mc[0] <= 1024u && p.mc[1] <= 1024u && p.mc[2] <= 1024u &&
+         p.mc[0] + p.mc[1] + p.mc[2] + 3u <= 2047u && nrect * (size_t)p.sCount < ((size_t)1 << 32);
+}
+
+template <int SK>
+int launch_resolve(const TrackParams &p, cudaStream_t st, int numSMs) {
+  const size_t npix = (size_t)p.W * (size_t)(p.rowHi - p.rowLo);
+  if (npix == 0) return (int)cudaGetLastError();
+  size_t g = (npix + 255) / 256;
+  if (g > (size_t)numSMs * 8) g = (size_t)numSMs * 8;
+  if (p.shadows || p.gradient) {
+    if (p.stats) resolve_kernel<true, true, SK><<<(unsigned)g, 256, 0, st>>>(p);
+    else resolve_kernel<false, true, SK><<<(unsigned)g, 256, 0, st>>>(p);
+  } else {
+    if (p.stats) resolve_kernel<true, false, SK><<<(unsigned)g, 256, 0, st>>>(p);
+    else resolve_kernel<false, false, SK><<<(unsigned)g, 256, 0, st>>>(p);
+  }
+  return (int)cudaGetLastError();
+}
+
+template <int SK>
+int launch_regroup(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
+  const int smem = (int)sizeof(rg::Slots);
+  cudaError_t e = cudaFuncSetAttribute(trace_regroup_kernel<SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return (int)e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_regroup_kernel<SK>, rg::kTPB, smem);
+  if (e != cudaSuccess) return (int)e;
+  if (bps < 1) bps = 1;
+  *grid = numSMs * bps;
+  if (p.numTiles > 0) trace_regroup_kernel<SK><<<*grid, rg::kTPB, smem, st>>>(p);
+  if (evMid) cudaEventRecord((cudaEvent_t)evMid, st);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  return launch_resolve<SK>(p, st, numSMs);
+}
+
 template <int MODE, int SK, bool STATS, bool SH>
 int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
+  if constexpr (MODE == 2 && !STATS && !SH) {
+    if (regroup_fits(p)) return launch_regroup<SK>(p, st, numSMs, grid, evMid);
+  }
   int bps = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_kernel<MODE, SK, STATS, SH>, kTPB, 0);
   if (e != cudaSuccess) return (int)e;
@@ -1004,13 +1320,7 @@ int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void 
   if (evMid) cudaEventRecord((cudaEvent_t)evMid, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  const size_t npix = (size_t)p.W * (size_t)(p.rowHi - p.rowLo);
-  if (npix == 0) return (int)cudaGetLastError();
-  size_t g = (npix + 255) / 256;
-  if (g > (size_t)numSMs * 8) g = (size_t)numSMs * 8;
-  if (p.shadows || p.gradient) resolve_kernel<STATS, true, SK><<<(unsigned)g, 256, 0, st>>>(p);
-  else resolve_kernel<STATS, false, SK><<<(unsigned)g, 256, 0, st>>>(p);
-  return (int)cudaGetLastError();
+  return launch_resolve<SK>(p, st, numSMs);
 }
 
 template <int MODE, int SK>
@@ -1101,7 +1411,7 @@ int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, 
     case 5: rc = u8 ? launch_s<4, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<4, kStoreF32>(p, st, numSMs, grid, evMid); break;
     default: return (int)cudaErrorInvalidValue;
   }
-  *block = kTPB;
+  *block = (regroup_fits(p) && !p.stats && !p.shadows && !p.recT) ? rg::kTPB : kTPB;
   if (launches) *launches += p.numTiles > 0 ? 2 : 1;
   return rc;
 }

@@ -380,8 +380,14 @@ class Renderer:
         return float(out[0]), float(out[1])
 
     def setTuning(self, key: int, value: int):
-        """Tracker tuning knob (0 = regeneration pool); results do not depend on it."""
+        """Tracker tuning knob (0 pool, 1 batch, 2 trips, 3 quorum, 4 regroup); results do
+        not depend on it."""
         self._call("set_tuning", C.c_int(key), C.c_int(value))
+
+    def getTuning(self, key: int) -> int:
+        v = C.c_int()
+        self._call("get_tuning", C.c_int(key), C.byref(v))
+        return v.value
 
     def renderInfo(self):
         """(kernels launched so far, per-frame parameter bytes, last grid, last block)."""

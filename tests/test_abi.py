@@ -107,3 +107,15 @@ def test_gpu_absent_is_an_error_not_a_fallback():
     with pytest.raises(MdwtError) as e:
         Renderer(0)
     assert e.value.status == 2
+
+
+def test_tuning_knobs_read_back():
+    r = Renderer(MDWT_HOST_ONLY)
+    assert [r.getTuning(k) for k in (0, 1, 2, 3, 4)] == [8, 0, 4, 16, 1]
+    r.setTuning(4, 0)
+    r.setTuning(2, 7)
+    assert r.getTuning(4) == 0 and r.getTuning(2) == 7
+    with pytest.raises(MdwtError):
+        r.setTuning(4, 2)
+    with pytest.raises(MdwtError):
+        r.getTuning(9)
