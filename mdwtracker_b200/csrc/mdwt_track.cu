@@ -848,8 +848,10 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel
   extern __shared__ __align__(16) unsigned char rgSmem[];
   rg::Slots &S = *reinterpret_cast<rg::Slots *>(rgSmem);
   __shared__ ChanSm sch[kMaxChannels];
+  __shared__ uint16_t selAll[rg::kTPB];                    // per warp: the slot each lane runs
   const unsigned tid = threadIdx.x, lane = tid & 31u;
   const unsigned wbase = (tid >> 5) * (32u * rg::kSPT);   // the warp's slots: group g is wbase + 32 g + lane
+  uint16_t *sel = selAll + (tid & ~31u);
   if (tid < (unsigned)P.C) sch[tid] = chan_params(P, (int)tid);
 #pragma unroll
   for (int g = 0; g < rg::kSPT; g++) S.meta[wbase + 32u * g + lane] = rg::NEED;
@@ -858,17 +860,19 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel
   const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
   uint32_t tot[5] = {0, 0, 0, 0, 0};
   while (true) {
-    // the warp's slots by stage; the most populated stage runs, one slot per lane
+    // the warp's slots by stage (two stage bits per slot); the most populated stage runs,
+    // lane i on the i-th slot of that stage in slot order
     unsigned ms[rg::kSPT][3];
     int n[3] = {0, 0, 0};
 #pragma unroll
     for (int g = 0; g < rg::kSPT; g++) {
-      const uint32_t st = S.meta[wbase + 32u * g + lane] & 3u;
+      const uint32_t st = S.meta[wbase + 32u * g + lane];
+      const unsigned b0 = __ballot_sync(kFull, st & 1u), b1 = __ballot_sync(kFull, st & 2u);
+      ms[g][rg::NEED] = ~b0 & ~b1;
+      ms[g][rg::WALK] = b0 & ~b1;
+      ms[g][rg::SAMPLE] = ~b0 & b1;
 #pragma unroll
-      for (int X = 0; X < 3; X++) {
-        ms[g][X] = __ballot_sync(kFull, st == (uint32_t)X);
-        n[X] += __popc(ms[g][X]);
-      }
+      for (int X = 0; X < 3; X++) n[X] += __popc(ms[g][X]);
     }
     if (n[0] + n[1] + n[2] == 0) break;   // every slot is out of work items
     int X = rg::SAMPLE, nX = n[rg::SAMPLE];
@@ -876,20 +880,18 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel
     if (n[rg::NEED] > nX) { X = rg::NEED; nX = n[rg::NEED]; }
     const int nx = nX < 32 ? nX : 32;
     const bool mine = (int)lane < nx;
-    // lane i takes the i-th slot of stage X in slot order
-    unsigned s = 0;
+    // each slot of stage X goes to the lane of its rank (the first 32 in slot order)
+    const unsigned lt = (1u << lane) - 1u;
     int below = 0;
-    bool found = false;
 #pragma unroll
     for (int g = 0; g < rg::kSPT; g++) {
       const unsigned m = X == rg::SAMPLE ? ms[g][rg::SAMPLE] : (X == rg::WALK ? ms[g][rg::WALK] : ms[g][rg::NEED]);
-      const int c = __popc(m);
-      if (mine && !found && (int)lane < below + c) {
-        s = wbase + 32u * g + (unsigned)__fns(m, 0u, (int)lane - below + 1);
-        found = true;
-      }
-      below += c;
+      const int r = below + __popc(m & lt);
+      if (((m >> lane) & 1u) && r < 32) sel[r] = (uint16_t)(wbase + 32u * g + lane);
+      below += __popc(m);
     }
+    __syncwarp();
+    const unsigned s = mine ? (unsigned)sel[lane] : 0u;
     if (X == rg::SAMPLE) {
       if (mine) rg::sample<SK>(P, S, sch, s, tot);
     } else if (X == rg::WALK) {
