@@ -1301,7 +1301,7 @@ mdwt_status grow_pair(mdwt_batch *b, T **h, T **d, size_t &cap, size_t n) {
 
 struct GroupPlan {
   int mode, store;
-  bool stats, ext, shade;
+  bool stats, ext, shade, regroup;
   int first, count;           // request slots [first, first + count) of the params array
   int pixFirst;               // offset of the group's nReq + 1 pixel offsets
   unsigned long long totalItems, totalPix;
@@ -1310,7 +1310,8 @@ struct GroupPlan {
 long long variant_key(const TrackParams &p, int store, bool stats) {
   const bool ext = p.shadows || p.recT;
   const bool shade = p.shadows || p.gradient;
-  return (long long)p.mode * 16 + store * 8 + (stats ? 4 : 0) + (ext ? 2 : 0) + (shade ? 1 : 0);
+  const bool rg = !stats && !ext && regroup_fits(p);
+  return (long long)p.mode * 32 + (rg ? 16 : 0) + store * 8 + (stats ? 4 : 0) + (ext ? 2 : 0) + (shade ? 1 : 0);
 }
 
 }  // namespace
@@ -1420,6 +1421,7 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
     GroupPlan g;
     g.mode = p0.mode; g.store = b->reqs[order[k]]->store; g.stats = b->reqs[order[k]]->statsOn;
     g.ext = p0.shadows || p0.recT; g.shade = p0.shadows || p0.gradient;
+    g.regroup = !g.stats && !g.ext && regroup_fits(p0);   // the whole group, by its key
     g.first = k; g.count = e - k;
     g.pixFirst = (int)pix.size();
     // the group's persistent grid: chunks sized like the single-request launch
@@ -1470,6 +1472,7 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
       const GroupPlan &g = groups[gi];
       BatchGroup bg;
       bg.mode = g.mode; bg.storeKind = g.store; bg.stats = g.stats; bg.ext = g.ext; bg.shade = g.shade;
+      bg.regroup = g.regroup;
       bg.reqs = b->dParams + g.first;
       bg.nReq = g.count;
       bg.dispensers = b->dDisp + g.first;

@@ -98,6 +98,7 @@ struct TrackParams {
 struct BatchGroup {
   int mode, storeKind;
   bool stats, ext, shade;                // per-pixel stats; extended trace; shaded resolve
+  bool regroup;                          // -m 2, every request regroupable (regroup_fits)
   const TrackParams *reqs;               // the group's requests (chunk = dispenser chunk)
   int nReq;
   unsigned *dispensers;                  // one work counter per request, zeroed before the launch
@@ -105,6 +106,8 @@ struct BatchGroup {
   const unsigned long long *pixOfs;      // nReq + 1 prefix offsets of W*H
   unsigned long long totalPix;
 };
+// -m 2 with MDWT_TUNE_REGROUP on and slot fields that fit the regrouped tracker's packing.
+bool regroup_fits(const TrackParams &p);
 // Blocks per SM of the batched trace kernel of a variant (for chunk sizing).
 int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext);
 int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launches, int *grid);

@@ -843,6 +843,65 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
 }
 }  // namespace rg
 
+namespace rg {
+// One warp's regrouped tracking loop over the work items [0, limit) of request P, drawn
+// from `dispenser`: its 64 slots start empty and the loop ends when each has run out of
+// items.  sel is the warp's 32-entry lane table in shared memory.
+template <int SK>
+__device__ __forceinline__ void run_warp(const TrackParams &P, Slots &S, uint16_t *sel, unsigned wbase, unsigned lane,
+                                         const ChanSm *sch, unsigned *dispenser, unsigned limit, uint32_t (&tot)[5]) {
+  const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
+#pragma unroll
+  for (int g = 0; g < kSPT; g++) S.meta[wbase + 32u * g + lane] = NEED;
+  __syncwarp();
+  while (true) {
+    // the warp's slots by stage (two stage bits per slot); the most populated stage runs,
+    // lane i on the i-th slot of that stage in slot order
+    unsigned ms[kSPT][3];
+    int n[3] = {0, 0, 0};
+#pragma unroll
+    for (int g = 0; g < kSPT; g++) {
+      const uint32_t st = S.meta[wbase + 32u * g + lane];
+      const unsigned b0 = __ballot_sync(kFull, st & 1u), b1 = __ballot_sync(kFull, st & 2u);
+      ms[g][NEED] = ~b0 & ~b1;
+      ms[g][WALK] = b0 & ~b1;
+      ms[g][SAMPLE] = ~b0 & b1;
+#pragma unroll
+      for (int X = 0; X < 3; X++) n[X] += __popc(ms[g][X]);
+    }
+    if (n[0] + n[1] + n[2] == 0) break;   // every slot is out of work items
+    int X = SAMPLE, nX = n[SAMPLE];
+    if (n[WALK] > nX) { X = WALK; nX = n[WALK]; }
+    if (n[NEED] > nX) { X = NEED; nX = n[NEED]; }
+    const int nx = nX < 32 ? nX : 32;
+    const bool mine = (int)lane < nx;
+    // each slot of stage X goes to the lane of its rank (the first 32 in slot order)
+    const unsigned lt = (1u << lane) - 1u;
+    int below = 0;
+#pragma unroll
+    for (int g = 0; g < kSPT; g++) {
+      const unsigned m = X == SAMPLE ? ms[g][SAMPLE] : (X == WALK ? ms[g][WALK] : ms[g][NEED]);
+      const int r = below + __popc(m & lt);
+      if (((m >> lane) & 1u) && r < 32) sel[r] = (uint16_t)(wbase + 32u * g + lane);
+      below += __popc(m);
+    }
+    __syncwarp();
+    const unsigned s = mine ? (unsigned)sel[lane] : 0u;
+    if (X == SAMPLE) {
+      if (mine) sample<SK>(P, S, sch, s, tot);
+    } else if (X == WALK) {
+      if (mine) walk(P, S, s, maxCells, tot);
+    } else {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(dispenser, (unsigned)nx);
+      base = __shfl_sync(kFull, base, 0);
+      if (mine) start(P, S, s, base + lane, limit, tot);
+    }
+    __syncwarp();
+  }
+}
+}  // namespace rg
+
 template <int SK>
 __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel(const __grid_constant__ TrackParams P) {
   extern __shared__ __align__(16) unsigned char rgSmem[];
@@ -851,60 +910,42 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel
   __shared__ uint16_t selAll[rg::kTPB];                    // per warp: the slot each lane runs
   const unsigned tid = threadIdx.x, lane = tid & 31u;
   const unsigned wbase = (tid >> 5) * (32u * rg::kSPT);   // the warp's slots: group g is wbase + 32 g + lane
-  uint16_t *sel = selAll + (tid & ~31u);
   if (tid < (unsigned)P.C) sch[tid] = chan_params(P, (int)tid);
-#pragma unroll
-  for (int g = 0; g < rg::kSPT; g++) S.meta[wbase + 32u * g + lane] = rg::NEED;
   __syncthreads();   // the channel table
-  const unsigned limit = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
-  const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
   uint32_t tot[5] = {0, 0, 0, 0, 0};
-  while (true) {
-    // the warp's slots by stage (two stage bits per slot); the most populated stage runs,
-    // lane i on the i-th slot of that stage in slot order
-    unsigned ms[rg::kSPT][3];
-    int n[3] = {0, 0, 0};
-#pragma unroll
-    for (int g = 0; g < rg::kSPT; g++) {
-      const uint32_t st = S.meta[wbase + 32u * g + lane];
-      const unsigned b0 = __ballot_sync(kFull, st & 1u), b1 = __ballot_sync(kFull, st & 2u);
-      ms[g][rg::NEED] = ~b0 & ~b1;
-      ms[g][rg::WALK] = b0 & ~b1;
-      ms[g][rg::SAMPLE] = ~b0 & b1;
-#pragma unroll
-      for (int X = 0; X < 3; X++) n[X] += __popc(ms[g][X]);
-    }
-    if (n[0] + n[1] + n[2] == 0) break;   // every slot is out of work items
-    int X = rg::SAMPLE, nX = n[rg::SAMPLE];
-    if (n[rg::WALK] > nX) { X = rg::WALK; nX = n[rg::WALK]; }
-    if (n[rg::NEED] > nX) { X = rg::NEED; nX = n[rg::NEED]; }
-    const int nx = nX < 32 ? nX : 32;
-    const bool mine = (int)lane < nx;
-    // each slot of stage X goes to the lane of its rank (the first 32 in slot order)
-    const unsigned lt = (1u << lane) - 1u;
-    int below = 0;
-#pragma unroll
-    for (int g = 0; g < rg::kSPT; g++) {
-      const unsigned m = X == rg::SAMPLE ? ms[g][rg::SAMPLE] : (X == rg::WALK ? ms[g][rg::WALK] : ms[g][rg::NEED]);
-      const int r = below + __popc(m & lt);
-      if (((m >> lane) & 1u) && r < 32) sel[r] = (uint16_t)(wbase + 32u * g + lane);
-      below += __popc(m);
-    }
+  rg::run_warp<SK>(P, S, selAll + (tid & ~31u), wbase, lane, sch, P.workCounter,
+                   (unsigned)P.numTiles * 32u * (unsigned)P.sCount, tot);
+  flush_counters(P.counters, tot);
+}
+
+// Batched variant of the regrouped tracker: a warp takes the requests in turn, as
+// trace_batch_kernel does, and runs the regrouped loop on each with that request's
+// dispenser and channel table.
+template <int SK>
+__global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks)
+    trace_batch_regroup_kernel(const TrackParams *__restrict__ reqs, int nReq, unsigned *dispensers) {
+  extern __shared__ __align__(16) unsigned char rgSmem[];
+  rg::Slots &S = *reinterpret_cast<rg::Slots *>(rgSmem);
+  __shared__ ChanSm sch[rg::kTPB / 32][kMaxChannels];
+  __shared__ uint16_t selAll[rg::kTPB];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned gw = blockIdx.x * (rg::kTPB / 32) + warp;
+  const unsigned wbase = warp * (32u * rg::kSPT);
+  for (int i = 0; i < nReq; i++) {
+    const int r = (int)((gw + (unsigned)i) % (unsigned)nReq);
+    const TrackParams &P = reqs[r];
+    const unsigned total = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
+    unsigned peek = 0;
+    if (lane == 0) peek = *(volatile unsigned *)(dispensers + r);
+    peek = __shfl_sync(kFull, peek, 0);
+    if (peek >= total) continue;   // nothing left of this request
+    if (lane < (unsigned)P.C) sch[warp][lane] = chan_params(P, (int)lane);
     __syncwarp();
-    const unsigned s = mine ? (unsigned)sel[lane] : 0u;
-    if (X == rg::SAMPLE) {
-      if (mine) rg::sample<SK>(P, S, sch, s, tot);
-    } else if (X == rg::WALK) {
-      if (mine) rg::walk(P, S, s, maxCells, tot);
-    } else {
-      unsigned base = 0;
-      if (lane == 0) base = atomicAdd(P.workCounter, (unsigned)nx);
-      base = __shfl_sync(kFull, base, 0);
-      if (mine) rg::start(P, S, s, base + lane, limit, tot);
-    }
+    uint32_t tot[5] = {0, 0, 0, 0, 0};
+    rg::run_warp<SK>(P, S, selAll + warp * 32u, wbase, lane, sch[warp], dispensers + r, total, tot);
+    flush_counters(P.counters, tot);
     __syncwarp();
   }
-  flush_counters(P.counters, tot);
 }
 
 // Batched variant: many requests (render contexts) in one persistent launch.  Every
@@ -1261,14 +1302,6 @@ __global__ void __launch_bounds__(256) resolve_batch_kernel(const TrackParams *_
   }
 }
 
-// The regrouped tracker's packed slot fields: cells < 1024 per axis, at most 2047 cells
-// entered, 32-bit record indices.
-bool regroup_fits(const TrackParams &p) {
-  const size_t nrect = (size_t)(p.cullX1 - p.cullX0 + 1) * (size_t)(p.cullY1 - p.cullY0 + 1);
-  return p.mode == 2 && p.regroup && p.mc[0] <= 1024u && p.mc[1] <= 1024u && p.mc[2] <= 1024u &&
-         p.mc[0] + p.mc[1] + p.mc[2] + 3u <= 2047u && nrect * (size_t)p.sCount < ((size_t)1 << 32);
-}
-
 template <int SK>
 int launch_resolve(const TrackParams &p, cudaStream_t st, int numSMs) {
   const size_t npix = (size_t)p.W * (size_t)(p.rowHi - p.rowLo);
@@ -1349,8 +1382,31 @@ int launch_tb(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
   return (int)cudaGetLastError();
 }
 
+template <int SK>
+int launch_tb_regroup(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
+  const int smem = (int)sizeof(rg::Slots);
+  cudaError_t e = cudaFuncSetAttribute(trace_batch_regroup_kernel<SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return (int)e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_regroup_kernel<SK>, rg::kTPB, smem);
+  if (e != cudaSuccess) return (int)e;
+  if (bps < 1) bps = 1;
+  *grid = numSMs * bps;
+  if (g.totalItems > 0) trace_batch_regroup_kernel<SK><<<*grid, rg::kTPB, smem, st>>>(g.reqs, g.nReq, g.dispensers);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  size_t rg = (size_t)((g.totalPix + 255) / 256);
+  if (rg > (size_t)numSMs * 8) rg = (size_t)numSMs * 8;
+  if (rg == 0) return (int)cudaSuccess;
+  resolve_batch_kernel<false, false, SK><<<(unsigned)rg, 256, 0, st>>>(g.reqs, g.pixOfs, g.nReq);
+  return (int)cudaGetLastError();
+}
+
 template <int MODE, int SK>
 int launch_tbs(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
+  if constexpr (MODE == 2) {
+    if (g.regroup && !g.stats && !g.ext) return launch_tb_regroup<SK>(g, st, numSMs, grid);
+  }
   if (g.ext) return g.stats ? launch_tb<MODE, SK, true, true>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, true>(g, st, numSMs, grid);
   return g.stats ? launch_tb<MODE, SK, true, false>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, false>(g, st, numSMs, grid);
 }
@@ -1367,6 +1423,14 @@ int occ_tbs(bool stats, bool ext) {
 }
 
 }  // namespace
+
+// The regrouped tracker's packed slot fields: cells < 1024 per axis, at most 2047 cells
+// entered, 32-bit record indices.
+bool regroup_fits(const TrackParams &p) {
+  const size_t nrect = (size_t)(p.cullX1 - p.cullX0 + 1) * (size_t)(p.cullY1 - p.cullY0 + 1);
+  return p.mode == 2 && p.regroup && p.mc[0] <= 1024u && p.mc[1] <= 1024u && p.mc[2] <= 1024u &&
+         p.mc[0] + p.mc[1] + p.mc[2] + 3u <= 2047u && nrect * (size_t)p.sCount < ((size_t)1 << 32);
+}
 
 int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext) {
   const bool u8 = storeKind == kStoreU8;
