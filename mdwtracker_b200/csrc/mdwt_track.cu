@@ -650,7 +650,6 @@ constexpr int kTPB = 256;
 constexpr int kSPT = 2;                  // path slots per thread
 constexpr int kSlots = kTPB * kSPT;
 constexpr int kMinBlocks = 4;            // 64 registers, 32 warps per SM
-constexpr int kWalkCells = 1 << 20;      // cells a walk may enter before it yields the lane
 enum : uint32_t { NEED = 0, WALK = 1, SAMPLE = 2, DONE = 3 };
 // meta word: bits 0-1 stage, bit 2 a channel is selected (free flights pending), bit 3
 // the cell's channels are exhausted (advance the walk), bits 4-7 channel, bit 8 capped,
@@ -748,16 +747,13 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
   DDA d;
   load_dda(S, s, d);
   d.visits = visits;
-  bool moved = false, paused = false;
-  int cellsLeft = kWalkCells;
+  bool moved = false;
   uint32_t stage = WALK;
   for (int k = 0;;) {
     if (!drawing) {
       bool ended = false;
       while (true) {
         if (advance) {
-          if (cellsLeft == 0) { paused = true; break; }   // bounded walk: resume at this cell boundary
-          cellsLeft--;
           if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ended = true; break; }
           float ct1;
           enter(P, d, ct1, cmask);
@@ -781,7 +777,6 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
         break;
       }
       if (ended) { finish(P, S, s, record, false, tot); return; }
-      if (paused) break;
       drawing = true;
     }
     // free-flight draw (deviceCode.cu:800-820)
