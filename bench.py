@@ -14,7 +14,9 @@ timed steps, outside the timed events.  `value` is device time (CUDA events on t
 render stream); `e2e` goes through the C ABI with host buffers: camera update (host to
 device), frame, framebuffer copy to pinned host memory.  Under torchrun every rank
 renders its own frames (different frame seeds) with no collective: per-GPU work is
-fixed, `scaling` is weak, and time is the max over ranks.
+fixed, `scaling` is weak, and time is the max over ranks.  Before timing, the tracker
+schedule is tuned for the workload (mdwt_autotune_schedule on launches of the step's
+shape; --no-autotune keeps the defaults) and reported in config.schedule.
 
 time_to_rmse (rank 0, one GPU; --no-ttr skips it): the first part of the headline metric
 -- how long plain accumulation takes at 1920x1080 (the 6 x 512^3 float32 log-normal scene,
@@ -565,7 +567,7 @@ def main():
     paths = w * h * sc.spp * sc.frames
     value = world * paths / (ms / 1e3) / 1e9
 
-    # algorithmic bytes of the dominant kernel (trace_kernel) per launch: 8*bpv per
+    # algorithmic bytes of the dominant kernel (the tracker) per launch: 8*bpv per
     # density sample (trilinear footprint), 4*C_read per macrocell visit (majorants;
     # C for syncDDA, 1 otherwise); the resolve pass (36 B per pixel) is timed apart
     bpv = 1 if all(v.dtype == np.uint8 for v in sc.volumes) else 4

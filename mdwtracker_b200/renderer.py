@@ -234,8 +234,10 @@ class Renderer:
         self._call("reset_accumulation")
 
     def autotuneSchedule(self, frames: int = 2):
-        """Time frames for each (trips, pool) candidate, keep the fastest; frame ids are
-        restored and the accumulation reset.  Returns (pool, trips)."""
+        """Time `frames`-frame launches for each schedule candidate and keep the fastest:
+        for -m 2 the tracker (regrouped or warp-local) first, then the trips, then the
+        warp-local tracker's pool and quorum.  Frame ids and counters are restored and the
+        accumulation reset.  Returns (pool, trips); getTuning(4) tells the tracker."""
         best = (C.c_int * 2)()
         self._call("autotune_schedule", C.c_int(frames), best)
         return tuple(best)
