@@ -50,6 +50,14 @@ mdwt_status mdwt_denoiser_get_grads(mdwt_denoiser *d, float *host_out);
 /* backward + one Adam step (beta 0.9 / 0.999, eps 1e-8) with learning rate lr. */
 mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *d_features, const float *d_target_rgba, int n,
                                      int h, int w, float lr, double *loss, void *stream);
+/* The pieces of a data-parallel training step (one process per GPU): backward on the
+ * rank's shard, copy_grads into a vector of num_params floats (get_params order; device or
+ * host memory), an all-reduce that averages it over the ranks, load_grads, adam_step.
+ * copy_grads / load_grads are asynchronous on `stream`; adam_step is the update of
+ * train_step, applied to the current gradient buffer. */
+mdwt_status mdwt_denoiser_copy_grads(mdwt_denoiser *d, float *out, void *stream);
+mdwt_status mdwt_denoiser_load_grads(mdwt_denoiser *d, const float *in, void *stream);
+mdwt_status mdwt_denoiser_adam_step(mdwt_denoiser *d, float lr, void *stream);
 
 /* Convolution path: 1 (default) = tcgen05 tensor-core kernels (persistent, warp-specialised;
  * two TMEM accumulators, so a tile's epilogue overlaps the next tile's MMAs) wherever the

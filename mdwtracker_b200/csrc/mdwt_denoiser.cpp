@@ -436,18 +436,55 @@ mdwt_status mdwt_denoiser_backward(mdwt_denoiser *d, const float *F, const float
   return MDWT_OK;
 }
 
-mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *F, const float *T, int n, int h, int w, float lr,
-                                     double *loss, void *stream) {
-  if (!d) return MDWT_ERR_BAD_ARG;
-  if (!(lr > 0.0f) || !std::isfinite(lr)) return fail(d, MDWT_ERR_BAD_ARG, "learning rate");
-  mdwt_status s = mdwt_denoiser_backward(d, F, T, n, h, w, loss, stream);
-  if (s) return s;
+// One Adam step of every layer from the gradient buffer, and the BF16 operand copies.
+static mdwt_status adam_all(mdwt_denoiser *d, float lr, void *stream) {
+  mdwt_status s;
   d->step++;
   for (auto &l : d->L) {
     DCKI(mdwt::nn::adam(l.W, l.mW, l.vW, l.gW, l.Wf, l.Wd, l.cin, l.cout, l.b, l.mb, l.vb, l.gb, lr, 0.9f, 0.999f,
                         1e-8f, d->step, d->numSMs, stream),
          "Adam");
     if (d->useTC && (s = umma_copies(d, l, stream))) return s;
+  }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoiser_train_step(mdwt_denoiser *d, const float *F, const float *T, int n, int h, int w, float lr,
+                                     double *loss, void *stream) {
+  if (!d) return MDWT_ERR_BAD_ARG;
+  if (!(lr > 0.0f) || !std::isfinite(lr)) return fail(d, MDWT_ERR_BAD_ARG, "learning rate");
+  mdwt_status s = mdwt_denoiser_backward(d, F, T, n, h, w, loss, stream);
+  if (s) return s;
+  return adam_all(d, lr, stream);
+}
+
+mdwt_status mdwt_denoiser_adam_step(mdwt_denoiser *d, float lr, void *stream) {
+  if (!d) return MDWT_ERR_BAD_ARG;
+  if (!(lr > 0.0f) || !std::isfinite(lr)) return fail(d, MDWT_ERR_BAD_ARG, "learning rate");
+  DCK(cudaSetDevice(d->device), "cudaSetDevice");
+  return adam_all(d, lr, stream);
+}
+
+mdwt_status mdwt_denoiser_copy_grads(mdwt_denoiser *d, float *out, void *stream) {
+  if (!d || !out) return MDWT_ERR_BAD_ARG;
+  DCK(cudaSetDevice(d->device), "cudaSetDevice");
+  for (auto &l : d->L) {
+    DCK(cudaMemcpyAsync(out, l.gW, l.nW() * 4, cudaMemcpyDefault, (cudaStream_t)stream), "copy gradients");
+    out += l.nW();
+    DCK(cudaMemcpyAsync(out, l.gb, (size_t)l.cout * 4, cudaMemcpyDefault, (cudaStream_t)stream), "copy gradients");
+    out += l.cout;
+  }
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_denoiser_load_grads(mdwt_denoiser *d, const float *in, void *stream) {
+  if (!d || !in) return MDWT_ERR_BAD_ARG;
+  DCK(cudaSetDevice(d->device), "cudaSetDevice");
+  for (auto &l : d->L) {
+    DCK(cudaMemcpyAsync(l.gW, in, l.nW() * 4, cudaMemcpyDefault, (cudaStream_t)stream), "load gradients");
+    in += l.nW();
+    DCK(cudaMemcpyAsync(l.gb, in, (size_t)l.cout * 4, cudaMemcpyDefault, (cudaStream_t)stream), "load gradients");
+    in += l.cout;
   }
   return MDWT_OK;
 }

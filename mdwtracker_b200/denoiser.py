@@ -99,6 +99,24 @@ class Denoiser:
                    C.c_void_p(stream or None))
         return loss.value
 
+    def _grad_buffer(self, x):
+        if hasattr(x, "numel") and x.numel() != self.numParams(self._lib):
+            raise ValueError(f"expected {self.numParams(self._lib)} gradient entries, got {x.numel()}")
+        return _ptr(x)
+
+    def copyGrads(self, out, stream: int = 0) -> None:
+        """The gradient buffer into `out` (a float32 CUDA tensor of numParams entries, in
+        params() order), asynchronously on `stream`."""
+        self._call("copy_grads", self._grad_buffer(out), C.c_void_p(stream or None))
+
+    def loadGrads(self, src, stream: int = 0) -> None:
+        """Replace the gradient buffer by `src` (as copyGrads lays it out), on `stream`."""
+        self._call("load_grads", self._grad_buffer(src), C.c_void_p(stream or None))
+
+    def adamStep(self, lr: float, stream: int = 0) -> None:
+        """One Adam step from the current gradient buffer (the update of trainStep)."""
+        self._call("adam_step", C.c_float(lr), C.c_void_p(stream or None))
+
     def trainStep(self, features, target, n: int, h: int, w: int, lr: float, stream: int = 0,
                   want_loss: bool = True) -> Optional[float]:
         loss = C.c_double()

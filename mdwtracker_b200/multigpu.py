@@ -1,5 +1,7 @@
-"""Multi-GPU frames: one process per GPU renders a band of image rows, and the bands are
-gathered with torch.distributed (NCCL between GPUs, gloo on CPU).
+"""Multi-GPU frames and denoiser training over torch.distributed (NCCL between GPUs, gloo on
+CPU).
+
+Frames: one process per GPU renders a band of image rows, and the bands are gathered.
 
 Pixels are independent in the tracker (every path-sample depends only on its pixel,
 sample index and frame id, deviceCode.cu:293-298), so disjoint row bands rendered by
@@ -85,3 +87,45 @@ class BandRenderer:
     def _on_gpu(self) -> bool:
         import torch.distributed as dist
         return dist.get_backend(self.group) == "nccl"
+
+
+class DataParallelTrainer:
+    """Data-parallel training of the learned denoiser, one process per GPU.
+
+    Every rank runs the backward pass on its shard of each minibatch.  One all-reduce
+    averages the gradient vector (470,640 floats for the committed network) over the ranks,
+    and every rank applies the same Adam step, so the parameters stay identical
+    everywhere.  With equal shard sizes the averaged gradient is the full minibatch's,
+    because the loss is a mean over the shard.  `denoiser` is a Denoiser, or any object
+    with its params / backward / copyGrads / loadGrads / adamStep calls."""
+
+    def __init__(self, denoiser, group=None):
+        import torch
+        import torch.distributed as dist
+        self.d = denoiser
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        p = np.asarray(denoiser.params())
+        dev = "cuda" if dist.is_initialized() and dist.get_backend(group) == "nccl" else getattr(denoiser, "device", "cuda")
+        self.g = torch.empty(p.size, dtype=torch.float32 if p.dtype == np.float32 else torch.float64, device=dev)
+
+    def step(self, features, target, n: int, h: int, w: int, lr: float, stream: int = 0) -> float:
+        """One training step on this rank's shard [n][h][w]; returns the loss averaged over
+        the ranks."""
+        import torch
+        import torch.distributed as dist
+        loss = self.d.backward(features, target, n, h, w, stream)
+        if self.world > 1:
+            self.d.copyGrads(self.g, stream)
+            if self.g.is_cuda:
+                torch.cuda.synchronize(self.g.device)   # the copy on `stream` before the collective
+            dist.all_reduce(self.g, group=self.group)
+            self.g /= self.world
+            if self.g.is_cuda:
+                torch.cuda.synchronize(self.g.device)   # the collective before the library reads it
+            self.d.loadGrads(self.g, stream)
+            t = torch.tensor([loss], dtype=torch.float64, device=self.g.device)
+            dist.all_reduce(t, group=self.group)
+            loss = float(t.item()) / self.world
+        self.d.adamStep(lr, stream)
+        return loss

@@ -1,6 +1,7 @@
 """Train the learned denoiser on frame pairs the tracker renders itself.
 
   python -m mdwtracker_b200.train_denoiser [--pairs 2000] [--steps 3000] [--out weights.npy]
+  torchrun --nproc-per-node N -m mdwtracker_b200.train_denoiser ...   (data-parallel, one GPU per rank)
 
 Data: the 6 x 512^3 float32 log-normal scene and the 3 x 256^3 uint8 sparse-noise scene
 (syncDDA; half the pairs each by default), random cameras around the volume
@@ -15,6 +16,11 @@ run in libmdwt's own kernels (include/mdwt_denoiser.h).
 
 Evaluation (--eval): on the default 1920x1080 view, the RMSE against the FP64 expected
 image of the plain k-spp frame and of its denoised version.
+
+Under torchrun (WORLD_SIZE > 1) every rank renders its share of the pairs (its own cameras
+and transfer functions), all ranks start from the same weights, and each minibatch of
+--batch crops is split over the ranks: multigpu.DataParallelTrainer averages the
+gradients with one all-reduce per step (NCCL).  Rank 0 saves and evaluates.
 """
 from __future__ import annotations
 
@@ -102,7 +108,9 @@ def render_pairs(r, n_pairs, res, spp_choices, target_spp, rng, log=None):
     return F, T
 
 
-def train(den, F, T, steps, batch, lr0, rng, log=None):
+def train(den, F, T, steps, batch, lr0, rng, log=None, trainer=None):
+    """Adam with cosine decay on minibatches of `batch` crops; with a data-parallel
+    `trainer`, `batch` is this rank's share of the minibatch."""
     import torch
     n, h, w = F.shape[0], F.shape[1], F.shape[2]
     losses = []
@@ -112,7 +120,10 @@ def train(den, F, T, steps, batch, lr0, rng, log=None):
         fb = F.index_select(0, idx).contiguous()
         tb = T.index_select(0, idx).contiguous()
         want = (s % 100 == 0) or s == steps - 1
-        loss = den.trainStep(fb, tb, batch, h, w, lr, want_loss=want)
+        if trainer is not None:
+            loss = trainer.step(fb, tb, batch, h, w, lr, torch.cuda.current_stream().cuda_stream)
+        else:
+            loss = den.trainStep(fb, tb, batch, h, w, lr, want_loss=want)
         if want:
             losses.append((s, loss))
             if log and s % 500 == 0:
@@ -166,14 +177,29 @@ def main(argv=None):
     ap.add_argument("--scenes", nargs="+", default=["c3", "c2"], choices=["c2", "c3"],
                     help="volumes of the training pairs (half the pairs each)")
     a = ap.parse_args(argv)
+    import os
     import torch
     from . import Denoiser, Renderer
     from . import synthetic as syn
 
-    def log(m):
-        print(m, file=sys.stderr, flush=True)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    trainer = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        if a.batch % world:
+            raise SystemExit(f"--batch {a.batch} must be a multiple of the {world} ranks")
+        torch.cuda.set_device(dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", dev))
 
-    rng = np.random.default_rng(a.seed)
+    def log(m):
+        if rank == 0:
+            print(m, file=sys.stderr, flush=True)
+
+    # each rank renders and samples its own data; the weights start identical on all ranks
+    rng = np.random.default_rng(a.seed + 7919 * rank)
     t0 = time.perf_counter()
     sc = syn.scene_c3(mode=2)
     scenes = [sc]
@@ -181,38 +207,46 @@ def main(argv=None):
         scenes.append(syn.scene_c2())
     if "c3" not in a.scenes:
         scenes = scenes[1:]
-    renderers = [s.setup(Renderer(0)) for s in scenes]
+    renderers = [s.setup(Renderer(dev)) for s in scenes]
     log(f"scenes ready in {time.perf_counter() - t0:.1f} s")
-    den = Denoiser(0, seed=a.seed)
+    den = Denoiser(dev, seed=a.seed)
     if a.init:
         den.load(a.init)
+    if world > 1:
+        from .multigpu import DataParallelTrainer
+        trainer = DataParallelTrainer(den)
     report = {"pairs": a.pairs, "res": a.res, "spp": a.spp, "target_spp": a.target_spp, "steps": a.steps,
-              "batch": a.batch, "lr": a.lr}
+              "batch": a.batch, "lr": a.lr, "ranks": world}
     if a.steps > 0:
         t0 = time.perf_counter()
-        import torch as _t
-        parts = [render_pairs(rr, a.pairs // len(renderers), a.res, a.spp, a.target_spp, rng, log) for rr in renderers]
-        F = _t.cat([p[0] for p in parts]) if len(parts) > 1 else parts[0][0]
-        T = _t.cat([p[1] for p in parts]) if len(parts) > 1 else parts[0][1]
+        share = a.pairs // world   # this rank's pairs
+        parts = [render_pairs(rr, share // len(renderers), a.res, a.spp, a.target_spp, rng, log) for rr in renderers]
+        F = torch.cat([p[0] for p in parts]) if len(parts) > 1 else parts[0][0]
+        T = torch.cat([p[1] for p in parts]) if len(parts) > 1 else parts[0][1]
         del parts
         report["data_s"] = time.perf_counter() - t0
         report["scenes"] = [s.name for s in scenes]
         t0 = time.perf_counter()
-        losses = train(den, F, T, a.steps, a.batch, a.lr, rng, log)
+        losses = train(den, F, T, a.steps, a.batch // world, a.lr, rng, log, trainer)
         torch.cuda.synchronize()
         report["train_s"] = time.perf_counter() - t0
         report["loss_first_last"] = [losses[0][1], losses[-1][1]]
         del F, T
-        if a.out:
+        if a.out and rank == 0:
             den.save(a.out)
-    if a.eval:
-        r2 = sc.setup(Renderer(0))
+    if a.eval and rank == 0:
+        r2 = sc.setup(Renderer(dev))
         r2.renderExpected(8, 0.25)
         report["eval"] = evaluate(r2, den, a.eval_spp)
         r2.close()
-    print(json.dumps(report))
+    if rank == 0:
+        print(json.dumps(report))
     for rr in renderers:
         rr.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 

@@ -199,3 +199,55 @@ def test_bounded_wait_gives_up_and_recovers():
     d.check()
     assert torch.equal(again, ref)
     d.close()
+
+
+@pytest.mark.gpu
+def test_gradient_copies_and_adam_step():
+    """copy_grads / load_grads move the gradient vector exactly; adam_step applies Adam's
+    update to it (first step from a fresh state, against a float32 restatement)."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    d = Denoiser(0, seed=3)
+    P0 = d.params()
+    G = (np.random.default_rng(0).standard_normal(P0.size) * 1e-2).astype(np.float32)
+    g = torch.from_numpy(G).cuda()
+    d.setParams(P0)   # fresh Adam state
+    d.loadGrads(g)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d.grads(), G)
+    back = torch.zeros_like(g)
+    d.copyGrads(back)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(back.cpu().numpy(), G)
+    with pytest.raises(ValueError):
+        d.copyGrads(back[:-1])
+    lr = 1e-3
+    d.adamStep(lr)
+    P1 = d.params()
+    f = np.float32
+    m = (f(1) - f(0.9)) * G
+    v = (f(1) - f(0.999)) * G * G
+    step = f(lr) * (m / (f(1) - f(0.9))) / (np.sqrt(v / (f(1) - f(0.999))) + f(1e-8))
+    np.testing.assert_allclose(P0 - P1, step, rtol=1e-4, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_shard_gradients_average_to_the_minibatch_gradient():
+    """The premise of data-parallel training (multigpu.DataParallelTrainer): the loss is a
+    mean over the shard, so the average of two equal shards' gradients is the whole
+    minibatch's gradient, up to summation order and BF16 rounding."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(4)
+    n, h, w = 4, 24, 32
+    F = torch.from_numpy(_features(rng, n, h, w)).cuda()
+    T = torch.from_numpy(rng.random((n, h, w, 4)).astype(np.float32)).cuda()
+    d = Denoiser(0, seed=5)
+    d.backward(F, T, n, h, w)
+    full = d.grads().astype(np.float64)
+    d.backward(F[:2].contiguous(), T[:2].contiguous(), 2, h, w)
+    a = d.grads().astype(np.float64)
+    d.backward(F[2:].contiguous(), T[2:].contiguous(), 2, h, w)
+    b = d.grads().astype(np.float64)
+    rel = np.linalg.norm(0.5 * (a + b) - full) / np.linalg.norm(full)
+    assert rel < 1e-2, rel
