@@ -238,3 +238,72 @@ def test_shadow_rays_back_towards_the_camera_follow_the_shared_shadow_seed(oracl
         assert abs(u - u1) < 4.5 * sigma + 0.01, (px, py, u, u1)
         us.append(u1)
     assert max(us) - min(us) > 0.05    # the pixels' generators differ
+
+
+def _two_channel_scene(oracle, mode, alphas, colours, spp, res=(33, 33)):
+    """Two constant channels over the unit cube with constant TF opacities `alphas` (cubed
+    on upload, so given as their cube roots) and flat colours."""
+    o = oracle.OracleRenderer()
+    for _ in alphas:
+        o.PushMesh(np.full((32, 32, 32), 128, np.uint8))
+    o.macrocellDims = (4, 4, 4)
+    o.Resize(res)
+    o.Init(mode)
+    for c, (a, rgb) in enumerate(zip(alphas, colours)):
+        tf = np.zeros((256, 4), np.float32)
+        tf[:, :3] = rgb
+        tf[:, 3] = np.float32(a) ** (1.0 / 3.0)
+        o.SetXFColormap(tf, c)
+        o.SetXFOpacityScale(1.0, c)
+        o.SetXFRange((0.0, 1.0), c)
+    o.setSpp(spp)
+    o.setBackground((0.0, 0.0, 0.0))
+    o.enablePixelStats(True)
+    return o
+
+
+def _path_length(o, px, py, res):
+    """Mean length through [0,1]^3 of the pixel's rays over its diagonal jitter."""
+    basis = o.cameraBasis()
+    org = basis[0].astype(np.float64)
+    out = []
+    for j in np.linspace(0.0, 1.0, 33)[:-1] + 1.0 / 64:
+        s = (np.array([px, py]) + j) / np.array(res)
+        d = basis[1] + s[0] * basis[2] + s[1] * basis[3] - org
+        d /= np.linalg.norm(d)
+        with np.errstate(divide="ignore"):
+            t0, t1 = (0.0 - org) / d, (1.0 - org) / d
+        out.append(max(0.0, np.min(np.maximum(t0, t1)) - np.max(np.minimum(t0, t1))))
+    return out
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
+def test_superposed_constant_channels(oracle, mode):
+    """Every tracker samples the first collision of the superposed medium: with constant
+    channel densities a0, a1 the hit probability is 1 - exp(-(a0 + a1) L / dt), and a hit
+    lands on channel c with probability a_c / (a0 + a1).  The blends (-m 4, -m 5) sample
+    the maximum channel opacity: 1 - exp(-max(a0, a1) L / dt)."""
+    alphas, colours, spp, res = (0.003, 0.006), ((1.0, 0.0, 0.0), (0.0, 1.0, 0.0)), 2048, (33, 33)
+    o = _two_channel_scene(oracle, mode, alphas, colours, spp, res)
+    o.Render()
+    st, acc, dt = o.pixelStats(), o.accum(), o.dt
+    density = max(alphas) if mode >= 4 else sum(alphas)
+    # the shaded colour of a hit on each channel: a single dense channel hits on every sample
+    hit_rgb = []
+    for rgb in colours:
+        d = _two_channel_scene(oracle, 2, (1.0,), (rgb,), 4, (3, 3))
+        d.Render()
+        hit_rgb.append(d.accum()[1, 1, :3].astype(np.float64))
+        assert d.pixelStats()[1, 1, 2] == 4
+    M = np.stack(hit_rgb, axis=1)[:2]          # [R, G] rows, channel columns
+    for (py, px) in [(16, 16), (14, 18), (10, 12), (20, 22)]:
+        p = float(np.mean([1.0 - math.exp(-density * L / dt) for L in _path_length(o, px, py, res)]))
+        hits = int(st[py, px, 2])
+        sigma = math.sqrt(p * (1 - p) / spp)
+        assert abs(hits / spp - p) < 4.5 * sigma, (mode, px, py, hits / spp, p)
+        if mode <= 3:   # channel shares from the colour: rgb = sum_c (hits_c / spp) * hit_rgb_c
+            n0, n1 = np.linalg.solve(M, acc[py, px, :2].astype(np.float64)) * spp
+            assert abs(n0 + n1 - hits) < 0.05 * hits + 1.0
+            share = alphas[0] / sum(alphas)
+            s_sigma = math.sqrt(share * (1 - share) / hits)
+            assert abs(n0 / (n0 + n1) - share) < 4.5 * s_sigma, (mode, px, py, n0 / (n0 + n1))
