@@ -307,3 +307,33 @@ def test_superposed_constant_channels(oracle, mode):
             share = alphas[0] / sum(alphas)
             s_sigma = math.sqrt(share * (1 - share) / hits)
             assert abs(n0 / (n0 + n1) - share) < 4.5 * s_sigma, (mode, px, py, n0 / (n0 + n1))
+
+
+def test_majorants_follow_the_tf_range_and_opacity_scale(oracle):
+    """renderer.cu:159-203: a cell's value range [lo, hi] is remapped through the TF range,
+    addr = r * N; the majorant is the largest TF opacity over texels floor(addr(lo)) ..
+    ceil(addr(hi)) (clamped), times the opacity scale.  With a monotone ramp that is the
+    texel at the ceiling.  Volume 16^3 float32: 0.33 for z < 8, 0.05 above; 4^3 cells; TF
+    range (0.1, 0.7): 0.33 -> r = 0.3833, addr 98.1 -> texels 98..99; 0.05 -> r < 0 ->
+    texel 0 (opacity 0)."""
+    vol = np.full((16, 16, 16), 0.05, np.float32)
+    vol[:8] = 0.33                                 # [z][y][x]
+    tf = np.zeros((256, 4), np.float32)
+    tf[:, 0] = 1.0
+    tf[:, 3] = np.arange(256, dtype=np.float32) / np.float32(255)   # cubed on upload
+    o = oracle.OracleRenderer()
+    o.PushMesh(vol)
+    o.macrocellDims = (4, 4, 4)
+    o.Resize((8, 8))
+    o.Init(2)
+    o.SetXFColormap(tf, 0)
+    o.SetXFOpacityScale(0.5, 0)
+    o.SetXFRange((0.1, 0.7), 0)
+    maj = o.majorants().reshape(4, 4, 4)           # [cz][cy][cx]
+    top = np.float32(0.5) * np.float32(np.float32(99) / np.float32(255)) ** 3
+    # cells 0..2 along z see 0.33 (cell 1 and 2 through the 27-neighbour boxes at z = 7|8)
+    np.testing.assert_allclose(maj[:3], top, rtol=1e-6)
+    np.testing.assert_array_equal(maj[3], 0.0)
+    # doubling the opacity scale doubles the majorants
+    o.SetXFOpacityScale(1.0, 0)
+    np.testing.assert_allclose(o.majorants().reshape(4, 4, 4)[:3], 2 * top, rtol=1e-6)
