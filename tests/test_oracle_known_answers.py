@@ -337,3 +337,35 @@ def test_majorants_follow_the_tf_range_and_opacity_scale(oracle):
     # doubling the opacity scale doubles the majorants
     o.SetXFOpacityScale(1.0, 0)
     np.testing.assert_allclose(o.majorants().reshape(4, 4, 4)[:3], 2 * top, rtol=1e-6)
+
+
+@pytest.mark.parametrize("cam", [((0.5, 0.5, -2.0), (0.5, 0.5, 0.5), (0.0, 1.0, 0.0), 30.0),
+                                 ((2.1, 1.3, 1.7), (0.4, 0.6, 0.3), (0.0, 1.0, 0.0), 45.0),
+                                 ((-1.0, 2.5, 0.2), (0.5, 0.5, 0.5), (0.0, 0.0, 1.0), 60.0)])
+def test_camera_is_a_pinhole(oracle, cam):
+    """UpdateCamera (renderer.cpp:1058-1092) with camera.h:83-110: pixel (sx, sy) looks
+    along llc + sx horiz + sy vert - from.  The image centre looks at the point of interest,
+    the image plane's axes are perpendicular to the view direction and to each other, the
+    vertical field of view is fovy, and the plane's extents have the ratio W / H."""
+    W, H = 64, 48
+    o = oracle.OracleRenderer()
+    o.PushMesh(np.zeros((8, 8, 8), np.uint8))
+    o.Resize((W, H))
+    o.Init(2, False)
+    frm, at, up, fovy = cam
+    o.setCamera(frm, at, up, fovy)
+    org, llc, hor, ver = (b.astype(np.float64) for b in o.cameraBasis())
+    np.testing.assert_allclose(org, frm, rtol=0, atol=1e-6)
+    fwd = np.asarray(at, np.float64) - org
+    fwd /= np.linalg.norm(fwd)
+    centre = llc + 0.5 * hor + 0.5 * ver - org
+    np.testing.assert_allclose(centre / np.linalg.norm(centre), fwd, atol=1e-5)
+    assert abs(np.dot(hor, fwd)) < 1e-4 * np.linalg.norm(hor)
+    assert abs(np.dot(ver, fwd)) < 1e-4 * np.linalg.norm(ver)
+    assert abs(np.dot(hor, ver)) < 1e-4 * np.linalg.norm(hor) * np.linalg.norm(ver)
+    top, bottom = llc + 0.5 * hor + ver - org, llc + 0.5 * hor - org
+    angle = math.degrees(math.acos(np.dot(top, bottom) / (np.linalg.norm(top) * np.linalg.norm(bottom))))
+    assert abs(angle - fovy) < 1e-3, angle
+    assert abs(np.linalg.norm(hor) / np.linalg.norm(ver) - W / H) < 1e-5
+    # up stays up: the vertical axis leans towards the up vector
+    assert np.dot(ver, np.asarray(up, np.float64)) > 0
