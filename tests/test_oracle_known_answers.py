@@ -369,3 +369,39 @@ def test_camera_is_a_pinhole(oracle, cam):
     assert abs(np.linalg.norm(hor) / np.linalg.norm(ver) - W / H) < 1e-5
     # up stays up: the vertical axis leans towards the up vector
     assert np.dot(ver, np.asarray(up, np.float64)) > 0
+
+
+def test_default_dt_follows_the_last_channel(oracle):
+    """Resetdt (renderer.cpp:1444-1454): dt = max(0.5 * min over axes of span / dims, 1e-4)
+    of the LAST channel pushed, not the finest one."""
+    for shapes, expect in [([(64, 64, 64), (16, 16, 16)], 0.5 / 16), ([(16, 16, 16), (64, 32, 128)], 0.5 / 128)]:
+        o = oracle.OracleRenderer()
+        for z, y, x in shapes:
+            o.PushMesh(np.zeros((z, y, x), np.uint8))
+        o.Resize((8, 8))
+        o.Init(2)
+        assert o.dt == np.float32(expect), (shapes, o.dt)
+
+
+def test_accumulation_is_the_running_mean_of_the_frames(oracle):
+    """deviceCode.cu:463-471: acc = (frame + a * acc) / (a + 1) with the frame's accumulation
+    id a.  Render k sees the ids the previous Render left (renderer.cpp:957-958), so renders
+    0 and 1 share frame and accumulation id 0: render 1 repeats render 0's frame and starts
+    the mean afresh.  After K renders the buffer is the mean of renders 1 .. K-1, each of
+    which is a frame of its own (checked by rendering every frame after a reset, which
+    keeps the frame ids running)."""
+    from mdwtracker_b200.synthetic import blobs
+    vol = blobs(24, 5, 2)
+    K = 5
+    acc_on = _scene(oracle, vol, ramp(), res=(20, 16), spp=2, mode=2)
+    for _ in range(K):
+        acc_on.Render()
+    ref = _scene(oracle, vol, ramp(), res=(20, 16), spp=2, mode=2)
+    single = []
+    for _ in range(K):
+        ref.ResetAccumulation()
+        ref.Render()
+        single.append(ref.accum().astype(np.float64))
+    np.testing.assert_array_equal(single[0], single[1])                 # the shared first seed
+    assert np.std([f[..., :3].mean() for f in single[1:]]) > 0           # later frames differ
+    np.testing.assert_allclose(acc_on.accum(), np.mean(single[1:], axis=0), rtol=1e-5, atol=1e-6)
