@@ -405,3 +405,31 @@ def test_accumulation_is_the_running_mean_of_the_frames(oracle):
     np.testing.assert_array_equal(single[0], single[1])                 # the shared first seed
     assert np.std([f[..., :3].mean() for f in single[1:]]) > 0           # later frames differ
     np.testing.assert_allclose(acc_on.accum(), np.mean(single[1:], axis=0), rtol=1e-5, atol=1e-6)
+
+
+def test_denoiser_features_at_the_extremes(oracle):
+    """The 16 per-pixel features (mean radiance RGB, depth, miss fraction, hit fractions of
+    channels 0..7, 1/sqrt(spp), two zeros): an empty volume gives the background, depth 0,
+    miss fraction 1 and no hits; a dense single-channel medium gives miss fraction 0, a hit
+    fraction of 1 on channel 0 and a positive depth."""
+    spp = 4
+    bg = (0.25, 0.5, 0.75)
+    empty = _scene(oracle, np.zeros((16, 16, 16), np.uint8), ramp(), res=(12, 10), spp=spp, mode=2, bg=bg)
+    empty.setFeatures(True)
+    empty.Render()
+    f = empty.features()
+    np.testing.assert_array_equal(f[..., :3], np.broadcast_to(np.float32(bg), f[..., :3].shape))
+    np.testing.assert_array_equal(f[..., 3], 0.0)
+    np.testing.assert_array_equal(f[..., 4], 1.0)
+    np.testing.assert_array_equal(f[..., 5:13], 0.0)
+    np.testing.assert_allclose(f[..., 13], 1.0 / math.sqrt(spp), rtol=1e-6)
+    np.testing.assert_array_equal(f[..., 14:], 0.0)
+    dense = _two_channel_scene(oracle, 2, (1.0,), ((1.0, 0.0, 0.0),), spp, (12, 10))
+    dense.setFeatures(True)
+    dense.Render()
+    g = dense.features()
+    centre = g[3:7, 4:8]
+    np.testing.assert_array_equal(centre[..., 4], 0.0)
+    np.testing.assert_array_equal(centre[..., 5], 1.0)
+    np.testing.assert_array_equal(centre[..., 6:13], 0.0)
+    assert np.all(centre[..., 3] > 0)
