@@ -1,6 +1,6 @@
 """Generates the golden fixtures of tests/test_golden.py from the reference's own code.
 
-  python tests/golden/make_golden.py [reference-source-dir]
+  python tests/golden/make_golden.py [reference-source-dir [output-dir]]
 
 Builds oracle/_ref/libref_pins.so (the reference's dda.h and rawFile.cpp compiled where they
 lie, `make -C oracle ref`) and records:
@@ -59,6 +59,7 @@ def rays(n=400, seed=23):
 
 def main(argv):
     ref = argv[1] if len(argv) > 1 else "/root/reference"
+    out = argv[2] if len(argv) > 2 else HERE
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref], check=True,
                    stdout=subprocess.DEVNULL)
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_pins.so"))
@@ -75,7 +76,7 @@ def main(argv):
         cells.append(np.frombuffer(cb, np.int32, 3 * k).reshape(-1, 3).copy())
         t0s.append(np.frombuffer(a, np.uint32, k).copy())
         t1s.append(np.frombuffer(b, np.uint32, k).copy())
-    np.savez_compressed(os.path.join(HERE, "dda_traces.npz"), org=np.array(orgs), dir=np.array(dirs),
+    np.savez_compressed(os.path.join(out, "dda_traces.npz"), org=np.array(orgs), dir=np.array(dirs),
                         tmax=np.array(tmaxs), grid=np.array(gss), count=np.array(counts, np.int32),
                         cells=np.concatenate(cells), t0_bits=np.concatenate(t0s), t1_bits=np.concatenate(t1s))
     rng = np.random.default_rng(29)
@@ -105,8 +106,8 @@ def main(argv):
             recs[f"{name}_format"] = np.array(fmt.value, np.int32)
             recs[f"{name}_bounds_bits"] = np.frombuffer(bounds, np.uint32, 8).copy()
             recs[f"{name}_values_bits"] = np.frombuffer(vals, np.uint32, n).copy()
-    np.savez_compressed(os.path.join(HERE, "raw_loader.npz"), **recs)
-    print("wrote", os.path.join(HERE, "dda_traces.npz"), "and", os.path.join(HERE, "raw_loader.npz"))
+    np.savez_compressed(os.path.join(out, "raw_loader.npz"), **recs)
+    print("wrote", os.path.join(out, "dda_traces.npz"), "and", os.path.join(out, "raw_loader.npz"))
     return 0
 
 

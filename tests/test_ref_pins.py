@@ -208,3 +208,17 @@ def test_unknown_type_token_is_an_error_here(tmp_path, ref, orc):
     with pytest.raises(MdwtError) as e:
         Renderer(MDWT_HOST_ONLY).PushMesh(path)
     assert e.value.status == 9
+
+
+def test_golden_fixtures_are_the_reference_outputs(ref, tmp_path):
+    """tests/golden holds what tests/golden/make_golden.py writes from the reference's code."""
+    import sys
+    gen = os.path.join(ROOT, "tests", "golden", "make_golden.py")
+    import __graft_entry__   # names the reference sources that build() compiles the pins from
+    r = subprocess.run([sys.executable, gen, __graft_entry__.REF_SOURCES, str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    for name in ("dda_traces.npz", "raw_loader.npz"):
+        new, old = np.load(tmp_path / name), np.load(os.path.join(ROOT, "tests", "golden", name))
+        assert sorted(new.files) == sorted(old.files)
+        for k in new.files:
+            np.testing.assert_array_equal(new[k], old[k], err_msg=f"{name}:{k}")
