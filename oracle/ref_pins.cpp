@@ -57,4 +57,16 @@ int64_t ref_raw_load(const char *path, int64_t dims[3], int *format, float bound
   return n;
 }
 
+// raw::RawR::reshapeBounds (rawFile.cpp:217-237, the viewer's -cb): the box4f bounds of the
+// loaded file after rescaling its xyz bounds by its dims (scale3 == nullptr) or by scale3.
+int ref_raw_reshape(const char *path, const float *scale3, float bounds8[8]) {
+  raw::RawR r(path, "rb");
+  if (scale3) r.reshapeBounds(owl::vec3f(scale3[0], scale3[1], scale3[2]));
+  else r.reshapeBounds();
+  const owl::box4f b = r.getBounds4f();
+  const float v[8] = {b.lower.x, b.lower.y, b.lower.z, b.lower.w, b.upper.x, b.upper.y, b.upper.z, b.upper.w};
+  std::memcpy(bounds8, v, sizeof(v));
+  return 0;
+}
+
 }  // extern "C"

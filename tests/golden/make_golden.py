@@ -7,7 +7,9 @@ lie, `make -C oracle ref`) and records:
   dda_traces.npz  -- dda::dda3 (dda.h:81-202) on a fixed, seeded set of rays: every visited
                      cell and its (t0, t1) as float32 bits;
   raw_loader.npz  -- raw::RawR (rawFile.cpp:31-128) on small files of all eight voxel types:
-                     the file bytes, dims, format, box4f bounds and converted values.
+                     the file bytes, dims, format, box4f bounds and converted values; and
+                     RawR::reshapeBounds (rawFile.cpp:217-237) of the float32 file, by its
+                     dims and by the factors in reshape_scale.
 The fixtures are reference outputs; the tests check the oracle against them where the
 reference sources are not available.
 """
@@ -64,6 +66,7 @@ def main(argv):
                    stdout=subprocess.DEVNULL)
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_pins.so"))
     lib.ref_raw_load.restype = C.c_int64
+    lib.ref_raw_reshape.restype = C.c_int
     R = rays()
     orgs, dirs, tmaxs, gss, counts, cells, t0s, t1s = [], [], [], [], [], [], [], []
     for org, d, tmax, gs in R:
@@ -106,6 +109,13 @@ def main(argv):
             recs[f"{name}_format"] = np.array(fmt.value, np.int32)
             recs[f"{name}_bounds_bits"] = np.frombuffer(bounds, np.uint32, 8).copy()
             recs[f"{name}_values_bits"] = np.frombuffer(vals, np.uint32, n).copy()
+            if name == "float32":
+                scale = np.array([0.5, 2.0, 1.25], np.float32)
+                for key, sc in (("reshape_dims_bits", None), ("reshape_scale_bits", scale)):
+                    rb = (C.c_float * 8)()
+                    assert lib.ref_raw_reshape(path.encode(), (C.c_float * 3)(*sc) if sc is not None else None, rb) == 0
+                    recs[key] = np.frombuffer(rb, np.uint32, 8).copy()
+                recs["reshape_scale"] = scale
     np.savez_compressed(os.path.join(out, "raw_loader.npz"), **recs)
     print("wrote", os.path.join(out, "dda_traces.npz"), "and", os.path.join(out, "raw_loader.npz"))
     return 0

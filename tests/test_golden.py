@@ -64,3 +64,17 @@ def test_loader_matches_the_reference_outputs(tmp_path, oracle, name):
     pd, pb = prod.channelInfo(0)
     assert pd == dims
     np.testing.assert_array_equal(pb.view(np.uint32), g[f"{name}_bounds_bits"])
+
+
+@pytest.mark.parametrize("by", ["dims", "scale"])
+def test_reshaped_bounds_match_the_reference_outputs(tmp_path, oracle, by):
+    g = np.load(os.path.join(GOLDEN, "raw_loader.npz"))
+    dims = tuple(int(x) for x in g["float32_dims"])
+    path = str(tmp_path / f"vol_{dims[0]}x{dims[1]}x{dims[2]}_float32.raw")
+    g["float32_bytes"].tofile(path)
+    scale = tuple(float(x) for x in g["reshape_scale"]) if by == "scale" else None
+    for r in (Renderer(MDWT_HOST_ONLY), oracle.OracleRenderer()):
+        r.PushMesh(path)
+        r.reshapeBounds(0, scale)
+        _, got = r.channelInfo(0)
+        np.testing.assert_array_equal(got.view(np.uint32), g[f"reshape_{by}_bits"])

@@ -222,3 +222,20 @@ def test_golden_fixtures_are_the_reference_outputs(ref, tmp_path):
         assert sorted(new.files) == sorted(old.files)
         for k in new.files:
             np.testing.assert_array_equal(new[k], old[k], err_msg=f"{name}:{k}")
+
+
+@pytest.mark.parametrize("scale", [None, (0.5, 2.0, 1.25), (3.0, 3.0, 3.0)])
+def test_reshaped_bounds_match_the_reference(tmp_path, ref, oracle, scale):
+    """raw::RawR::reshapeBounds (rawFile.cpp:217-237, the -cb flag): xyz bounds times the dims,
+    or times the given factors; the value range is kept."""
+    arr = (np.arange(6 * 3 * 11, dtype=np.float32) * 0.37).reshape(11, 3, 6)
+    path = str(tmp_path / "vol_6x3x11_float32.raw")
+    arr.tofile(path)
+    b = (C.c_float * 8)()
+    assert ref.ref_raw_reshape(os.fsencode(path), (C.c_float * 3)(*scale) if scale else None, b) == 0
+    want = np.frombuffer(b, np.uint32, 8).copy()
+    for r in (Renderer(MDWT_HOST_ONLY), oracle.OracleRenderer()):
+        r.PushMesh(path)
+        r.reshapeBounds(0, scale)
+        _, got = r.channelInfo(0)
+        np.testing.assert_array_equal(got.view(np.uint32), want)
