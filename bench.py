@@ -7,16 +7,22 @@ the tracker (Renderer::Render, renderer.cpp:944-973).  Metric: Gpath-samples/s
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1|c3] [--impl mdwt|reference]
 
-Default workload (c2): syncDDA (-m 2), 3 channels of 256^3 uint8 sparse value noise,
-16^3-voxel macrocells, 1024x1024, 64 spp.  Inputs (volumes, majorants) are resident in
-HBM before timing; L2 (126 MB > the 48 MB volume) is flushed by a 512 MiB write between
-timed steps, outside the timed events.  `value` is device time (CUDA events on the
-render stream); `e2e` goes through the C ABI with host buffers: camera update (host to
-device), frame, framebuffer copy to pinned host memory.  Under torchrun every rank
-renders its own frames (different frame seeds) with no collective: per-GPU work is
-fixed, `scaling` is weak, and time is the max over ranks.  Before timing, the tracker
-schedule is tuned for the workload (mdwt_autotune_schedule on launches of the step's
-shape; --no-autotune keeps the defaults) and reported in config.schedule.
+Default workload (c3): syncDDA (-m 2), 6 channels of 512^3 float32 log-normal fields,
+16-voxel macrocells, 1920x1080, 256 spp -- the configuration the headline metric is
+quoted on.  Inputs (volumes, majorants) are resident in HBM before timing; L2 is flushed
+by a 512 MiB write between timed steps, outside the timed events (the 3.2 GB volume is
+larger than L2 in any case).  `value` is device time (CUDA events on the render stream);
+`e2e` goes through the C ABI with host buffers: camera update (host to device), frame,
+framebuffer copy to pinned host memory.  Under torchrun every rank renders its own frames
+(different frame seeds) with no collective: per-GPU work is fixed, `scaling` is weak,
+and time is the max over ranks.  Before timing, the tracker schedule is tuned for the
+workload (mdwt_autotune_schedule on launches of the step's shape; --no-autotune keeps
+the defaults) and reported in config.schedule.
+
+Extra keys on the same line (rank 0, one GPU): `c2` -- the 3 x 256^3 uint8 syncDDA
+scene at 1024^2 and 64 spp, timed the same way; `edge_sweep` -- the 1080p scene's
+macrocell sweep over edges 4/8/16/32 voxels for syncDDA and N-DDA (--no-sweep skips
+it); `--edge` sets the headline scene's edge.
 
 time_to_rmse (rank 0, one GPU; --no-ttr skips it): the first part of the headline metric
 -- how long plain accumulation takes at 1920x1080 (the 6 x 512^3 float32 log-normal scene,
@@ -32,7 +38,7 @@ same requests rendered one after the other.
 
 --impl reference times the reference's path restated on the CPU (the OpenMP oracle,
 the reference itself cannot be built: no OptiX/OWL) on the same scene, on all host
-cores, each step a band of image rows; rank 0 only.
+cores, each step a set of image rows spread evenly over the frame; rank 0 only.
 """
 import argparse
 import json
@@ -53,7 +59,11 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c3ndda", "c3b", "c3bndda"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c3ndda", "c3b", "c3bndda"])
+    ap.add_argument("--edge", type=int, default=16, choices=[4, 8, 16, 32],
+                    help="macrocell edge in voxels of the c3/c3b scenes")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the c3 macrocell-edge sweep")
+    ap.add_argument("--no-c2", action="store_true", help="skip the extra c2 line")
     ap.add_argument("--impl", default="mdwt", choices=["mdwt", "reference"])
     ap.add_argument("--flush-mib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
@@ -72,20 +82,20 @@ def parse_args():
     return ap.parse_args()
 
 
-def make_scene(name, res=None, spp=None):
+def make_scene(name, res=None, spp=None, edge=16):
     from mdwtracker_b200 import synthetic as syn
     if name == "c1":
         sc = syn.scene_c1()
     elif name == "c2":
         sc = syn.scene_c2()
     elif name == "c3":
-        sc = syn.scene_c3(mode=2)
+        sc = syn.scene_c3(mode=2, edge=edge)
     elif name == "c3ndda":
-        sc = syn.scene_c3(mode=0)
+        sc = syn.scene_c3(mode=0, edge=edge)
     elif name == "c3b":
-        sc = syn.scene_c3b(mode=2)
+        sc = syn.scene_c3b(mode=2, edge=edge)
     elif name == "c3bndda":
-        sc = syn.scene_c3b(mode=0)
+        sc = syn.scene_c3b(mode=0, edge=edge)
     else:
         raise ValueError(name)
     if res is not None:
@@ -209,25 +219,32 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(sc, budget_s, full=False):
-    """Oracle on the host cores over a band of rows of the same frame."""
+def spread_rows(o, h, budget_s):
+    """Rows spread evenly over the frame for a CPU sample of about `budget_s` seconds:
+    calibrated on one row at the middle of the frame (among the heaviest), then every
+    stride-th row from stride // 2.  Returns (row0, stride)."""
+    t0 = time.perf_counter()
+    o.renderRowStride(h // 2, h)
+    dt1 = max(time.perf_counter() - t0, 1e-4)
+    rows = int(max(1, min(h, budget_s / dt1)))
+    stride = max(1, h // rows)
+    return stride // 2, stride
+
+
+def cpu_baseline(sc, budget_s):
+    """Oracle on the host cores over rows spread evenly over the same frame."""
     from oracle import oracle as orc
     threads = orc.set_threads(len(os.sched_getaffinity(0)))
     o = sc.setup(orc.OracleRenderer())
     w, h = sc.resolution
-    # calibrate on 1 row, then size the band for the budget
+    r0, stride = spread_rows(o, h, budget_s)
     t0 = time.perf_counter()
-    o.renderRows(h // 2, h // 2 + 1)
-    dt1 = max(time.perf_counter() - t0, 1e-4)
-    rows = int(max(1, min(h, budget_s / dt1)))
-    r0 = max(0, h // 2 - rows // 2)
-    t0 = time.perf_counter()
-    o.renderRows(r0, r0 + rows)
+    rows = o.renderRowStride(r0, stride)
     el = time.perf_counter() - t0
     ps = rows * w * sc.spp
     return {"value": ps / el / 1e9, "unit": "Gpath-samples/s", "cores": threads, "kind": "port",
-            "sample": f"rows {r0}..{r0 + rows - 1} of the {w}x{h} frame at {sc.spp} spp "
-                      f"({ps} path-samples, {el:.1f} s)"}, o
+            "sample": f"{rows} rows spread over the {w}x{h} frame (every {stride}th from row {r0}) at "
+                      f"{sc.spp} spp ({ps} path-samples, {el:.1f} s)"}, o
 
 
 def time_to_rmse(name, target, device_index, max_frames=20000):
@@ -425,22 +442,20 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sc = make_scene(args.config, args.res, args.spp)
+    sc = make_scene(args.config, args.res, args.spp, args.edge)
     from oracle import oracle as orc
     threads = orc.set_threads(len(os.sched_getaffinity(0)))
     o = sc.setup(orc.OracleRenderer())
     w, h = sc.resolution
-    t0 = time.perf_counter()
-    o.renderRows(h // 2, h // 2 + 1)
-    dt1 = max(time.perf_counter() - t0, 1e-4)
-    rows = int(max(1, min(h, 6.0 / dt1)))
-    r0 = max(0, h // 2 - rows // 2)
+    # each step: rows spread evenly over the frame, about 6 s of host work
+    r0, stride = spread_rows(o, h, 6.0)
     for _ in range(args.warmup):
-        o.renderRows(r0, r0 + min(rows, 2))
+        o.renderRowStride(r0, max(stride, h // 2))
     times = []
+    rows = 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        o.renderRows(r0, r0 + rows)
+        rows = o.renderRowStride(r0, stride)
         times.append(time.perf_counter() - t0)
     ps = rows * w * sc.spp
     value = ps / statistics.mean(times) / 1e9
@@ -452,8 +467,8 @@ def run_reference(args):
         "data": "synthetic (seeded)",
         "config": scene_config(sc, "host caches", "host threads"),
         "cpu_baseline": {"value": value, "unit": "Gpath-samples/s", "cores": threads, "kind": "port",
-                         "sample": f"each step: rows {r0}..{r0 + rows - 1} of the {w}x{h} frame at {sc.spp} spp "
-                                   f"({ps} path-samples)"},
+                         "sample": f"each step: {rows} rows spread over the {w}x{h} frame (every {stride}th "
+                                   f"from row {r0}) at {sc.spp} spp ({ps} path-samples)"},
         "e2e": {"value": value, "unit": "Gpath-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (OptiX 7 + OWL, GL viewer) cannot be built here; its tracking path "
                 "is restated in C++/OpenMP (oracle/mdwt_oracle.cpp) and timed on the host cores",
@@ -468,6 +483,123 @@ def schedule_of(r, by):
     names = {4: "regroup", 2: "trips", 0: "pool", 3: "quorum"}
     out = {v: r.getTuning(k) for k, v in names.items()}
     out["by"] = by
+    return out
+
+
+def algorithmic_bytes(sc, cnt):
+    """Algorithmic bytes of the tracker over the counted work: 8*bpv per density sample
+    (trilinear footprint), 4*C_read per macrocell visit (majorants; C for syncDDA, 1
+    otherwise).  The resolve pass (36 B per pixel) is timed apart."""
+    bpv = 1 if all(v.dtype == np.uint8 for v in sc.volumes) else 4
+    creads = len(sc.volumes) if sc.mode == 2 else 1
+    return 8.0 * bpv * float(cnt[0]) + 4.0 * creads * float(cnt[2])
+
+
+def timed_frames(r, sc, steps, warmup, flush, stream, barrier=lambda: None, clocks=None):
+    """`warmup` untimed steps, then `steps` timed ones (one step = the workload's frames),
+    each bracketed by CUDA events on the render stream, with an L2 flush before each step
+    outside the events.  Returns the step times, the tracker kernel's times, the counters
+    of the timed steps and the number of library launches inside them."""
+    import torch
+    sptr = stream.cuda_stream
+
+    def step():
+        if sc.frames > 1:
+            r.RenderFrames(sc.frames, sptr)
+        else:
+            r.Render(sptr)
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            flush.fill_(1)
+            step()
+    torch.cuda.synchronize()
+    r.resetCounters()
+    timed = True
+    try:
+        r.setTiming(True)
+    except Exception:
+        timed = False
+    launches0 = r.renderInfo()[0]
+    # the tracker kernel the frames run: the regrouped one launches 256-thread blocks
+    tracker = "trace_regroup_kernel" if r.renderInfo()[3] == 256 else "trace_kernel"
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.mark()
+    trace_ms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+            if timed and sc.frames == 1:
+                trace_ms.append(r.kernelTimes()[0])  # trace kernel, CUDA events on the render stream
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop() if clocks is not None else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    return {"step_ms": step_ms, "trace_ms": trace_ms, "counters": r.counters(),
+            "launches": r.renderInfo()[0] - launches0, "tracker": tracker, "clocks": clk, "step": step}
+
+
+def throughput_summary(sc, t, peak):
+    """Gpath-samples/s, the tracker's algorithmic GB/s and its roofline fraction."""
+    w, h = sc.resolution
+    steps = len(t["step_ms"])
+    ms = statistics.mean(t["step_ms"])
+    kernel_ms = statistics.mean(t["trace_ms"]) if t["trace_ms"] else ms
+    alg = algorithmic_bytes(sc, t["counters"]) / steps
+    cnt = t["counters"]
+    return {"workload": workload_name(sc), "Gpath_samples_per_s": w * h * sc.spp * sc.frames / (ms / 1e3) / 1e9,
+            "ms_per_step": ms, "kernel": t["tracker"], "kernel_ms": kernel_ms,
+            "algorithmic_GB_per_s": alg / (kernel_ms / 1e3) / 1e9, "frac_of_measured_hbm": alg / (kernel_ms / 1e3) / 1e9 / peak,
+            "density_samples_per_path": float(cnt[0]) / max(1, int(cnt[3])),
+            "cells_per_path": float(cnt[2]) / max(1, int(cnt[3]))}
+
+
+def extra_c2(args, local, flush, stream, peak):
+    """The 3 x 256^3 uint8 syncDDA scene at 1024^2 and 64 spp (L2-resident volume),
+    tuned and timed like the headline line."""
+    from mdwtracker_b200 import Renderer
+    sc = make_scene("c2")
+    r = sc.setup(Renderer(local))
+    if not args.no_autotune:
+        r.autotuneSchedule(frames=sc.frames)
+    t = timed_frames(r, sc, args.steps, args.warmup, flush, stream)
+    out = throughput_summary(sc, t, peak)
+    out["schedule"] = schedule_of(r, "default" if args.no_autotune else "mdwt_autotune_schedule")
+    r.close()
+    return out
+
+
+def edge_sweep(args, local, flush, stream, peak, edges=(4, 8, 16, 32), steps=3):
+    """The 1080p scene (6 x 512^3 float32, 256 spp) over macrocell edges of 4/8/16/32
+    voxels, syncDDA and N-DDA: the grid is rebuilt on the same context (mdwt_set_macrocells
+    keeps the TFs) and the schedule tuned for each edge; `steps` timed frames each."""
+    from mdwtracker_b200 import Renderer
+    out = {}
+    for name in ("c3", "c3ndda"):
+        sc = make_scene(name, args.res, args.spp, 16)
+        r = sc.setup(Renderer(local))
+        rows = []
+        n = sc.volumes[0].shape[0]
+        for e in edges:
+            mc = max(1, n // e)
+            r.macrocellDims = (mc, mc, mc)
+            sc.macrocells = (mc, mc, mc)
+            sc.name = sc.name.rsplit("_e", 1)[0] + f"_e{e}"
+            if not args.no_autotune:
+                r.autotuneSchedule(frames=1)
+            t = timed_frames(r, sc, steps, 1, flush, stream)
+            row = throughput_summary(sc, t, peak)
+            row["edge"] = e
+            row["schedule"] = schedule_of(r, "default" if args.no_autotune else "mdwt_autotune_schedule")
+            rows.append(row)
+        out["syncdda" if sc.mode == 2 else "ndda"] = rows
+        r.close()
     return out
 
 
@@ -491,7 +623,7 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    sc = make_scene(args.config, args.res, args.spp)
+    sc = make_scene(args.config, args.res, args.spp, args.edge)
     r = sc.setup(Renderer(local))
     w, h = sc.resolution
     # the tracker schedule is tuned for the workload first (outside the timed region), on
@@ -505,8 +637,7 @@ def main():
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream
     flush = torch.empty(args.flush_mib << 20, dtype=torch.uint8, device=dev)
-    # one step = the workload's frames (several successive frames in one launch through
-    # mdwt_render_frames when the configuration renders more than one)
+
     def step():
         if sc.frames > 1:
             r.RenderFrames(sc.frames, sptr)
@@ -526,57 +657,24 @@ def main():
     # region); only the samples written after mark() are counted
     clocks = ClockSampler(torch.cuda.get_device_properties(dev).uuid and f"GPU-{torch.cuda.get_device_properties(dev).uuid}")
     clocks.start()
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            flush.fill_(1)
-            step()
-    torch.cuda.synchronize(dev)
-    r.resetCounters()
-    timed = True
-    try:
-        r.setTiming(True)
-    except Exception:
-        timed = False
-    launches0 = r.renderInfo()[0]
-    # the tracker kernel the frames run: the regrouped one launches 256-thread blocks
-    tracker = "trace_regroup_kernel" if r.renderInfo()[3] == 256 else "trace_kernel"
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    barrier()
-    torch.cuda.synchronize(dev)
-    clocks.mark()
-    trace_ms = []
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.fill_(k & 0xff)
-            ev[k][0].record(stream)
-            step()
-            ev[k][1].record(stream)
-            if timed and sc.frames == 1:
-                trace_ms.append(r.kernelTimes()[0])  # trace kernel, CUDA events on the render stream
-    torch.cuda.synchronize(dev)
-    barrier()
-    clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    launches = r.renderInfo()[0] - launches0
-    cnt = r.counters()
+    t = timed_frames(r, sc, args.steps, args.warmup, flush, stream, barrier, clocks)
+    clk = t["clocks"]
+    step_ms = t["step_ms"]
+    cnt = t["counters"]
     ms = statistics.mean(step_ms)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
     paths = w * h * sc.spp * sc.frames
     value = world * paths / (ms / 1e3) / 1e9
 
-    # algorithmic bytes of the dominant kernel (the tracker) per launch: 8*bpv per
-    # density sample (trilinear footprint), 4*C_read per macrocell visit (majorants;
-    # C for syncDDA, 1 otherwise); the resolve pass (36 B per pixel) is timed apart
-    bpv = 1 if all(v.dtype == np.uint8 for v in sc.volumes) else 4
-    creads = len(sc.volumes) if sc.mode == 2 else 1
     steps = args.steps
-    alg_bytes = (8.0 * bpv * float(cnt[0]) + 4.0 * creads * float(cnt[2])) / steps
-    kernel_ms = statistics.mean(trace_ms) if trace_ms else statistics.mean(step_ms)
+    alg_bytes = algorithmic_bytes(sc, cnt) / steps
+    kernel_ms = statistics.mean(t["trace_ms"]) if t["trace_ms"] else statistics.mean(step_ms)
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
+    tracker = t["tracker"]
 
     # ---- end to end through the C ABI with host buffers
     pinned = torch.empty(w * h, dtype=torch.int32, pin_memory=True)
@@ -594,10 +692,11 @@ def main():
     barrier()
     e2e = statistics.mean(e2e_ms)
     if world > 1:
-        t = torch.tensor([e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+        tt = torch.tensor([e2e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = float(tt.item())
     h2d = r.renderInfo()[1] + 48  # kernel parameter block + camera vectors
+    r.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -605,6 +704,19 @@ def main():
             cpu, _ = cpu_baseline(sc, args.cpu_seconds)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "error": str(ex)}
+
+    extras = {}
+    if rank == 0 and world == 1:
+        if not args.no_c2 and args.config != "c2":
+            try:
+                extras["c2"] = extra_c2(args, local, flush, stream, peak)
+            except Exception as ex:  # reported beside the throughput line, never required
+                extras["c2"] = {"error": str(ex)}
+        if not args.no_sweep and args.config in ("c3", "c3ndda"):
+            try:
+                extras["edge_sweep"] = edge_sweep(args, local, flush, stream, peak)
+            except Exception as ex:
+                extras["edge_sweep"] = {"error": str(ex)}
 
     ttr = None
     if rank == 0 and world == 1 and not args.no_ttr:
@@ -646,15 +758,15 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": w * h * 4, "ms_per_step": e2e},
         "time_to_rmse": ttr,
         "batch": batch,
-        "gpu_launches": int(launches),
+        "gpu_launches": int(t["launches"]),
         "clocks": clk,
         "counters": {"density_samples": int(cnt[0]), "rejections": int(cnt[1]), "cells": int(cnt[2]),
                      "path_samples": int(cnt[3]), "samples_per_path": float(cnt[0]) / max(1, int(cnt[3]))},
         "step_ms": step_ms,
     }
+    line.update(extras)
     if rank == 0:
         print(json.dumps(line))
-    r.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -206,7 +206,7 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * MDWT_TUNE_POOL: a warp starts new paths only when at least `value` (1..32) of its
  * lanes wait for one, or when no lane is busy.
  * MDWT_TUNE_BATCH: at most `value` samples per pixel per trace pass (0 = as many as the
- * 1 GiB path-record budget allows); the per-pixel sums still run in sample order.
+ * 4 GiB path-record budget allows); the per-pixel sums still run in sample order.
  * MDWT_TUNE_TRIPS: transition/free-flight trips (1..64) a warp takes per round before
  * it evaluates its pending density samples together.
  * MDWT_TUNE_QUORUM: a round's trips also end once `value` (1..33; 33 = never) of the
@@ -223,9 +223,10 @@ mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
 mdwt_status mdwt_get_tuning(const mdwt_ctx *ctx, int key, int *value);
 
 /* No reference counterpart: CUDA events on the render stream around the trace kernel
- * (with the work-counter reset before it) and the resolve kernel of each frame whose
- * samples fit one trace pass; mdwt_get_kernel_times returns the last frame's
- * {trace, resolve} milliseconds (it waits for that frame). */
+ * (with the work-counter reset before it) and the resolve kernel of every sample pass of
+ * each frame of at most 8 passes (a pass holds the samples whose path records fit
+ * 2^30 records); mdwt_get_kernel_times returns the last frame's {trace, resolve}
+ * milliseconds summed over its passes (it waits for that frame). */
 mdwt_status mdwt_set_timing(mdwt_ctx *ctx, int enable);
 mdwt_status mdwt_get_kernel_times(mdwt_ctx *ctx, float out_ms2[2]);
 
@@ -281,10 +282,16 @@ mdwt_status mdwt_accum_rmse(mdwt_ctx *ctx, double *rmse);
  * cell, cell-major).  The result equals the ranges mdwt_init builds for that channel.
  * Work is enqueued on `cuda_stream` (a cudaStream_t; NULL = legacy default stream).
  * Limits: at most 1024 macrocells per axis and dims[2] * mc[1] * mc[0] <= 2^20, else
- * MDWT_ERR_SCRATCH_LIMIT.  The scratch is fixed device memory inside the library (8 MiB +
- * 24 KiB, held by every GPU that loads the library until the process exits); the first
- * call on a device looks up its address, so make that first call before any stream
- * capture.  Calls share the scratch: calls that overlap on the GPU race. */
+ * MDWT_ERR_SCRATCH_LIMIT.  Bounds for which some voxel's neighbour box is empty in float
+ * or the cells touched are not non-decreasing along an axis give MDWT_ERR_UNSUPPORTED
+ * (mdwt_init rejects the non-monotone ones too).  The scratch is fixed device memory
+ * inside the library (8 MiB + 24 KiB, held by every GPU that loads the library until the
+ * process exits).  A call outside stream capture looks up its address on the current
+ * device; a call under capture reuses the address found by the last call on that device
+ * and fails with MDWT_ERR_STATE if there was none, so make the first call on a device
+ * before any stream capture.  An error left pending by earlier CUDA work is reported as
+ * MDWT_ERR_CUDA before anything is launched and is not cleared.  Calls share the
+ * scratch: calls that overlap on the GPU race. */
 mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int format, const int64_t dims[3],
                                       const uint32_t macrocells[3], const float world_lo[3],
                                       const float world_hi[3], float *d_ranges_out, void *cuda_stream);

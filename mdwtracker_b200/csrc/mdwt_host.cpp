@@ -168,7 +168,9 @@ struct mdwt_ctx {
   int regroup = 1;    // -m 2: the tracker that regroups each warp's paths by operation (MDWT_TUNE_REGROUP)
   int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
   bool timing = false;        // CUDA events around the trace and resolve kernels
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  static constexpr int kTimedPasses = 8;   // sample passes of a frame that can be timed
+  cudaEvent_t ev[3 * kTimedPasses] = {};   // per pass: start, trace end, resolve end
+  int timedPasses = 0;
   bool timed = false;
 };
 
@@ -1089,23 +1091,27 @@ mdwt_status mdwt_render(mdwt_ctx *c, void *stream) {
   int batch = 0;
   mdwt_status s = prepare_frame(c, p, &batch);
   if (s) return s;
-  // kernel timing: events around the trace and the resolve pass of a one-batch frame
-  const bool timeIt = c->timing && batch >= c->spp;
+  // kernel timing: events around the trace and the resolve kernel of every sample pass
+  // of the frame (frames of up to kTimedPasses passes)
+  const int passes = (c->spp + batch - 1) / batch;
+  const bool timeIt = c->timing && passes <= mdwt_ctx::kTimedPasses;
   c->timed = false;
   if (timeIt) {
-    for (auto &e : c->ev)
-      if (!e) CK(cudaEventCreate(&e), "cudaEventCreate");
-    CK(cudaEventRecord(c->ev[0], st), "event");
+    for (int i = 0; i < 3 * passes; i++)
+      if (!c->ev[i]) CK(cudaEventCreate(&c->ev[i]), "cudaEventCreate");
   }
-  for (int s0 = 0; s0 < c->spp; s0 += batch) {
+  for (int s0 = 0, b = 0; s0 < c->spp; s0 += batch, b++) {
     p.sBase = s0;
     p.sCount = std::min(batch, c->spp - s0);
+    if (timeIt) CK(cudaEventRecord(c->ev[3 * b], st), "event");
     CK(cudaMemsetAsync(c->dWork, 0, sizeof(unsigned int), st), "reset work counter");
-    CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock, timeIt ? c->ev[1] : nullptr),
+    CKI(launch_track(p, c->store, st, c->numSMs, &c->launches, &c->lastGrid, &c->lastBlock,
+                     timeIt ? c->ev[3 * b + 1] : nullptr),
         "tracker kernels");
+    if (timeIt) CK(cudaEventRecord(c->ev[3 * b + 2], st), "event");
   }
   if (timeIt) {
-    CK(cudaEventRecord(c->ev[2], st), "event");
+    c->timedPasses = passes;
     c->timed = true;
   }
   // Renderer::Render (renderer.cpp:957-958): the ids the next frame sees are the
@@ -1871,10 +1877,16 @@ mdwt_status mdwt_set_timing(mdwt_ctx *c, int enable) {
 
 mdwt_status mdwt_get_kernel_times(mdwt_ctx *c, float out_ms[2]) {
   if (!c || !out_ms) return MDWT_ERR_BAD_ARG;
-  if (!c->timed) return fail(c, MDWT_ERR_STATE, "no timed frame (enable timing; frames of one sample batch)");
-  CK(cudaEventSynchronize(c->ev[2]), "event sync");
-  CK(cudaEventElapsedTime(&out_ms[0], c->ev[0], c->ev[1]), "elapsed");
-  CK(cudaEventElapsedTime(&out_ms[1], c->ev[1], c->ev[2]), "elapsed");
+  if (!c->timed) return fail(c, MDWT_ERR_STATE, "no timed frame (enable timing; frames of at most 8 sample passes)");
+  CK(cudaEventSynchronize(c->ev[3 * c->timedPasses - 1]), "event sync");
+  out_ms[0] = out_ms[1] = 0.0f;
+  for (int b = 0; b < c->timedPasses; b++) {
+    float a = 0.0f, r = 0.0f;
+    CK(cudaEventElapsedTime(&a, c->ev[3 * b], c->ev[3 * b + 1]), "elapsed");
+    CK(cudaEventElapsedTime(&r, c->ev[3 * b + 1], c->ev[3 * b + 2]), "elapsed");
+    out_ms[0] += a;
+    out_ms[1] += r;
+  }
   return MDWT_OK;
 }
 

@@ -113,7 +113,7 @@ int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext);
 int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launches, int *grid);
 
 constexpr int kMaxTexels = 16384;          // TF texels addressable by a path record
-constexpr size_t kRecordBudget = size_t(1) << 28;   // records per batch (1 GiB)
+constexpr size_t kRecordBudget = size_t(1) << 30;   // records per sample pass (4 GiB)
 
 // Per-axis voxel intervals of the separable range build: for macrocell index k on
 // one axis, voxels [lo[k], hi[k]] (empty when lo > hi) enter its value range.

@@ -240,10 +240,42 @@ void *g_noalloc_pairs_ptr[kNoAllocMaxDevices];
 int *g_noalloc_iv_ptr[kNoAllocMaxDevices];
 bool g_noalloc_ready[kNoAllocMaxDevices];
 
-bool bounds_ok(float lo, float hi, int64_t D) {
-  if (!std::isfinite(lo) || !std::isfinite(hi) || !(hi > lo)) return false;
-  const float scale = std::fmax(std::fabs(lo), std::fabs(hi));
-  return (hi - lo) / (float)D >= 1e-6f * scale;
+int f2i_h(float x) {
+  if (!(x == x)) return 0;
+  if (x >= 2147483648.0f) return 2147483647;
+  if (x <= -2147483648.0f) return (-2147483647 - 1);
+  return (int)x;
+}
+
+int project_h(float f, float lo, float hi, int dim) {
+  int v = f2i_h((float)dim * (f - lo) / (hi - lo));
+  v = v < dim - 1 ? v : dim - 1;
+  return v > 0 ? v : 0;
+}
+
+// The device search of noalloc_intervals_kernel finds, for each cell k, the run of voxels
+// whose neighbour boxes reach k.  It gives the voxel set that mdwt_init's scan finds when
+// every voxel's neighbour box is non-empty and the cells it touches are non-decreasing
+// in the voxel index.  Checked here over every voxel of the axis, with the arithmetic
+// of voxel_cells (fmaf corners, IEEE division, truncating conversion).
+bool axis_searchable(int64_t D, int md, float wlo, float whi) {
+  if (!std::isfinite(wlo) || !std::isfinite(whi) || !(whi > wlo)) return false;
+  const float len = (whi - wlo) / (float)D;
+  int pclo = 0, pchi = 0;
+  for (int64_t p = 0; p < D; p++) {
+    const float vlo = std::fma((float)p, len, wlo);
+    float blo = vlo, bhi = vlo + len;
+    if (p - 1 >= 0) { const float nl = std::fma((float)(p - 1), len, wlo); blo = std::fmin(blo, nl); bhi = std::fmax(bhi, nl); }
+    if (p + 1 < D) { const float nl = std::fma((float)(p + 1), len, wlo); blo = std::fmin(blo, nl); bhi = std::fmax(bhi, nl); }
+    if (!(blo < bhi)) return false;
+    const int clo = project_h(blo, wlo, whi, md);
+    const int h = project_h(bhi, wlo, whi, md);
+    const int chi = h < md - 1 ? h : md - 1;
+    if (clo < pclo || chi < pchi) return false;
+    pclo = clo;
+    pchi = chi;
+  }
+  return true;
 }
 }  // namespace
 
@@ -253,9 +285,11 @@ bool bounds_ok(float lo, float hi, int64_t D) {
 // must not allocate device memory: code running inside an application's own memory pool
 // or under an allocator that forbids cudaMalloc, or plug-ins that are handed device
 // buffers and a stream but no allocation rights.  The scratch is the module-global
-// g_noalloc_pairs / g_noalloc_iv; the first call on a device looks up their addresses
-// (cudaGetSymbolAddress), so make that first call before any stream capture.  All calls
-// share the scratch: calls that overlap on the GPU (two streams, two threads) race.
+// g_noalloc_pairs / g_noalloc_iv; a call outside stream capture looks up their addresses
+// on the current device (cudaGetSymbolAddress), and a call under capture reuses the
+// addresses of the last call on that device, so make the first call on a device before
+// any stream capture.  All calls share the scratch: calls that overlap on the GPU (two
+// streams, two threads) race.
 extern "C" mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int format, const int64_t dims[3],
                                                  const uint32_t macrocells[3], const float world_lo[3],
                                                  const float world_hi[3], float *d_ranges_out, void *cuda_stream) {
@@ -265,14 +299,25 @@ extern "C" mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int forma
   for (int a = 0; a < 3; a++) {
     if (dims[a] <= 0 || dims[a] > (1 << 20) || macrocells[a] == 0) return MDWT_ERR_BAD_ARG;
     if (macrocells[a] > (uint32_t)kNoAllocMaxCells) return MDWT_ERR_SCRATCH_LIMIT;
-    if (!bounds_ok(world_lo[a], world_hi[a], dims[a])) return MDWT_ERR_UNSUPPORTED;
   }
   if ((size_t)dims[2] * macrocells[1] * macrocells[0] > kNoAllocPairs) return MDWT_ERR_SCRATCH_LIMIT;
+  for (int a = 0; a < 3; a++)
+    if (!axis_searchable(dims[a], (int)macrocells[a], world_lo[a], world_hi[a])) return MDWT_ERR_UNSUPPORTED;
+  // an error that earlier work left pending is reported here and left for its owner:
+  // nothing is launched, and the check after the launches sees only this call's errors
+  if (cudaPeekAtLastError() != cudaSuccess) return MDWT_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) { cudaGetLastError(); return MDWT_ERR_CUDA; }
+  cudaStream_t st = (cudaStream_t)cuda_stream;
   {
+    // The scratch addresses are looked up on every call outside stream capture (a
+    // cudaDeviceReset reloads the module and moves them); under capture the last
+    // looked-up address of this device is used.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) { cudaGetLastError(); return MDWT_ERR_CUDA; }
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ready[dev]) {
+    if (cap == cudaStreamCaptureStatusNone || !g_noalloc_ready[dev]) {
+      if (cap != cudaStreamCaptureStatusNone) return MDWT_ERR_STATE;
       void *p = nullptr, *q = nullptr;
       if (cudaGetSymbolAddress(&p, g_noalloc_pairs) != cudaSuccess ||
           cudaGetSymbolAddress(&q, g_noalloc_iv) != cudaSuccess) {
@@ -284,7 +329,6 @@ extern "C" mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int forma
       g_noalloc_ready[dev] = true;
     }
   }
-  cudaStream_t st = (cudaStream_t)cuda_stream;
   const int mx = (int)macrocells[0], my = (int)macrocells[1], mz = (int)macrocells[2];
   int *iv = g_noalloc_iv_ptr[dev];
   noalloc_intervals_kernel<<<(mx + my + mz + 127) / 128, 128, 0, st>>>(

@@ -1400,10 +1400,9 @@ int orc_enable_pixel_stats(Oracle *o, int e) {
   return ORC_OK;
 }
 
-// Render one frame over the pixel rows [row0, row1) (all rows when row1 <= row0).
-int orc_render_rows(Oracle *o, int row0, int row1) {
-  if (!o->inited) return ORC_STATE;
-  if (row1 <= row0) { row0 = 0; row1 = o->H; }
+// Render one frame over the pixel rows row0, row0 + stride, ... (nrows of them, all
+// inside the frame); the frame ids advance as for a whole frame.
+static int render_row_set(Oracle *o, int row0, int stride, int nrows) {
   if (o->featOn) {
     // depth-feature scale: 1 / (camera-to-root-box-centre distance + box diagonal)
     const float cx = (o->rootLo[0] + o->rootHi[0]) * 0.5f, cy = (o->rootLo[1] + o->rootHi[1]) * 0.5f,
@@ -1415,12 +1414,12 @@ int orc_render_rows(Oracle *o, int row0, int row1) {
   }
   uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0, cap = 0;
   const int W = o->W;
-  const int64_t n = (int64_t)(row1 - row0) * W;
+  const int64_t n = (int64_t)nrows * W;
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : c0, c1, c2, c3, cap)
   for (int64_t i = 0; i < n; i++) {
     uint64_t cnt[4] = {0, 0, 0, 0};
     uint64_t capped = 0;
-    render_pixel(*o, (int)(i % W), row0 + (int)(i / W), cnt, capped);
+    render_pixel(*o, (int)(i % W), row0 + stride * (int)(i / W), cnt, capped);
     c0 += cnt[0]; c1 += cnt[1]; c2 += cnt[2]; c3 += cnt[3]; cap += capped;
   }
   o->counters[0] += c0; o->counters[1] += c1; o->counters[2] += c2; o->counters[3] += c3;
@@ -1429,6 +1428,21 @@ int orc_render_rows(Oracle *o, int row0, int row1) {
   o->accumParam = o->accumID++;
   o->frameParam = o->frameID++;
   return ORC_OK;
+}
+
+// Render one frame over the pixel rows [row0, row1) (all rows when row1 <= row0).
+int orc_render_rows(Oracle *o, int row0, int row1) {
+  if (!o->inited) return ORC_STATE;
+  if (row1 <= row0) { row0 = 0; row1 = o->H; }
+  if (row0 < 0 || row1 > o->H) return ORC_BAD;
+  return render_row_set(o, row0, 1, row1 - row0);
+}
+// Render one frame over the rows row0, row0 + stride, ... below the frame's height
+// (rows spread over the frame, for timing samples).
+int orc_render_row_stride(Oracle *o, int row0, int stride) {
+  if (!o->inited) return ORC_STATE;
+  if (row0 < 0 || row0 >= o->H || stride <= 0) return ORC_BAD;
+  return render_row_set(o, row0, stride, (o->H - 1 - row0) / stride + 1);
 }
 int orc_render(Oracle *o) { return orc_render_rows(o, 0, 0); }
 int orc_set_features(Oracle *o, int e) { o->featOn = e != 0; return ORC_OK; }

@@ -73,6 +73,12 @@ class OracleRenderer(Renderer):
         """One frame restricted to pixel rows [row0, row1) (frame ids still advance)."""
         self._call("render_rows", C.c_int(row0), C.c_int(row1))
 
+    def renderRowStride(self, row0: int, stride: int) -> int:
+        """One frame over the rows row0, row0 + stride, ... of the frame (frame ids still
+        advance); returns how many rows were rendered."""
+        self._call("render_row_stride", C.c_int(row0), C.c_int(stride))
+        return (self.fbSize[1] - 1 - row0) // stride + 1
+
     _band = (0, 0)
 
     def setRenderRows(self, row0: int, row1: int):

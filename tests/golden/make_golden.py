@@ -60,7 +60,7 @@ def rays(n=400, seed=23):
 
 
 def main(argv):
-    ref = argv[1] if len(argv) > 1 else "/root/reference"
+    ref = argv[1] if len(argv) > 1 else os.path.normpath(os.path.join(ROOT, "..", "reference"))
     out = argv[2] if len(argv) > 2 else HERE
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref], check=True,
                    stdout=subprocess.DEVNULL)

@@ -44,7 +44,7 @@ def test_reference_arm_other_ranks_exit_quietly():
 def test_defaults(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse_args()
-    assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1 and a.config == "c2" and a.impl == "mdwt"
+    assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1 and a.config == "c3" and a.edge == 16 and a.impl == "mdwt"
     assert not a.no_autotune and a.regroup is None
 
 
