@@ -1470,6 +1470,46 @@ int orc_set_frame_id(Oracle *o, int f) {
   o->frameID = f + 1;
   return ORC_OK;
 }
+// The state a launch of the reference's mainRG reads (for the pins against the
+// reference's own device code): f = dt, root box lo[3] hi[3] (union of the channels),
+// last channel's box4f lo[4] hi[4], background[3], light direction[3], intensity, ambient;
+// i = mode, spp, accumulation, shadows, gradient shading, W, H, channels.
+int orc_get_launch_state(Oracle *o, float f[23], int i[8]) {
+  if (!o->inited) return ORC_STATE;
+  int k = 0;
+  f[k++] = o->dt;
+  for (int a = 0; a < 3; a++) f[k++] = o->rootLo[a];
+  for (int a = 0; a < 3; a++) f[k++] = o->rootHi[a];
+  for (int a = 0; a < 4; a++) f[k++] = o->gLo[a];
+  for (int a = 0; a < 4; a++) f[k++] = o->gHi[a];
+  f[k++] = o->bg.x; f[k++] = o->bg.y; f[k++] = o->bg.z;
+  f[k++] = o->lightDir.x; f[k++] = o->lightDir.y; f[k++] = o->lightDir.z;
+  f[k++] = o->lightIntensity;
+  f[k++] = o->ambient;
+  i[0] = o->mode; i[1] = o->spp; i[2] = o->accum; i[3] = o->shadows; i[4] = o->gradient;
+  i[5] = o->W; i[6] = o->H; i[7] = (int)o->ch.size();
+  return ORC_OK;
+}
+// Channel c's transfer function as uploaded (alpha cubed): texels (4 floats each, at
+// most cap texels written), count, volume domain, TF range and opacity scale.
+int orc_get_tf(Oracle *o, int c, float *rgba, int cap, int *n, float vd[2], float xd[2], float *os) {
+  if (c < 0 || c >= (int)o->tf.size()) return ORC_BAD;
+  const TFData &t = o->tf[c];
+  *n = t.n;
+  if (rgba) std::memcpy(rgba, t.rgba.data(), sizeof(float) * 4 * (size_t)std::min(cap, t.n));
+  vd[0] = t.vd[0]; vd[1] = t.vd[1]; xd[0] = t.xd[0]; xd[1] = t.xd[1];
+  *os = t.os;
+  return ORC_OK;
+}
+// Channel c's material: diffuse, specular, shininess, gradient step, specular colour.
+int orc_get_material(Oracle *o, int c, float out[7]) {
+  if (c < 0 || c >= (int)o->mats.size()) return ORC_BAD;
+  const Material &m = o->mats[c];
+  out[0] = m.diffuse; out[1] = m.specular; out[2] = m.shininess; out[3] = m.gradStep;
+  out[4] = m.spec.x; out[5] = m.spec.y; out[6] = m.spec.z;
+  return ORC_OK;
+}
+float orc_pow(float x, float y) { return mpow(x, y); }
 int orc_get_frame_ids(Oracle *o, int out[4]) {
   out[0] = o->frameID; out[1] = o->accumID; out[2] = o->frameParam; out[3] = o->accumParam; return ORC_OK;
 }

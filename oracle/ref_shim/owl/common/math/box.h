@@ -1,5 +1,6 @@
 // TEST INFRASTRUCTURE ONLY.  Stand-in for OWL's box types (owl/common/math/box.h):
-// the lower/upper pairs the reference's dda.h and rawFile.h construct and read.
+// the lower/upper pairs the reference's dda.h, rawFile.h and deviceCode.cu construct and
+// read, and box3f::including (the bounds programs of deviceCode.cu).
 #pragma once
 
 #include "vec.h"
@@ -11,6 +12,8 @@ struct box3f {
   vec3f lower, upper;
   box3f() = default;
   box3f(const vec3f &lo, const vec3f &hi) : lower(lo), upper(hi) {}
+  box3f including(const vec3f &p) const { return box3f(min(lower, p), max(upper, p)); }
+  box3f &extend(const vec3f &p) { lower = min(lower, p); upper = max(upper, p); return *this; }
 };
 
 struct box4f {

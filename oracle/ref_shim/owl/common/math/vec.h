@@ -1,21 +1,33 @@
 // TEST INFRASTRUCTURE ONLY.  A minimal stand-in for the vector types of OWL's math
 // library (owl-project/owl, owl/common/math/vec.h), which the reference's sources include
-// but whose submodule is empty and whose commit is unpinned.  It declares only what the
-// reference's dda.h and rawFile.h use, so that oracle/Makefile can compile those reference
-// files where they lie (into oracle/_ref/) and the oracle can be checked against them.
+// but whose submodule is empty and whose commit is unpinned.  It declares what the
+// reference's dda.h, rawFile.h, camera.h and deviceCode.cu use, so that oracle/Makefile
+// can compile those reference files where they lie (into oracle/_ref/) and the oracle can
+// be checked against them.
 //
 // Element-wise semantics are those of the reference's CUDA device code, where OWL's
 // helpers resolve to CUDA's float overloads: scalar min/max are fminf/fmaxf, abs is
-// fabsf, and rcp is the correctly rounded 1/x.
+// fabsf, rcp is the correctly rounded 1/x, and sqrt is the correctly rounded square root.
+// length(v) = sqrt(dot(v, v)) and normalize(v) = v * (1 / sqrt(dot(v, v))), the
+// arithmetic this project fixes for OWL's helpers (the oracle and the kernels use it).
 #pragma once
 
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 
+#include <vector_types.h>   // CUDA's float3 / float4 / uint3 (host-usable plain structs)
+
 #ifndef __CUDACC__
+#ifndef __device__
 #define __device__
+#endif
+#ifndef __host__
 #define __host__
+#endif
+#endif
+#ifndef __both__
+#define __both__
 #endif
 #ifndef CUDART_INF
 #define CUDART_INF __builtin_inf()   // a double, like CUDA's math_constants.h
@@ -26,31 +38,69 @@ namespace common {
 
 inline float min(float a, float b) { return fminf(a, b); }
 inline float max(float a, float b) { return fmaxf(a, b); }
+inline int min(int a, int b) { return a < b ? a : b; }
+inline int max(int a, int b) { return a > b ? a : b; }
 inline float abs(float a) { return fabsf(a); }
 inline float rcp(float a) { return 1.0f / a; }
 
+// ---------------------------------------------------------------- 2-D
+struct vec2i;
+struct vec2f {
+  union { float x; float u; };
+  union { float y; float v; };
+  vec2f() : x(0.f), y(0.f) {}
+  explicit vec2f(float s) : x(s), y(s) {}
+  vec2f(float a, float b) : x(a), y(b) {}
+  explicit vec2f(const vec2i &o);
+  vec2f(const float2 &o) : x(o.x), y(o.y) {}
+};
+struct vec2i {
+  int x = 0, y = 0;
+  vec2i() = default;
+  vec2i(int a, int b) : x(a), y(b) {}
+};
+inline vec2f::vec2f(const vec2i &o) : x((float)o.x), y((float)o.y) {}
+inline vec2f operator+(const vec2f &a, float s) { return vec2f(a.x + s, a.y + s); }
+inline vec2f operator+(const vec2f &a, const vec2f &b) { return vec2f(a.x + b.x, a.y + b.y); }
+inline vec2f operator/(const vec2f &a, const vec2f &b) { return vec2f(a.x / b.x, a.y / b.y); }
+
+// ---------------------------------------------------------------- 3-D
 struct vec3ui {
   uint32_t x = 0, y = 0, z = 0;
   vec3ui() = default;
   vec3ui(uint32_t a, uint32_t b, uint32_t c) : x(a), y(b), z(c) {}
+  const uint32_t &operator[](unsigned i) const { return i == 0 ? x : (i == 1 ? y : z); }
 };
 
 struct vec3i;
+struct vec4f;
 
 struct vec3f {
   float x = 0.f, y = 0.f, z = 0.f;
   vec3f() = default;
-  explicit vec3f(float s) : x(s), y(s), z(s) {}
+  vec3f(float s) : x(s), y(s), z(s) {}
   vec3f(float a, float b, float c) : x(a), y(b), z(c) {}
   explicit vec3f(const vec3ui &v) : x((float)v.x), y((float)v.y), z((float)v.z) {}
   explicit vec3f(const vec3i &v);
+  explicit vec3f(const vec4f &v);
+  vec3f(const float3 &v) : x(v.x), y(v.y), z(v.z) {}
+  explicit vec3f(const float4 &v) : x(v.x), y(v.y), z(v.z) {}
+  operator float3() const { return make_float3_(x, y, z); }
+  float &operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+  const float &operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+
+ private:
+  static float3 make_float3_(float a, float b, float c) { float3 r; r.x = a; r.y = b; r.z = c; return r; }
 };
 
 struct vec3i {
   int x = 0, y = 0, z = 0;
   vec3i() = default;
+  explicit vec3i(int s) : x(s), y(s), z(s) {}
   vec3i(int a, int b, int c) : x(a), y(b), z(c) {}
   explicit vec3i(const vec3f &v) : x((int)v.x), y((int)v.y), z((int)v.z) {}
+  int &operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+  const int &operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
 };
 inline vec3f::vec3f(const vec3i &v) : x((float)v.x), y((float)v.y), z((float)v.z) {}
 
@@ -60,20 +110,24 @@ struct vec3l {
   vec3l(int64_t a, int64_t b, int64_t c) : x(a), y(b), z(c) {}
 };
 
-struct vec4f {
-  float x = 0.f, y = 0.f, z = 0.f, w = 0.f;
-  vec4f() = default;
-  vec4f(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
-};
-
 inline vec3f operator+(const vec3f &a, const vec3f &b) { return vec3f(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline vec3f operator-(const vec3f &a, const vec3f &b) { return vec3f(a.x - b.x, a.y - b.y, a.z - b.z); }
 inline vec3f operator*(const vec3f &a, const vec3f &b) { return vec3f(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline vec3f operator/(const vec3f &a, const vec3f &b) { return vec3f(a.x / b.x, a.y / b.y, a.z / b.z); }
 inline vec3f operator*(float s, const vec3f &b) { return vec3f(s * b.x, s * b.y, s * b.z); }
 inline vec3f operator*(const vec3f &a, float s) { return vec3f(a.x * s, a.y * s, a.z * s); }
+inline vec3f operator/(const vec3f &a, float s) { return vec3f(a.x / s, a.y / s, a.z / s); }
+inline vec3f operator/(float s, const vec3f &b) { return vec3f(s / b.x, s / b.y, s / b.z); }
 inline vec3f operator+(const vec3f &a, float s) { return vec3f(a.x + s, a.y + s, a.z + s); }
 inline vec3f operator-(const vec3f &a, float s) { return vec3f(a.x - s, a.y - s, a.z - s); }
+inline vec3f operator-(const vec3f &a) { return vec3f(-a.x, -a.y, -a.z); }
+inline vec3f &operator+=(vec3f &a, const vec3f &b) { a = a + b; return a; }
+inline vec3f &operator-=(vec3f &a, const vec3f &b) { a = a - b; return a; }
+inline vec3f &operator*=(vec3f &a, float s) { a = a * s; return a; }
+inline vec3f &operator/=(vec3f &a, float s) { a = a / s; return a; }
 inline bool operator==(const vec3f &a, const vec3f &b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+inline vec3i operator+(const vec3i &a, const vec3i &b) { return vec3i(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline vec3i operator-(const vec3i &a, const vec3i &b) { return vec3i(a.x - b.x, a.y - b.y, a.z - b.z); }
 
 inline vec3f min(const vec3f &a, const vec3f &b) { return vec3f(min(a.x, b.x), min(a.y, b.y), min(a.z, b.z)); }
 inline vec3f max(const vec3f &a, const vec3f &b) { return vec3f(max(a.x, b.x), max(a.y, b.y), max(a.z, b.z)); }
@@ -81,6 +135,30 @@ inline vec3f abs(const vec3f &a) { return vec3f(abs(a.x), abs(a.y), abs(a.z)); }
 inline vec3f rcp(const vec3f &a) { return vec3f(rcp(a.x), rcp(a.y), rcp(a.z)); }
 inline float reduce_min(const vec3f &a) { return min(min(a.x, a.y), a.z); }
 inline float reduce_max(const vec3f &a) { return max(max(a.x, a.y), a.z); }
+inline float dot(const vec3f &a, const vec3f &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline vec3f cross(const vec3f &a, const vec3f &b) {
+  return vec3f(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+inline float length(const vec3f &a) { return sqrtf(dot(a, a)); }
+inline vec3f normalize(const vec3f &a) { return a * (1.0f / sqrtf(dot(a, a))); }
+
+// ---------------------------------------------------------------- 4-D
+struct vec4f {
+  float x = 0.f, y = 0.f, z = 0.f, w = 0.f;
+  vec4f() = default;
+  explicit vec4f(float s) : x(s), y(s), z(s), w(s) {}
+  vec4f(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+  vec4f(const vec3f &v, float d) : x(v.x), y(v.y), z(v.z), w(d) {}
+  vec4f(const float4 &v) : x(v.x), y(v.y), z(v.z), w(v.w) {}
+  operator float4() const { float4 r; r.x = x; r.y = y; r.z = z; r.w = w; return r; }
+};
+inline vec3f::vec3f(const vec4f &v) : x(v.x), y(v.y), z(v.z) {}
+inline vec4f operator+(const vec4f &a, const vec4f &b) { return vec4f(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+inline vec4f operator*(const vec4f &a, float s) { return vec4f(a.x * s, a.y * s, a.z * s, a.w * s); }
+inline vec4f operator*(float s, const vec4f &a) { return vec4f(s * a.x, s * a.y, s * a.z, s * a.w); }
+inline vec4f operator/(const vec4f &a, float s) { return vec4f(a.x / s, a.y / s, a.z / s, a.w / s); }
+inline vec4f &operator+=(vec4f &a, const vec4f &b) { a = a + b; return a; }
+inline vec4f &operator/=(vec4f &a, float s) { a = a / s; return a; }
 
 }  // namespace common
 using namespace common;
