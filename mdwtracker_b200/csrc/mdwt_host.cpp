@@ -155,6 +155,7 @@ struct mdwt_ctx {
   float *dRanges = nullptr;
   float *dMaj = nullptr;
   uint16_t *dMask = nullptr;    // per-cell non-zero-majorant channel mask
+  float *dMajRcp = nullptr;     // recip_for_div of each majorant (the trackers' free flights)
   size_t M = 0;
   float rootLo[3] = {0, 0, 0}, rootHi[3] = {1, 1, 1};
   float gLo[4] = {0, 0, 0, 0}, gHi[4] = {1, 1, 1, 1};
@@ -458,6 +459,8 @@ void free_device(mdwt_ctx *c) {
   if (c->dMaj) cudaFree(c->dMaj);
   if (c->dMask) cudaFree(c->dMask);
   c->dMask = nullptr;
+  if (c->dMajRcp) cudaFree(c->dMajRcp);
+  c->dMajRcp = nullptr;
   if (c->dRec) cudaFree(c->dRec);
   if (c->dRecStats) cudaFree(c->dRecStats);
   if (c->dRecT) cudaFree(c->dRecT);
@@ -505,6 +508,7 @@ mdwt_status recalc(mdwt_ctx *c) {
   std::memset(&p, 0, sizeof(p));
   p.ranges = c->dRanges;
   p.majorants = c->dMaj;
+  p.majRcp = c->dMajRcp;
   p.mask = c->dMask;
   p.C = (int)c->ch.size();
   p.mode = c->mode;
@@ -761,6 +765,7 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  CK(cudaMalloc(&c->dMajRcp, c->M * (mode >= 3 ? 1 : C) * 4), "cudaMalloc majorant reciprocals");
   CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
   c->inited = true;
   mdwt_status s = build_ranges(c);
@@ -979,6 +984,7 @@ static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   p.mode = c->mode;
   p.dt = c->dt;
   p.majorants = c->dMaj;
+  p.majRcp = c->dMajRcp;
   p.mask = c->dMask;
   for (int i = 0; i < p.C; i++) {
     p.vol[i] = c->ch[i].dVol;
@@ -1240,12 +1246,14 @@ static mdwt_status regrid(mdwt_ctx *c) {
   if (c->dRanges) cudaFree(c->dRanges);
   if (c->dMaj) cudaFree(c->dMaj);
   if (c->dMask) cudaFree(c->dMask);
-  c->dRanges = nullptr; c->dMaj = nullptr; c->dMask = nullptr;
+  if (c->dMajRcp) cudaFree(c->dMajRcp);
+  c->dRanges = nullptr; c->dMaj = nullptr; c->dMask = nullptr; c->dMajRcp = nullptr;
   for (int a = 0; a < 3; a++) c->mc[a] = mc[a];
   c->M = (size_t)mc[0] * mc[1] * mc[2];
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (c->mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
+  CK(cudaMalloc(&c->dMajRcp, c->M * (c->mode >= 3 ? 1 : C) * 4), "cudaMalloc majorant reciprocals");
   CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
   mdwt_status s = build_ranges(c);
   if (s) return s;

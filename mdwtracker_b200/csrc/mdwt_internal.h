@@ -43,6 +43,7 @@ struct TrackParams {
   int C, mode;
   float dt;
   const float *majorants;      // [cell*C + ch] (modes 0..2) or [cell] (mode 3)
+  const float *majRcp;         // the same layout: recip_for_div of each majorant
   const uint16_t *mask;        // per cell: bit c set when majorants[cell*C + c] != 0
   // channels
   const void *vol[kMaxChannels];
@@ -146,6 +147,7 @@ int launch_ranges_init(float *ranges, size_t count, void *stream, int *launches)
 struct MajorantParams {
   const float *ranges;
   float *majorants;
+  float *majRcp;               // recip_for_div of each majorant (the free flights divide by it)
   uint16_t *mask;              // per cell: bit c set when channel c's majorant is non-zero
   int C, mode;
   size_t M;

@@ -118,6 +118,7 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
         sum += channel_majorant(p, c, rc.x, rc.y);
       }
       p.majorants[cell] = sum;
+      if (p.majRcp) p.majRcp[cell] = recip_for_div(sum);
       if (p.mask) p.mask[cell] = sum != 0.0f ? 1 : 0;
     } else {
       uint32_t m = 0;
@@ -125,6 +126,7 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
         const float2 rc = r[c];
         const float v = channel_majorant(p, c, rc.x, rc.y);
         p.majorants[cell * C + c] = v;
+        if (p.majRcp) p.majRcp[cell * C + c] = recip_for_div(v);
         if (v != 0.0f) m |= 1u << c;
       }
       if (p.mask) p.mask[cell] = (uint16_t)m;

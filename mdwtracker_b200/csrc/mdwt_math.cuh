@@ -80,6 +80,30 @@ __device__ __forceinline__ float mpow(float x, float y) {
   return mexp(y * mlog(x));
 }
 
+// a / b correctly rounded, from y = RN(1/b): q = RN(a*y), then one correction with the
+// exact residual a - q*b (Markstein 1990: with y the correctly rounded reciprocal and no
+// underflow or overflow, RN(q + y*(a - q*b)) is the correctly rounded quotient).  The
+// correction runs where |a| >= 2^-80 and 2^-80 <= |q| <= 2^80, so the residual stays a
+// normal number; elsewhere (y = 0 included, and NaN) the IEEE division itself.
+__device__ __forceinline__ float div_by(float a, float b, float y) {
+  const float q = a * y;
+  const float aq = fabsf(q);
+  if (fabsf(a) >= 8.271806125530277e-25f && aq >= 8.271806125530277e-25f && aq <= 1.2089258196146292e24f)
+    return fmaf(fmaf(-q, b, a), y, q);
+  return a / b;
+}
+// RN(1/b) for 2^-80 <= |b| <= 2^80, else 0 (div_by then divides).
+__device__ __forceinline__ float recip_for_div(float b) {
+  const float ab = fabsf(b);
+  return (ab >= 8.271806125530277e-25f && ab <= 1.2089258196146292e24f) ? 1.0f / b : 0.0f;
+}
+
+// One Woodcock free flight t - (log(1 - u) / majorant) * dt * w2g (deviceCode.cu:805),
+// the quotient from the majorant's reciprocal rmaj = recip_for_div(maj).
+__device__ __forceinline__ float flight(float t, float u, float maj, float rmaj, float dt, float w2g) {
+  return fmaf(-(div_by(mlog(1.0f - u), maj, rmaj) * dt), w2g, t);
+}
+
 __device__ __forceinline__ float quant(float a) { return rintf(a * 256.0f) * (1.0f / 256.0f); }
 __device__ __forceinline__ float lerpf(float a, float p, float q) { return fmaf(a, q, (1.0f - a) * p); }
 

@@ -77,6 +77,7 @@ struct ChanSm {
   const float *tfAlpha;
   int X, Y, Z, n;
   float vd0, vd1, xd0, xd1, os;
+  float ry1, ry2;   // recip_for_div of the TF remap divisors vd1 - vd0 and xd1 - xd0
 };
 
 // sampleVolumeTexture (deviceCode.cu:122-132): NaN outside [0,1]^3, else trilinear.
@@ -93,8 +94,8 @@ __device__ __forceinline__ float sample_volume(const TrackParams &P, const ChanS
 __device__ __forceinline__ float tf_alpha(const ChanSm &cs, float f, Axis &ax) {
   if (cs.n <= 0) return 0.f;
   if (f < cs.vd0 || f > cs.vd1) return 0.f;
-  const float r1 = (f - cs.vd0) / (cs.vd1 - cs.vd0);
-  const float r2 = (r1 - cs.xd0) / (cs.xd1 - cs.xd0);
+  const float r1 = div_by(f - cs.vd0, cs.vd1 - cs.vd0, cs.ry1);
+  const float r2 = div_by(r1 - cs.xd0, cs.xd1 - cs.xd0, cs.ry2);
   ax = axis(r2, cs.n);
   return lerpf(ax.a, __ldg(cs.tfAlpha + ax.i0), __ldg(cs.tfAlpha + ax.i1)) * cs.os;
 }
@@ -223,6 +224,8 @@ __device__ __forceinline__ ChanSm chan_params(const TrackParams &P, int c) {
   cs.vd0 = P.vd[c][0]; cs.vd1 = P.vd[c][1];
   cs.xd0 = P.xd[c][0]; cs.xd1 = P.xd[c][1];
   cs.os = P.os[c];
+  cs.ry1 = recip_for_div(cs.vd1 - cs.vd0);
+  cs.ry2 = recip_for_div(cs.xd1 - cs.xd0);
   return cs;
 }
 
@@ -250,7 +253,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
   d.visits = 0;
   int ch = 0, cellID = 0;
   uint32_t cmask = 0;                          // non-zero-majorant channels of the current cell
-  float maj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f, tW = 0.f;
+  float maj = 0.f, rmaj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f, tW = 0.f;
   float rnd = 0.f;                              // -m 1: the draw taken before a selection
   float majs[MODE == 1 ? kMaxChannels : 1], ts[MODE == 1 ? kMaxChannels : 1];   // -m 1 per-channel state
   bool capped = false;
@@ -417,6 +420,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             }
             ch += __ffs(rem) - 1;
             maj = __ldg(P.majorants + (size_t)cellID * C + ch);
+            rmaj = __ldg(P.majRcp + (size_t)cellID * C + ch);
             t = ct0;
             stepping = true;
             break;
@@ -437,6 +441,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             act = A_CHAN;
             if ((cmask >> ch) & 1u) {  // zero-majorant cells are skipped (deviceCode.cu:893-894)
               maj = __ldg(P.majorants + (size_t)cellID * C + ch);
+              rmaj = __ldg(P.majRcp + (size_t)cellID * C + ch);
               t = ct0;
               stepping = true;
               break;
@@ -451,6 +456,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             if constexpr (MODE >= 3) {  // summed majorant (deviceCode.cu:541-548, 1003-1007)
               if (cmask & 1u) {
                 maj = __ldg(P.majorants + cellID);
+                rmaj = __ldg(P.majRcp + cellID);
                 t = ct0;
                 stepping = true;
                 break;
@@ -492,7 +498,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             exitCell = minT >= ct1;
           } else {
             const float u = rng_next(rng);
-            t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+            t = flight(t, u, maj, rmaj, P.dt, w2g);
             exitCell = MODE == 2 ? (t >= lim) : (t >= ct1);
             if (MODE == 0 && !exitCell && lim < t) skipChannel = true;
           }
@@ -659,7 +665,7 @@ struct Slots {
   uint32_t meta[kSlots], recIdx[kSlots], rng[kSlots], steps[kSlots], record[kSlots], cell[kSlots];
   float wdx[kSlots], wdy[kSlots], wdz[kSlots], t1w[kSlots], w2g[kSlots], g2w[kSlots];
   float tnx[kSlots], tny[kSlots], tnz[kSlots], tsx[kSlots], tsy[kSlots], tsz[kSlots];
-  float rt0[kSlots], ncb[kSlots], maj[kSlots], t[kSlots], lim[kSlots];
+  float rt0[kSlots], ncb[kSlots], maj[kSlots], rmaj[kSlots], t[kSlots], lim[kSlots];
 };
 __device__ __forceinline__ uint32_t pack_meta(uint32_t stage, uint32_t flags, int ch, uint32_t cmask, uint32_t visits) {
   return stage | flags | ((uint32_t)ch << 4) | ((cmask & 0xfffu) << 9) | (visits << 21);
@@ -741,7 +747,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
   int ch = (int)((m0 >> 4) & 15u);
   uint32_t cmask = (m0 >> 9) & 0xfffu, visits = m0 >> 21;
   uint32_t record = S.record[s], steps = S.steps[s], rng = S.rng[s];
-  float maj = S.maj[s], t = S.t[s], lim = S.lim[s];
+  float maj = S.maj[s], rmaj = S.rmaj[s], t = S.t[s], lim = S.lim[s];
   const float w2g = S.w2g[s];
   const float wdx = S.wdx[s], wdy = S.wdy[s], wdz = S.wdz[s];
   DDA d;
@@ -773,6 +779,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
         ch += __ffs(rem) - 1;
         const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
         maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
+        rmaj = __ldg(P.majRcp + (size_t)cellID * P.C + ch);
         t = d.rt0 + d.ncb;   // the cell's entry distance
         break;
       }
@@ -782,7 +789,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     // free-flight draw (deviceCode.cu:800-820)
     if (++steps >= kMaxStepsPerSample) { finish(P, S, s, record, true, tot); return; }
     const float u = rng_next(rng);
-    t = fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+    t = flight(t, u, maj, rmaj, P.dt, w2g);
     if (t >= lim) {
       ch++;
       drawing = false;
@@ -801,7 +808,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     if (++k >= P.trips) break;
   }
   S.meta[s] = pack_meta(stage, (drawing ? kDraw : 0u) | (advance ? kAdvance : 0u), ch, cmask, d.visits);
-  S.steps[s] = steps; S.rng[s] = rng; S.maj[s] = maj; S.t[s] = t; S.lim[s] = lim;
+  S.steps[s] = steps; S.rng[s] = rng; S.maj[s] = maj; S.rmaj[s] = rmaj; S.t[s] = t; S.lim[s] = lim;
   if (moved) {
     S.tnx[s] = d.tnx; S.tny[s] = d.tny; S.tnz[s] = d.tnz;
     S.cell[s] = (uint32_t)d.cx | ((uint32_t)d.cy << 10) | ((uint32_t)d.cz << 20);
