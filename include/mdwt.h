@@ -211,7 +211,7 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * it evaluates its pending density samples together.
  * MDWT_TUNE_QUORUM: a round's trips also end once `value` (1..33; 33 = never) of the
  * warp's lanes hold a pending density sample.
- * MDWT_TUNE_REGROUP: 1 (default) = -m 2 frames without shadows, features or per-pixel
+ * MDWT_TUNE_REGROUP: 1 (default) = -m 2 and -m 0 frames without shadow rays or per-pixel
  * statistics run the tracker that keeps 64 paths per warp and runs, at each step, the
  * operation most of them need next (path start, walk, density sample), one path per
  * lane; a walk takes at most TRIPS free-flight draws.  0 = the warp-local tracker (32
@@ -270,6 +270,15 @@ mdwt_status mdwt_copy_features(mdwt_ctx *ctx, void *d_dst, void *stream);
 mdwt_status mdwt_render_expected(mdwt_ctx *ctx, int jitter, float step_voxels, void *stream);
 mdwt_status mdwt_get_expected(mdwt_ctx *ctx, double *host_out);
 mdwt_status mdwt_accum_rmse(mdwt_ctx *ctx, double *rmse);
+
+/* No counterpart in the reference: a self-check of the trackers' free-flight exit filter.
+ * A flight t - log(1 - u) / majorant * dt * w2g (deviceCode.cu:805, 915) that certainly
+ * leaves the current cell is decided from the hardware log2 with a margin, without the
+ * exact log; the margin assumes |log2_hw(x) - log2(x)| <= 2^-20 * (1 + |log2 x|) for every
+ * flight argument x = 1 - k 2^-24.  Writes the largest observed value of
+ * |log2_hw(x) - log2(x)| / (1 + |log2 x|) over all 2^24 of them on the current device
+ * (synchronous; allocates 4 bytes). */
+mdwt_status mdwt_check_flight_filter(float *worst_out);
 
 /* No counterpart in the reference.  The value ranges of ONE channel, built on the GPU
  * without allocating any memory, for callers that may not allocate device memory: code

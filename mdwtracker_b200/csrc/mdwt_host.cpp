@@ -1654,9 +1654,9 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
   const int tripsC[] = {1, 2, 3, 4, 6, 8};
   const int poolsC[] = {4, 8, 16, 32};
   const int quorumC[] = {8, 16, 24, 33};
-  // the regrouped tracker runs -m 2 frames without shadows, gradient shading, features or
-  // per-pixel statistics; other frames run the warp-local tracker whatever the knob says
-  const bool regroupable = c->mode == 2 && !c->shadows && !c->gradient && !c->featOn && !c->statsOn;
+  // the regrouped tracker runs -m 2 and -m 0 frames without shadow rays or per-pixel
+  // statistics; other frames run the warp-local tracker whatever the knob says
+  const bool regroupable = (c->mode == 2 || c->mode == 0) && !c->shadows && !c->statsOn;
   if (regroupable) s = tune(&c->regroup, regroupC, 2);
   if (!s && !(s = tune(&c->trips, tripsC, 6)) && !(regroupable && c->regroup)) {
     // the regeneration pool and the sample quorum belong to the warp-local tracker

@@ -104,6 +104,29 @@ __device__ __forceinline__ float flight(float t, float u, float maj, float rmaj,
   return fmaf(-(div_by(mlog(1.0f - u), maj, rmaj) * dt), w2g, t);
 }
 
+// Exit filter of a free flight: true only when flight(t, u, maj, rmaj, dt, w2g) >= lim is
+// certain, decided from the hardware log2 (lg2.approx) instead of the exact chain; a
+// false answer means "run the exact flight".  k = rmaj * dt * w2g * ln 2.
+//   The estimate xf = -log2(1 - u) * k of the flight length differs from the exact chain's
+// length by at most xf * kFlightRel + k * kFlightAbs, where
+//   - mlog's relative error over every 1 - u of the 24-bit draw grid is <= 1.6e-7
+//     (checked exhaustively against a double-precision log on the host),
+//   - lg2.approx's error over the same 2^24 inputs is below 2^-20 * (1 + |log2 x|)
+//     (checked exhaustively on the GPU by the tests),
+//   - the roundings of the exact chain (quotient, product by dt) and of k add a few 2^-24,
+// and the constants take 2^-18 for both, four times those bounds and more.  The terms
+// |tf| * 2^-22 cover the roundings of tf and of the final comparison.  Since the exact
+// t' = RN(t + length) and RN is monotone, t + length >= lim implies t' >= lim.
+constexpr float kFlightRel = 3.814697265625e-06f;   // 2^-18
+constexpr float kFlightAbs = 3.814697265625e-06f;   // 2^-18 (log2 units, times k)
+constexpr float kLn2 = 0.693147182464599609375f;     // RN(ln 2)
+__device__ __forceinline__ bool flight_surely_exits(float t, float u, float k, float lim) {
+  const float xf = -__log2f(1.0f - u) * k;
+  const float tf = t + xf;
+  const float m = fmaf(xf, kFlightRel, fmaf(k, kFlightAbs, fabsf(tf) * 2.384185791015625e-07f));
+  return tf - m >= lim;
+}
+
 __device__ __forceinline__ float quant(float a) { return rintf(a * 256.0f) * (1.0f / 256.0f); }
 __device__ __forceinline__ float lerpf(float a, float p, float q) { return fmaf(a, q, (1.0f - a) * p); }
 

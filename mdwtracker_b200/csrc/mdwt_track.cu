@@ -23,6 +23,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstring>
+
+#include "../../include/mdwt.h"
 #include "mdwt_internal.h"
 #include "mdwt_math.cuh"
 
@@ -255,6 +258,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
   uint32_t cmask = 0;                          // non-zero-majorant channels of the current cell
   float maj = 0.f, rmaj = 0.f, t = 0.f, lim = 0.f, ct0 = 0.f, ct1 = 0.f, tW = 0.f;
   float rnd = 0.f;                              // -m 1: the draw taken before a selection
+  float pendU = 0.f;                            // the draw of a flight pending in phase 2
   float majs[MODE == 1 ? kMaxChannels : 1], ts[MODE == 1 ? kMaxChannels : 1];   // -m 1 per-channel state
   bool capped = false;
   float tHitW = 0.f;                            // world t of the recorded hit
@@ -497,10 +501,16 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             t = minT;
             exitCell = minT >= ct1;
           } else {
-            const float u = rng_next(rng);
-            t = flight(t, u, maj, rmaj, P.dt, w2g);
-            exitCell = MODE == 2 ? (t >= lim) : (t >= ct1);
-            if (MODE == 0 && !exitCell && lim < t) skipChannel = true;
+            // A flight that certainly leaves the cell needs no exact length (the next
+            // channel or cell starts again from its entry distance).  The others -- the
+            // few that end inside the cell -- compute it in phase 2, together, before
+            // their density sample.
+            pendU = rng_next(rng);
+            exitCell = flight_surely_exits(t, pendU, rmaj * (P.dt * w2g * kLn2), MODE == 2 ? lim : ct1);
+            if (!exitCell) {
+              st = S_SAMPLE;
+              continue;
+            }
           }
           if (exitCell) {
             if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
@@ -523,7 +533,24 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
     }
     __syncwarp();
 
-    // ---------------- phase 2: the pending density samples, together
+    // ---------------- phase 2: the pending flights and density samples, together
+    if (MODE != 1 && st == S_SAMPLE) {   // the exact flight and its tests (deviceCode.cu:805-821, 915-931)
+      t = flight(t, pendU, maj, rmaj, P.dt, w2g);
+      if (t >= (MODE == 2 ? lim : ct1)) {   // leaves the cell after all
+        if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
+        st = S_TRANS;
+      } else if (MODE == 0 && lim < t) {    // beyond the closest hit so far: next channel
+        ch++; act = A_NEWDDA; st = S_TRANS;
+      } else {
+        tW = t * g2w;
+        if (tW >= t1w) {  // world exit
+          if (STATS) pRej++;
+          totRej++;
+          if ((MODE == 2 && ch == C - 1) || MODE >= 3) finish();
+          else { ch++; act = MODE == 2 ? A_CHAN : A_NEWDDA; st = S_TRANS; }
+        }
+      }
+    }
     if (st == S_SAMPLE) {
       const float xs = fmaf(tW, wdx, SH ? lox : P.camOrg.x) * P.w2u.x;
       const float ys = fmaf(tW, wdy, SH ? loy : P.camOrg.y) * P.w2u.y;
@@ -640,17 +667,21 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
 }
 
 // ------------------------------------------------------------------ regrouped tracker
-// trace_regroup_kernel: the syncDDA tracker (-m 2; no shadows, features or per-pixel
-// statistics) with each warp's paths regrouped by their next operation.  A warp keeps 64
-// path states in shared memory (structure of arrays), twice its lanes.  Each iteration it
-// counts its slots per stage -- start a path, walk (cell and channel transitions with
-// free-flight draws, at most `trips` draws), evaluate a pending density sample -- and runs
-// the most populated stage with lane i on the i-th slot of that stage, so at least 22 of
-// its 32 lanes work on the same operation.  Warps run independently (no block barrier).
-// Every path runs exactly the arithmetic of trace_items (the same helpers, in the same
-// order), so records and counters are identical; only which lane runs which path when
-// changes.  The loop ends when every slot has run out of work items; each path is
-// bounded by kMaxStepsPerSample draws and maxCells cells.
+// trace_regroup_kernel: the syncDDA (-m 2) and N-DDA (-m 0) trackers, without shadow rays
+// or per-pixel statistics, with each warp's paths regrouped by their next operation.  A
+// warp keeps 64 path states in shared memory (structure of arrays), twice its lanes.
+// Each iteration it counts its slots per stage -- start a path, walk (cell and channel
+// transitions with free-flight draws, at most `trips` draws), evaluate a pending density
+// sample -- and runs the most populated stage with lane i on the i-th slot of that stage,
+// so at least 22 of its 32 lanes work on the same operation.  Warps run independently (no
+// block barrier).  Every path runs exactly the arithmetic of trace_items (the same
+// helpers, in the same order), so records, hit distances and counters are identical;
+// only which lane runs which path when changes.  The loop ends when every slot has run
+// out of work items; each path is bounded by kMaxStepsPerSample draws and maxCells cells
+// per traversal.
+//   -m 2: one traversal; `lim` is min(the cell's exit, the closest hit so far).
+//   -m 0: one traversal per channel (deviceCode.cu:965-969); `lim` is the closest hit so
+//   far (1e20 before the first), the cell's exit comes from the walk's DDA state.
 namespace rg {
 constexpr int kTPB = 256;
 constexpr int kSPT = 2;                  // path slots per thread
@@ -658,14 +689,17 @@ constexpr int kSlots = kTPB * kSPT;
 constexpr int kMinBlocks = 4;            // 64 registers, 32 warps per SM
 enum : uint32_t { NEED = 0, WALK = 1, SAMPLE = 2, DONE = 3 };
 // meta word: bits 0-1 stage, bit 2 a channel is selected (free flights pending), bit 3
-// the cell's channels are exhausted (advance the walk), bits 4-7 channel, bit 8 capped,
-// bits 9-20 the cell's non-zero-majorant channels, bits 21-31 cells entered
-constexpr uint32_t kDraw = 4u, kAdvance = 8u, kCapped = 256u;
+// the cell's channels are exhausted (advance the walk), bits 4-7 channel, bit 8 (-m 0)
+// start the next channel's traversal, bits 9-20 the cell's non-zero-majorant channels,
+// bits 21-31 cells entered by the current traversal
+constexpr uint32_t kDraw = 4u, kAdvance = 8u, kNewDda = 256u;
 struct Slots {
   uint32_t meta[kSlots], recIdx[kSlots], rng[kSlots], steps[kSlots], record[kSlots], cell[kSlots];
   float wdx[kSlots], wdy[kSlots], wdz[kSlots], t1w[kSlots], w2g[kSlots], g2w[kSlots];
   float tnx[kSlots], tny[kSlots], tnz[kSlots], tsx[kSlots], tsy[kSlots], tsz[kSlots];
   float rt0[kSlots], ncb[kSlots], maj[kSlots], rmaj[kSlots], t[kSlots], lim[kSlots];
+  float u[kSlots];    // the draw of the flight the sample stage completes
+  float xa[kSlots];   // -m 0: the exit distance of the cell that flight started in
 };
 __device__ __forceinline__ uint32_t pack_meta(uint32_t stage, uint32_t flags, int ch, uint32_t cmask, uint32_t visits) {
   return stage | flags | ((uint32_t)ch << 4) | ((cmask & 0xfffu) << 9) | (visits << 21);
@@ -677,23 +711,35 @@ __device__ __forceinline__ void load_dda(const Slots &S, unsigned s, DDA &d) {
   d.cx = (int)(c & 1023u); d.cy = (int)((c >> 10) & 1023u); d.cz = (int)(c >> 20);
   d.rt0 = S.rt0[s]; d.ncb = S.ncb[s];
 }
-// enter_cell of trace_items: the cell's exit distance, id and channel mask
-__device__ __forceinline__ int enter(const TrackParams &P, const DDA &d, float &ct1, uint32_t &cmask) {
-  const float tc = fminf(fminf(d.tnx, d.tny), d.tnz);
-  ct1 = d.rt0 + fminf(tc, 1e20f);
+__device__ __forceinline__ void store_dda(Slots &S, unsigned s, const DDA &d) {
+  S.tnx[s] = d.tnx; S.tny[s] = d.tny; S.tnz[s] = d.tnz;
+  S.cell[s] = (uint32_t)d.cx | ((uint32_t)d.cy << 10) | ((uint32_t)d.cz << 20);
+  S.ncb[s] = d.ncb;
+}
+// the exit distance of the DDA's current cell (cell_t1 of dda.h:164-170)
+__device__ __forceinline__ float cell_exit(const DDA &d) {
+  return d.rt0 + fminf(fminf(fminf(d.tnx, d.tny), d.tnz), 1e20f);
+}
+// enter_cell of trace_items: the cell's id and channel mask
+__device__ __forceinline__ int enter(const TrackParams &P, const DDA &d, uint32_t &cmask) {
   const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
   cmask = __ldg(P.mask + cellID);
   return cellID;
 }
+// End of a path: its record and, for features and gradient shading, the world distance
+// of its hit (0 for a miss); `lim` holds the grid distance of the recorded hit.
 __device__ __forceinline__ void finish(const TrackParams &P, Slots &S, unsigned s, uint32_t record, bool capped,
-                                       uint32_t (&tot)[5]) {
-  P.records[S.recIdx[s]] = capped ? 0u : record;
+                                       float lim, uint32_t (&tot)[5]) {
+  const uint32_t i = S.recIdx[s];
+  P.records[i] = capped ? 0u : record;
+  if (P.recT) P.recT[i] = record ? lim * S.g2w[s] : 0.f;
   tot[3]++;
   if (capped) tot[4]++;
   S.meta[s] = NEED;
 }
 
 // Start the path of work item `item` in slot s (the pooled start of trace_items).
+template <int MODE>
 __device__ __forceinline__ void start(const TrackParams &P, Slots &S, unsigned s, unsigned item, unsigned limit,
                                       uint32_t (&tot)[5]) {
   if (item >= limit) { S.meta[s] = DONE; return; }
@@ -718,37 +764,43 @@ __device__ __forceinline__ void start(const TrackParams &P, Slots &S, unsigned s
   const float t5 = (P.rootLo.z - P.camOrg.z) * frz, t6 = (P.rootHi.z - P.camOrg.z) * frz;
   const float th0 = fmaxf(fmaxf(fminf(t1, t2), fminf(t3, t4)), fminf(t5, t6));
   const float th1 = fminf(fminf(fmaxf(t1, t2), fmaxf(t3, t4)), fmaxf(t5, t6));
-  if (th1 < 0 || th0 >= th1) { finish(P, S, s, 0u, false, tot); return; }
+  if (th1 < 0 || th0 >= th1) { finish(P, S, s, 0u, false, 0.f, tot); return; }
   float gx, gy, gz, w2g, g2w;
   grid_dir(P, wdx, wdy, wdz, gx, gy, gz, w2g, g2w);
-  DDA d;
-  if (!dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) { finish(P, S, s, 0u, false, tot); return; }
-  float ct1;
-  uint32_t cmask;
-  enter(P, d, ct1, cmask);
-  tot[2]++;
   S.rng[s] = rng; S.steps[s] = 0u; S.record[s] = 0u;
   S.wdx[s] = wdx; S.wdy[s] = wdy; S.wdz[s] = wdz;
   S.t1w[s] = fminf(1e20f, th1); S.w2g[s] = w2g; S.g2w[s] = g2w;
-  S.tnx[s] = d.tnx; S.tny[s] = d.tny; S.tnz[s] = d.tnz;
+  if constexpr (MODE == 0) {   // the first channel's traversal starts in the walk
+    S.lim[s] = 1e20f;
+    S.meta[s] = pack_meta(WALK, kNewDda, 0, 0u, 0u);
+    return;
+  }
+  DDA d;
+  if (!dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) { finish(P, S, s, 0u, false, 0.f, tot); return; }
+  uint32_t cmask;
+  enter(P, d, cmask);
+  tot[2]++;
+  store_dda(S, s, d);
   S.tsx[s] = d.tsx; S.tsy[s] = d.tsy; S.tsz[s] = d.tsz;
-  S.cell[s] = (uint32_t)d.cx | ((uint32_t)d.cy << 10) | ((uint32_t)d.cz << 20);
-  S.rt0[s] = d.rt0; S.ncb[s] = d.ncb;
-  S.lim[s] = ct1;
+  S.rt0[s] = d.rt0;
+  S.lim[s] = cell_exit(d);
   S.meta[s] = pack_meta(WALK, 0u, 0, cmask, 1u);
 }
 
-// Walk: transitions to the next channel with a non-zero majorant, then free-flight draws,
-// until a tentative collision (-> SAMPLE), the end of the path, or `trips` draws.
+// Walk: transitions to the next channel (-m 2) or cell (-m 0) with a non-zero majorant,
+// then free-flight draws, until a tentative collision (-> SAMPLE), the end of the path,
+// or `trips` draws.
+template <int MODE>
 __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s, uint32_t maxCells,
                                      uint32_t (&tot)[5]) {
   const uint32_t m0 = S.meta[s];
-  bool drawing = (m0 & kDraw) != 0u, advance = (m0 & kAdvance) != 0u;
+  bool drawing = (m0 & kDraw) != 0u, advance = (m0 & kAdvance) != 0u, newdda = (m0 & kNewDda) != 0u;
   int ch = (int)((m0 >> 4) & 15u);
   uint32_t cmask = (m0 >> 9) & 0xfffu, visits = m0 >> 21;
   uint32_t record = S.record[s], steps = S.steps[s], rng = S.rng[s];
   float maj = S.maj[s], rmaj = S.rmaj[s], t = S.t[s], lim = S.lim[s];
   const float w2g = S.w2g[s];
+  const float kd = P.dt * w2g * kLn2;   // the exit filter's scale, times the majorant's reciprocal
   const float wdx = S.wdx[s], wdy = S.wdy[s], wdz = S.wdz[s];
   DDA d;
   load_dda(S, s, d);
@@ -759,70 +811,114 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     if (!drawing) {
       bool ended = false;
       while (true) {
-        if (advance) {
-          if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ended = true; break; }
-          float ct1;
-          enter(P, d, ct1, cmask);
-          d.visits++;
-          tot[2]++;
-          moved = true;
-          lim = ct1;
-          ch = 0;
-          advance = false;
-        }
-        const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
-        if (rem == 0u) {   // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
-          if (record) { ended = true; break; }
+        if constexpr (MODE == 0) {
+          if (newdda) {   // the next channel's traversal (deviceCode.cu:965-969)
+            if (ch >= P.C) { ended = true; break; }
+            float gx, gy, gz, a, b;
+            grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
+            if (!dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) { ch++; continue; }
+            enter(P, d, cmask);
+            d.visits = 1u;
+            tot[2]++;
+            moved = true;
+            newdda = false;
+            S.rt0[s] = d.rt0;   // the same for every channel's traversal of the ray
+            S.tsx[s] = d.tsx; S.tsy[s] = d.tsy; S.tsz[s] = d.tsz;
+          } else if (advance) {
+            advance = false;
+            if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; newdda = true; continue; }
+            enter(P, d, cmask);
+            d.visits++;
+            tot[2]++;
+            moved = true;
+          }
+          if ((cmask >> ch) & 1u) {   // zero-majorant cells are skipped (deviceCode.cu:893-894)
+            const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
+            maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
+            rmaj = __ldg(P.majRcp + (size_t)cellID * P.C + ch);
+            t = d.rt0 + d.ncb;   // the cell's entry distance
+            break;
+          }
           advance = true;
-          continue;
+        } else {
+          if (advance) {
+            if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ended = true; break; }
+            enter(P, d, cmask);
+            d.visits++;
+            tot[2]++;
+            moved = true;
+            lim = cell_exit(d);
+            ch = 0;
+            advance = false;
+          }
+          const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
+          if (rem == 0u) {   // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
+            if (record) { ended = true; break; }
+            advance = true;
+            continue;
+          }
+          ch += __ffs(rem) - 1;
+          const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
+          maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
+          rmaj = __ldg(P.majRcp + (size_t)cellID * P.C + ch);
+          t = d.rt0 + d.ncb;   // the cell's entry distance
+          break;
         }
-        ch += __ffs(rem) - 1;
-        const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-        maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
-        rmaj = __ldg(P.majRcp + (size_t)cellID * P.C + ch);
-        t = d.rt0 + d.ncb;   // the cell's entry distance
-        break;
       }
-      if (ended) { finish(P, S, s, record, false, tot); return; }
+      if (ended) { finish(P, S, s, record, false, lim, tot); return; }
       drawing = true;
     }
-    // free-flight draw (deviceCode.cu:800-820)
-    if (++steps >= kMaxStepsPerSample) { finish(P, S, s, record, true, tot); return; }
+    // free-flight draw (deviceCode.cu:800-820, 908-930).  A flight that certainly leaves
+    // the cell needs no exact length: the next channel or cell starts again from its
+    // entry distance.  The others -- the few that end inside the cell -- go to the sample
+    // stage, which computes the exact flight, its tests and the density sample together.
+    if (++steps >= kMaxStepsPerSample) { finish(P, S, s, record, true, lim, tot); return; }
     const float u = rng_next(rng);
-    t = flight(t, u, maj, rmaj, P.dt, w2g);
-    if (t >= lim) {
-      ch++;
-      drawing = false;
-    } else {
-      const float tW = t * S.g2w[s];
-      if (tW >= S.t1w[s]) {   // world exit
-        tot[1]++;
-        if (ch == P.C - 1) { finish(P, S, s, record, false, tot); return; }
-        ch++;
-        drawing = false;
-      } else {
-        stage = SAMPLE;
-        break;
-      }
+    const float exitAt = MODE == 0 ? cell_exit(d) : lim;
+    if (!flight_surely_exits(t, u, rmaj * kd, exitAt)) {
+      S.u[s] = u;
+      if (MODE == 0) S.xa[s] = exitAt;
+      stage = SAMPLE;
+      break;
     }
+    if (MODE == 0) advance = true;
+    else ch++;
+    drawing = false;
     if (++k >= P.trips) break;
   }
-  S.meta[s] = pack_meta(stage, (drawing ? kDraw : 0u) | (advance ? kAdvance : 0u), ch, cmask, d.visits);
+  S.meta[s] = pack_meta(stage, (drawing ? kDraw : 0u) | (advance ? kAdvance : 0u) | (newdda ? kNewDda : 0u), ch,
+                        cmask, d.visits);
   S.steps[s] = steps; S.rng[s] = rng; S.maj[s] = maj; S.rmaj[s] = rmaj; S.t[s] = t; S.lim[s] = lim;
-  if (moved) {
-    S.tnx[s] = d.tnx; S.tny[s] = d.tny; S.tnz[s] = d.tnz;
-    S.cell[s] = (uint32_t)d.cx | ((uint32_t)d.cy << 10) | ((uint32_t)d.cz << 20);
-    S.ncb[s] = d.ncb;
-  }
+  if (moved) store_dda(S, s, d);
 }
 
-// The pending density sample of slot s (phase 2 of trace_items, -m 2).
-template <int SK>
+// The pending flight of slot s, then its density sample (phase 2 of trace_items, -m 2
+// and -m 0): the exact free flight from the walk's draw and its tests (cell exit, -m 0's
+// closest hit, world exit, deviceCode.cu:805-821, 915-931), then the collision test.
+template <int MODE, int SK>
 __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const ChanSm *sch, unsigned s,
                                        uint32_t (&tot)[5]) {
   const uint32_t m0 = S.meta[s];
   const int ch = (int)((m0 >> 4) & 15u);
-  const float tW = S.t[s] * S.g2w[s];
+  const float lim = S.lim[s];
+  const float t = flight(S.t[s], S.u[s], S.maj[s], S.rmaj[s], P.dt, S.w2g[s]);
+  S.t[s] = t;
+  const uint32_t keep = m0 & ~(0xfu | kNewDda);   // channel, cell channels and cells entered
+  if (t >= (MODE == 0 ? S.xa[s] : lim)) {   // leaves the cell after all
+    S.meta[s] = MODE == 0 ? (keep | WALK | kAdvance) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
+    return;
+  }
+  if (MODE == 0 && lim < t) {   // beyond the closest hit so far: the next channel's traversal
+    S.meta[s] = pack_meta(WALK, kNewDda, ch + 1, 0u, 0u);
+    return;
+  }
+  const float tW = t * S.g2w[s];
+  if (tW >= S.t1w[s]) {   // world exit
+    tot[1]++;
+    if (MODE == 2 && ch == P.C - 1) { finish(P, S, s, S.record[s], false, lim, tot); return; }
+    S.meta[s] = MODE == 0 ? pack_meta(WALK, kNewDda, ch + 1, 0u, 0u) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
+    return;
+  }
   const float xs = fmaf(tW, S.wdx[s], P.camOrg.x) * P.w2u.x;
   const float ys = fmaf(tW, S.wdy[s], P.camOrg.y) * P.w2u.y;
   const float zs = fmaf(tW, S.wdz[s], P.camOrg.z) * P.w2u.z;
@@ -831,17 +927,23 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
   const ChanSm &cs = sch[ch];
   const float v = sample_volume<SK>(P, cs, xs, ys, zs);
   tot[0]++;
+  uint32_t next = (m0 & ~3u) | WALK | kDraw;
   if (v == v) {
     Axis tax;
     const float a = tf_alpha(cs, v, tax);
     if (a > 0.0f && thr < a) {
       S.record[s] = make_record(ch, tax);
-      S.lim[s] = fminf(S.t[s], S.lim[s]);
+      S.lim[s] = fminf(t, lim);
+      if (MODE == 0) {   // the channel's traversal ends at its hit; the next channel's starts
+        next = pack_meta(WALK, kNewDda, ch + 1, 0u, 0u);
+      }
+    } else if (MODE == 0) {
+      tot[1]++;
     }
   }
-  tot[1]++;   // -m 2 counts every sample as a rejection, hits included (deviceCode.cu:836-846)
+  if (MODE == 2) tot[1]++;   // -m 2 counts every sample as a rejection, hits included (deviceCode.cu:836-846)
   S.rng[s] = rng;
-  S.meta[s] = (m0 & ~3u) | WALK | kDraw;
+  S.meta[s] = next;
 }
 }  // namespace rg
 
@@ -849,7 +951,7 @@ namespace rg {
 // One warp's regrouped tracking loop over the work items [0, limit) of request P, drawn
 // from `dispenser`: its 64 slots start empty and the loop ends when each has run out of
 // items.  sel is the warp's 32-entry lane table in shared memory.
-template <int SK>
+template <int MODE, int SK>
 __device__ __forceinline__ void run_warp(const TrackParams &P, Slots &S, uint16_t *sel, unsigned wbase, unsigned lane,
                                          const ChanSm *sch, unsigned *dispenser, unsigned limit, uint32_t (&tot)[5]) {
   const uint32_t maxCells = P.mc[0] + P.mc[1] + P.mc[2] + 3u;
@@ -890,21 +992,21 @@ __device__ __forceinline__ void run_warp(const TrackParams &P, Slots &S, uint16_
     __syncwarp();
     const unsigned s = mine ? (unsigned)sel[lane] : 0u;
     if (X == SAMPLE) {
-      if (mine) sample<SK>(P, S, sch, s, tot);
+      if (mine) sample<MODE, SK>(P, S, sch, s, tot);
     } else if (X == WALK) {
-      if (mine) walk(P, S, s, maxCells, tot);
+      if (mine) walk<MODE>(P, S, s, maxCells, tot);
     } else {
       unsigned base = 0;
       if (lane == 0) base = atomicAdd(dispenser, (unsigned)nx);
       base = __shfl_sync(kFull, base, 0);
-      if (mine) start(P, S, s, base + lane, limit, tot);
+      if (mine) start<MODE>(P, S, s, base + lane, limit, tot);
     }
     __syncwarp();
   }
 }
 }  // namespace rg
 
-template <int SK>
+template <int MODE, int SK>
 __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel(const __grid_constant__ TrackParams P) {
   extern __shared__ __align__(16) unsigned char rgSmem[];
   rg::Slots &S = *reinterpret_cast<rg::Slots *>(rgSmem);
@@ -915,15 +1017,15 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks) trace_regroup_kernel
   if (tid < (unsigned)P.C) sch[tid] = chan_params(P, (int)tid);
   __syncthreads();   // the channel table
   uint32_t tot[5] = {0, 0, 0, 0, 0};
-  rg::run_warp<SK>(P, S, selAll + (tid & ~31u), wbase, lane, sch, P.workCounter,
-                   (unsigned)P.numTiles * 32u * (unsigned)P.sCount, tot);
+  rg::run_warp<MODE, SK>(P, S, selAll + (tid & ~31u), wbase, lane, sch, P.workCounter,
+                         (unsigned)P.numTiles * 32u * (unsigned)P.sCount, tot);
   flush_counters(P.counters, tot);
 }
 
 // Batched variant of the regrouped tracker: a warp takes the requests in turn, as
 // trace_batch_kernel does, and runs the regrouped loop on each with that request's
 // dispenser and channel table.
-template <int SK>
+template <int MODE, int SK>
 __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks)
     trace_batch_regroup_kernel(const TrackParams *__restrict__ reqs, int nReq, unsigned *dispensers) {
   extern __shared__ __align__(16) unsigned char rgSmem[];
@@ -944,12 +1046,11 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks)
     if (lane < (unsigned)P.C) sch[warp][lane] = chan_params(P, (int)lane);
     __syncwarp();
     uint32_t tot[5] = {0, 0, 0, 0, 0};
-    rg::run_warp<SK>(P, S, selAll + warp * 32u, wbase, lane, sch[warp], dispensers + r, total, tot);
+    rg::run_warp<MODE, SK>(P, S, selAll + warp * 32u, wbase, lane, sch[warp], dispensers + r, total, tot);
     flush_counters(P.counters, tot);
     __syncwarp();
   }
 }
-
 // Batched variant: many requests (render contexts) in one persistent launch.  Every
 // request has its own work dispenser; a warp starts at request (global warp id mod nReq),
 // takes chunks of that request's items until they run out, then moves on to the next
@@ -1320,17 +1421,17 @@ int launch_resolve(const TrackParams &p, cudaStream_t st, int numSMs) {
   return (int)cudaGetLastError();
 }
 
-template <int SK>
+template <int MODE, int SK>
 int launch_regroup(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
   const int smem = (int)sizeof(rg::Slots);
-  cudaError_t e = cudaFuncSetAttribute(trace_regroup_kernel<SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(trace_regroup_kernel<MODE, SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return (int)e;
   int bps = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_regroup_kernel<SK>, rg::kTPB, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_regroup_kernel<MODE, SK>, rg::kTPB, smem);
   if (e != cudaSuccess) return (int)e;
   if (bps < 1) bps = 1;
   *grid = numSMs * bps;
-  if (p.numTiles > 0) trace_regroup_kernel<SK><<<*grid, rg::kTPB, smem, st>>>(p);
+  if (p.numTiles > 0) trace_regroup_kernel<MODE, SK><<<*grid, rg::kTPB, smem, st>>>(p);
   if (evMid) cudaEventRecord((cudaEvent_t)evMid, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
@@ -1339,8 +1440,8 @@ int launch_regroup(const TrackParams &p, cudaStream_t st, int numSMs, int *grid,
 
 template <int MODE, int SK, bool STATS, bool SH>
 int launch_t(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
-  if constexpr (MODE == 2 && !STATS && !SH) {
-    if (regroup_fits(p)) return launch_regroup<SK>(p, st, numSMs, grid, evMid);
+  if constexpr ((MODE == 2 || MODE == 0) && !STATS) {
+    if (!p.shadows && regroup_fits(p)) return launch_regroup<MODE, SK>(p, st, numSMs, grid, evMid);
   }
   int bps = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_kernel<MODE, SK, STATS, SH>, kTPB, 0);
@@ -1384,17 +1485,17 @@ int launch_tb(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
   return (int)cudaGetLastError();
 }
 
-template <int SK>
+template <int MODE, int SK>
 int launch_tb_regroup(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
   const int smem = (int)sizeof(rg::Slots);
-  cudaError_t e = cudaFuncSetAttribute(trace_batch_regroup_kernel<SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(trace_batch_regroup_kernel<MODE, SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return (int)e;
   int bps = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_regroup_kernel<SK>, rg::kTPB, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_regroup_kernel<MODE, SK>, rg::kTPB, smem);
   if (e != cudaSuccess) return (int)e;
   if (bps < 1) bps = 1;
   *grid = numSMs * bps;
-  if (g.totalItems > 0) trace_batch_regroup_kernel<SK><<<*grid, rg::kTPB, smem, st>>>(g.reqs, g.nReq, g.dispensers);
+  if (g.totalItems > 0) trace_batch_regroup_kernel<MODE, SK><<<*grid, rg::kTPB, smem, st>>>(g.reqs, g.nReq, g.dispensers);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   size_t rg = (size_t)((g.totalPix + 255) / 256);
@@ -1406,8 +1507,8 @@ int launch_tb_regroup(const BatchGroup &g, cudaStream_t st, int numSMs, int *gri
 
 template <int MODE, int SK>
 int launch_tbs(const BatchGroup &g, cudaStream_t st, int numSMs, int *grid) {
-  if constexpr (MODE == 2) {
-    if (g.regroup && !g.stats && !g.ext) return launch_tb_regroup<SK>(g, st, numSMs, grid);
+  if constexpr (MODE == 2 || MODE == 0) {
+    if (g.regroup && !g.stats && !g.ext) return launch_tb_regroup<MODE, SK>(g, st, numSMs, grid);
   }
   if (g.ext) return g.stats ? launch_tb<MODE, SK, true, true>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, true>(g, st, numSMs, grid);
   return g.stats ? launch_tb<MODE, SK, true, false>(g, st, numSMs, grid) : launch_tb<MODE, SK, false, false>(g, st, numSMs, grid);
@@ -1430,7 +1531,7 @@ int occ_tbs(bool stats, bool ext) {
 // entered, 32-bit record indices.
 bool regroup_fits(const TrackParams &p) {
   const size_t nrect = (size_t)(p.cullX1 - p.cullX0 + 1) * (size_t)(p.cullY1 - p.cullY0 + 1);
-  return p.mode == 2 && p.regroup && p.mc[0] <= 1024u && p.mc[1] <= 1024u && p.mc[2] <= 1024u &&
+  return (p.mode == 2 || p.mode == 0) && p.regroup && p.mc[0] <= 1024u && p.mc[1] <= 1024u && p.mc[2] <= 1024u &&
          p.mc[0] + p.mc[1] + p.mc[2] + 3u <= 2047u && nrect * (size_t)p.sCount < ((size_t)1 << 32);
 }
 
@@ -1479,9 +1580,47 @@ int launch_track(const TrackParams &p, int storeKind, void *stream, int numSMs, 
     case 5: rc = u8 ? launch_s<4, kStoreU8>(p, st, numSMs, grid, evMid) : launch_s<4, kStoreF32>(p, st, numSMs, grid, evMid); break;
     default: return (int)cudaErrorInvalidValue;
   }
-  *block = (regroup_fits(p) && !p.stats && !p.shadows && !p.recT) ? rg::kTPB : kTPB;
+  *block = (regroup_fits(p) && !p.stats && !p.shadows) ? rg::kTPB : kTPB;
   if (launches) *launches += p.numTiles > 0 ? 2 : 1;
   return rc;
 }
 
 }  // namespace mdwt
+
+// ------------------------------------------------------------------ exit-filter premise
+namespace mdwt {
+namespace {
+// The largest |lg2.approx(x) - log2(x)| / (1 + |log2 x|) over every argument a free
+// flight takes, x = 1 - k 2^-24 for k < 2^24, against the double-precision log2.
+__global__ void flight_log2_bound_kernel(unsigned *worst) {
+  float w = 0.f;
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < (1u << 24); k += gridDim.x * blockDim.x) {
+    const float x = 1.0f - (float)k * (1.0f / 16777216.0f);
+    const double e = log2((double)x);
+    const double g = (double)__log2f(x);
+    w = fmaxf(w, (float)(fabs(g - e) / (1.0 + fabs(e))));
+  }
+  for (int o = 16; o > 0; o >>= 1) w = fmaxf(w, __shfl_xor_sync(kFull, w, o));
+  if ((threadIdx.x & 31u) == 0) atomicMax(worst, __float_as_uint(w));   // w >= 0: bit order is value order
+}
+}  // namespace
+}  // namespace mdwt
+
+// Checks the premise of the trackers' free-flight exit filter on this device: writes the
+// largest relative error of the hardware log2 over the 2^24 flight arguments.
+extern "C" mdwt_status mdwt_check_flight_filter(float *worst_out) {
+  if (!worst_out) return MDWT_ERR_BAD_ARG;
+  unsigned *d = nullptr;
+  if (cudaMalloc(&d, sizeof(unsigned)) != cudaSuccess) { cudaGetLastError(); return MDWT_ERR_CUDA; }
+  unsigned h = 0;
+  cudaError_t e = cudaMemset(d, 0, sizeof(unsigned));
+  if (e == cudaSuccess) {
+    mdwt::flight_log2_bound_kernel<<<1184, 256>>>(d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return MDWT_ERR_CUDA;
+  std::memcpy(worst_out, &h, sizeof(float));
+  return MDWT_OK;
+}

@@ -176,8 +176,10 @@ static inline Axis axis(float u, int n) {
 // ---------------------------------------------------------------- scene state
 struct Channel {
   int64_t dims[3];
-  std::vector<float> data;   // converted to float exactly like RawR (rawFile.cpp:98-121)
-  float lo[4], hi[4];        // box4f bounds_ = {{0,0,0,0},{1,1,1,1}} (rawFile.h:162)
+  std::vector<float> data;     // converted to float exactly like RawR (rawFile.cpp:98-121)
+  std::vector<uint8_t> bytes;  // uint8 channels: the bytes, value = byte * 255 (exact in float)
+  float lo[4], hi[4];          // box4f bounds_ = {{0,0,0,0},{1,1,1,1}} (rawFile.h:162)
+  float at(size_t i) const { return bytes.empty() ? data[i] : (float)bytes[i] * 255; }
 };
 
 struct TFData {
@@ -290,9 +292,18 @@ static int fmt_bytes(int f) {
 }
 
 static void convert(Channel &c, const void *buf, int fmt, size_t n) {
-  c.data.resize(n);
   c.lo[0] = c.lo[1] = c.lo[2] = c.lo[3] = 0.f;
   c.hi[0] = c.hi[1] = c.hi[2] = c.hi[3] = 1.f;
+  if (fmt == 4) {  // uint8 kept as bytes (a quarter of the memory); the values are the same
+    c.bytes.assign((const uint8_t *)buf, (const uint8_t *)buf + n);
+    for (size_t i = 0; i < n; i++) {
+      const float v = (float)c.bytes[i] * 255;
+      if (v > c.hi[3]) c.hi[3] = v;
+      if (v < c.lo[3]) c.lo[3] = v;
+    }
+    return;
+  }
+  c.data.resize(n);
   for (size_t i = 0; i < n; i++) {
     float v = 0.f;
     switch (fmt) {
@@ -372,7 +383,7 @@ static void build_ranges(Oracle &o) {
           for (int64_t x = 0; x < X; x++) {
             // renderer.cu:835-893, one voxel
             const int64_t p[3] = {x, y, z};
-            const float s = chn.data[(size_t)((z * Y + y) * X + x)];
+            const float s = chn.at((size_t)((z * Y + y) * X + x));
             float blo[4], bhi[4];
             for (int a = 0; a < 3; a++) {
               blo[a] = std::fma((float)p[a], len[a], wlo[a]);
@@ -386,7 +397,7 @@ static void build_ranges(Oracle &o) {
                   if (n[0] < 0 || n[0] >= X || n[1] < 0 || n[1] >= Y || n[2] < 0 || n[2] >= Z) continue;
                   float pt[4];
                   for (int a = 0; a < 3; a++) pt[a] = std::fma((float)n[a], len[a], wlo[a]);
-                  pt[3] = chn.data[(size_t)((n[2] * Y + n[1]) * X + n[0])];
+                  pt[3] = chn.at((size_t)((n[2] * Y + n[1]) * X + n[0]));
                   for (int a = 0; a < 4; a++) { blo[a] = std::fmin(blo[a], pt[a]); bhi[a] = std::fmax(bhi[a], pt[a]); }
                 }
             // rasterBox(float2*) renderer.cu:487-519
@@ -508,7 +519,7 @@ static inline float sample_volume(const Oracle &o, int c, V3 p) {
   const Channel &h = o.ch[c];
   const int X = (int)h.dims[0], Y = (int)h.dims[1], Z = (int)h.dims[2];
   Axis ax = axis(p.x, X), ay = axis(p.y, Y), az = axis(p.z, Z);
-  auto at = [&](int x, int y, int z) { return h.data[((size_t)z * Y + y) * X + x]; };
+  auto at = [&](int x, int y, int z) { return h.at(((size_t)z * Y + y) * X + x); };
   float c00 = lerpf(ax.a, at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0));
   float c10 = lerpf(ax.a, at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0));
   float c01 = lerpf(ax.a, at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1));
@@ -1102,7 +1113,7 @@ static double volume_d(const Oracle &o, int c, const double p[3]) {
   const Channel &h = o.ch[c];
   const int X = (int)h.dims[0], Y = (int)h.dims[1], Z = (int)h.dims[2];
   const AxisD ax = axis_d(p[0], X), ay = axis_d(p[1], Y), az = axis_d(p[2], Z);
-  auto at = [&](int x, int y, int z) { return (double)h.data[((size_t)z * Y + y) * X + x]; };
+  auto at = [&](int x, int y, int z) { return (double)h.at(((size_t)z * Y + y) * X + x); };
   const double c00 = lerp_d(ax.a, at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0));
   const double c10 = lerp_d(ax.a, at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0));
   const double c01 = lerp_d(ax.a, at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1));
@@ -1529,7 +1540,9 @@ int orc_num_channels(Oracle *o, int *n) { *n = (int)o->ch.size(); return ORC_OK;
 // The converted float values of channel c (RawR::getDataVector, rawFile.cpp:201-204).
 int orc_get_channel_data(Oracle *o, int c, float *out) {
   if (c < 0 || c >= (int)o->ch.size()) return ORC_BAD;
-  std::memcpy(out, o->ch[c].data.data(), o->ch[c].data.size() * sizeof(float));
+  const Channel &h = o->ch[c];
+  const size_t n = (size_t)(h.dims[0] * h.dims[1] * h.dims[2]);
+  for (size_t i = 0; i < n; i++) out[i] = h.at(i);
   return ORC_OK;
 }
 // The oracle's dda3 over a grid of gs cells: the cells visited and their (t0, t1), at
@@ -1548,6 +1561,25 @@ int orc_dda_trace(const float org[3], const float dir[3], float tMax, const uint
 
 // Test hooks: the primitives of the arithmetic specification.
 float orc_log(float x) { return mlog(x); }
+// The largest relative error of mlog against a double-precision log over every argument
+// a free flight takes, 1 - k 2^-24 for k < 2^24 (the premise of the tracker kernels'
+// exit filter, which bounds it by 2^-18); also counts k where mlog increases with k.
+double orc_flight_log_bound(uint64_t *nonmonotone) {
+  double worst = 0.0;
+  uint64_t up = 0;
+  float prev = 1.0f;
+  for (uint32_t k = 0; k < (1u << 24); k++) {
+    const float x = 1.0f - (float)k * (1.0f / 16777216.0f);
+    const float L = mlog(x);
+    const double e = std::log((double)x);
+    if (e != 0.0) worst = std::max(worst, std::fabs((double)L - e) / std::fabs(e));
+    else if (L != 0.0f) worst = INFINITY;
+    if (k > 0 && L > prev) up++;
+    prev = L;
+  }
+  if (nonmonotone) *nonmonotone = up;
+  return worst;
+}
 // Published-algorithm checks: TEA with an arbitrary key and round count (32 rounds is
 // the cipher of Wheeler & Needham), and the raw LCG state sequence.
 void orc_tea(uint32_t v0, uint32_t v1, const uint32_t k[4], int rounds, uint32_t out[2]) {

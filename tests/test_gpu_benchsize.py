@@ -3,8 +3,8 @@
 Each case sets up the configured scene at its full size in both renderers, renders
 whole frames on the GPU and a set of rows spread over the frame in the oracle, and
 compares those rows bit for bit: the accumulation buffer (float4) and the RGBA8
-framebuffer.  With per-pixel statistics off, syncDDA frames run the regrouped tracker
-(trace_regroup_kernel, launched as 256-thread blocks) -- the kernel `bench.py` times; a
+framebuffer.  With per-pixel statistics off, syncDDA and N-DDA frames run the regrouped
+tracker (trace_regroup_kernel, launched as 256-thread blocks) -- the kernel `bench.py` times; a
 second frame with statistics on runs the warp-local tracker and also compares the
 per-pixel event counts (density samples, rejections, hits, hit channels).  The
 per-pixel loop both follow is the reference's mainRG and its closest-hit trackers
@@ -111,7 +111,7 @@ def test_c3_full_size(orc, c3_scenes, mode):
     o = sc.setup(orc.OracleRenderer())
     np.testing.assert_array_equal(p.ranges(), o.ranges())
     np.testing.assert_array_equal(p.majorants(), o.majorants())
-    regrouped_then_warp_local(p, o, sc.spp, 72, f"c3 -m {mode}", expect_regroup=(mode == 2))
+    regrouped_then_warp_local(p, o, sc.spp, 72, f"c3 -m {mode}")
     p.close()
 
 
