@@ -13,9 +13,13 @@ quoted on.  Inputs (volumes, majorants) are resident in HBM before timing; L2 is
 by a 512 MiB write between timed steps, outside the timed events (the 3.2 GB volume is
 larger than L2 in any case).  `value` is device time (CUDA events on the render stream);
 `e2e` goes through the C ABI with host buffers: camera update (host to device), frame,
-framebuffer copy to pinned host memory.  Under torchrun every rank renders its own frames
-(different frame seeds) with no collective: per-GPU work is fixed, `scaling` is weak,
-and time is the max over ranks.  Before timing, the tracker schedule is tuned for the
+framebuffer copy to pinned host memory.  Under torchrun (--split rows, the default) the
+ranks render ONE frame together: each renders a band of rows (mdwtracker_b200.multigpu.
+BandRenderer; the bands are re-cut from measured render times during the warm-up so that
+each carries an equal share of the work) and the RGBA8 bands are all-gathered over NCCL
+inside the timed region -- total work is fixed, `scaling` is strong, time is the max over
+ranks.  --split replicas: every rank renders its own whole frames (different frame
+seeds) with no collective (`scaling` weak).  Before timing, the tracker schedule is tuned for the
 workload (mdwt_autotune_schedule on launches of the step's shape; --no-autotune keeps
 the defaults) and reported in config.schedule.
 
@@ -65,6 +69,8 @@ def parse_args():
     ap.add_argument("--no-sweep", action="store_true", help="skip the c3 macrocell-edge sweep")
     ap.add_argument("--no-c2", action="store_true", help="skip the extra c2 line")
     ap.add_argument("--impl", default="mdwt", choices=["mdwt", "reference"])
+    ap.add_argument("--split", default="rows", choices=["rows", "replicas"],
+                    help="N > 1: one frame in row bands over the ranks (gathered), or whole frames per rank")
     ap.add_argument("--flush-mib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -463,8 +469,8 @@ def run_reference(args):
         "impl": "reference",
         "metric": "Gpath-samples/s", "value": value, "unit": "Gpath-samples/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded)",
+        "higher_is_better": True, "scaling": "strong" if args.split == "rows" else "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded)",
         "config": scene_config(sc, "host caches", "host threads"),
         "cpu_baseline": {"value": value, "unit": "Gpath-samples/s", "cores": threads, "kind": "port",
                          "sample": f"each step: {rows} rows spread over the {w}x{h} frame (every {stride}th "
@@ -543,6 +549,57 @@ def timed_frames(r, sc, steps, warmup, flush, stream, barrier=lambda: None, cloc
     step_ms = [a.elapsed_time(b) for a, b in ev]
     return {"step_ms": step_ms, "trace_ms": trace_ms, "counters": r.counters(),
             "launches": r.renderInfo()[0] - launches0, "tracker": tracker, "clocks": clk, "step": step}
+
+
+def timed_split_frames(br, sc, steps, warmup, flush, stream, barrier, clocks=None):
+    """One frame across the ranks: each renders its row band, then the RGBA8 bands are
+    all-gathered (NCCL) -- both inside the CUDA events of a step.  The warm-up frames
+    re-cut the bands from each rank's measured band time (BandRenderer.rebalance)."""
+    import torch
+    sptr = stream.cuda_stream
+    r = br.r
+    bands_seen = []
+    for _ in range(warmup):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            br.render(sptr)
+            e1.record(stream)
+            br.gather_framebuffer(sptr)
+        torch.cuda.synchronize()
+        bands_seen.append(br.rebalance(e0.elapsed_time(e1) / 1e3))
+    torch.cuda.synchronize()
+    r.resetCounters()
+    timed = True
+    try:
+        r.setTiming(True)
+    except Exception:
+        timed = False
+    launches0 = r.renderInfo()[0]
+    tracker = "trace_regroup_kernel" if r.renderInfo()[3] == 256 else "trace_kernel"
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.mark()
+    trace_ms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(stream)
+            br.render(sptr)
+            br.gather_framebuffer(sptr)
+            ev[k][1].record(stream)
+            if timed:
+                trace_ms.append(r.kernelTimes()[0])
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop() if clocks is not None else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    return {"step_ms": step_ms, "trace_ms": trace_ms, "counters": r.counters(),
+            "launches": r.renderInfo()[0] - launches0, "tracker": tracker, "clocks": clk,
+            "bands": br.bands, "bands_warmup": bands_seen}
 
 
 def throughput_summary(sc, t, peak):
@@ -644,9 +701,15 @@ def main():
         else:
             r.Render(sptr)
 
-    # distinct frame seeds per rank: rank r starts r*(warmup+steps) frames later
-    for _ in range(rank * (args.warmup + args.steps)):
-        step()
+    split = world > 1 and args.split == "rows" and sc.frames == 1
+    br = None
+    if split:
+        from mdwtracker_b200.multigpu import BandRenderer
+        br = BandRenderer(r)
+    else:
+        # distinct frame seeds per rank: rank r starts r*(warmup+steps) frames later
+        for _ in range(rank * (args.warmup + args.steps)):
+            step()
     torch.cuda.synchronize(dev)
 
     def barrier():
@@ -657,7 +720,10 @@ def main():
     # region); only the samples written after mark() are counted
     clocks = ClockSampler(torch.cuda.get_device_properties(dev).uuid and f"GPU-{torch.cuda.get_device_properties(dev).uuid}")
     clocks.start()
-    t = timed_frames(r, sc, args.steps, args.warmup, flush, stream, barrier, clocks)
+    if split:
+        t = timed_split_frames(br, sc, args.steps, args.warmup, flush, stream, barrier, clocks)
+    else:
+        t = timed_frames(r, sc, args.steps, args.warmup, flush, stream, barrier, clocks)
     clk = t["clocks"]
     step_ms = t["step_ms"]
     cnt = t["counters"]
@@ -667,12 +733,16 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     paths = w * h * sc.spp * sc.frames
-    value = world * paths / (ms / 1e3) / 1e9
+    value = (1 if split else world) * paths / (ms / 1e3) / 1e9
 
     steps = args.steps
     alg_bytes = algorithmic_bytes(sc, cnt) / steps
     kernel_ms = statistics.mean(t["trace_ms"]) if t["trace_ms"] else statistics.mean(step_ms)
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    if world > 1:   # the mean over the ranks of each one's achieved GB/s
+        tt = torch.tensor([achieved], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt)
+        achieved = float(tt.item()) / world
     peak, peak_kind = measured_peak_hbm()
     tracker = t["tracker"]
 
@@ -686,8 +756,15 @@ def main():
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         r.setCamera(*cam)
-        step()
-        r._call("get_framebuffer", C.cast(C.c_void_p(pinned.data_ptr()), C.POINTER(C.c_uint32)))
+        if split:   # this rank's band, the gathered frame, to pinned host memory
+            br.render(sptr)
+            with torch.cuda.stream(stream):
+                fb = br.gather_framebuffer(sptr)
+                pinned.copy_(fb.reshape(-1), non_blocking=True)
+            stream.synchronize()
+        else:
+            step()
+            r._call("get_framebuffer", C.cast(C.c_void_p(pinned.data_ptr()), C.POINTER(C.c_uint32)))
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     barrier()
     e2e = statistics.mean(e2e_ms)
@@ -743,18 +820,19 @@ def main():
         "warmup": args.warmup,
         "ms_per_step": ms,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if (split or (world == 1 and args.split == "rows")) else "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded generators in mdwtracker_b200/synthetic.py)",
-        "config": dict(scene_config(sc, l2note, f"replicas x{world}" if world > 1 else "single GPU"),
+        "config": dict(scene_config(sc, l2note, (f"row bands x{world}, NCCL all_gather of the RGBA8 frame" if split
+                                                 else f"replicas x{world}") if world > 1 else "single GPU"),
                        schedule=schedule),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profiled_traffic(tracker, workload_name(sc)),
                      "peak_source": peak_kind, "kernel": tracker,
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": alg_bytes},
         "cpu_baseline": cpu,
-        "e2e": {"value": world * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",
+        "e2e": {"value": (1 if split else world) * paths / (e2e / 1e3) / 1e9, "unit": "Gpath-samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": w * h * 4, "ms_per_step": e2e},
         "time_to_rmse": ttr,
         "batch": batch,
@@ -764,6 +842,8 @@ def main():
                      "path_samples": int(cnt[3]), "samples_per_path": float(cnt[0]) / max(1, int(cnt[3]))},
         "step_ms": step_ms,
     }
+    if split:
+        line["config"]["bands"] = [list(b) for b in t["bands"]]
     line.update(extras)
     if rank == 0:
         print(json.dumps(line))

@@ -28,7 +28,7 @@ def test_reference_arm_prints_the_contract_line():
     assert len(lines) == 1
     line = lines[0]
     assert line["impl"] == "reference" and line["metric"] == "Gpath-samples/s" and line["unit"] == "Gpath-samples/s"
-    assert line["value"] > 0 and line["higher_is_better"] is True and line["scaling"] == "weak"
+    assert line["value"] > 0 and line["higher_is_better"] is True and line["scaling"] == "strong"
     assert line["n_gpus"] == 1 and line["steps"] == 1 and line["warmup"] == 1 and line["vs_baseline"] is None
     assert line["config"]["workload"].startswith("c1_")
     cb = line["cpu_baseline"]
@@ -45,7 +45,7 @@ def test_defaults(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse_args()
     assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1 and a.config == "c3" and a.edge == 16 and a.impl == "mdwt"
-    assert not a.no_autotune and a.regroup is None
+    assert not a.no_autotune and a.regroup is None and a.split == "rows"
 
 
 def test_schedule_report_reads_the_knobs():

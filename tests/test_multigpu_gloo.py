@@ -1,6 +1,7 @@
 """The multi-process row split (mdwtracker_b200.multigpu) on CPU: two gloo ranks each render
 a band of every frame with the oracle and gather the bands; the assembled frames must
-equal a single-process render bit for bit."""
+equal a single-process render bit for bit, also when the bands are re-cut between frames
+from measured render times."""
 import os
 import tempfile
 
@@ -8,7 +9,7 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
-from mdwtracker_b200.multigpu import band
+from mdwtracker_b200.multigpu import band, split_by_cost
 
 
 def test_band_partition():
@@ -20,6 +21,35 @@ def test_band_partition():
                 assert b == c
             sizes = [b - a for a, b in bands]
             assert max(sizes) - min(sizes) <= 1
+
+
+def test_split_by_cost_balances_and_covers():
+    rng = np.random.default_rng(3)
+    for H in (8, 37, 1080):
+        for world in (1, 2, 3, 8):
+            for cost in (np.ones(H), rng.random(H) ** 4, np.r_[np.zeros(H // 2), np.ones(H - H // 2)]):
+                bands = split_by_cost(cost, world)
+                assert len(bands) == world and bands[0][0] == 0 and bands[-1][1] == H
+                for (a, b), (c, d) in zip(bands, bands[1:]):
+                    assert b == c and a <= b
+                for a, b in bands:
+                    assert b - a >= (4 if H >= 4 * world else 0)
+                for a, b in bands[:-1]:
+                    assert b % 4 == 0 or H < 4 * world
+                share = [cost[a:b].sum() for a, b in bands]
+                # each share is within one 4-row alignment step (either side) of the mean
+                if H >= 16 * world:
+                    step = 8 * float(cost.max())
+                    assert max(share) <= cost.sum() / world + step + 1e-9
+
+
+def test_split_follows_a_centre_heavy_cost():
+    H = 1080
+    y = np.arange(H)
+    cost = np.exp(-((y - H / 2) / (H / 8)) ** 2) + 1e-3
+    bands = split_by_cost(cost, 4)
+    sizes = [b - a for a, b in bands]
+    assert sizes[0] > 2 * sizes[1] and sizes[3] > 2 * sizes[2]   # wide outer bands, narrow centre bands
 
 
 def _scene():
@@ -43,7 +73,7 @@ def _setup(r, vols, tfs, res):
     return r
 
 
-def _worker(rank, world, port, out_dir, frames, res):
+def _worker(rank, world, port, out_dir, frames, res, rebalance=False):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -53,25 +83,33 @@ def _worker(rank, world, port, out_dir, frames, res):
     set_threads(1)
     vols, tfs = _scene()
     br = BandRenderer(_setup(OracleRenderer(), vols, tfs, res))
-    accs, fbs = [], []
+    accs, fbs, bands = [], [], []
+    import time
     for _ in range(frames):
+        t0 = time.perf_counter()
         br.render()
+        dt = time.perf_counter() - t0
         accs.append(br.gather_accum().numpy())
         fbs.append(br.gather_framebuffer().numpy())
+        if rebalance:   # a skewed time so that the bands move
+            bands.append(br.rebalance(dt * (1.0 + 3.0 * rank)))
     cnt = br.reduce_counters()
     if rank == 0:
-        np.savez(os.path.join(out_dir, "dist.npz"), acc=np.stack(accs), fb=np.stack(fbs), cnt=cnt)
+        np.savez(os.path.join(out_dir, "dist.npz"), acc=np.stack(accs), fb=np.stack(fbs), cnt=cnt,
+                 bands=np.asarray(bands, dtype=np.int64).reshape(-1, world, 2))
     dist.barrier()
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2])
-def test_row_split_equals_single_process(oracle, world):
+@pytest.mark.parametrize("world,rebalance", [(2, False), (2, True)])
+def test_row_split_equals_single_process(oracle, world, rebalance):
     res, frames = (21, 17), 3
-    port = 29500 + (os.getpid() % 2000)
+    port = 29500 + (os.getpid() % 2000) + (7 if rebalance else 0)
     with tempfile.TemporaryDirectory() as d:
-        mp.spawn(_worker, args=(world, port, d, frames, res), nprocs=world, join=True)
+        mp.spawn(_worker, args=(world, port, d, frames, res, rebalance), nprocs=world, join=True)
         got = np.load(os.path.join(d, "dist.npz"))
+    if rebalance:   # the bands moved off the equal split
+        assert any(tuple(map(tuple, b)) != tuple(band(res[1], world, k) for k in range(world)) for b in got["bands"])
     vols, tfs = _scene()
     o = _setup(oracle.OracleRenderer(), vols, tfs, res)
     for f in range(frames):
