@@ -33,7 +33,8 @@ time_to_rmse (rank 0, one GPU; --no-ttr skips it): the first part of the headlin
 syncDDA) until the accumulation buffer is within RMSE 0.01 of the FP64 expected image of
 the estimator (libmdwt's mdwt_render_expected) -- and how long one low-spp frame plus the
 learned denoiser (weights in mdwtracker_b200/weights, trained by
-mdwtracker_b200/train_denoiser.py) takes to get there.
+mdwtracker_b200/train_denoiser.py) takes to get there; `held_out` repeats it on volumes
+generated from a seed the denoiser's training never used.
 
 batch (--no-batch skips it): 64 render requests of mixed resolution, channel count,
 voxel format, method, camera and spp rendered per frame through the batch API (one
@@ -88,22 +89,26 @@ def parse_args():
     return ap.parse_args()
 
 
-def make_scene(name, res=None, spp=None, edge=16):
+def make_scene(name, res=None, spp=None, edge=16, seed=None):
+    """The named scene; `seed` (c2, c3) regenerates its volumes from another seed."""
     from mdwtracker_b200 import synthetic as syn
+    kw = {} if seed is None else {"seed": seed}
     if name == "c1":
         sc = syn.scene_c1()
     elif name == "c2":
-        sc = syn.scene_c2()
+        sc = syn.scene_c2(**kw)
     elif name == "c3":
-        sc = syn.scene_c3(mode=2, edge=edge)
+        sc = syn.scene_c3(mode=2, edge=edge, **kw)
     elif name == "c3ndda":
-        sc = syn.scene_c3(mode=0, edge=edge)
+        sc = syn.scene_c3(mode=0, edge=edge, **kw)
     elif name == "c3b":
         sc = syn.scene_c3b(mode=2, edge=edge)
     elif name == "c3bndda":
         sc = syn.scene_c3b(mode=0, edge=edge)
     else:
         raise ValueError(name)
+    if seed is not None:
+        sc.name += f"_seed{seed}"
     if res is not None:
         sc.resolution = (int(res[0]), int(res[1]))
     if spp is not None:
@@ -253,7 +258,12 @@ def cpu_baseline(sc, budget_s):
                       f"{sc.spp} spp ({ps} path-samples, {el:.1f} s)"}, o
 
 
-def time_to_rmse(name, target, device_index, max_frames=20000):
+# volume seed of the held-out time-to-RMSE scene: the denoiser's training frames came from
+# the default c3 (seed 3) and c2 (seed 2) volumes only
+HELD_OUT_SEED = 11
+
+
+def time_to_rmse(name, target, device_index, max_frames=20000, seed=None):
     """Plain accumulation until the accumulation buffer's RGB is within `target` RMSE of
     the FP64 expected image: one sample per frame (frame f draws with seed factor f+1, so
     no two samples of the run share a seed); the first 16 frames one by one, then blocks
@@ -262,7 +272,7 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
     first check that meets the target."""
     import torch
     from mdwtracker_b200 import Renderer
-    sc = make_scene(name)
+    sc = make_scene(name, seed=seed)
     r = sc.setup(Renderer(device_index))
     w, h = sc.resolution
     r.setSpp(1)
@@ -311,6 +321,7 @@ def time_to_rmse(name, target, device_index, max_frames=20000):
         denoised["speedup_vs_plain"] = dev_ms / denoised["device_ms"]
     return {
         "target": target, "metric": "RMSE of linear RGB (accumulation buffer) vs the FP64 expected image",
+        "volume_seed": seed if seed is not None else "default (the denoiser's training volumes)",
         "workload": workload_name(sc).replace(f"_{sc.spp}spp", ""), "resolution": [w, h], "mode": sc.mode,
         "schedule": plain_schedule,
         "reference": {"kind": "FP64 expected image of the estimator (mdwt_render_expected)",
@@ -801,6 +812,11 @@ def main():
             ttr = time_to_rmse(args.ttr_config, args.ttr_target, local)
         except Exception as ex:  # reported beside the throughput line, never required
             ttr = {"error": str(ex)}
+        # the same measurement on volumes the denoiser never saw in training
+        try:
+            ttr["held_out"] = time_to_rmse(args.ttr_config, args.ttr_target, local, seed=HELD_OUT_SEED)
+        except Exception as ex:
+            ttr["held_out"] = {"error": str(ex)}
 
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:

@@ -56,6 +56,16 @@ class Batch:
     def setGraph(self, enable: bool) -> None:
         self._call("set_graph", C.c_int(1 if enable else 0))
 
+    def setFusion(self, enable: bool) -> None:
+        """Regroupable requests in one shared launch (default) or one launch per variant."""
+        self._call("set_fusion", C.c_int(1 if enable else 0))
+
+    def traceLaunches(self) -> int:
+        """Trace-kernel launches of the last batch frame."""
+        out = (C.c_int * 2)()
+        self._call("fusion_info", out)
+        return int(out[0])
+
     def lastMs(self) -> float:
         v = C.c_float()
         self._call("last_ms", C.byref(v))

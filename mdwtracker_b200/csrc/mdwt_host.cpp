@@ -1036,6 +1036,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   p.trips = c->trips;
   p.quorum = c->quorum;
   p.regroup = c->regroup;
+  p.store = c->store;
   p.vol32 = 1;
   for (auto &h : c->ch)
     if ((uint64_t)h.dims[0] * h.dims[1] * h.dims[2] >= (1ull << 32)) p.vol32 = 0;
@@ -1273,6 +1274,7 @@ struct mdwt_batch {
   std::vector<mdwt_ctx *> reqs;
   int unitItems = 0, pool = 0, trips = 0;   // unitItems: dispenser chunk (0 = sized per request)
   bool useGraph = true;
+  bool fuse = true;                          // regroupable requests share one launch (mdwt_batch_set_fusion)
   // pinned host staging and device copies: params, units, pixel offsets, unit counters
   TrackParams *hParams = nullptr, *dParams = nullptr;
   unsigned long long *hPix = nullptr, *dPix = nullptr;
@@ -1283,7 +1285,7 @@ struct mdwt_batch {
   cudaStream_t graphStream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t launches = 0, replays = 0, captures = 0, lastUnitsLaunch = 0;
-  int lastGroups = 0, lastUnits = 0;
+  int lastGroups = 0, lastUnits = 0, lastTraceLaunches = 0;
   std::string err;
 };
 
@@ -1321,11 +1323,14 @@ struct GroupPlan {
   unsigned long long totalItems, totalPix;
 };
 
+// Kernel variant of a batched request; the regroupable variants sort first (bit 40 clear)
+// so that they form one prefix of the batch, which a fused launch covers.
 long long variant_key(const TrackParams &p, int store, bool stats) {
   const bool ext = p.shadows || p.recT;
   const bool shade = p.shadows || p.gradient;
   const bool rg = !stats && !ext && regroup_fits(p);
-  return (long long)p.mode * 32 + (rg ? 16 : 0) + store * 8 + (stats ? 4 : 0) + (ext ? 2 : 0) + (shade ? 1 : 0);
+  return (rg ? 0LL : (1LL << 40)) + (long long)p.mode * 32 + (rg ? 16 : 0) + store * 8 + (stats ? 4 : 0) +
+         (ext ? 2 : 0) + (shade ? 1 : 0);
 }
 
 }  // namespace
@@ -1401,6 +1406,12 @@ mdwt_status mdwt_batch_set_graph(mdwt_batch *b, int enable) {
   return MDWT_OK;
 }
 
+mdwt_status mdwt_batch_set_fusion(mdwt_batch *b, int enable) {
+  if (!b) return MDWT_ERR_BAD_ARG;
+  b->fuse = enable != 0;
+  return MDWT_OK;
+}
+
 mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
   if (!b) return MDWT_ERR_BAD_ARG;
   if (b->reqs.empty()) return bfail(b, MDWT_ERR_STATE, "empty batch");
@@ -1457,6 +1468,26 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
     groups.push_back(g);
     k = e;
   }
+  // the regroupable prefix (its groups come first in key order): one fused launch with
+  // pixel offsets over all its requests
+  int nFused = 0, fusedGroups = 0, fusedPixFirst = 0;
+  unsigned long long fusedItems = 0, fusedPix = 0;
+  if (b->fuse) {
+    for (auto &g : groups) {
+      if (!g.regroup) break;
+      nFused += g.count;
+      fusedGroups++;
+      fusedItems += g.totalItems;
+    }
+    if (fusedGroups >= 1) {
+      fusedPixFirst = (int)pix.size();
+      for (int j = 0; j < nFused; j++) {
+        pix.push_back(fusedPix);
+        fusedPix += (unsigned long long)ps[order[j]].W * ps[order[j]].H;
+      }
+      pix.push_back(fusedPix);
+    }
+  }
   mdwt_status s;
   if ((s = grow_pair(b, &b->hParams, &b->dParams, b->capParams, (size_t)n))) return s;
   if ((s = grow_pair(b, &b->hPix, &b->dPix, b->capPix, pix.size()))) return s;
@@ -1470,7 +1501,7 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
   for (int j = 0; j < n; j++) b->hParams[j] = ps[order[j]];
   std::copy(pix.begin(), pix.end(), b->hPix);
   // structure signature: what a captured graph bakes in
-  std::vector<long long> sig = {n, (long long)pix.size(), (long long)b->numSMs};
+  std::vector<long long> sig = {n, (long long)pix.size(), (long long)b->numSMs, (long long)fusedGroups};
   for (auto &g : groups) {
     sig.push_back(keys[order[g.first]]);
     sig.push_back(g.count);
@@ -1482,7 +1513,14 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
     BCK(cudaMemcpyAsync(b->dParams, b->hParams, (size_t)n * sizeof(TrackParams), cudaMemcpyHostToDevice, st), "params");
     BCK(cudaMemcpyAsync(b->dPix, b->hPix, pix.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, st), "pix");
     BCK(cudaMemsetAsync(b->dDisp, 0, (size_t)n * sizeof(unsigned), st), "dispensers");
-    for (size_t gi = 0; gi < groups.size(); gi++) {
+    if (fusedGroups >= 1) {   // every regroupable request: one trace launch, one resolve launch
+      int launches = 0, grid = 0;
+      const int rc = launch_track_batch_fused(b->dParams, nFused, b->dDisp, fusedItems, b->dPix + fusedPixFirst,
+                                              fusedPix, st, b->numSMs, &launches, &grid);
+      if (rc) return bfail(b, MDWT_ERR_CUDA, std::string("batched tracker: ") + cudaGetErrorString((cudaError_t)rc));
+      b->launches += launches;
+    }
+    for (size_t gi = (size_t)fusedGroups; gi < groups.size(); gi++) {
       const GroupPlan &g = groups[gi];
       BatchGroup bg;
       bg.mode = g.mode; bg.storeKind = g.store; bg.stats = g.stats; bg.ext = g.ext; bg.shade = g.shade;
@@ -1536,6 +1574,7 @@ mdwt_status mdwt_batch_render(mdwt_batch *b, void *stream) {
     c->frameParam = c->frameID++;
   }
   b->lastGroups = (int)groups.size();
+  b->lastTraceLaunches = (int)groups.size() - (fusedGroups >= 1 ? fusedGroups - 1 : 0);
   b->lastUnits = n;
   return MDWT_OK;
 }
@@ -1558,6 +1597,13 @@ mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]) {
   if (!b || !out) return MDWT_ERR_BAD_ARG;
   out[0] = b->launches; out[1] = b->lastGroups; out[2] = b->lastUnits; out[3] = b->replays; out[4] = b->captures;
   out[5] = b->unitItems; out[6] = b->pool; out[7] = b->trips;
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_batch_fusion_info(mdwt_batch *b, int out[2]) {
+  if (!b || !out) return MDWT_ERR_BAD_ARG;
+  out[0] = b->lastTraceLaunches;
+  out[1] = b->fuse ? 1 : 0;
   return MDWT_OK;
 }
 

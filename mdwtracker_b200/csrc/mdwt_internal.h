@@ -83,6 +83,7 @@ struct TrackParams {
   int quorum;                    // ... ending early once this many lanes hold a pending sample
   int regroup;                   // -m 2: regroup paths across the block's warps (trace_regroup_kernel)
   int vol32;                     // every channel has < 2^32 voxels: 32-bit voxel offsets
+  int store;                     // voxel format of every channel: kStoreU8 or kStoreF32
   // sample batch [sBase, sBase + sCount) of the frame; one 4-byte record per traced
   // path, [k * nrect + rect-local pixel], nrect = pixels of the traced rectangle
   int sBase, sCount;
@@ -109,6 +110,11 @@ struct BatchGroup {
 };
 // -m 2 with MDWT_TUNE_REGROUP on and slot fields that fit the regrouped tracker's packing.
 bool regroup_fits(const TrackParams &p);
+// Regroupable requests of any method (-m 0, -m 2) and voxel format in ONE persistent trace
+// launch and one resolve launch (no per-pixel statistics, shadows or hit distances).
+int launch_track_batch_fused(const TrackParams *reqs, int nReq, unsigned *dispensers, unsigned long long totalItems,
+                             const unsigned long long *pixOfs, unsigned long long totalPix, void *stream, int numSMs,
+                             int *launches, int *grid);
 // Blocks per SM of the batched trace kernel of a variant (for chunk sizing).
 int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext);
 int launch_track_batch(const BatchGroup &g, void *stream, int numSMs, int *launches, int *grid);

@@ -698,9 +698,10 @@ struct Slots {
   float wdx[kSlots], wdy[kSlots], wdz[kSlots], t1w[kSlots], w2g[kSlots], g2w[kSlots];
   float tnx[kSlots], tny[kSlots], tnz[kSlots], tsx[kSlots], tsy[kSlots], tsz[kSlots];
   float rt0[kSlots], ncb[kSlots], maj[kSlots], rmaj[kSlots], t[kSlots], lim[kSlots];
-  float u[kSlots];    // the draw of the flight the sample stage completes
-  float xa[kSlots];   // -m 0: the exit distance of the cell that flight started in
 };
+// The draw a generator state was left at by its last rng_next: the top 24 bits of the
+// state (the sample stage re-reads the walk's pending flight draw this way).
+__device__ __forceinline__ float last_draw(uint32_t s) { return (float)(s >> 8) * (1.0f / 16777216.0f); }
 __device__ __forceinline__ uint32_t pack_meta(uint32_t stage, uint32_t flags, int ch, uint32_t cmask, uint32_t visits) {
   return stage | flags | ((uint32_t)ch << 4) | ((cmask & 0xfffu) << 9) | (visits << 21);
 }
@@ -876,9 +877,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     const float u = rng_next(rng);
     const float exitAt = MODE == 0 ? cell_exit(d) : lim;
     if (!flight_surely_exits(t, u, rmaj * kd, exitAt)) {
-      S.u[s] = u;
-      if (MODE == 0) S.xa[s] = exitAt;
-      stage = SAMPLE;
+      stage = SAMPLE;   // the state left at this draw (S.rng) gives it back to the sample stage
       break;
     }
     if (MODE == 0) advance = true;
@@ -901,10 +900,17 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
   const uint32_t m0 = S.meta[s];
   const int ch = (int)((m0 >> 4) & 15u);
   const float lim = S.lim[s];
-  const float t = flight(S.t[s], S.u[s], S.maj[s], S.rmaj[s], P.dt, S.w2g[s]);
+  uint32_t rng = S.rng[s];
+  const float t = flight(S.t[s], last_draw(rng), S.maj[s], S.rmaj[s], P.dt, S.w2g[s]);
   S.t[s] = t;
+  float exitAt = lim;
+  if (MODE == 0) {   // the walk's current cell: its exit distance from the DDA state
+    DDA d;
+    d.tnx = S.tnx[s]; d.tny = S.tny[s]; d.tnz = S.tnz[s]; d.rt0 = S.rt0[s];
+    exitAt = cell_exit(d);
+  }
   const uint32_t keep = m0 & ~(0xfu | kNewDda);   // channel, cell channels and cells entered
-  if (t >= (MODE == 0 ? S.xa[s] : lim)) {   // leaves the cell after all
+  if (t >= exitAt) {   // leaves the cell after all
     S.meta[s] = MODE == 0 ? (keep | WALK | kAdvance) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
     return;
   }
@@ -922,7 +928,6 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
   const float xs = fmaf(tW, S.wdx[s], P.camOrg.x) * P.w2u.x;
   const float ys = fmaf(tW, S.wdy[s], P.camOrg.y) * P.w2u.y;
   const float zs = fmaf(tW, S.wdz[s], P.camOrg.z) * P.w2u.z;
-  uint32_t rng = S.rng[s];
   const float thr = rng_next(rng) * S.maj[s];
   const ChanSm &cs = sch[ch];
   const float v = sample_volume<SK>(P, cs, xs, ys, zs);
@@ -1051,6 +1056,44 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks)
     __syncwarp();
   }
 }
+// The regroupable requests of a whole batch in ONE persistent launch, whatever their
+// method (-m 0 or -m 2) and voxel format: a warp takes the requests in turn, as
+// trace_batch_regroup_kernel does, and runs the regrouped loop of each request's variant,
+// so every request shares the launch's single tail.
+__global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks)
+    trace_batch_fused_kernel(const TrackParams *__restrict__ reqs, int nReq, unsigned *dispensers) {
+  extern __shared__ __align__(16) unsigned char rgSmem[];
+  rg::Slots &S = *reinterpret_cast<rg::Slots *>(rgSmem);
+  __shared__ ChanSm sch[rg::kTPB / 32][kMaxChannels];
+  __shared__ uint16_t selAll[rg::kTPB];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned gw = blockIdx.x * (rg::kTPB / 32) + warp;
+  const unsigned wbase = warp * (32u * rg::kSPT);
+  for (int i = 0; i < nReq; i++) {
+    const int r = (int)((gw + (unsigned)i) % (unsigned)nReq);
+    const TrackParams &P = reqs[r];
+    const unsigned total = (unsigned)P.numTiles * 32u * (unsigned)P.sCount;
+    unsigned peek = 0;
+    if (lane == 0) peek = *(volatile unsigned *)(dispensers + r);
+    peek = __shfl_sync(kFull, peek, 0);
+    if (peek >= total) continue;   // nothing left of this request
+    if (lane < (unsigned)P.C) sch[warp][lane] = chan_params(P, (int)lane);
+    __syncwarp();
+    uint32_t tot[5] = {0, 0, 0, 0, 0};
+    uint16_t *sel = selAll + warp * 32u;
+    const bool u8 = P.store == kStoreU8;
+    if (P.mode == 0) {
+      if (u8) rg::run_warp<0, kStoreU8>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
+      else rg::run_warp<0, kStoreF32>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
+    } else {
+      if (u8) rg::run_warp<2, kStoreU8>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
+      else rg::run_warp<2, kStoreF32>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
+    }
+    flush_counters(P.counters, tot);
+    __syncwarp();
+  }
+}
+
 // Batched variant: many requests (render contexts) in one persistent launch.  Every
 // request has its own work dispenser; a warp starts at request (global warp id mod nReq),
 // takes chunks of that request's items until they run out, then moves on to the next
@@ -1526,6 +1569,30 @@ int occ_tbs(bool stats, bool ext) {
 }
 
 }  // namespace
+
+int launch_track_batch_fused(const TrackParams *reqs, int nReq, unsigned *dispensers, unsigned long long totalItems,
+                             const unsigned long long *pixOfs, unsigned long long totalPix, void *stream, int numSMs,
+                             int *launches, int *grid) {
+  cudaStream_t st = (cudaStream_t)stream;
+  const int smem = (int)sizeof(rg::Slots);
+  cudaError_t e = cudaFuncSetAttribute(trace_batch_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return (int)e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_batch_fused_kernel, rg::kTPB, smem);
+  if (e != cudaSuccess) return (int)e;
+  if (bps < 1) bps = 1;
+  *grid = numSMs * bps;
+  if (totalItems > 0) trace_batch_fused_kernel<<<*grid, rg::kTPB, smem, st>>>(reqs, nReq, dispensers);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  size_t g = (size_t)((totalPix + 255) / 256);
+  if (g > (size_t)numSMs * 8) g = (size_t)numSMs * 8;
+  // the resolve pass of -m 0 / -m 2 without shading extras reads no voxels: one variant
+  // serves every voxel format
+  if (g > 0) resolve_batch_kernel<false, false, kStoreF32><<<(unsigned)g, 256, 0, st>>>(reqs, pixOfs, nReq);
+  if (launches) *launches += (totalItems > 0 ? 1 : 0) + (g > 0 ? 1 : 0);
+  return (int)cudaGetLastError();
+}
 
 // The regrouped tracker's packed slot fields: cells < 1024 per axis, at most 2047 cells
 // entered, 32-bit record indices.

@@ -53,13 +53,14 @@ def _same(a, b, stats):
     assert a.frameIds() == b.frameIds()
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_batch_equals_individual_renders(graph):
+@pytest.mark.parametrize("graph,fusion", [(True, True), (False, True), (True, False)])
+def test_batch_equals_individual_renders(graph, fusion):
     specs = _requests()
     batched = [_setup(s) for s in specs]
     alone = [_setup(s) for s in specs]
     b = Batch(0)
     b.setGraph(graph)
+    b.setFusion(fusion)
     for r in batched:
         b.add(r)
     for f in range(3):
@@ -73,6 +74,8 @@ def test_batch_equals_individual_renders(graph):
         np.testing.assert_array_equal(x.counters(), y.counters())
     info = b.info()
     assert info["groups"] >= 4 and info["requests"] == len(specs)
+    # the three regroupable variants (-m 0 uint8, -m 2 float32, -m 2 uint8) share one launch
+    assert b.traceLaunches() == info["groups"] - (2 if fusion else 0)
     if graph:
         assert info["graph_captures"] == 1 and info["graph_replays"] == 3
 
