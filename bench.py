@@ -497,7 +497,7 @@ def run_reference(args):
 def schedule_of(r, by):
     """The context's tracker schedule (MDWT_TUNE_*): which tracker, its trips, and the
     warp-local tracker's pool and quorum."""
-    names = {4: "regroup", 2: "trips", 0: "pool", 3: "quorum"}
+    names = {4: "regroup", 5: "rg_blocks", 2: "trips", 0: "pool", 3: "quorum"}
     out = {v: r.getTuning(k) for k, v in names.items()}
     out["by"] = by
     return out

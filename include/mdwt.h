@@ -215,8 +215,12 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * statistics run the tracker that keeps 64 paths per warp and runs, at each step, the
  * operation most of them need next (path start, walk, density sample), one path per
  * lane; a walk takes at most TRIPS free-flight draws.  0 = the warp-local tracker (32
- * paths per warp; POOL and QUORUM apply to it only). */
-enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2, MDWT_TUNE_QUORUM = 3, MDWT_TUNE_REGROUP = 4 };
+ * paths per warp; POOL and QUORUM apply to it only).
+ * MDWT_TUNE_RG_BLOCKS: blocks of 256 threads per SM the regrouped tracker runs (0, the
+ * default: as many as its path slots' shared memory allows, 4); fewer blocks leave more of
+ * the SM's 256 KB of L1/shared memory to the L1 cache, which holds the majorant grid. */
+enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2, MDWT_TUNE_QUORUM = 3, MDWT_TUNE_REGROUP = 4,
+       MDWT_TUNE_RG_BLOCKS = 5 };
 mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
 /* The current value of a tuning knob (defaults: pool 8, batch 0, trips 4, quorum 16,
  * regroup 1). */

@@ -67,8 +67,9 @@ mdwt_status mdwt_batch_info(mdwt_batch *b, int64_t out[8]);
  * accumulation reset afterwards.  best[3] (optional) = chunk items, pool, trips. */
 mdwt_status mdwt_batch_autotune(mdwt_batch *b, int frames, int best[3]);
 
-/* Schedule autotuner for one context: coordinate descent over, for -m 2, the tracker
- * (MDWT_TUNE_REGROUP {1, 0}), then the trips {1, 2, 3, 4, 6, 8}, then -- for the
+/* Schedule autotuner for one context: coordinate descent over, for -m 2 and -m 0, the tracker
+ * (MDWT_TUNE_REGROUP {1, 0}), for the regrouped tracker its blocks per SM
+ * (MDWT_TUNE_RG_BLOCKS {0, 3, 2}), then the trips {1, 2, 3, 4, 6, 8, 12, 16}, then -- for the
  * warp-local tracker -- the regeneration pool {4, 8, 16, 32} and the sample quorum
  * {8, 16, 24, never} (MDWT_TUNE_*), each candidate timed on `frames` frames rendered by
  * mdwt_render_frames (after a warm-up of the same), so pass the frames per call of the

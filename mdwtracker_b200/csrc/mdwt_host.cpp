@@ -166,7 +166,8 @@ struct mdwt_ctx {
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
   int trips = 4;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
   int quorum = 16;    // end a round's trips early once this many lanes wait to sample (33: never)
-  int regroup = 1;    // -m 2: the tracker that regroups each warp's paths by operation (MDWT_TUNE_REGROUP)
+  int regroup = 1;    // -m 2 / -m 0: the tracker that regroups each warp's paths by operation (MDWT_TUNE_REGROUP)
+  int rgBlocks = 0;   // its blocks per SM, 0 = as many as fit (MDWT_TUNE_RG_BLOCKS)
   int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
   bool timing = false;        // CUDA events around the trace and resolve kernels
   static constexpr int kTimedPasses = 8;   // sample passes of a frame that can be timed
@@ -1036,6 +1037,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   p.trips = c->trips;
   p.quorum = c->quorum;
   p.regroup = c->regroup;
+  p.rgBlocks = c->rgBlocks;
   p.store = c->store;
   p.vol32 = 1;
   for (auto &h : c->ch)
@@ -1697,14 +1699,16 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
     return MDWT_OK;
   };
   const int regroupC[] = {1, 0};
-  const int tripsC[] = {1, 2, 3, 4, 6, 8};
+  const int tripsC[] = {1, 2, 3, 4, 6, 8, 12, 16};
   const int poolsC[] = {4, 8, 16, 32};
   const int quorumC[] = {8, 16, 24, 33};
+  const int rgBlocksC[] = {0, 3, 2};
   // the regrouped tracker runs -m 2 and -m 0 frames without shadow rays or per-pixel
   // statistics; other frames run the warp-local tracker whatever the knob says
   const bool regroupable = (c->mode == 2 || c->mode == 0) && !c->shadows && !c->statsOn;
   if (regroupable) s = tune(&c->regroup, regroupC, 2);
-  if (!s && !(s = tune(&c->trips, tripsC, 6)) && !(regroupable && c->regroup)) {
+  if (!s && regroupable && c->regroup) s = tune(&c->rgBlocks, rgBlocksC, 3);
+  if (!s && !(s = tune(&c->trips, tripsC, 8)) && !(regroupable && c->regroup)) {
     // the regeneration pool and the sample quorum belong to the warp-local tracker
     if (!(s = tune(&c->pool, poolsC, 4))) s = tune(&c->quorum, quorumC, 4);
   }
@@ -1966,6 +1970,11 @@ mdwt_status mdwt_set_tuning(mdwt_ctx *c, int key, int value) {
     c->regroup = value;
     return MDWT_OK;
   }
+  if (key == MDWT_TUNE_RG_BLOCKS) {
+    if (value < 0 || value > 8) return fail(c, MDWT_ERR_BAD_ARG, "regrouped-tracker blocks per SM must be in 0..8");
+    c->rgBlocks = value;
+    return MDWT_OK;
+  }
   if (key == MDWT_TUNE_BATCH) {
     if (value < 0) return fail(c, MDWT_ERR_BAD_ARG, "batch must be >= 0");
     c->batchCap = value;
@@ -1982,6 +1991,7 @@ mdwt_status mdwt_get_tuning(const mdwt_ctx *c, int key, int *value) {
     case MDWT_TUNE_TRIPS: *value = c->trips; return MDWT_OK;
     case MDWT_TUNE_QUORUM: *value = c->quorum; return MDWT_OK;
     case MDWT_TUNE_REGROUP: *value = c->regroup; return MDWT_OK;
+    case MDWT_TUNE_RG_BLOCKS: *value = c->rgBlocks; return MDWT_OK;
     default: return MDWT_ERR_BAD_ARG;
   }
 }

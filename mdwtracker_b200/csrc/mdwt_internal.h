@@ -81,7 +81,8 @@ struct TrackParams {
   int chunk;                     // work items a warp takes from the dispenser at once
   int trips;                     // phase-1 transition/draw trips per warp round (at most)
   int quorum;                    // ... ending early once this many lanes hold a pending sample
-  int regroup;                   // -m 2: regroup paths across the block's warps (trace_regroup_kernel)
+  int regroup;                   // -m 2 / -m 0: the regrouped tracker (trace_regroup_kernel)
+  int rgBlocks;                  // its blocks per SM (0: as many as fit); fewer leave more L1 cache
   int vol32;                     // every channel has < 2^32 voxels: 32-bit voxel offsets
   int store;                     // voxel format of every channel: kStoreU8 or kStoreF32
   // sample batch [sBase, sBase + sCount) of the frame; one 4-byte record per traced

@@ -1464,15 +1464,35 @@ int launch_resolve(const TrackParams &p, cudaStream_t st, int numSMs) {
   return (int)cudaGetLastError();
 }
 
+// The shared-memory carveout for `blocks` regrouped-tracker blocks per SM, in percent of
+// the largest carveout (the rest of the SM's 256 KB is L1 cache); -1 = the default.
+template <typename K>
+int regroup_carveout(K kernel, int blocks, int smem) {
+  if (blocks <= 0) return -1;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return -1;
+  int dev = 0, maxSm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (maxSm <= 0) return -1;
+  const long need = (long)blocks * ((long)smem + (long)fa.sharedSizeBytes + 1024L);   // 1 KB reserved per block
+  const int pct = (int)((need * 100 + maxSm - 1) / maxSm);
+  return pct > 100 ? 100 : pct;
+}
+
 template <int MODE, int SK>
 int launch_regroup(const TrackParams &p, cudaStream_t st, int numSMs, int *grid, void *evMid) {
   const int smem = (int)sizeof(rg::Slots);
   cudaError_t e = cudaFuncSetAttribute(trace_regroup_kernel<MODE, SK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(trace_regroup_kernel<MODE, SK>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           regroup_carveout(trace_regroup_kernel<MODE, SK>, p.rgBlocks, smem));
+  if (e != cudaSuccess) return (int)e;
   int bps = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, trace_regroup_kernel<MODE, SK>, rg::kTPB, smem);
   if (e != cudaSuccess) return (int)e;
   if (bps < 1) bps = 1;
+  if (p.rgBlocks > 0 && p.rgBlocks < bps) bps = p.rgBlocks;
   *grid = numSMs * bps;
   if (p.numTiles > 0) trace_regroup_kernel<MODE, SK><<<*grid, rg::kTPB, smem, st>>>(p);
   if (evMid) cudaEventRecord((cudaEvent_t)evMid, st);

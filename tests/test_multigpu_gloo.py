@@ -3,6 +3,7 @@ a band of every frame with the oracle and gather the bands; the assembled frames
 equal a single-process render bit for bit, also when the bands are re-cut between frames
 from measured render times."""
 import os
+import socket
 import tempfile
 
 import numpy as np
@@ -21,6 +22,13 @@ def test_band_partition():
                 assert b == c
             sizes = [b - a for a, b in bands]
             assert max(sizes) - min(sizes) <= 1
+
+
+def _free_port() -> int:
+    """A TCP port on 127.0.0.1 that nothing listens on now (for the gloo rendezvous)."""
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
 
 
 def test_split_by_cost_balances_and_covers():
@@ -104,7 +112,7 @@ def _worker(rank, world, port, out_dir, frames, res, rebalance=False):
 @pytest.mark.parametrize("world,rebalance", [(2, False), (2, True)])
 def test_row_split_equals_single_process(oracle, world, rebalance):
     res, frames = (21, 17), 3
-    port = 29500 + (os.getpid() % 2000) + (7 if rebalance else 0)
+    port = _free_port()
     with tempfile.TemporaryDirectory() as d:
         mp.spawn(_worker, args=(world, port, d, frames, res, rebalance), nprocs=world, join=True)
         got = np.load(os.path.join(d, "dist.npz"))
@@ -189,7 +197,7 @@ def test_data_parallel_training_equals_full_batch_training():
     """Two ranks, each training on half of every minibatch, keep identical parameters and
     follow single-process training on the whole minibatch."""
     world, steps = 2, 25
-    port = 31500 + (os.getpid() % 2000)
+    port = _free_port()
     with tempfile.TemporaryDirectory() as d:
         mp.spawn(_dp_worker, args=(world, port, d, steps), nprocs=world, join=True)
         got = np.load(os.path.join(d, "dp.npz"))
