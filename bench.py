@@ -377,6 +377,17 @@ def batch_throughput(device_index, n_requests, frames=3, small=False):
         b.render(st.cuda_stream)
         bat.append(b.lastMs())
     info = b.info()
+    launches = b.traceLaunches()
+    # the same schedule with one trace launch per kernel variant (no fused launch)
+    b.setFusion(False)
+    b.render(st.cuda_stream)
+    torch.cuda.synchronize()
+    unf = []
+    for _ in range(frames):
+        b.render(st.cuda_stream)
+        unf.append(b.lastMs())
+    launches_unf = b.traceLaunches()
+    b.setFusion(True)
     b.close()
     for r in reqs:
         r.close()
@@ -384,9 +395,10 @@ def batch_throughput(device_index, n_requests, frames=3, small=False):
     return {"workload": f"c4_{n_requests}req_{'256x256_1-4spp' if small else 'mixed'}", "requests": n_requests,
             "path_samples_per_frame": paths,
             "batched": {"ms_per_frame": ms_bat, "Gpath_samples_per_s": paths / ms_bat / 1e6,
-                        "kernel_variant_groups": info["groups"],
+                        "kernel_variant_groups": info["groups"], "trace_launches": launches,
                         "graph_replays": info["graph_replays"], "autotuned": {"chunk_items": best[0] or "per request", "pool": best[1],
                                                                               "trips": best[2], "seconds": tune_s}},
+            "batched_per_variant": {"ms_per_frame": min(unf), "trace_launches": launches_unf},
             "one_by_one": {"ms_per_frame": ms_seq, "Gpath_samples_per_s": paths / ms_seq / 1e6},
             "speedup": ms_seq / ms_bat, "setup_s": setup_s}
 

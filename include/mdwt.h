@@ -211,11 +211,13 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * it evaluates its pending density samples together.
  * MDWT_TUNE_QUORUM: a round's trips also end once `value` (1..33; 33 = never) of the
  * warp's lanes hold a pending density sample.
- * MDWT_TUNE_REGROUP: 1 (default) = -m 2 and -m 0 frames without shadow rays or per-pixel
+ * MDWT_TUNE_REGROUP: 1 = -m 2 and -m 0 frames without shadow rays or per-pixel
  * statistics run the tracker that keeps 64 paths per warp and runs, at each step, the
  * operation most of them need next (path start, walk, density sample), one path per
  * lane; a walk takes at most TRIPS free-flight draws.  0 = the warp-local tracker (32
- * paths per warp; POOL and QUORUM apply to it only).
+ * paths per warp; POOL and QUORUM apply to it only).  Until set: 1 for -m 2, 0 for -m 0
+ * (the warp-local tracker is the faster N-DDA tracker on the scenes measured); the
+ * schedule autotuner tries both.
  * MDWT_TUNE_RG_BLOCKS: blocks of 256 threads per SM the regrouped tracker runs (0, the
  * default: as many as its path slots' shared memory allows, 4); fewer blocks leave more of
  * the SM's 256 KB of L1/shared memory to the L1 cache, which holds the majorant grid. */
@@ -223,7 +225,7 @@ enum { MDWT_TUNE_POOL = 0, MDWT_TUNE_BATCH = 1, MDWT_TUNE_TRIPS = 2, MDWT_TUNE_Q
        MDWT_TUNE_RG_BLOCKS = 5 };
 mdwt_status mdwt_set_tuning(mdwt_ctx *ctx, int key, int value);
 /* The current value of a tuning knob (defaults: pool 8, batch 0, trips 4, quorum 16,
- * regroup 1). */
+ * regroup 1 for -m 2 and 0 otherwise, regrouped-tracker blocks 0). */
 mdwt_status mdwt_get_tuning(const mdwt_ctx *ctx, int key, int *value);
 
 /* No reference counterpart: CUDA events on the render stream around the trace kernel

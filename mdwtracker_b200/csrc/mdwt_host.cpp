@@ -154,8 +154,7 @@ struct mdwt_ctx {
   int expW = 0, expH = 0;
   float *dRanges = nullptr;
   float *dMaj = nullptr;
-  uint16_t *dMask = nullptr;    // per-cell non-zero-majorant channel mask
-  float *dMajRcp = nullptr;     // recip_for_div of each majorant (the trackers' free flights)
+  float2 *dCellTab = nullptr;   // the trackers' per-cell table: channel mask, (majorant, reciprocal) pairs
   size_t M = 0;
   float rootLo[3] = {0, 0, 0}, rootHi[3] = {1, 1, 1};
   float gLo[4] = {0, 0, 0, 0}, gHi[4] = {1, 1, 1, 1};
@@ -166,7 +165,8 @@ struct mdwt_ctx {
   int batchCap = 0;   // samples per trace pass, 0 = automatic (MDWT_TUNE_BATCH)
   int trips = 4;      // transition/draw trips per warp round (MDWT_TUNE_TRIPS)
   int quorum = 16;    // end a round's trips early once this many lanes wait to sample (33: never)
-  int regroup = 1;    // -m 2 / -m 0: the tracker that regroups each warp's paths by operation (MDWT_TUNE_REGROUP)
+  int regroup = -1;   // the tracker that regroups each warp's paths by operation (MDWT_TUNE_REGROUP);
+                      // -1 until set: on for -m 2, off for -m 0 (see regroup_on)
   int rgBlocks = 0;   // its blocks per SM, 0 = as many as fit (MDWT_TUNE_RG_BLOCKS)
   int rowLo = 0, rowHi = 0;   // rendered row band, empty = all rows (mdwt_set_render_rows)
   bool timing = false;        // CUDA events around the trace and resolve kernels
@@ -458,10 +458,8 @@ void free_device(mdwt_ctx *c) {
   if (c->dWork) cudaFree(c->dWork);
   if (c->dRanges) cudaFree(c->dRanges);
   if (c->dMaj) cudaFree(c->dMaj);
-  if (c->dMask) cudaFree(c->dMask);
-  c->dMask = nullptr;
-  if (c->dMajRcp) cudaFree(c->dMajRcp);
-  c->dMajRcp = nullptr;
+  if (c->dCellTab) cudaFree(c->dCellTab);
+  c->dCellTab = nullptr;
   if (c->dRec) cudaFree(c->dRec);
   if (c->dRecStats) cudaFree(c->dRecStats);
   if (c->dRecT) cudaFree(c->dRecT);
@@ -509,8 +507,7 @@ mdwt_status recalc(mdwt_ctx *c) {
   std::memset(&p, 0, sizeof(p));
   p.ranges = c->dRanges;
   p.majorants = c->dMaj;
-  p.majRcp = c->dMajRcp;
-  p.mask = c->dMask;
+  p.cellTab = c->dCellTab;
   p.C = (int)c->ch.size();
   p.mode = c->mode;
   p.M = c->M;
@@ -766,8 +763,7 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
-  CK(cudaMalloc(&c->dMajRcp, c->M * (mode >= 3 ? 1 : C) * 4), "cudaMalloc majorant reciprocals");
-  CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
+  CK(cudaMalloc(&c->dCellTab, c->M * ((mode >= 3 ? 1 : C) + 1) * sizeof(float2)), "cudaMalloc cell table");
   c->inited = true;
   mdwt_status s = build_ranges(c);
   if (s) { c->inited = false; return s; }
@@ -965,6 +961,12 @@ static float feature_scale(const mdwt_ctx *c) {
 }
 
 // Scene, camera, transfer functions and shading of the next frame.
+// Whether frames run the regrouped tracker (MDWT_TUNE_REGROUP): as set, or by default for
+// syncDDA only -- for N-DDA the warp-local tracker measured faster (2.20 vs 1.54 Gpath/s
+// on the 1080p 6 x 512^3 float32 scene), its per-cell majorant reads hitting the L1 cache
+// that the regrouped tracker's path slots take as shared memory.
+static int regroup_on(const mdwt_ctx *c) { return c->regroup >= 0 ? c->regroup : (c->mode == 2 ? 1 : 0); }
+
 static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   std::memset(&p, 0, sizeof(p));
   p.W = c->W; p.H = c->H; p.spp = c->spp;
@@ -985,8 +987,8 @@ static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   p.mode = c->mode;
   p.dt = c->dt;
   p.majorants = c->dMaj;
-  p.majRcp = c->dMajRcp;
-  p.mask = c->dMask;
+  p.cellTab = c->dCellTab;
+  p.tabStride = (c->mode >= 3 ? 1 : p.C) + 1;
   for (int i = 0; i < p.C; i++) {
     p.vol[i] = c->ch[i].dVol;
     for (int a = 0; a < 3; a++) p.dims[i][a] = (int)c->ch[i].dims[a];
@@ -1036,7 +1038,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   p.pool = c->pool;
   p.trips = c->trips;
   p.quorum = c->quorum;
-  p.regroup = c->regroup;
+  p.regroup = regroup_on(c);
   p.rgBlocks = c->rgBlocks;
   p.store = c->store;
   p.vol32 = 1;
@@ -1248,16 +1250,14 @@ static mdwt_status regrid(mdwt_ctx *c) {
   CK(cudaStreamSynchronize(c->stream), "regrid");
   if (c->dRanges) cudaFree(c->dRanges);
   if (c->dMaj) cudaFree(c->dMaj);
-  if (c->dMask) cudaFree(c->dMask);
-  if (c->dMajRcp) cudaFree(c->dMajRcp);
-  c->dRanges = nullptr; c->dMaj = nullptr; c->dMask = nullptr; c->dMajRcp = nullptr;
+  if (c->dCellTab) cudaFree(c->dCellTab);
+  c->dRanges = nullptr; c->dMaj = nullptr; c->dCellTab = nullptr;
   for (int a = 0; a < 3; a++) c->mc[a] = mc[a];
   c->M = (size_t)mc[0] * mc[1] * mc[2];
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (c->mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
-  CK(cudaMalloc(&c->dMajRcp, c->M * (c->mode >= 3 ? 1 : C) * 4), "cudaMalloc majorant reciprocals");
-  CK(cudaMalloc(&c->dMask, c->M * 2), "cudaMalloc majorant mask");
+  CK(cudaMalloc(&c->dCellTab, c->M * ((c->mode >= 3 ? 1 : C) + 1) * sizeof(float2)), "cudaMalloc cell table");
   mdwt_status s = build_ranges(c);
   if (s) return s;
   s = recalc(c);
@@ -1707,8 +1707,8 @@ mdwt_status mdwt_autotune_schedule(mdwt_ctx *c, int frames, int best[2]) {
   // statistics; other frames run the warp-local tracker whatever the knob says
   const bool regroupable = (c->mode == 2 || c->mode == 0) && !c->shadows && !c->statsOn;
   if (regroupable) s = tune(&c->regroup, regroupC, 2);
-  if (!s && regroupable && c->regroup) s = tune(&c->rgBlocks, rgBlocksC, 3);
-  if (!s && !(s = tune(&c->trips, tripsC, 8)) && !(regroupable && c->regroup)) {
+  if (!s && regroupable && regroup_on(c)) s = tune(&c->rgBlocks, rgBlocksC, 3);
+  if (!s && !(s = tune(&c->trips, tripsC, 8)) && !(regroupable && regroup_on(c))) {
     // the regeneration pool and the sample quorum belong to the warp-local tracker
     if (!(s = tune(&c->pool, poolsC, 4))) s = tune(&c->quorum, quorumC, 4);
   }
@@ -1990,7 +1990,7 @@ mdwt_status mdwt_get_tuning(const mdwt_ctx *c, int key, int *value) {
     case MDWT_TUNE_BATCH: *value = c->batchCap; return MDWT_OK;
     case MDWT_TUNE_TRIPS: *value = c->trips; return MDWT_OK;
     case MDWT_TUNE_QUORUM: *value = c->quorum; return MDWT_OK;
-    case MDWT_TUNE_REGROUP: *value = c->regroup; return MDWT_OK;
+    case MDWT_TUNE_REGROUP: *value = regroup_on(c); return MDWT_OK;
     case MDWT_TUNE_RG_BLOCKS: *value = c->rgBlocks; return MDWT_OK;
     default: return MDWT_ERR_BAD_ARG;
   }

@@ -43,8 +43,12 @@ struct TrackParams {
   int C, mode;
   float dt;
   const float *majorants;      // [cell*C + ch] (modes 0..2) or [cell] (mode 3)
-  const float *majRcp;         // the same layout: recip_for_div of each majorant
-  const uint16_t *mask;        // per cell: bit c set when majorants[cell*C + c] != 0
+  // The trackers' per-cell table, tabStride = Ce + 1 float2 per cell (Ce = C, or 1 for the
+  // summed majorant): entry 0 holds the cell's non-zero-majorant channel mask (as bits in
+  // .x), entry 1 + c the majorant of channel c and its recip_for_div -- the mask and the
+  // first majorants share a sector, and a majorant comes with its reciprocal in one load.
+  const float2 *cellTab;
+  int tabStride;
   // channels
   const void *vol[kMaxChannels];
   int dims[kMaxChannels][3];
@@ -154,8 +158,7 @@ int launch_ranges_init(float *ranges, size_t count, void *stream, int *launches)
 struct MajorantParams {
   const float *ranges;
   float *majorants;
-  float *majRcp;               // recip_for_div of each majorant (the free flights divide by it)
-  uint16_t *mask;              // per cell: bit c set when channel c's majorant is non-zero
+  float2 *cellTab;             // the trackers' per-cell table (TrackParams::cellTab), or null
   int C, mode;
   size_t M;
   const float *tfAlpha[kMaxChannels];

@@ -118,18 +118,21 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
         sum += channel_majorant(p, c, rc.x, rc.y);
       }
       p.majorants[cell] = sum;
-      if (p.majRcp) p.majRcp[cell] = recip_for_div(sum);
-      if (p.mask) p.mask[cell] = sum != 0.0f ? 1 : 0;
+      if (p.cellTab) {
+        p.cellTab[cell * 2] = make_float2(__uint_as_float(sum != 0.0f ? 1u : 0u), 0.0f);
+        p.cellTab[cell * 2 + 1] = make_float2(sum, recip_for_div(sum));
+      }
     } else {
       uint32_t m = 0;
+      float2 *tab = p.cellTab ? p.cellTab + cell * (C + 1) : nullptr;
       for (int c = 0; c < C; c++) {
         const float2 rc = r[c];
         const float v = channel_majorant(p, c, rc.x, rc.y);
         p.majorants[cell * C + c] = v;
-        if (p.majRcp) p.majRcp[cell * C + c] = recip_for_div(v);
+        if (tab) tab[1 + c] = make_float2(v, recip_for_div(v));
         if (v != 0.0f) m |= 1u << c;
       }
-      if (p.mask) p.mask[cell] = (uint16_t)m;
+      if (tab) tab[0] = make_float2(__uint_as_float(m), 0.0f);
     }
   }
 }

@@ -83,6 +83,15 @@ struct ChanSm {
   float ry1, ry2;   // recip_for_div of the TF remap divisors vd1 - vd0 and xd1 - xd0
 };
 
+// The per-cell table (TrackParams::cellTab): a cell's non-zero-majorant channel mask, and
+// channel c's (majorant, reciprocal) pair.
+__device__ __forceinline__ uint32_t cell_mask(const TrackParams &P, int cellID) {
+  return __float_as_uint(__ldg(reinterpret_cast<const float *>(P.cellTab + (size_t)cellID * P.tabStride)));
+}
+__device__ __forceinline__ float2 cell_maj(const TrackParams &P, int cellID, int c) {
+  return __ldg(P.cellTab + (size_t)cellID * P.tabStride + 1 + c);
+}
+
 // sampleVolumeTexture (deviceCode.cu:122-132): NaN outside [0,1]^3, else trilinear.
 template <int SK>
 __device__ __forceinline__ float sample_volume(const TrackParams &P, const ChanSm &cs, float px, float py, float pz) {
@@ -276,7 +285,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
     d.visits++;
     totCell++;
     cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-    cmask = __ldg(P.mask + cellID);
+    cmask = cell_mask(P, cellID);
   };
   // Start a tracking leg (volumeIntersection + the tracker's set-up, deviceCode.cu:759-778,
   // 1676-1726) from the leg origin along (dx, dy, dz); false when it misses the volume.
@@ -423,8 +432,9 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
               continue;
             }
             ch += __ffs(rem) - 1;
-            maj = __ldg(P.majorants + (size_t)cellID * C + ch);
-            rmaj = __ldg(P.majRcp + (size_t)cellID * C + ch);
+            const float2 mr = cell_maj(P, cellID, ch);
+            maj = mr.x;
+            rmaj = mr.y;
             t = ct0;
             stepping = true;
             break;
@@ -444,8 +454,9 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             }
             act = A_CHAN;
             if ((cmask >> ch) & 1u) {  // zero-majorant cells are skipped (deviceCode.cu:893-894)
-              maj = __ldg(P.majorants + (size_t)cellID * C + ch);
-              rmaj = __ldg(P.majRcp + (size_t)cellID * C + ch);
+              const float2 mr = cell_maj(P, cellID, ch);
+              maj = mr.x;
+              rmaj = mr.y;
               t = ct0;
               stepping = true;
               break;
@@ -459,8 +470,9 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             }
             if constexpr (MODE >= 3) {  // summed majorant (deviceCode.cu:541-548, 1003-1007)
               if (cmask & 1u) {
-                maj = __ldg(P.majorants + cellID);
-                rmaj = __ldg(P.majRcp + cellID);
+                const float2 mr = cell_maj(P, cellID, 0);
+                maj = mr.x;
+                rmaj = mr.y;
                 t = ct0;
                 stepping = true;
                 break;
@@ -469,7 +481,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
             } else {  // MODE 1: per-channel free flights from the cell entry (deviceCode.cu:652-674)
               float sum = 0.0f;
               for (int i = 0; i < C; i++) {
-                majs[i] = __ldg(P.majorants + (size_t)cellID * C + i);
+                majs[i] = cell_maj(P, cellID, i).x;
                 sum += majs[i];
                 ts[i] = ct0;
               }
@@ -724,7 +736,7 @@ __device__ __forceinline__ float cell_exit(const DDA &d) {
 // enter_cell of trace_items: the cell's id and channel mask
 __device__ __forceinline__ int enter(const TrackParams &P, const DDA &d, uint32_t &cmask) {
   const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-  cmask = __ldg(P.mask + cellID);
+  cmask = cell_mask(P, cellID);
   return cellID;
 }
 // End of a path: its record and, for features and gradient shading, the world distance
@@ -835,8 +847,9 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
           }
           if ((cmask >> ch) & 1u) {   // zero-majorant cells are skipped (deviceCode.cu:893-894)
             const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-            maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
-            rmaj = __ldg(P.majRcp + (size_t)cellID * P.C + ch);
+            const float2 mr = cell_maj(P, cellID, ch);
+            maj = mr.x;
+            rmaj = mr.y;
             t = d.rt0 + d.ncb;   // the cell's entry distance
             break;
           }
@@ -860,8 +873,9 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
           }
           ch += __ffs(rem) - 1;
           const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-          maj = __ldg(P.majorants + (size_t)cellID * P.C + ch);
-          rmaj = __ldg(P.majRcp + (size_t)cellID * P.C + ch);
+          const float2 mr = cell_maj(P, cellID, ch);
+          maj = mr.x;
+          rmaj = mr.y;
           t = d.rt0 + d.ncb;   // the cell's entry distance
           break;
         }

@@ -111,11 +111,15 @@ def test_gpu_absent_is_an_error_not_a_fallback():
 
 def test_tuning_knobs_read_back():
     r = Renderer(MDWT_HOST_ONLY)
-    assert [r.getTuning(k) for k in (0, 1, 2, 3, 4)] == [8, 0, 4, 16, 1]
-    r.setTuning(4, 0)
+    # pool, batch, trips, quorum, regroup (off by default without -m 2), regrouped-tracker blocks
+    assert [r.getTuning(k) for k in (0, 1, 2, 3, 4, 5)] == [8, 0, 4, 16, 0, 0]
+    r.setTuning(4, 1)
     r.setTuning(2, 7)
-    assert r.getTuning(4) == 0 and r.getTuning(2) == 7
+    r.setTuning(5, 3)
+    assert r.getTuning(4) == 1 and r.getTuning(2) == 7 and r.getTuning(5) == 3
     with pytest.raises(MdwtError):
         r.setTuning(4, 2)
+    with pytest.raises(MdwtError):
+        r.setTuning(5, 9)
     with pytest.raises(MdwtError):
         r.getTuning(9)

@@ -50,7 +50,8 @@ def test_defaults(monkeypatch):
 
 def test_schedule_report_reads_the_knobs():
     r = Renderer(MDWT_HOST_ONLY)
-    assert bench.schedule_of(r, "default") == {"regroup": 1, "rg_blocks": 0, "trips": 4, "pool": 8, "quorum": 16,
+    # a host-only context has no method yet (-m 0): the warp-local tracker by default
+    assert bench.schedule_of(r, "default") == {"regroup": 0, "rg_blocks": 0, "trips": 4, "pool": 8, "quorum": 16,
                                                "by": "default"}
     r.setTuning(4, 0)
     r.setTuning(2, 6)

@@ -108,6 +108,7 @@ def test_c3_full_size(orc, c3_scenes, mode):
     sc = c3_scenes[mode]
     assert sc.resolution == (1920, 1080) and sc.spp == 256 and sc.macrocells == (32, 32, 32)
     p = sc.setup(Renderer(0))
+    p.setTuning(4, 1)   # the regrouped tracker for N-DDA too (its default there is the warp-local one)
     o = sc.setup(orc.OracleRenderer())
     np.testing.assert_array_equal(p.ranges(), o.ranges())
     np.testing.assert_array_equal(p.majorants(), o.majorants())
