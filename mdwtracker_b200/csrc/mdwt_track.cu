@@ -711,6 +711,16 @@ struct Slots {
   float tnx[kSlots], tny[kSlots], tnz[kSlots], tsx[kSlots], tsy[kSlots], tsz[kSlots];
   float rt0[kSlots], ncb[kSlots], maj[kSlots], rmaj[kSlots], t[kSlots], lim[kSlots];
 };
+// MODE of the regrouped loop: 0 (N-DDA) or 2 (syncDDA) at compile time, or -1 to read the
+// request's method at run time (the fused batch kernel: one copy of the code for every
+// request).  SK likewise: a store kind, or -1 for the request's.
+template <int MODE>
+__device__ __forceinline__ bool ndda(const TrackParams &P) { return MODE == 0 || (MODE < 0 && P.mode == 0); }
+template <int SK>
+__device__ __forceinline__ float sample_any(const TrackParams &P, const ChanSm &cs, float x, float y, float z) {
+  if constexpr (SK >= 0) return sample_volume<SK>(P, cs, x, y, z);
+  else return P.store == kStoreU8 ? sample_volume<kStoreU8>(P, cs, x, y, z) : sample_volume<kStoreF32>(P, cs, x, y, z);
+}
 // The draw a generator state was left at by its last rng_next: the top 24 bits of the
 // state (the sample stage re-reads the walk's pending flight draw this way).
 __device__ __forceinline__ float last_draw(uint32_t s) { return (float)(s >> 8) * (1.0f / 16777216.0f); }
@@ -783,7 +793,7 @@ __device__ __forceinline__ void start(const TrackParams &P, Slots &S, unsigned s
   S.rng[s] = rng; S.steps[s] = 0u; S.record[s] = 0u;
   S.wdx[s] = wdx; S.wdy[s] = wdy; S.wdz[s] = wdz;
   S.t1w[s] = fminf(1e20f, th1); S.w2g[s] = w2g; S.g2w[s] = g2w;
-  if constexpr (MODE == 0) {   // the first channel's traversal starts in the walk
+  if (ndda<MODE>(P)) {   // the first channel's traversal starts in the walk
     S.lim[s] = 1e20f;
     S.meta[s] = pack_meta(WALK, kNewDda, 0, 0u, 0u);
     return;
@@ -824,7 +834,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     if (!drawing) {
       bool ended = false;
       while (true) {
-        if constexpr (MODE == 0) {
+        if (ndda<MODE>(P)) {
           if (newdda) {   // the next channel's traversal (deviceCode.cu:965-969)
             if (ch >= P.C) { ended = true; break; }
             float gx, gy, gz, a, b;
@@ -889,12 +899,12 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     // stage, which computes the exact flight, its tests and the density sample together.
     if (++steps >= kMaxStepsPerSample) { finish(P, S, s, record, true, lim, tot); return; }
     const float u = rng_next(rng);
-    const float exitAt = MODE == 0 ? cell_exit(d) : lim;
+    const float exitAt = ndda<MODE>(P) ? cell_exit(d) : lim;
     if (!flight_surely_exits(t, u, rmaj * kd, exitAt)) {
       stage = SAMPLE;   // the state left at this draw (S.rng) gives it back to the sample stage
       break;
     }
-    if (MODE == 0) advance = true;
+    if (ndda<MODE>(P)) advance = true;
     else ch++;
     drawing = false;
     if (++k >= P.trips) break;
@@ -918,25 +928,26 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
   const float t = flight(S.t[s], last_draw(rng), S.maj[s], S.rmaj[s], P.dt, S.w2g[s]);
   S.t[s] = t;
   float exitAt = lim;
-  if (MODE == 0) {   // the walk's current cell: its exit distance from the DDA state
+  const bool n0 = ndda<MODE>(P);
+  if (n0) {   // the walk's current cell: its exit distance from the DDA state
     DDA d;
     d.tnx = S.tnx[s]; d.tny = S.tny[s]; d.tnz = S.tnz[s]; d.rt0 = S.rt0[s];
     exitAt = cell_exit(d);
   }
   const uint32_t keep = m0 & ~(0xfu | kNewDda);   // channel, cell channels and cells entered
   if (t >= exitAt) {   // leaves the cell after all
-    S.meta[s] = MODE == 0 ? (keep | WALK | kAdvance) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
+    S.meta[s] = n0 ? (keep | WALK | kAdvance) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
     return;
   }
-  if (MODE == 0 && lim < t) {   // beyond the closest hit so far: the next channel's traversal
+  if (n0 && lim < t) {   // beyond the closest hit so far: the next channel's traversal
     S.meta[s] = pack_meta(WALK, kNewDda, ch + 1, 0u, 0u);
     return;
   }
   const float tW = t * S.g2w[s];
   if (tW >= S.t1w[s]) {   // world exit
     tot[1]++;
-    if (MODE == 2 && ch == P.C - 1) { finish(P, S, s, S.record[s], false, lim, tot); return; }
-    S.meta[s] = MODE == 0 ? pack_meta(WALK, kNewDda, ch + 1, 0u, 0u) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
+    if (!n0 && ch == P.C - 1) { finish(P, S, s, S.record[s], false, lim, tot); return; }
+    S.meta[s] = n0 ? pack_meta(WALK, kNewDda, ch + 1, 0u, 0u) : ((keep & ~0xf0u) | WALK | ((uint32_t)(ch + 1) << 4));
     return;
   }
   const float xs = fmaf(tW, S.wdx[s], P.camOrg.x) * P.w2u.x;
@@ -944,7 +955,7 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
   const float zs = fmaf(tW, S.wdz[s], P.camOrg.z) * P.w2u.z;
   const float thr = rng_next(rng) * S.maj[s];
   const ChanSm &cs = sch[ch];
-  const float v = sample_volume<SK>(P, cs, xs, ys, zs);
+  const float v = sample_any<SK>(P, cs, xs, ys, zs);
   tot[0]++;
   uint32_t next = (m0 & ~3u) | WALK | kDraw;
   if (v == v) {
@@ -953,14 +964,14 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
     if (a > 0.0f && thr < a) {
       S.record[s] = make_record(ch, tax);
       S.lim[s] = fminf(t, lim);
-      if (MODE == 0) {   // the channel's traversal ends at its hit; the next channel's starts
+      if (n0) {   // the channel's traversal ends at its hit; the next channel's starts
         next = pack_meta(WALK, kNewDda, ch + 1, 0u, 0u);
       }
-    } else if (MODE == 0) {
+    } else if (n0) {
       tot[1]++;
     }
   }
-  if (MODE == 2) tot[1]++;   // -m 2 counts every sample as a rejection, hits included (deviceCode.cu:836-846)
+  if (!n0) tot[1]++;   // -m 2 counts every sample as a rejection, hits included (deviceCode.cu:836-846)
   S.rng[s] = rng;
   S.meta[s] = next;
 }
@@ -1094,15 +1105,9 @@ __global__ void __launch_bounds__(rg::kTPB, rg::kMinBlocks)
     if (lane < (unsigned)P.C) sch[warp][lane] = chan_params(P, (int)lane);
     __syncwarp();
     uint32_t tot[5] = {0, 0, 0, 0, 0};
-    uint16_t *sel = selAll + warp * 32u;
-    const bool u8 = P.store == kStoreU8;
-    if (P.mode == 0) {
-      if (u8) rg::run_warp<0, kStoreU8>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
-      else rg::run_warp<0, kStoreF32>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
-    } else {
-      if (u8) rg::run_warp<2, kStoreU8>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
-      else rg::run_warp<2, kStoreF32>(P, S, sel, wbase, lane, sch[warp], dispensers + r, total, tot);
-    }
+    // one copy of the loop for every request: method and voxel format are read at run
+    // time, so the kernel's code stays the size of one variant
+    rg::run_warp<-1, -1>(P, S, selAll + warp * 32u, wbase, lane, sch[warp], dispensers + r, total, tot);
     flush_counters(P.counters, tot);
     __syncwarp();
   }
