@@ -1561,6 +1561,64 @@ int orc_dda_trace(const float org[3], const float dir[3], float tMax, const uint
 
 // Test hooks: the primitives of the arithmetic specification.
 float orc_log(float x) { return mlog(x); }
+// The trackers' quotient from a stored reciprocal (Markstein 1990: q = RN(a y), then
+// RN(q + y (a - q b)) with y = RN(1/b); the IEEE division outside the safe range), restated
+// on the host, against the IEEE quotient: the number of mismatches over `n` seeded pairs
+// with random mantissas and exponents in [-40, 40], plus every divisor mantissa in [1, 2)
+// with `per` dividends each.
+static inline float host_recip_for_div(float b) {
+  const float ab = std::fabs(b);
+  return (ab >= 8.271806125530277e-25f && ab <= 1.2089258196146292e24f) ? 1.0f / b : 0.0f;
+}
+static inline float host_div_by(float a, float b, float y) {
+  const float q = a * y;
+  const float aq = std::fabs(q);
+  if (std::fabs(a) >= 8.271806125530277e-25f && aq >= 8.271806125530277e-25f && aq <= 1.2089258196146292e24f)
+    return std::fma(std::fma(-q, b, a), y, q);
+  return a / b;
+}
+uint64_t orc_quotient_check(uint64_t n, int per, uint64_t seed) {
+  uint64_t bad = 0;
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+  for (int64_t t = 0; t < 64; t++) {
+    uint64_t s = seed + 0x9e3779b97f4a7c15ull * (uint64_t)(t + 1);
+    auto next = [&s]() {
+      uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+      return z ^ (z >> 31);
+    };
+    for (uint64_t i = 0; i < n / 64; i++) {
+      const uint64_t r = next();
+      const uint32_t ea = 127u + (uint32_t)((r >> 8) % 81u) - 40u, eb = 127u + (uint32_t)((r >> 16) % 81u) - 40u;
+      float a, b;
+      const uint32_t ua = (ea << 23) | (uint32_t)((r >> 40) & 0x7fffffu) | ((uint32_t)(r & 1u) << 31);
+      const uint32_t ub = (eb << 23) | (uint32_t)((r >> 20) & 0x7fffffu);
+      std::memcpy(&a, &ua, 4);
+      std::memcpy(&b, &ub, 4);
+      const float q1 = host_div_by(a, b, host_recip_for_div(b)), q2 = a / b;
+      if (std::memcmp(&q1, &q2, 4) != 0) bad++;
+    }
+  }
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+  for (int64_t m = 0; m < (1 << 23); m++) {
+    const uint32_t ub = (127u << 23) | (uint32_t)m;
+    float b;
+    std::memcpy(&b, &ub, 4);
+    const float y = host_recip_for_div(b);
+    uint32_t st = (uint32_t)m * 2654435761u + (uint32_t)seed;
+    for (int k = 0; k < per; k++) {
+      st = 1664525u * st + 1013904223u;
+      const uint32_t ua = (127u << 23) | (st >> 9);
+      float a;
+      std::memcpy(&a, &ua, 4);
+      const float q1 = host_div_by(a, b, y), q2 = a / b;
+      if (std::memcmp(&q1, &q2, 4) != 0) bad++;
+    }
+  }
+  return bad;
+}
+
 // The largest relative error of mlog against a double-precision log over every argument
 // a free flight takes, 1 - k 2^-24 for k < 2^24 (the premise of the tracker kernels'
 // exit filter, which bounds it by 2^-18); also counts k where mlog increases with k.

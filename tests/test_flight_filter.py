@@ -25,6 +25,16 @@ def test_project_log_bound_over_every_flight_argument(oracle):
     assert up.value == 0
 
 
+def test_quotient_from_the_stored_reciprocal_is_the_ieee_quotient(oracle):
+    """The trackers divide by a majorant (and the TF remap by its spans) as q = RN(a y),
+    RN(q + y (a - q b)) with the stored y = RN(1/b) (Markstein 1990): the same bits as the
+    IEEE quotient, here over 64 M random pairs and every divisor mantissa x 16 dividends."""
+    lib = oracle.load_oracle()
+    lib.orc_quotient_check.restype = C.c_uint64
+    lib.orc_quotient_check.argtypes = [C.c_uint64, C.c_int, C.c_uint64]
+    assert lib.orc_quotient_check(64 << 20, 16, 12345) == 0
+
+
 @pytest.mark.gpu
 def test_hardware_log2_bound_over_every_flight_argument(mdwt_lib):
     worst = C.c_float(-1.0)
