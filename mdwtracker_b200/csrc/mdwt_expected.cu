@@ -45,7 +45,7 @@ __device__ double volume_d(const TrackParams &P, int c, const double p[3]) {
   const int X = P.dims[c][0], Y = P.dims[c][1], Z = P.dims[c][2];
   const AxisD ax = axis_d(p[0], X), ay = axis_d(p[1], Y), az = axis_d(p[2], Z);
   const void *v = P.vol[c];
-  auto at = [&](int x, int y, int z) { return (double)vox<SK>(v, ((size_t)z * Y + y) * X + x); };
+  auto at = [&](int x, int y, int z) { return (double)vox<SK>(v, vidx<SK, size_t>(x, y, z, X, Y)); };
   const double c00 = lerp_d(ax.a, at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0));
   const double c10 = lerp_d(ax.a, at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0));
   const double c01 = lerp_d(ax.a, at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1));

@@ -755,10 +755,22 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
       h.u8.clear(); h.u8.shrink_to_fit();
       h.store = kStoreF32;
     }
-    const size_t bytes = n * (c->store == kStoreU8 ? 1 : 4);
-    CK(cudaMalloc(&h.dVol, bytes), "cudaMalloc volume");
-    CK(cudaMemcpyAsync(h.dVol, c->store == kStoreU8 ? (const void *)h.u8.data() : (const void *)h.f32.data(), bytes,
-                       cudaMemcpyHostToDevice, c->stream), "upload volume");
+    if (c->store == kStoreU8) {
+      CK(cudaMalloc(&h.dVol, n), "cudaMalloc volume");
+      CK(cudaMemcpyAsync(h.dVol, h.u8.data(), n, cudaMemcpyHostToDevice, c->stream), "upload volume");
+    } else {
+      // float32: uploaded x fastest, then rearranged into 2x2x2 micro-bricks on the device
+      // (kStoreF32); the linear copy lives only for this channel's upload
+      const int d3[3] = {(int)h.dims[0], (int)h.dims[1], (int)h.dims[2]};
+      float *lin = nullptr;
+      CK(cudaMalloc(&lin, n * 4), "cudaMalloc volume upload");
+      cudaError_t e = cudaMemcpyAsync(lin, h.f32.data(), n * 4, cudaMemcpyHostToDevice, c->stream);
+      if (e == cudaSuccess) e = cudaMalloc(&h.dVol, stored_voxels(kStoreF32, h.dims) * 4);
+      if (e == cudaSuccess) e = (cudaError_t)launch_brick_f32(lin, (float *)h.dVol, d3, c->stream, &c->launches);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      cudaFree(lin);
+      CK(e, "micro-brick upload");
+    }
   }
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
@@ -1043,7 +1055,7 @@ static mdwt_status prepare_frame(mdwt_ctx *c, TrackParams &p, int *batchOut) {
   p.store = c->store;
   p.vol32 = 1;
   for (auto &h : c->ch)
-    if ((uint64_t)h.dims[0] * h.dims[1] * h.dims[2] >= (1ull << 32)) p.vol32 = 0;
+    if ((uint64_t)stored_voxels(c->store, h.dims) >= (1ull << 32)) p.vol32 = 0;
   // samples in batches whose path records fit the record budget; the resolve pass
   // carries the per-pixel running sums across batches in sample order
   const size_t nrect = p.numTiles > 0 ? (size_t)rw * (size_t)rh : 0;
@@ -1276,7 +1288,7 @@ struct mdwt_batch {
   std::vector<mdwt_ctx *> reqs;
   int unitItems = 0, pool = 0, trips = 0;   // unitItems: dispenser chunk (0 = sized per request)
   bool useGraph = true;
-  bool fuse = true;                          // regroupable requests share one launch (mdwt_batch_set_fusion)
+  bool fuse = false;                         // regroupable requests share one launch (mdwt_batch_set_fusion)
   // pinned host staging and device copies: params, units, pixel offsets, unit counters
   TrackParams *hParams = nullptr, *dParams = nullptr;
   unsigned long long *hPix = nullptr, *dPix = nullptr;

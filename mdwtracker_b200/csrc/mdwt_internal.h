@@ -13,7 +13,13 @@ constexpr uint32_t kMaxStepsPerSample = 1u << 22;
 // Device voxel storage.  uint8 channels stay one byte per voxel (value = b * 255,
 // the exact float the reference's RawR conversion produces, rawFile.cpp:103-105);
 // everything else is stored as the float32 the reference would have uploaded.
-enum StoreKind : int { kStoreU8 = 0, kStoreF32 = 1 };
+// Voxel storage on the device.  kStoreU8: bytes, x fastest (value = byte * 255).
+// kStoreF32: float32 in 2x2x2 micro-bricks -- voxel (x, y, z) at
+// ((((z>>1) * Yb + (y>>1)) * Xb + (x>>1)) * 8) + 4 (z&1) + 2 (y&1) + (x&1), with
+// Xb = ceil(X/2), Yb = ceil(Y/2): a trilinear footprint whose lower corner has even
+// coordinates is one 32-byte sector, and any footprint spans at most eight.
+// kStoreF32Lin: float32, x fastest (a caller's buffer: mdwt_build_ranges_noalloc).
+enum StoreKind : int { kStoreU8 = 0, kStoreF32 = 1, kStoreF32Lin = 2 };
 
 struct F3 { float x, y, z; };
 
@@ -88,7 +94,7 @@ struct TrackParams {
   int regroup;                   // -m 2 / -m 0: the regrouped tracker (trace_regroup_kernel)
   int rgBlocks;                  // its blocks per SM (0: as many as fit); fewer leave more L1 cache
   int vol32;                     // every channel has < 2^32 voxels: 32-bit voxel offsets
-  int store;                     // voxel format of every channel: kStoreU8 or kStoreF32
+  int store;                     // voxel storage of every channel: kStoreU8 or kStoreF32 (micro-bricks)
   // sample batch [sBase, sBase + sCount) of the frame; one 4-byte record per traced
   // path, [k * nrect + rect-local pixel], nrect = pixels of the traced rectangle
   int sBase, sCount;
@@ -168,5 +174,10 @@ struct MajorantParams {
   float os[kMaxChannels];
 };
 int launch_majorants(const MajorantParams &p, void *stream, int *launches);
+// Float32 voxels, x fastest, into the micro-brick layout of kStoreF32 (dst holds
+// 8 ceil(X/2) ceil(Y/2) ceil(Z/2) floats; the padding voxels are written as 0).
+int launch_brick_f32(const float *src, float *dst, const int dims[3], void *stream, int *launches);
+// Floats of a channel's device buffer in the layout of `storeKind` (bytes / 4 for uint8).
+size_t stored_voxels(int storeKind, const int64_t dims[3]);
 
 }  // namespace mdwt

@@ -40,14 +40,25 @@ __global__ void range_xy_kernel(const void *__restrict__ vol, int X, int Y, int 
     const int y0 = __ldg(ivy + 2 * cy), y1 = __ldg(ivy + 2 * cy + 1);
     float mn = __int_as_float(0x7f800000), mx = __int_as_float(0xff800000);
     for (int y = y0; y <= y1; y++) {
-      const size_t row = ((size_t)z * Y + y) * X;
       for (int x = x0; x <= x1; x++) {
-        const float v = vox<SK>(vol, row + x);
+        const float v = vox<SK>(vol, vidx<SK, size_t>(x, y, z, X, Y));
         if (v < mn) mn = v;   // NaN never enters (atomicMin CAS loop: `while (val < old)`)
         if (v > mx) mx = v;
       }
     }
     out[i] = make_float2(mn, mx);
+  }
+}
+
+// Float32 voxels, x fastest, into the micro-brick layout (kStoreF32): one thread per
+// voxel, reads coalesced along x, writes two floats apart within a brick.
+__global__ void brick_f32_kernel(const float *__restrict__ src, float *__restrict__ dst, int X, int Y, int Z) {
+  const size_t n = (size_t)X * Y * Z;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % (size_t)X);
+    const size_t r = i / (size_t)X;
+    const int y = (int)(r % (size_t)Y), z = (int)(r / (size_t)Y);
+    dst[vidx<kStoreF32, size_t>(x, y, z, X, Y)] = __ldg(src + i);
   }
 }
 
@@ -161,14 +172,34 @@ int launch_ranges(const void *vol, int storeKind, const int dims[3], const uint3
   float2 *A = reinterpret_cast<float2 *>(scratchA);
   if (storeKind == kStoreU8)
     range_xy_kernel<kStoreU8><<<grid_for(n1, 256, 148 * 64), 256, 0, st>>>(vol, dims[0], dims[1], dims[2], ivx, ivy, (int)mc[0], (int)mc[1], A);
-  else
+  else if (storeKind == kStoreF32)
     range_xy_kernel<kStoreF32><<<grid_for(n1, 256, 148 * 64), 256, 0, st>>>(vol, dims[0], dims[1], dims[2], ivx, ivy, (int)mc[0], (int)mc[1], A);
+  else
+    range_xy_kernel<kStoreF32Lin><<<grid_for(n1, 256, 148 * 64), 256, 0, st>>>(vol, dims[0], dims[1], dims[2], ivx, ivy, (int)mc[0], (int)mc[1], A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   const size_t n2 = (size_t)mc[2] * mc[1] * mc[0];
   range_z_kernel<<<grid_for(n2, 256, 148 * 64), 256, 0, st>>>(A, ivz, (int)mc[0], (int)mc[1], (int)mc[2], C, ch,
                                                               reinterpret_cast<float2 *>(ranges));
   if (launches) *launches += 2;
+  return (int)cudaGetLastError();
+}
+
+size_t stored_voxels(int storeKind, const int64_t dims[3]) {
+  if (storeKind == kStoreF32)
+    return (size_t)8 * (size_t)((dims[0] + 1) / 2) * (size_t)((dims[1] + 1) / 2) * (size_t)((dims[2] + 1) / 2);
+  return (size_t)dims[0] * (size_t)dims[1] * (size_t)dims[2];
+}
+
+int launch_brick_f32(const float *src, float *dst, const int dims[3], void *stream, int *launches) {
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t d64[3] = {dims[0], dims[1], dims[2]};
+  const size_t nb = stored_voxels(kStoreF32, d64), n = (size_t)dims[0] * dims[1] * dims[2];
+  cudaError_t e = cudaSuccess;
+  if (nb > n) e = cudaMemsetAsync(dst, 0, nb * sizeof(float), st);   // the padding voxels of odd dims
+  if (e != cudaSuccess) return (int)e;
+  brick_f32_kernel<<<grid_for(n, 256, 148 * 64), 256, 0, st>>>(src, dst, dims[0], dims[1], dims[2]);
+  if (launches) *launches += 1;
   return (int)cudaGetLastError();
 }
 
@@ -344,7 +375,7 @@ extern "C" mdwt_status mdwt_build_ranges_noalloc(const void *d_volume, int forma
   if (launch_ranges_init(d_ranges_out, M, st, nullptr) != 0) return MDWT_ERR_CUDA;
   const int d3[3] = {(int)dims[0], (int)dims[1], (int)dims[2]};
   const uint32_t mc3[3] = {macrocells[0], macrocells[1], macrocells[2]};
-  const int sk = format == MDWT_FMT_UINT8 ? kStoreU8 : kStoreF32;
+  const int sk = format == MDWT_FMT_UINT8 ? kStoreU8 : kStoreF32Lin;   // the caller's layout: x fastest
   if (launch_ranges(d_volume, sk, d3, mc3, iv, iv + 2 * mx, iv + 2 * (mx + my), 1, 0, d_ranges_out,
                     (float *)g_noalloc_pairs_ptr[dev], nullptr, st, nullptr) != 0)
     return MDWT_ERR_CUDA;

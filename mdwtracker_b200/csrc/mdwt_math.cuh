@@ -147,6 +147,15 @@ __device__ __forceinline__ float vox(const void *base, size_t idx) {
   if (SK == kStoreU8) return (float)__ldg(reinterpret_cast<const uint8_t *>(base) + idx) * 255.0f;
   return __ldg(reinterpret_cast<const float *>(base) + idx);
 }
+// The element index of voxel (x, y, z) in the storage layout SK (StoreKind).
+template <int SK, typename IDX>
+__device__ __forceinline__ IDX vidx(int x, int y, int z, int X, int Y) {
+  if (SK == kStoreF32) {
+    const IDX Xb = (IDX)((X + 1) >> 1), Yb = (IDX)((Y + 1) >> 1);
+    return (((IDX)(z >> 1) * Yb + (IDX)(y >> 1)) * Xb + (IDX)(x >> 1)) * 8u + (IDX)(((z & 1) << 2) | ((y & 1) << 1) | (x & 1));
+  }
+  return ((IDX)z * (IDX)Y + (IDX)y) * (IDX)X + (IDX)x;
+}
 
 }  // namespace
 }  // namespace mdwt

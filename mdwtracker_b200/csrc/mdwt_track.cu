@@ -57,13 +57,21 @@ __device__ __forceinline__ Axis axis_in_range(float u, int n) {
 
 template <int SK, typename IDX>
 __device__ __forceinline__ float trilinear(const void *base, int X, int Y, const Axis &ax, const Axis &ay, const Axis &az) {
-  const IDX sXY = (IDX)X * (IDX)Y;
-  const IDX z0 = (IDX)az.i0 * sXY, z1 = (IDX)az.i1 * sXY;
-  const IDX y0 = (IDX)ay.i0 * (IDX)X, y1 = (IDX)ay.i1 * (IDX)X;
-  const float v000 = vox<SK>(base, z0 + y0 + ax.i0), v100 = vox<SK>(base, z0 + y0 + ax.i1);
-  const float v010 = vox<SK>(base, z0 + y1 + ax.i0), v110 = vox<SK>(base, z0 + y1 + ax.i1);
-  const float v001 = vox<SK>(base, z1 + y0 + ax.i0), v101 = vox<SK>(base, z1 + y0 + ax.i1);
-  const float v011 = vox<SK>(base, z1 + y1 + ax.i0), v111 = vox<SK>(base, z1 + y1 + ax.i1);
+  float v000, v100, v010, v110, v001, v101, v011, v111;
+  if (SK == kStoreF32) {   // micro-bricks: the eight corners from at most eight 8-voxel bricks
+    v000 = vox<SK>(base, vidx<SK, IDX>(ax.i0, ay.i0, az.i0, X, Y)); v100 = vox<SK>(base, vidx<SK, IDX>(ax.i1, ay.i0, az.i0, X, Y));
+    v010 = vox<SK>(base, vidx<SK, IDX>(ax.i0, ay.i1, az.i0, X, Y)); v110 = vox<SK>(base, vidx<SK, IDX>(ax.i1, ay.i1, az.i0, X, Y));
+    v001 = vox<SK>(base, vidx<SK, IDX>(ax.i0, ay.i0, az.i1, X, Y)); v101 = vox<SK>(base, vidx<SK, IDX>(ax.i1, ay.i0, az.i1, X, Y));
+    v011 = vox<SK>(base, vidx<SK, IDX>(ax.i0, ay.i1, az.i1, X, Y)); v111 = vox<SK>(base, vidx<SK, IDX>(ax.i1, ay.i1, az.i1, X, Y));
+  } else {
+    const IDX sXY = (IDX)X * (IDX)Y;
+    const IDX z0 = (IDX)az.i0 * sXY, z1 = (IDX)az.i1 * sXY;
+    const IDX y0 = (IDX)ay.i0 * (IDX)X, y1 = (IDX)ay.i1 * (IDX)X;
+    v000 = vox<SK>(base, z0 + y0 + ax.i0); v100 = vox<SK>(base, z0 + y0 + ax.i1);
+    v010 = vox<SK>(base, z0 + y1 + ax.i0); v110 = vox<SK>(base, z0 + y1 + ax.i1);
+    v001 = vox<SK>(base, z1 + y0 + ax.i0); v101 = vox<SK>(base, z1 + y0 + ax.i1);
+    v011 = vox<SK>(base, z1 + y1 + ax.i0); v111 = vox<SK>(base, z1 + y1 + ax.i1);
+  }
   const float c00 = lerpf(ax.a, v000, v100);
   const float c10 = lerpf(ax.a, v010, v110);
   const float c01 = lerpf(ax.a, v001, v101);

@@ -59,7 +59,7 @@ def test_schedule_report_reads_the_knobs():
     assert s["regroup"] == 0 and s["trips"] == 6
 
 
-@pytest.mark.parametrize("kernel,bytes_", [("trace_regroup_kernel", 93842176.0), ("trace_kernel", 92951552.0)])
+@pytest.mark.parametrize("kernel,bytes_", [("trace_regroup_kernel", 94480640.0), ("trace_kernel", 92951552.0)])
 def test_profiled_traffic_reads_the_committed_summaries(kernel, bytes_):
     assert bench.profiled_traffic(kernel, "c2_syncdda_3x256u8_mc16_1024x1024_64spp") == bytes_
     assert bench.profiled_traffic(kernel, "no_such_workload") is None
