@@ -153,6 +153,15 @@ mdwt_status mdwt_set_material(mdwt_ctx *ctx, int ch, float diffuse, float specul
                               float shininess, float gradient_step, const float spec_rgb[3]);
 /* Renderer::mirrorFramebuffer (renderer.h:177, renderer.cpp:962-972). */
 mdwt_status mdwt_set_mirror(mdwt_ctx *ctx, int enable);
+/* Seed words of the per-sample generator.  The reference seeds LCG<4>(threadIdx.x + seed,
+ * threadIdx.y + seed) for the camera ray and (threadIdx.x + seed + 1, threadIdx.y + seed + 1)
+ * for the shadow ray (deviceCode.cu:296-297, 385-386); under OptiX threadIdx is not a
+ * function of the pixel.  edge 0 (the default): the pixel's coordinates stand for
+ * threadIdx.  edge = a power of two in 1..1024: the pixel's position inside an edge x edge
+ * thread block, as a 2-D CUDA launch of such blocks would give threadIdx -- pixels at the
+ * same position in different blocks then share their generator streams, as they would in
+ * that launch.  Other values: MDWT_ERR_BAD_ARG. */
+mdwt_status mdwt_set_seed_block(mdwt_ctx *ctx, int edge);
 
 /* ---- frames ------------------------------------------------------------------ */
 
@@ -175,6 +184,12 @@ mdwt_status mdwt_set_render_rows(mdwt_ctx *ctx, int row0, int row1);
  * memory (device or pinned/pageable host; either pointer may be NULL), enqueued on
  * `cuda_stream` (NULL = the context's stream). */
 mdwt_status mdwt_copy_frame_rows(mdwt_ctx *ctx, int row0, int row1, float *accum_dst, uint32_t *fb_dst,
+                                 void *cuda_stream);
+/* No counterpart in the reference (row bands).  The inverse of mdwt_copy_frame_rows: rows
+ * [row0, row1) of the accumulation (float4) and RGBA8 buffers from caller memory (either
+ * pointer may be NULL), enqueued on `cuda_stream` (NULL = the context's stream).  A
+ * context whose band grows takes over the running mean of its new rows this way. */
+mdwt_status mdwt_load_frame_rows(mdwt_ctx *ctx, int row0, int row1, const float *accum_src, const uint32_t *fb_src,
                                  void *cuda_stream);
 /* Wait for every frame issued on the context's streams; reports device-side errors. */
 mdwt_status mdwt_sync(mdwt_ctx *ctx);

@@ -129,6 +129,7 @@ struct mdwt_ctx {
   std::vector<Material> mats;
   std::vector<TFState> tf;
   bool mirror = false;
+  uint32_t seedMask = 0xffffffffu;   // mdwt_set_seed_block: the pixel's coordinates, or its position in a block
   Camera cam;
   V3 cOrg{}, cLlc{}, cHor{}, cVer{};
   int frameID = 0, accumID = 0, frameParam = 0, accumParam = 0;
@@ -962,6 +963,15 @@ mdwt_status mdwt_set_mirror(mdwt_ctx *c, int e) {
   return MDWT_OK;
 }
 
+mdwt_status mdwt_set_seed_block(mdwt_ctx *c, int edge) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (edge == 0) { c->seedMask = 0xffffffffu; return MDWT_OK; }
+  if (edge < 1 || edge > 1024 || (edge & (edge - 1)) != 0)
+    return fail(c, MDWT_ERR_BAD_ARG, "seed block edge must be 0 or a power of two in 1..1024");
+  c->seedMask = (uint32_t)edge - 1u;
+  return MDWT_OK;
+}
+
 // Depth-feature scale: 1 / (distance from the camera to the root-box centre + the box
 // diagonal), so that hit distances map into [0, 1].
 static float feature_scale(const mdwt_ctx *c) {
@@ -986,6 +996,7 @@ static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   p.accumParam = (uint32_t)c->accumParam;
   p.accumulate = c->accum ? 1 : 0;
   p.mirror = c->mirror ? 1 : 0;
+  p.seedMask = c->seedMask;
   p.bg = f3(c->bg);
   p.camOrg = f3(c->cOrg); p.camLlc = f3(c->cLlc); p.camHor = f3(c->cHor); p.camVer = f3(c->cVer);
   p.rootLo = {c->rootLo[0], c->rootLo[1], c->rootLo[2]};
@@ -1936,6 +1947,19 @@ mdwt_status mdwt_copy_frame_rows(mdwt_ctx *c, int row0, int row1, float *accum_d
   const size_t off = (size_t)row0 * c->W, n = (size_t)(row1 - row0) * c->W;
   if (accum_dst) CK(cudaMemcpyAsync(accum_dst, c->dAccum + 4 * off, n * 16, cudaMemcpyDefault, st), "copy accum rows");
   if (fb_dst) CK(cudaMemcpyAsync(fb_dst, c->dFb + off, n * 4, cudaMemcpyDefault, st), "copy framebuffer rows");
+  return MDWT_OK;
+}
+
+mdwt_status mdwt_load_frame_rows(mdwt_ctx *c, int row0, int row1, const float *accum_src, const uint32_t *fb_src,
+                                 void *stream) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (!c->inited) return fail(c, MDWT_ERR_STATE, "mdwt_init first");
+  if (row0 < 0 || row1 > c->H || row0 > row1) return fail(c, MDWT_ERR_BAD_ARG, "row range outside the frame");
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const size_t off = (size_t)row0 * c->W, n = (size_t)(row1 - row0) * c->W;
+  if (accum_src) CK(cudaMemcpyAsync(c->dAccum + 4 * off, accum_src, n * 16, cudaMemcpyDefault, st), "load accum rows");
+  if (fb_src) CK(cudaMemcpyAsync(c->dFb + off, fb_src, n * 4, cudaMemcpyDefault, st), "load framebuffer rows");
   return MDWT_OK;
 }
 

@@ -35,6 +35,7 @@ struct TrackParams {
   int nFrames;
   uint32_t frameParam1, accumParam1;
   int accumulate, mirror;
+  uint32_t seedMask;             // seed words from (pixel & seedMask): ~0 per pixel, edge - 1 per thread block
   F3 bg;
   // camera basis (LaunchParams::camera)
   F3 camOrg, camLlc, camHor, camVer;

@@ -205,7 +205,7 @@ __device__ __forceinline__ void grid_dir(const TrackParams &P, float wdx, float 
 __device__ __forceinline__ uint32_t primary_ray(const TrackParams &P, int px, int py, uint32_t frame, int s, float &wdx,
                                                 float &wdy, float &wdz) {
   const uint32_t seed = (uint32_t)P.W * (uint32_t)P.H * (frame + 1u) * (uint32_t)(s + 1);
-  uint32_t rng = tea4((uint32_t)px + seed, (uint32_t)py + seed);
+  uint32_t rng = tea4(((uint32_t)px & P.seedMask) + seed, ((uint32_t)py & P.seedMask) + seed);
   const float jit = rng_next(rng);
   const float sxf = ((float)px + jit) / (float)P.W;
   const float syf = ((float)py + jit) / (float)P.H;
@@ -342,7 +342,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
         loy = fmaf(tHitW, wdy, P.camOrg.y);
         loz = fmaf(tHitW, wdz, P.camOrg.z);
         const uint32_t sseed = (uint32_t)P.W * (uint32_t)P.H * pathFrame;
-        rng = tea4((pxy & 0xffffu) + sseed + 1u, (pxy >> 16) + sseed + 1u);
+        rng = tea4((pxy & 0xffffu & P.seedMask) + sseed + 1u, ((pxy >> 16) & P.seedMask) + sseed + 1u);
         if (start_leg(-P.lightDir.x, -P.lightDir.y, -P.lightDir.z)) return;
         record = 0u;
         capped = false;

@@ -78,7 +78,10 @@ class BandRenderer:
         """Re-split the frame from this rank's last render time (every rank calls this with
         its own time): the times are all-gathered, each spread evenly over its band's rows
         into the per-row cost estimate, and the bands re-cut at equal shares of it.  The
-        next `render` uses the new band.  Returns the bands."""
+        next `render` uses the new band.  When the bands move, each rank takes over the
+        accumulation buffer of the rows it gains (the running mean continues there: the
+        whole buffer is all-gathered once and each rank loads its new rows).  Returns the
+        bands."""
         import torch
         import torch.distributed as dist
         dev = "cuda" if self._on_gpu() else "cpu"
@@ -92,7 +95,16 @@ class BandRenderer:
         # rows never measured keep their old estimate; no row is free
         floor = 1e-3 * float(self.cost.mean()) if self.cost.mean() > 0 else 1.0
         self.cost = np.maximum(self.cost, floor)
-        self.bands = split_by_cost(self.cost, self.world)
+        bands = split_by_cost(self.cost, self.world)
+        if bands != self.bands:
+            whole = self.gather_accum()   # the old bands' rows, on every rank
+            lo, hi = bands[self.rank]
+            if hi > lo:
+                rows = whole[lo:hi].contiguous()
+                self.r.loadFrameRows(lo, hi, rows.data_ptr(), None)
+                if self._on_gpu():
+                    self.r.sync()
+            self.bands = bands
         self.lo, self.hi = self.bands[self.rank]
         return list(self.bands)
 

@@ -222,6 +222,11 @@ class Renderer:
     def setMirror(self, enable: bool):
         self._call("set_mirror", C.c_int(1 if enable else 0))
 
+    def setSeedBlock(self, edge: int):
+        """Seed the generator from the pixel (0) or from its position in an edge x edge
+        thread block, the reference's threadIdx under such a launch (deviceCode.cu:297)."""
+        self._call("set_seed_block", C.c_int(edge))
+
     # ---------------------------------------------------------------- frames
     def Render(self, stream: Optional[int] = None):
         """Renderer::Render (renderer.cpp:944-973); asynchronous on ``stream``."""
@@ -370,6 +375,13 @@ class Renderer:
         """Copy rows [row0, row1) of the accumulation / RGBA8 buffers to raw (device or
         host) pointers."""
         self._call("copy_frame_rows", C.c_int(row0), C.c_int(row1), C.c_void_p(accum_ptr), C.c_void_p(fb_ptr),
+                   C.c_void_p(stream) if stream else None)
+
+    def loadFrameRows(self, row0: int, row1: int, accum_ptr: Optional[int], fb_ptr: Optional[int],
+                      stream: Optional[int] = None):
+        """Write rows [row0, row1) of the accumulation / RGBA8 buffers from raw (device or
+        host) pointers: the inverse of copyFrameRows."""
+        self._call("load_frame_rows", C.c_int(row0), C.c_int(row1), C.c_void_p(accum_ptr), C.c_void_p(fb_ptr),
                    C.c_void_p(stream) if stream else None)
 
     def setTiming(self, enable: bool = True):

@@ -240,6 +240,7 @@ struct Oracle {
   V3 lightDir = {0.0001f, -1.f, 0.0001f};
   float lightIntensity = 1.0f, ambient = 0.1f;
   bool mirror = false;
+  uint32_t seedMask = 0xffffffffu;   // orc_set_seed_block
   Camera cam;
   V3 cOrg{}, cLlc{}, cHor{}, cVer{};
   int frameID = 0, accumID = 0, frameParam = 0, accumParam = 0;
@@ -950,7 +951,7 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
   for (int sampleID = 0; sampleID < o.spp; sampleID++) {
     uint32_t seed = (uint32_t)o.W * (uint32_t)o.H * (uint32_t)(o.frameParam + 1) * (uint32_t)(sampleID + 1);
     Rng rng;
-    rng.init((uint32_t)px + seed, (uint32_t)py + seed);
+    rng.init(((uint32_t)px & o.seedMask) + seed, ((uint32_t)py & o.seedMask) + seed);
     float jit = rng.next();
     const float sx = ((float)px + jit) / (float)o.W;
     const float sy = ((float)py + jit) / (float)o.H;
@@ -1020,7 +1021,7 @@ static void render_pixel(Oracle &o, int px, int py, uint64_t cnt[4], uint64_t &c
         sh.t0 = 0.f;
         sh.t1 = 1e20f;
         const uint32_t sseed = (uint32_t)o.W * (uint32_t)o.H * (uint32_t)o.frameParam;
-        sh.rng.init((uint32_t)px + sseed + 1u, (uint32_t)py + sseed + 1u);
+        sh.rng.init(((uint32_t)px & o.seedMask) + sseed + 1u, ((uint32_t)py & o.seedMask) + sseed + 1u);
         sh.steps = 0;
         sh.capped = false;
         V3 so;
@@ -1405,6 +1406,14 @@ int orc_set_material(Oracle *o, int c, float di, float sp, float shin, float gs,
   return ORC_OK;
 }
 int orc_set_mirror(Oracle *o, int e) { o->mirror = e != 0; return ORC_OK; }
+// The reference seeds from threadIdx (deviceCode.cu:296-297, 385-386): 0 = the pixel's
+// coordinates, a power of two = the pixel's position in an edge x edge thread block.
+int orc_set_seed_block(Oracle *o, int edge) {
+  if (edge == 0) { o->seedMask = 0xffffffffu; return ORC_OK; }
+  if (edge < 1 || edge > 1024 || (edge & (edge - 1)) != 0) { o->err = "bad seed block"; return ORC_BAD; }
+  o->seedMask = (uint32_t)edge - 1u;
+  return ORC_OK;
+}
 int orc_enable_pixel_stats(Oracle *o, int e) {
   o->statsOn = e != 0;
   if (o->statsOn) o->stats.assign(4 * (size_t)o->W * o->H, 0u);
@@ -1456,6 +1465,15 @@ int orc_render_row_stride(Oracle *o, int row0, int stride) {
   return render_row_set(o, row0, stride, (o->H - 1 - row0) / stride + 1);
 }
 int orc_render(Oracle *o) { return orc_render_rows(o, 0, 0); }
+// Rows [row0, row1) of the accumulation and RGBA8 buffers from caller memory (the row-band
+// hand-over of mdwt_load_frame_rows; the stream argument is ignored on the host).
+int orc_load_frame_rows(Oracle *o, int row0, int row1, const float *accum, const uint32_t *fb, void * /*stream*/) {
+  if (row0 < 0 || row1 > o->H || row0 > row1) return ORC_BAD;
+  const size_t off = (size_t)row0 * o->W, n = (size_t)(row1 - row0) * o->W;
+  if (accum) std::memcpy(o->accumBuf.data() + 4 * off, accum, n * 16);
+  if (fb) std::memcpy(o->fb.data() + off, fb, n * 4);
+  return ORC_OK;
+}
 int orc_set_features(Oracle *o, int e) { o->featOn = e != 0; return ORC_OK; }
 int orc_get_features(Oracle *o, float *out) {
   if (!o->featOn || o->feat.empty()) return ORC_STATE;

@@ -72,6 +72,7 @@ thread_local TraceState g_trace;
 thread_local owl::vec2i g_launchIndex;
 owl::vec2i g_launchDims;
 MacrocellData g_rootData;   // the root macrocell's program data
+unsigned g_seedMask = 0xffffffffu;   // threadIdx = launch index & g_seedMask
 box4f g_rootBox;
 
 // renderer.cpp:671-685
@@ -160,6 +161,10 @@ struct RefScene {
   float lightDir[3], lightIntensity, ambient, bg[3];
 };
 
+// threadIdx for the launches that follow: the launch index (edge 0), or its position in an
+// edge x edge thread block (edge a power of two).
+void ref_set_seed_block(int edge) { g_seedMask = edge > 0 ? (unsigned)edge - 1u : 0xffffffffu; }
+
 // One launch of mainRG (owlLaunch2D(rayGen, W, H), renderer.cpp:949) with frameID and
 // accumID as the launch parameters, over the rows row0, row0 + stride, ... of the frame.
 // accum (W*H float4) is read and written, fb (W*H RGBA8) written, for those rows.
@@ -224,11 +229,11 @@ int ref_mainrg_frame(const RefScene *s, int frameID, int accumID, float *accum, 
 #pragma omp parallel for schedule(dynamic, 8)
   for (int64_t i = 0; i < n; i++) {
     const int x = (int)(i % s->W), y = row0 + stride * (int)(i / s->W);
-    // the project seeds from the pixel (the reference's threadIdx under OptiX is not a
-    // function of the pixel): threadIdx = launch index
+    // the reference's threadIdx under OptiX is not a function of the pixel: the launch
+    // index stands for it, or (ref_set_seed_block) the pixel's position in a thread block
     g_launchIndex = owl::vec2i(x, y);
-    threadIdx.x = (unsigned)x;
-    threadIdx.y = (unsigned)y;
+    threadIdx.x = (unsigned)x & g_seedMask;
+    threadIdx.y = (unsigned)y & g_seedMask;
     threadIdx.z = 0;
     __raygen__mainRG();
   }

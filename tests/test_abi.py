@@ -109,6 +109,15 @@ def test_gpu_absent_is_an_error_not_a_fallback():
     assert e.value.status == 2
 
 
+def test_seed_block_accepts_powers_of_two_only():
+    r = Renderer(MDWT_HOST_ONLY)
+    for edge in (0, 1, 16, 1024):
+        r.setSeedBlock(edge)
+    for edge in (-1, 3, 12, 2048):
+        with pytest.raises(MdwtError):
+            r.setSeedBlock(edge)
+
+
 def test_tuning_knobs_read_back():
     r = Renderer(MDWT_HOST_ONLY)
     # pool, batch, trips, quorum, regroup (off by default without -m 2), regrouped-tracker blocks

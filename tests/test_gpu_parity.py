@@ -324,3 +324,26 @@ def test_render_frames_equals_successive_renders(oracle, mode, extra):
     o.RenderFrames(4)
     assert_same_frame(p, o, "no accumulation")
     np.testing.assert_array_equal(p.counters(), o.counters())
+
+
+@pytest.mark.parametrize("mode", [0, 2, 3])
+@pytest.mark.parametrize("shadows", [False, True])
+def test_thread_block_seeding(oracle, mode, shadows):
+    """Seed words from the pixel's position in a 16 x 16 thread block (mdwt_set_seed_block,
+    the reference's threadIdx seeding, deviceCode.cu:296-297, 385-386), with and without
+    shadow rays, on both trackers, bit for bit; pixels 16 apart share their streams."""
+    vols = [noise_u8(40, occ, 60 + i) for i, occ in enumerate([0.2, 0.3])]
+    tfs = [syn.ramp_tf(syn.HUES[i], alpha_max=0.9) for i in range(2)]
+    p, o = make_pair(oracle, vols, tfs, mode, (5, 5, 5), (50, 38), 3)
+    for r in (p, o):
+        r.setSeedBlock(16)
+        if shadows:
+            _shade(r, True, False, (0.35, -0.8, 0.25), 2)
+    run_frames(p, o, 2)
+    # per-pixel seeding gives another frame
+    q, _ = make_pair(oracle, vols, tfs, mode, (5, 5, 5), (50, 38), 3)
+    if shadows:
+        _shade(q, True, False, (0.35, -0.8, 0.25), 2)
+    q.Render()
+    q.Render()
+    assert not np.array_equal(q.accum(), p.accum())

@@ -45,6 +45,7 @@ def ref():
     if r.returncode != 0 and not os.path.exists(REF_LIB):
         pytest.skip("the reference sources are not available to build oracle/_ref")
     lib = C.CDLL(REF_LIB)
+    lib.ref_set_seed_block.argtypes = [C.c_int]
     lib.ref_mainrg_frame.restype = C.c_int
     lib.ref_mainrg_frame.argtypes = [C.POINTER(RefScene), C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                      C.c_int, C.c_int]
@@ -199,6 +200,22 @@ def test_shadows_and_gradient_shading(oracle, ref, mode):
     o = setup(oracle, vols, tfs, mode, (4, 4, 4), (40, 32), 2, light=(True, True, (0.3, -1.0, 0.2), 1.2, 0.15),
               mats=[(0.8, 0.4, 16.0, 0.01, (1.0, 0.9, 0.8)), (0.6, 0.2, 4.0, 0.02, (0.7, 0.8, 1.0))])
     assert_pinned(ref, o)
+
+
+@pytest.mark.parametrize("mode", [0, 2])
+def test_thread_block_seeding(oracle, ref, mode):
+    """With 16 x 16 thread-block seeding (mdwt_set_seed_block), the reference's own
+    LCG<4>(threadIdx.x + seed, threadIdx.y + seed) and shadow-ray seeding (deviceCode.cu:
+    296-297, 385-386) run with threadIdx = the pixel's position in its block."""
+    vols = [noise_u8(32, 0.3, 85), noise_u8(32, 0.25, 86)]
+    tfs = [syn.ramp_tf(syn.HUES[i]) for i in range(2)]
+    o = setup(oracle, vols, tfs, mode, (4, 4, 4), (40, 34), 2, light=(True, False, (0.3, -1.0, 0.2), 1.2, 0.15))
+    o.setSeedBlock(16)
+    ref.ref_set_seed_block(16)
+    try:
+        assert_pinned(ref, o)
+    finally:
+        ref.ref_set_seed_block(0)
 
 
 def test_accumulation_off_and_frame_ids(oracle, ref):
