@@ -776,7 +776,7 @@ mdwt_status mdwt_init(mdwt_ctx *c, int mode, int auto_camera) {
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
-  CK(cudaMalloc(&c->dCellTab, c->M * cell_tab_stride(mode >= 3 ? 1 : C) * sizeof(float2)), "cudaMalloc cell table");
+  CK(cudaMalloc(&c->dCellTab, c->M * ((mode >= 3 ? 1 : C) + 1) * sizeof(float2)), "cudaMalloc cell table");
   c->inited = true;
   mdwt_status s = build_ranges(c);
   if (s) { c->inited = false; return s; }
@@ -1011,7 +1011,7 @@ static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   p.dt = c->dt;
   p.majorants = c->dMaj;
   p.cellTab = c->dCellTab;
-  p.tabStride = cell_tab_stride(c->mode >= 3 ? 1 : p.C);
+  p.tabStride = (c->mode >= 3 ? 1 : p.C) + 1;
   for (int i = 0; i < p.C; i++) {
     p.vol[i] = c->ch[i].dVol;
     for (int a = 0; a < 3; a++) p.dims[i][a] = (int)c->ch[i].dims[a];
@@ -1280,7 +1280,7 @@ static mdwt_status regrid(mdwt_ctx *c) {
   const int C = (int)c->ch.size();
   CK(cudaMalloc(&c->dRanges, c->M * C * 8), "cudaMalloc ranges");
   CK(cudaMalloc(&c->dMaj, c->M * (c->mode >= 3 ? 1 : C) * 4), "cudaMalloc majorants");
-  CK(cudaMalloc(&c->dCellTab, c->M * cell_tab_stride(c->mode >= 3 ? 1 : C) * sizeof(float2)), "cudaMalloc cell table");
+  CK(cudaMalloc(&c->dCellTab, c->M * ((c->mode >= 3 ? 1 : C) + 1) * sizeof(float2)), "cudaMalloc cell table");
   mdwt_status s = build_ranges(c);
   if (s) return s;
   s = recalc(c);

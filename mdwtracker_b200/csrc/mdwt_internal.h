@@ -50,12 +50,10 @@ struct TrackParams {
   int C, mode;
   float dt;
   const float *majorants;      // [cell*C + ch] (modes 0..2) or [cell] (mode 3)
-  // The trackers' per-cell table, tabStride = cell_tab_stride(Ce) float2 per cell (Ce = C,
-  // or 1 for the summed majorant; an even count, so every cell starts 16-byte aligned): a
-  // 16-byte header -- the cell's non-zero-majorant channel mask (as bits in .x), then the
-  // majorant and recip_for_div of its first such channel -- and at 2 + c the majorant of
-  // channel c and its reciprocal.  A cell's mask and first majorant come in one load, any
-  // other majorant with its reciprocal in one more.
+  // The trackers' per-cell table, tabStride = Ce + 1 float2 per cell (Ce = C, or 1 for the
+  // summed majorant): entry 0 holds the cell's non-zero-majorant channel mask (as bits in
+  // .x), entry 1 + c the majorant of channel c and its recip_for_div -- the mask and the
+  // first majorants share a sector, and a majorant comes with its reciprocal in one load.
   const float2 *cellTab;
   int tabStride;
   // channels
@@ -177,11 +175,6 @@ struct MajorantParams {
   float os[kMaxChannels];
 };
 int launch_majorants(const MajorantParams &p, void *stream, int *launches);
-// float2 entries per cell of the trackers' cell table for Ce majorants per cell.
-#ifdef __CUDACC__
-__host__ __device__
-#endif
-inline int cell_tab_stride(int Ce) { return (2 + Ce + 1) & ~1; }
 // Float32 voxels, x fastest, into the micro-brick layout of kStoreF32 (dst holds
 // 8 ceil(X/2) ceil(Y/2) ceil(Z/2) floats; the padding voxels are written as 0).
 int launch_brick_f32(const float *src, float *dst, const int dims[3], void *stream, int *launches);

@@ -130,31 +130,20 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
       }
       p.majorants[cell] = sum;
       if (p.cellTab) {
-        float2 *tab = p.cellTab + cell * (size_t)cell_tab_stride(1);
-        const float2 pr = make_float2(sum, recip_for_div(sum));
-        tab[0] = make_float2(__uint_as_float(sum != 0.0f ? 1u : 0u), 0.0f);
-        tab[1] = sum != 0.0f ? pr : make_float2(0.0f, 0.0f);
-        tab[2] = pr;
+        p.cellTab[cell * 2] = make_float2(__uint_as_float(sum != 0.0f ? 1u : 0u), 0.0f);
+        p.cellTab[cell * 2 + 1] = make_float2(sum, recip_for_div(sum));
       }
     } else {
       uint32_t m = 0;
-      float2 *tab = p.cellTab ? p.cellTab + cell * (size_t)cell_tab_stride(C) : nullptr;
-      float2 first = make_float2(0.0f, 0.0f);
+      float2 *tab = p.cellTab ? p.cellTab + cell * (C + 1) : nullptr;
       for (int c = 0; c < C; c++) {
         const float2 rc = r[c];
         const float v = channel_majorant(p, c, rc.x, rc.y);
         p.majorants[cell * C + c] = v;
-        const float2 pr = make_float2(v, recip_for_div(v));
-        if (tab) tab[2 + c] = pr;
-        if (v != 0.0f) {
-          if (m == 0u) first = pr;
-          m |= 1u << c;
-        }
+        if (tab) tab[1 + c] = make_float2(v, recip_for_div(v));
+        if (v != 0.0f) m |= 1u << c;
       }
-      if (tab) {
-        tab[0] = make_float2(__uint_as_float(m), 0.0f);
-        tab[1] = first;
-      }
+      if (tab) tab[0] = make_float2(__uint_as_float(m), 0.0f);
     }
   }
 }

@@ -97,12 +97,7 @@ __device__ __forceinline__ uint32_t cell_mask(const TrackParams &P, int cellID) 
   return __float_as_uint(__ldg(reinterpret_cast<const float *>(P.cellTab + (size_t)cellID * P.tabStride)));
 }
 __device__ __forceinline__ float2 cell_maj(const TrackParams &P, int cellID, int c) {
-  return __ldg(P.cellTab + (size_t)cellID * P.tabStride + 2 + c);
-}
-// The cell's header in one 16-byte load: .x the channel mask (bits), .z/.w the majorant and
-// reciprocal of its first non-zero-majorant channel.
-__device__ __forceinline__ float4 cell_head(const TrackParams &P, int cellID) {
-  return __ldg(reinterpret_cast<const float4 *>(P.cellTab + (size_t)cellID * P.tabStride));
+  return __ldg(P.cellTab + (size_t)cellID * P.tabStride + 1 + c);
 }
 
 // sampleVolumeTexture (deviceCode.cu:122-132): NaN outside [0,1]^3, else trilinear.
@@ -843,8 +838,6 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
   d.visits = visits;
   bool moved = false;
   uint32_t stage = WALK;
-  float2 pn = make_float2(0.0f, 0.0f);   // syncDDA: the majorant pair of channel pnc, loaded ahead
-  int pnc = 16;
   for (int k = 0;;) {
     if (!drawing) {
       bool ended = false;
@@ -882,11 +875,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
         } else {
           if (advance) {
             if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ended = true; break; }
-            // the new cell's header: channel mask and first majorant in one load
-            const float4 hd = cell_head(P, d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1]);
-            cmask = __float_as_uint(hd.x);
-            pn = make_float2(hd.z, hd.w);
-            pnc = cmask ? __ffs(cmask) - 1 : 16;
+            enter(P, d, cmask);
             d.visits++;
             tot[2]++;
             moved = true;
@@ -902,14 +891,9 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
           }
           ch += __ffs(rem) - 1;
           const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-          const float2 mr = ch == pnc ? pn : cell_maj(P, cellID, ch);
+          const float2 mr = cell_maj(P, cellID, ch);
           maj = mr.x;
           rmaj = mr.y;
-          // the cell's next non-zero-majorant channel: its majorant is loaded now and used
-          // when this channel's flights leave the cell
-          const uint32_t rest = ch < 15 ? (cmask >> (ch + 1)) : 0u;
-          pnc = rest ? ch + __ffs(rest) : 16;
-          if (rest) pn = cell_maj(P, cellID, pnc);
           t = d.rt0 + d.ncb;   // the cell's entry distance
           break;
         }
