@@ -218,7 +218,10 @@ mdwt_status forward(mdwt_denoiser *d, const float *F, int N, int H, int W, void 
 // dx (optional) = data gradient
 mdwt_status layer_bwd(mdwt_denoiser *d, const Layer &l, const void *x, const void *dy, void *dx, int N, int H, int W,
                       void *st) {
-  DCKI(mdwt::nn::conv3x3_wgrad(x, dy, l.gW, N, H, W, l.cin, l.cout, st), "weight gradient");
+  if (d->useTC && mdwt::nn::conv3x3_wgrad_tc_supported(l.cin, l.cout))
+    DCKI(mdwt::nn::conv3x3_wgrad_tc(x, dy, l.gW, N, H, W, l.cin, l.cout, d->dErr, st), "weight gradient (tcgen05)");
+  else
+    DCKI(mdwt::nn::conv3x3_wgrad(x, dy, l.gW, N, H, W, l.cin, l.cout, st), "weight gradient");
   DCKI(mdwt::nn::bias_grad(dy, l.gb, (size_t)N * H * W, l.cout, d->numSMs, st), "bias gradient");
   if (dx) {
     const int li = (int)(&l - d->L);

@@ -55,6 +55,12 @@ void conv3x3_tc_policy(int policy);
 // Test hook: the next `launches` tensor-core convolutions issue no input loads, so their
 // bounded waits give up and set *err (0 = off).
 void conv3x3_tc_stall_test(int launches);
+// Weight gradient on the tensor cores (tcgen05, MN-major operands from NHWC by TMA):
+// dW[tap][co][ci] += sum_p dY[p][co] X[p + tap][ci], the same contract as conv3x3_wgrad.
+// Supported for Cout in 8..128 (multiples of 8) and Cin with a chunk of 16, 32 or 48.
+bool conv3x3_wgrad_tc_supported(int Cin, int Cout);
+int conv3x3_wgrad_tc(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin, int Cout, int *err,
+                     void *stream);
 int umma_weights(const void *Wf, void *Wu, int Cin, int Cout, int numSMs, void *stream);
 // Residual output fused into the epilogue (the denoiser's last layer, inference): instead of
 // storing Y, out4[n][y][x] = (F[n][y][x][0..2] + conv[0..2], 1) for y < H, x < W (F has 16

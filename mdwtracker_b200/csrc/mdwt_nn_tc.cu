@@ -558,6 +558,187 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
   }
 }
 
+// ------------------------------------------------------------------ weight gradient
+// dW[tap][co][ci] += sum over pixels p of dY[p][co] X[p + tap][ci] (tap = 3 dy + dx) on the
+// tensor cores: per input-channel chunk g of KN channels, a GEMM D_tap[co][ci] with M = 128
+// output channels (rows beyond Cout are discarded), N = KN, K = pixels, accumulated in
+// tensor memory over the CTA's tiles for all nine taps at once (9 KN <= 432 columns).
+//   A = dY of one image row segment (128 pixels), B = X of the three rows y - 1 .. y + 1
+//   with a one-pixel halo; both are NHWC in global memory, so the TMA boxes (8 channels x
+//   pixels) land as MN-major core matrices (8 pixels x 8 channels, 128 contiguous bytes):
+//   the K (pixel) direction steps 128 B, the M / N (channel group) direction a group.
+//   Tap (dy, dx) of output pixel p reads staged row dy, pixel p + dx.
+//   CTA b takes chunk b mod NG and the row segments of its slice; the epilogue adds its
+//   nine accumulators into dW with atomics.
+constexpr int kWgEpiWarps = 4;
+constexpr int kWgThreads = 32 * (2 + kWgEpiWarps);   // producer, MMA issuer, epilogue
+constexpr uint32_t kWgDyGroup = kTM * 16;            // 8 channels of a 128-pixel row segment: 2048 B
+constexpr uint32_t kWgXBox = 3 * kRowBytes;          // 8 channels of three 130-pixel rows: 6240 B
+constexpr uint32_t kWgXGroup = (kWgXBox + 127u) & ~127u;   // its slot: TMA destinations are 128-byte aligned
+constexpr int kWgMaxStages = 4;
+
+struct WgradArgs {
+  float *dW;
+  int *err;
+  int N, H, W, Cin, Cout, KN, NG, SA, tilesX, tiles;
+};
+
+// one stage: 16 dY channel groups (M = 128; those at and beyond Cout stay zero) and the
+// chunk's KN / 8 X channel groups, every group 128-byte aligned
+__host__ __device__ inline uint32_t wg_stage_bytes(int KN) {
+  return 16u * kWgDyGroup + (uint32_t)(KN / 8) * kWgXGroup;
+}
+
+// One MMA with its own high descriptor word for each operand (their strides differ).
+__device__ __forceinline__ void umma_f16_ab(uint32_t dtmem, uint32_t alo, uint32_t ahi, uint32_t blo, uint32_t bhi,
+                                            uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p, e;\n\t.reg .b64 a, b;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "setp.ne.b32 p, %6, 0;\n\t"
+      "mov.b64 a, {%1, %2};\n\t"
+      "mov.b64 b, {%3, %4};\n\t"
+      "@e tcgen05.mma.cta_group::1.kind::f16 [%0], a, b, %5, p;\n\t}\n" ::"r"(dtmem),
+      "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(idesc), "r"(acc));
+}
+
+__global__ void __launch_bounds__(kWgThreads, 1) conv3x3_wgrad_tc_kernel(const __grid_constant__ CUtensorMap mapDY,
+                                                                         const __grid_constant__ CUtensorMap mapX,
+                                                                         const WgradArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full[kWgMaxStages], empty[kWgMaxStages], done;
+  __shared__ uint32_t tmemBase;
+  __shared__ volatile int abortFlag;
+  uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = (int)blockIdx.x % a.NG, slice = (int)blockIdx.x / a.NG, slices = (int)gridDim.x / a.NG;
+  const uint32_t stB = wg_stage_bytes(a.KN);
+  const int gDy = a.Cout / 8, gX = a.KN / 8;
+  // the dY groups the TMA never writes (channels >= Cout) are zero in every stage
+  for (int st = 0; st < a.SA; st++)
+    for (uint32_t i = (uint32_t)gDy * kWgDyGroup / 16u + threadIdx.x; i < 16u * kWgDyGroup / 16u; i += kWgThreads)
+      reinterpret_cast<uint4 *>(smem + (size_t)st * stB)[i] = make_uint4(0u, 0u, 0u, 0u);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < a.SA; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(&done, 1);
+    abortFlag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmemBase)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // the zeroed groups, for the tensor cores
+  asm volatile("tcgen05.fence::before_thread_sync;\n");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n");
+  const uint32_t tmem = tmemBase;
+  auto fail = [&]() {
+    abortFlag = 1;
+    atomicExch(a.err, 1);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------------------------------------------------------- producer
+      bool ok = true;
+      uint32_t it = 0;
+      for (int t = slice; t < a.tiles && ok; t += slices, it++) {
+        if (abortFlag) break;
+        const uint32_t s = it % (uint32_t)a.SA, use = it / (uint32_t)a.SA;
+        if (use > 0 && !mbar_wait_ab(&empty[s], (use - 1) & 1u, &abortFlag)) { ok = false; break; }
+        const int tx = t % a.tilesX, y = (t / a.tilesX) % a.H, n = t / (a.tilesX * a.H);
+        const int x0 = tx * kTM;
+        uint8_t *st = smem + (size_t)s * stB;
+        if ((smem_u32(st) & 127u) != 0u) { ok = false; break; }   // every slot below is then 128-byte aligned
+        mbar_expect_tx(&full[s], (uint32_t)gDy * kWgDyGroup + (uint32_t)gX * kWgXBox);
+        for (int q = 0; q < gDy; q++) tma_load_4d(st + q * kWgDyGroup, &mapDY, 8 * q, x0, y, n, &full[s]);
+        for (int h = 0; h < gX; h++)
+          tma_load_4d(st + 16 * kWgDyGroup + h * kWgXGroup, &mapX, g * a.KN + 8 * h, x0 - 1, y - 1, n, &full[s]);
+      }
+      if (!ok) fail();
+      // wait for every load issued (the last one into each stage may still be in flight)
+      for (uint32_t st = 0; st < (uint32_t)a.SA; st++)
+        if (it > st && !mbar_wait(&full[st], ((it - 1 - st) / (uint32_t)a.SA) & 1u)) fail();
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------------------------ MMA issuer
+    auto warpWait = [&](uint64_t *bar, uint32_t parity) -> bool {
+      int okw = 0;
+      if (lane == 0) okw = mbar_wait_ab(bar, parity, &abortFlag) ? 1 : 0;
+      return __shfl_sync(0xffffffffu, okw, 0) != 0;
+    };
+    // both operands MN-major (instruction descriptor bits 15 and 16); leading (K) byte
+    // offset 128, stride (M / N) byte offsets one channel group
+    const uint32_t idesc = instr_desc(kTM, a.KN) | (1u << 15) | (1u << 16);
+    const uint32_t aHi = smem_desc_hi(kWgDyGroup), bHi = smem_desc_hi(kWgXGroup);
+    const uint32_t aLo0 = smem_desc_lo(smem_u32(smem), 128), bLo0 = smem_desc_lo(smem_u32(smem + 16 * kWgDyGroup), 128);
+    const uint32_t stU = stB >> 4;
+    bool ok = true;
+    uint32_t it = 0;
+    for (int t = slice; t < a.tiles && ok; t += slices, it++) {
+      const uint32_t s = it % (uint32_t)a.SA;
+      if (!warpWait(&full[s], (it / (uint32_t)a.SA) & 1u)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;\n");
+      const uint32_t aSt = aLo0 + s * stU, bSt = bLo0 + s * stU;
+      for (int k = 0; k < kTM / 16; k++) {
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+          const uint32_t dy = (uint32_t)(tap / 3), dx = (uint32_t)(tap % 3);
+          umma_f16_ab(tmem + (uint32_t)(tap * a.KN), aSt + 16u * (uint32_t)k, aHi,
+                      bSt + dy * (kRowBytes >> 4) + 16u * (uint32_t)k + dx, bHi, idesc, (it > 0 || k > 0) ? 1u : 0u);
+        }
+      }
+      if (lane == 0) umma_commit(&empty[s]);
+      __syncwarp();
+    }
+    if (lane == 0) {
+      if (!ok) fail();
+      umma_commit(&done);   // every MMA issued by this warp has completed
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------------ epilogue
+    int go = 1;
+    if (lane == 0) go = mbar_wait_ab(&done, 0, &abortFlag) ? 1 : 0;
+    go = __shfl_sync(0xffffffffu, go, 0);
+    if (go && !abortFlag && slice < a.tiles) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n");
+      const int qd = warp & 3, co = qd * 32 + lane;
+      const uint32_t tBase = tmem + ((uint32_t)(qd * 32) << 16);
+      for (int tap = 0; tap < 9; tap++)
+        for (int c0 = 0; c0 < a.KN; c0 += 16) {
+          uint32_t v32[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+              : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
+                "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]),
+                "=r"(v32[14]), "=r"(v32[15])
+              : "r"(tBase + (uint32_t)(tap * a.KN + c0)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          if (co < a.Cout) {
+            float *d = a.dW + ((size_t)tap * a.Cout + co) * a.Cin + (size_t)g * a.KN + c0;
+#pragma unroll
+            for (int j = 0; j < 16; j++) atomicAdd(d + j, __uint_as_float(v32[j]));
+          }
+        }
+    } else if (!go && lane == 0) {
+      fail();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
+  }
+}
+
 // weights [tap][co][ci] (forward layout, tap = 3 dy + dx) -> operand layout
 // [dx][ci / 8][dy][co][8]: for one horizontal tap and 8 input channels the three vertical
 // taps' Cout rows are contiguous, so one MMA can take all three (N = 3 Cout)
@@ -716,6 +897,55 @@ bool conv3x3_tc_supported(int Cin, int Cout) {
 }
 
 void conv3x3_tc_stall_test(int launches) { g_tcStall = launches > 0 ? launches : 0; }
+
+// The weight gradient's input-channel chunk: the largest divisor of Cin that is a multiple
+// of 16 and at most 48 (nine taps' accumulators then fit the 512 TMEM columns); 0 if none.
+int wgrad_tc_chunk(int Cin) {
+  for (int kn = 48; kn >= 16; kn -= 16)
+    if (Cin % kn == 0) return kn;
+  return 0;
+}
+
+bool conv3x3_wgrad_tc_supported(int Cin, int Cout) {
+  return Cout % 8 == 0 && Cout >= 8 && Cout <= 128 && wgrad_tc_chunk(Cin) > 0 && encode_fn() != nullptr;
+}
+
+int conv3x3_wgrad_tc(const void *X, const void *dY, float *dW, int N, int H, int W, int Cin, int Cout, int *err,
+                     void *stream) {
+  if (!conv3x3_wgrad_tc_supported(Cin, Cout) || N <= 0 || H <= 0 || W <= 0 || !err) return (int)cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(dY) & 15)) return (int)cudaErrorInvalidValue;
+  WgradArgs a;
+  a.dW = dW; a.err = err;
+  a.N = N; a.H = H; a.W = W; a.Cin = Cin; a.Cout = Cout;
+  a.KN = wgrad_tc_chunk(Cin);
+  a.NG = Cin / a.KN;
+  const uint32_t stB = wg_stage_bytes(a.KN);
+  a.SA = (int)(kSmemBudget / stB);
+  if (a.SA > kWgMaxStages) a.SA = kWgMaxStages;
+  if (a.SA < 2) return (int)cudaErrorInvalidValue;
+  a.tilesX = (W + kTM - 1) / kTM;
+  a.tiles = N * H * a.tilesX;
+  auto encode = [&](CUtensorMap *m, const void *base, int C, int boxW, int boxH) -> bool {
+    const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)boxW, (cuuint32_t)boxH, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  CUtensorMap mapDY, mapX;
+  if (!encode(&mapDY, dY, Cout, kTM, 1) || !encode(&mapX, X, Cin, kHalo, 3)) return (int)cudaErrorInvalidValue;
+  const size_t smem = (size_t)a.SA * stB + 1024;
+  cudaError_t e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(kSmemBudget + 1024));
+  if (e != cudaSuccess) return (int)e;
+  int slices = num_sms() / a.NG;
+  if (slices > a.tiles) slices = a.tiles;
+  if (slices < 1) slices = 1;
+  conv3x3_wgrad_tc_kernel<<<(unsigned)(slices * a.NG), kWgThreads, smem, (cudaStream_t)stream>>>(mapDY, mapX, a);
+  return (int)cudaGetLastError();
+}
 
 void conv3x3_tc_policy(int policy) { g_tcPolicy = policy == 1 ? 1 : 0; }
 

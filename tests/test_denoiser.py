@@ -144,6 +144,33 @@ def test_tensor_core_and_mma_paths_agree(n, h, w, overlap):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,h,w", [(1, 7, 20), (2, 9, 150), (1, 12, 256)])
+def test_tensor_core_weight_gradients_agree_with_mma_path(n, h, w):
+    """The tcgen05 weight gradient (MN-major operands staged by TMA from the NHWC tensors,
+    the nine taps accumulated in tensor memory) against the mma.sync one, layer by layer:
+    the same BF16 operands and FP32 accumulation in another order (the data gradients
+    feeding the earlier layers differ in rounding the same way)."""
+    import torch
+    from mdwtracker_b200 import Denoiser
+    rng = np.random.default_rng(n * 7 + h * 5 + w)
+    d = Denoiser(0)
+    d.setParams(R.init_params(17))
+    F = torch.from_numpy(_features(rng, n, h, w)).cuda()
+    T = torch.from_numpy(rng.random((n, h, w, 4)).astype(np.float32)).cuda()
+    grads = []
+    for tc in (False, True):
+        d.setTensorCores(tc)
+        d.backward(F, T, n, h, w)
+        d.check()
+        grads.append(d.grads().astype(np.float64))
+    for i, sl in enumerate(_layer_slices()):
+        a, b = grads[1][sl], grads[0][sl]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert rel < 2e-2, (i, rel)
+    d.setTensorCores(True)
+
+
+@pytest.mark.gpu
 def test_autotuned_tilings_agree_with_mma_path():
     """After the tiling autotuner (forward and data gradients), inference and gradients
     still agree with the mma.sync path."""
