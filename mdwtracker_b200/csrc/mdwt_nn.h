@@ -44,10 +44,8 @@ int weight_copies(const float *Wm, void *Wf, void *Wd, int Cin, int Cout, int nu
 // tile overlaps the MMAs of the next), NS weight stages (NS >= 9 x chunks keeps all the
 // weights resident for the launch).
 // ST = 1 stacks the three vertical taps into one MMA (N = 3 Cout; needs 3 Cout <= 256).
-// CT: CTAs per SM (1, or 2 when two fit: at most 110 KB of shared memory and 256 tensor-
-// memory columns each), so that one CTA's MMAs run while the other waits.
 struct TcTiling {
-  int R = 0, KC = 0, NS = 0, SA = 0, AB = 0, ST = 0, CT = 1;
+  int R = 0, KC = 0, NS = 0, SA = 0, AB = 0, ST = 0;
 };
 bool conv3x3_tc_supported(int Cin, int Cout);
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t);

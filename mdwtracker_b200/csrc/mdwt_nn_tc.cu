@@ -778,8 +778,7 @@ int tmem_cols_for(int cols) {
 }
 
 constexpr size_t kSmemBudget = 224 * 1024;     // dynamic shared memory of one CTA (one per SM)
-constexpr size_t kSmemBudget2 = 110 * 1024;    // ... of each of two CTAs per SM
-constexpr size_t kSmemFloor = 120 * 1024;      // requested at least with one CTA per SM: keeps a second off
+constexpr size_t kSmemFloor = 120 * 1024;      // requested at least: keeps a second CTA off the SM
 constexpr size_t kResidentMax = 112 * 1024;    // weights kept resident up to this size
 
 int chunks_of(int Cin, const TcTiling &t) { return t.KC > 0 ? Cin / t.KC : 0; }
@@ -796,14 +795,14 @@ int g_tcPolicy = 1;   // 1: two accumulators (the epilogue overlaps the next til
 
 // Largest input-channel chunk (a divisor of Cin, multiple of 16) that fits the budget with
 // SA input stages and the given weight staging (NS = 0: resident); 0 when none does.
-int fit_kc(int Cin, int Cout, int R, int SA, int NS, int AB, size_t budget = kSmemBudget) {
+int fit_kc(int Cin, int Cout, int R, int SA, int NS, int AB) {
   for (int KC = Cin; KC >= 16; KC -= 16) {
     if (Cin % KC) continue;
     TcTiling t;
     t.R = R; t.KC = KC; t.SA = SA; t.AB = AB;
     t.NS = NS > 0 ? NS : Cin / KC;
     if (Cin / KC > kMaxWStages && NS == 0) continue;
-    if (tc_smem(Cin, Cout, t) <= budget) return KC;
+    if (tc_smem(Cin, Cout, t) <= kSmemBudget) return KC;
   }
   return 0;
 }
@@ -853,8 +852,6 @@ int num_sms() {
 
 bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t) {
   if (t.R < 1 || t.R > 8 || t.R > (H > 0 ? H : 1) || (t.AB != 1 && t.AB != 2) || t.AB * t.R * Cout > 512) return false;
-  if (t.CT != 1 && t.CT != 2) return false;
-  if (t.CT == 2 && (tmem_cols_for(t.AB * t.R * Cout) > 256 || tc_smem(Cin, Cout, t) > kSmemBudget2)) return false;
   if (t.KC < 16 || t.KC % 16 || Cin % t.KC || t.SA < 2 || t.SA > kMaxAStages) return false;
   if (t.ST && 3 * Cout > 256) return false;
   if (resident_of(Cin, t) ? chunks_of(Cin, t) > kMaxWStages : (t.NS < 2 || t.NS > kMaxWStages)) return false;
@@ -866,24 +863,19 @@ bool conv3x3_tc_valid(int Cin, int Cout, int H, const TcTiling &t) {
 // ring of 2 or 3 chunk stages, each with the largest chunk that fits.
 int conv3x3_tc_candidates(int Cin, int Cout, int H, TcTiling *out, int maxOut) {
   int n = 0;
-  auto add1 = [&](int R, int AB, int SA, int NS, int ST, int CT) {
+  auto add = [&](int R, int AB, int SA, int NS, int ST) {
     if (R < 1 || n >= maxOut) return;
-    const int KC = fit_kc(Cin, Cout, R, SA, NS, AB, CT == 2 ? kSmemBudget2 : kSmemBudget);
+    const int KC = fit_kc(Cin, Cout, R, SA, NS, AB);
     if (!KC) return;
     TcTiling t;
-    t.R = R; t.KC = KC; t.SA = SA; t.AB = AB; t.ST = ST; t.CT = CT;
+    t.R = R; t.KC = KC; t.SA = SA; t.AB = AB; t.ST = ST;
     t.NS = NS > 0 ? NS : Cin / KC;
     if (!conv3x3_tc_valid(Cin, Cout, H, t)) return;
     for (int i = 0; i < n; i++)
       if (out[i].R == t.R && out[i].KC == t.KC && out[i].SA == t.SA && out[i].AB == t.AB && out[i].NS == t.NS &&
-          out[i].ST == t.ST && out[i].CT == t.CT)
+          out[i].ST == t.ST)
         return;
     out[n++] = t;
-  };
-  // each tiling with one CTA per SM, and with two where two fit (half the rows)
-  auto add = [&](int R, int AB, int SA, int NS, int ST) {
-    add1(R, AB, SA, NS, ST, 1);
-    add1(R / 2, AB, SA, NS, ST, 2);
   };
   const int h = H > 0 ? H : 1;
   for (int ST = 3 * Cout <= 256 ? 1 : 0; ST >= 0; ST--)
@@ -1013,11 +1005,11 @@ int conv3x3_tc(const void *X, const void *Wu, const float *bias, void *Y, int N,
   a.tilesY = (H + tl.R - 1) / tl.R;
   a.tiles = N * a.tilesX * a.tilesY;
   size_t smem = tc_smem(Cin, Cout, tl) + 1024;
-  if (tl.CT == 1 && smem < kSmemFloor) smem = kSmemFloor;
+  if (smem < kSmemFloor) smem = kSmemFloor;
   cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kSmemBudget + 1024));
   if (e != cudaSuccess) return (int)e;
-  int grid = num_sms() * tl.CT;
+  int grid = num_sms();
   if (grid > a.tiles) grid = a.tiles;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
