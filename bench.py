@@ -82,7 +82,9 @@ def parse_args():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tracker schedule (regrouped tracker, trips 4) instead of tuning it")
     ap.add_argument("--regroup", type=int, choices=[0, 1], default=None,
-                    help="force the -m 2 tracker after tuning: 1 regrouped, 0 warp-local")
+                    help="force the tracker after tuning: 1 regrouped, 0 warp-local")
+    ap.add_argument("--rg-blocks", type=int, choices=[0, 1, 2, 3, 4], default=None,
+                    help="force the regrouped tracker's blocks per SM after tuning (0: as many as fit)")
     ap.add_argument("--batch-requests", type=int, default=64)
     ap.add_argument("--ttr-config", default="c3", choices=["c1", "c2", "c3", "c3ndda"])
     ap.add_argument("--ttr-target", type=float, default=0.01)
@@ -711,8 +713,11 @@ def main():
         r.autotuneSchedule(frames=sc.frames)
     if args.regroup is not None:
         r.setTuning(4, args.regroup)
+    if args.rg_blocks is not None:
+        r.setTuning(5, args.rg_blocks)
     schedule = schedule_of(r, ("default" if args.no_autotune else "mdwt_autotune_schedule") +
-                           ("" if args.regroup is None else f", regroup forced to {args.regroup}"))
+                           ("" if args.regroup is None else f", regroup forced to {args.regroup}") +
+                           ("" if args.rg_blocks is None else f", blocks per SM forced to {args.rg_blocks}"))
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream
     flush = torch.empty(args.flush_mib << 20, dtype=torch.uint8, device=dev)
@@ -823,11 +828,16 @@ def main():
             ttr = time_to_rmse(args.ttr_config, args.ttr_target, local)
         except Exception as ex:  # reported beside the throughput line, never required
             ttr = {"error": str(ex)}
-        # the same measurement on volumes the denoiser never saw in training
+        # the same measurement on volumes the denoiser never saw in training: the 1080p
+        # scene's generator and the uint8 C2 scene's, from another seed
         try:
             ttr["held_out"] = time_to_rmse(args.ttr_config, args.ttr_target, local, seed=HELD_OUT_SEED)
         except Exception as ex:
             ttr["held_out"] = {"error": str(ex)}
+        try:
+            ttr["held_out_c2"] = time_to_rmse("c2", args.ttr_target, local, seed=HELD_OUT_SEED)
+        except Exception as ex:
+            ttr["held_out_c2"] = {"error": str(ex)}
 
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
