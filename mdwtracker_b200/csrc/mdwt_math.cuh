@@ -108,7 +108,7 @@ __device__ __forceinline__ float flight(float t, float u, float maj, float rmaj,
 // certain, decided from the hardware log2 (lg2.approx) instead of the exact chain; a
 // false answer means "run the exact flight".  k = rmaj * dt * w2g * ln 2.
 //   The estimate xf = -log2(1 - u) * k of the flight length differs from the exact chain's
-// length by at most xf * kFlightRel + k * kFlightAbs, where
+// length by at most |xf| * kFlightRel + |k| * kFlightAbs (negative majorants included), where
 //   - mlog's relative error over every 1 - u of the 24-bit draw grid is <= 1.6e-7
 //     (checked exhaustively against a double-precision log on the host),
 //   - lg2.approx's error over the same 2^24 inputs is below 2^-20 * (1 + |log2 x|)
@@ -123,7 +123,7 @@ constexpr float kLn2 = 0.693147182464599609375f;     // RN(ln 2)
 __device__ __forceinline__ bool flight_surely_exits(float t, float u, float k, float lim) {
   const float xf = -__log2f(1.0f - u) * k;
   const float tf = t + xf;
-  const float m = fmaf(xf, kFlightRel, fmaf(k, kFlightAbs, fabsf(tf) * 2.384185791015625e-07f));
+  const float m = fmaf(fabsf(xf), kFlightRel, fmaf(fabsf(k), kFlightAbs, fabsf(tf) * 2.384185791015625e-07f));
   return tf - m >= lim;
 }
 
