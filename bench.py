@@ -26,7 +26,11 @@ the defaults) and reported in config.schedule.
 Extra keys on the same line (rank 0, one GPU): `c2` -- the 3 x 256^3 uint8 syncDDA
 scene at 1024^2 and 64 spp, timed the same way; `edge_sweep` -- the 1080p scene's
 macrocell sweep over edges 4/8/16/32 voxels for syncDDA and N-DDA (--no-sweep skips
-it); `--edge` sets the headline scene's edge.
+it); `--edge` sets the headline scene's edge; `fast_arith` -- the headline scene and C2
+with the fast free-flight arithmetic (mdwt_set_arithmetic: hardware-log2 flight lengths,
+per-pixel events equal to the oracle's on >= 99.9 % of pixels; --no-fast skips it).  The
+headline line itself runs the exact arithmetic (bit-identical to the oracle) unless
+--arith fast.
 
 time_to_rmse (rank 0, one GPU; --no-ttr skips it): the first part of the headline metric
 -- how long plain accumulation takes at 1920x1080 (the 6 x 512^3 float32 log-normal scene,
@@ -85,6 +89,9 @@ def parse_args():
                     help="force the tracker after tuning: 1 regrouped, 0 warp-local")
     ap.add_argument("--rg-blocks", type=int, choices=[0, 1, 2, 3, 4], default=None,
                     help="force the regrouped tracker's blocks per SM after tuning (0: as many as fit)")
+    ap.add_argument("--arith", default="exact", choices=["exact", "fast"],
+                    help="free-flight arithmetic of the headline line (exact: bit-identical to the oracle)")
+    ap.add_argument("--no-fast", action="store_true", help="skip the extra fast-arithmetic lines")
     ap.add_argument("--batch-requests", type=int, default=64)
     ap.add_argument("--ttr-config", default="c3", choices=["c1", "c2", "c3", "c3ndda"])
     ap.add_argument("--ttr-target", type=float, default=0.01)
@@ -656,6 +663,27 @@ def extra_c2(args, local, flush, stream, peak):
     return out
 
 
+def extra_fast(args, local, flush, stream, peak):
+    """The headline scene and the C2 scene with the fast free-flight arithmetic
+    (mdwt_set_arithmetic: hardware-log2 flight lengths; per-pixel events match the oracle
+    on >= 99.9 % of pixels, tested), tuned and timed like the headline line."""
+    from mdwtracker_b200 import Renderer
+    out = {}
+    for name in dict.fromkeys((args.config, "c2")):
+        sc = make_scene(name, args.res if name == args.config else None, args.spp if name == args.config else None,
+                        args.edge if name == args.config else 16)
+        r = sc.setup(Renderer(local))
+        r.setArithmetic(True)
+        if not args.no_autotune:
+            r.autotuneSchedule(frames=sc.frames)
+        t = timed_frames(r, sc, args.steps, args.warmup, flush, stream)
+        row = throughput_summary(sc, t, peak)
+        row["schedule"] = schedule_of(r, "default" if args.no_autotune else "mdwt_autotune_schedule")
+        out[name] = row
+        r.close()
+    return out
+
+
 def edge_sweep(args, local, flush, stream, peak, edges=(4, 8, 16, 32), steps=3):
     """The 1080p scene (6 x 512^3 float32, 256 spp) over macrocell edges of 4/8/16/32
     voxels, syncDDA and N-DDA: the grid is rebuilt on the same context (mdwt_set_macrocells
@@ -706,6 +734,8 @@ def main():
 
     sc = make_scene(args.config, args.res, args.spp, args.edge)
     r = sc.setup(Renderer(local))
+    if args.arith == "fast":
+        r.setArithmetic(True)
     w, h = sc.resolution
     # the tracker schedule is tuned for the workload first (outside the timed region), on
     # launches of the step's shape
@@ -816,6 +846,11 @@ def main():
                 extras["c2"] = extra_c2(args, local, flush, stream, peak)
             except Exception as ex:  # reported beside the throughput line, never required
                 extras["c2"] = {"error": str(ex)}
+        if not args.no_fast and args.arith == "exact":
+            try:
+                extras["fast_arith"] = extra_fast(args, local, flush, stream, peak)
+            except Exception as ex:
+                extras["fast_arith"] = {"error": str(ex)}
         if not args.no_sweep and args.config in ("c3", "c3ndda"):
             try:
                 extras["edge_sweep"] = edge_sweep(args, local, flush, stream, peak)
@@ -863,7 +898,7 @@ def main():
         "data": "synthetic (seeded generators in mdwtracker_b200/synthetic.py)",
         "config": dict(scene_config(sc, l2note, (f"row bands x{world}, NCCL all_gather of the RGBA8 frame" if split
                                                  else f"replicas x{world}") if world > 1 else "single GPU"),
-                       schedule=schedule),
+                       schedule=schedule, arithmetic=args.arith),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profiled_traffic(tracker, workload_name(sc)),
                      "peak_source": peak_kind, "kernel": tracker,

@@ -162,6 +162,27 @@ mdwt_status mdwt_set_mirror(mdwt_ctx *ctx, int enable);
  * same position in different blocks then share their generator streams, as they would in
  * that launch.  Other values: MDWT_ERR_BAD_ARG. */
 mdwt_status mdwt_set_seed_block(mdwt_ctx *ctx, int edge);
+/* No reference counterpart: the arithmetic of the free flights t - log(1 - u) / majorant
+ * * dt * w2g (deviceCode.cu:564, 676, 739, 805, 913, 1023).
+ * MDWT_ARITH_EXACT (the default): the project's own log and correctly rounded quotients,
+ * the same on the CPU oracle and the GPU, so frames are bit-identical to the oracle's; a
+ * flight that certainly leaves its macrocell is still decided from the hardware log2,
+ * within a proven margin.
+ * MDWT_ARITH_FAST: a flight length is the hardware log2 (lg2.approx) times
+ * dt * w2g * ln 2 / majorant, with no exact chain.  Lengths differ from the exact ones
+ * by a few units in the last place, so a path's events differ only where a flight ends
+ * that close to a cell or volume boundary or a density lands that close to its
+ * acceptance threshold: per-pixel collision events match the oracle on at least 99.9 %
+ * of pixels at equal spp (tested), and converged images match the exact ones within
+ * their noise.  Most flights leave their cell and are settled by the same exit filter
+ * under both arithmetics, so the fast one gains little time (its flights inside a cell
+ * skip the exact chain).
+ * The accumulation is not reset.  After mdwt_init, the call rebuilds the majorant
+ * table (the fast flights use 1 / majorant); other values: MDWT_ERR_BAD_ARG. */
+#define MDWT_ARITH_EXACT 0
+#define MDWT_ARITH_FAST 1
+mdwt_status mdwt_set_arithmetic(mdwt_ctx *ctx, int arith);
+mdwt_status mdwt_get_arithmetic(const mdwt_ctx *ctx, int *arith);
 
 /* ---- frames ------------------------------------------------------------------ */
 

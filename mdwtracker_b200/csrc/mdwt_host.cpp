@@ -130,6 +130,7 @@ struct mdwt_ctx {
   std::vector<TFState> tf;
   bool mirror = false;
   uint32_t seedMask = 0xffffffffu;   // mdwt_set_seed_block: the pixel's coordinates, or its position in a block
+  int arith = MDWT_ARITH_EXACT;      // mdwt_set_arithmetic
   Camera cam;
   V3 cOrg{}, cLlc{}, cHor{}, cVer{};
   int frameID = 0, accumID = 0, frameParam = 0, accumParam = 0;
@@ -509,6 +510,7 @@ mdwt_status recalc(mdwt_ctx *c) {
   p.ranges = c->dRanges;
   p.majorants = c->dMaj;
   p.cellTab = c->dCellTab;
+  p.fast = c->arith == MDWT_ARITH_FAST ? 1 : 0;
   p.C = (int)c->ch.size();
   p.mode = c->mode;
   p.M = c->M;
@@ -972,6 +974,23 @@ mdwt_status mdwt_set_seed_block(mdwt_ctx *c, int edge) {
   return MDWT_OK;
 }
 
+mdwt_status mdwt_set_arithmetic(mdwt_ctx *c, int arith) {
+  if (!c) return MDWT_ERR_BAD_ARG;
+  if (arith != MDWT_ARITH_EXACT && arith != MDWT_ARITH_FAST)
+    return fail(c, MDWT_ERR_BAD_ARG, "arithmetic must be MDWT_ARITH_EXACT or MDWT_ARITH_FAST");
+  if (arith == c->arith) return MDWT_OK;
+  c->arith = arith;
+  if (!c->inited) return MDWT_OK;
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  return recalc(c);   // the cell table's reciprocals follow the arithmetic
+}
+
+mdwt_status mdwt_get_arithmetic(const mdwt_ctx *c, int *arith) {
+  if (!c || !arith) return MDWT_ERR_BAD_ARG;
+  *arith = c->arith;
+  return MDWT_OK;
+}
+
 // Depth-feature scale: 1 / (distance from the camera to the root-box centre + the box
 // diagonal), so that hit distances map into [0, 1].
 static float feature_scale(const mdwt_ctx *c) {
@@ -997,6 +1016,7 @@ static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
   p.accumulate = c->accum ? 1 : 0;
   p.mirror = c->mirror ? 1 : 0;
   p.seedMask = c->seedMask;
+  p.fast = c->arith == MDWT_ARITH_FAST ? 1 : 0;
   p.bg = f3(c->bg);
   p.camOrg = f3(c->cOrg); p.camLlc = f3(c->cLlc); p.camHor = f3(c->cHor); p.camVer = f3(c->cVer);
   p.rootLo = {c->rootLo[0], c->rootLo[1], c->rootLo[2]};

@@ -9,6 +9,11 @@ namespace mdwt {
 
 constexpr int kMaxChannels = 12;          // deviceCode.h:13
 constexpr uint32_t kMaxStepsPerSample = 1u << 22;
+// Margin terms of the free-flight exit filter (flight_surely_exits in mdwt_math.cuh):
+// factors of |xf|, |k| and |tf|.
+constexpr float kFlightRel = 3.814697265625e-06f;   // 2^-18
+constexpr float kFlightAbs = 3.814697265625e-06f;   // 2^-18 (log2 units, times k)
+constexpr float kFlightTf = 2.384185791015625e-07f;  // 2^-22
 
 // Device voxel storage.  uint8 channels stay one byte per voxel (value = b * 255,
 // the exact float the reference's RawR conversion produces, rawFile.cpp:103-105);
@@ -56,6 +61,11 @@ struct TrackParams {
   // first majorants share a sector, and a majorant comes with its reciprocal in one load.
   const float2 *cellTab;
   int tabStride;
+  // Free-flight arithmetic (mdwt_set_arithmetic).  fast = 0: the flights the exit filter
+  // does not settle run the exact chain.  fast = 1: they run the filter's hardware-log2
+  // estimate as the flight itself, and cellTab holds 1 / majorant for every non-zero
+  // majorant.
+  int fast;
   // channels
   const void *vol[kMaxChannels];
   int dims[kMaxChannels][3];
@@ -166,6 +176,7 @@ struct MajorantParams {
   const float *ranges;
   float *majorants;
   float2 *cellTab;             // the trackers' per-cell table (TrackParams::cellTab), or null
+  int fast;                    // TrackParams::fast: the table's reciprocals are 1 / majorant
   int C, mode;
   size_t M;
   const float *tfAlpha[kMaxChannels];

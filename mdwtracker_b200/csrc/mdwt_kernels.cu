@@ -117,6 +117,13 @@ __device__ float channel_majorant(const MajorantParams &p, int c, float mn, floa
   return m;
 }
 
+// The reciprocal the trackers' table holds beside a majorant: recip_for_div for the exact
+// chain's quotients, or 1 / majorant for the fast arithmetic's flights.
+__device__ __forceinline__ float table_recip(const MajorantParams &p, float v) {
+  if (p.fast) return v != 0.0f ? 1.0f / v : 0.0f;
+  return recip_for_div(v);
+}
+
 __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
   const int C = p.C;
   for (size_t cell = (size_t)blockIdx.x * blockDim.x + threadIdx.x; cell < p.M; cell += (size_t)gridDim.x * blockDim.x) {
@@ -131,7 +138,7 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
       p.majorants[cell] = sum;
       if (p.cellTab) {
         p.cellTab[cell * 2] = make_float2(__uint_as_float(sum != 0.0f ? 1u : 0u), 0.0f);
-        p.cellTab[cell * 2 + 1] = make_float2(sum, recip_for_div(sum));
+        p.cellTab[cell * 2 + 1] = make_float2(sum, table_recip(p, sum));
       }
     } else {
       uint32_t m = 0;
@@ -140,7 +147,7 @@ __global__ void majorant_kernel(const __grid_constant__ MajorantParams p) {
         const float2 rc = r[c];
         const float v = channel_majorant(p, c, rc.x, rc.y);
         p.majorants[cell * C + c] = v;
-        if (tab) tab[1 + c] = make_float2(v, recip_for_div(v));
+        if (tab) tab[1 + c] = make_float2(v, table_recip(p, v));
         if (v != 0.0f) m |= 1u << c;
       }
       if (tab) tab[0] = make_float2(__uint_as_float(m), 0.0f);

@@ -114,17 +114,26 @@ __device__ __forceinline__ float flight(float t, float u, float maj, float rmaj,
 //   - lg2.approx's error over the same 2^24 inputs is below 2^-20 * (1 + |log2 x|)
 //     (checked exhaustively on the GPU by the tests),
 //   - the roundings of the exact chain (quotient, product by dt) and of k add a few 2^-24,
-// and the constants take 2^-18 for both, four times those bounds and more.  The terms
-// |tf| * 2^-22 cover the roundings of tf and of the final comparison.  Since the exact
-// t' = RN(t + length) and RN is monotone, t + length >= lim implies t' >= lim.
-constexpr float kFlightRel = 3.814697265625e-06f;   // 2^-18
-constexpr float kFlightAbs = 3.814697265625e-06f;   // 2^-18 (log2 units, times k)
+// and the constants kFlightRel = kFlightAbs = 2^-18 (mdwt_internal.h) take four times
+// those bounds and more.  The term |tf| * kFlightTf (2^-22) covers the roundings of tf and
+// of the final comparison.  Since the exact t' = RN(t + length) and RN is monotone,
+// t + length >= lim implies t' >= lim.
+//   Under the fast arithmetic (TrackParams::fast) the flight is fast_flight(t, u, k) = tf
+// itself, and a true answer (tf - m >= lim with m >= 0) implies tf >= lim there too.
 constexpr float kLn2 = 0.693147182464599609375f;     // RN(ln 2)
 __device__ __forceinline__ bool flight_surely_exits(float t, float u, float k, float lim) {
   const float xf = -__log2f(1.0f - u) * k;
   const float tf = t + xf;
-  const float m = fmaf(fabsf(xf), kFlightRel, fmaf(fabsf(k), kFlightAbs, fabsf(tf) * 2.384185791015625e-07f));
+  const float m = fmaf(fabsf(xf), kFlightRel, fmaf(fabsf(k), kFlightAbs, fabsf(tf) * kFlightTf));
   return tf - m >= lim;
+}
+// The fast arithmetic's free flight (TrackParams::fast): the exit filter's estimate
+// t + xf itself, k = rmaj * dt * w2g * ln 2 with rmaj = 1 / majorant.  The reference
+// computes log(1 - u) / majorant (deviceCode.cu:564, 805, 913, 1023); this is the same
+// length from the hardware log2, within lg2.approx's error.
+__device__ __forceinline__ float fast_flight(float t, float u, float k) {
+  const float xf = -__log2f(1.0f - u) * k;
+  return t + xf;
 }
 
 __device__ __forceinline__ float quant(float a) { return rintf(a * 256.0f) * (1.0f / 256.0f); }

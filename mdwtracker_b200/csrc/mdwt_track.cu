@@ -38,6 +38,20 @@ constexpr unsigned kFull = 0xffffffffu;
 
 // Path record: bit 31 hit, bits 27..30 channel, bits 13..26 TF texel i0, bit 12 set when
 // i1 == i0 (clamped edge), bits 0..8 quantized weight * 256.  0 = miss.
+// A free flight from t with draw u (deviceCode.cu:564, 805, 913, 1023) in the arithmetic of
+// the request: the exact chain, or the fast arithmetic's length (fast_flight; rmaj = 1 / maj
+// there).  The exit filter runs unchanged under both: a flight it passes as leaving the
+// cell leaves it in either arithmetic (its margin is non-negative), and the others reach
+// this function, whose length the sample stage tests against the cell exit itself.
+__device__ __forceinline__ float any_flight(const TrackParams &P, float t, float u, float maj, float rmaj, float w2g) {
+  if (P.fast) return fast_flight(t, u, rmaj * (P.dt * w2g * kLn2));
+  return flight(t, u, maj, rmaj, P.dt, w2g);
+}
+// -m 1's per-channel flights (deviceCode.cu:676, 739): t - (log(1 - u) / maj) * dt * w2g.
+__device__ __forceinline__ float mode1_flight(const TrackParams &P, float t, float u, float maj, float w2g) {
+  if (P.fast) return fast_flight(t, u, (P.dt * w2g * kLn2) / maj);
+  return fmaf(-((mlog(1.0f - u) / maj) * P.dt), w2g, t);
+}
 __device__ __forceinline__ uint32_t make_record(int ch, const Axis &a) {
   const uint32_t k = (uint32_t)(a.a * 256.0f);
   return 0x80000000u | ((uint32_t)ch << 27) | ((uint32_t)a.i0 << 13) | ((a.i1 == a.i0) ? (1u << 12) : 0u) | k;
@@ -495,7 +509,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
               }
               if (sum <= 0.0000001f) { act = A_ADVANCE; continue; }
               for (int i = 0; i < C; i++)
-                ts[i] = majs[i] > 0.0f ? fmaf(-((mlog(1.0f - rng_next(rng)) / majs[i]) * P.dt), w2g, ts[i]) : 1e20f;
+                ts[i] = majs[i] > 0.0f ? mode1_flight(P, ts[i], rng_next(rng), majs[i], w2g) : 1e20f;
               stepping = true;
               break;
             }
@@ -555,7 +569,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
 
     // ---------------- phase 2: the pending flights and density samples, together
     if (MODE != 1 && st == S_SAMPLE) {   // the exact flight and its tests (deviceCode.cu:805-821, 915-931)
-      t = flight(t, pendU, maj, rmaj, P.dt, w2g);
+      t = any_flight(P, t, pendU, maj, rmaj, w2g);
       if (t >= (MODE == 2 ? lim : ct1)) {   // leaves the cell after all
         if (MODE == 2) { ch++; act = A_CHAN; } else act = A_ADVANCE;
         st = S_TRANS;
@@ -650,7 +664,7 @@ __device__ __forceinline__ void trace_items(const TrackParams &P, const ChanSm *
           totRej++;
         }
         if constexpr (MODE == 1) {
-          if (st == S_STEP) ts[ch] = fmaf(-((mlog(1.0f - rnd) / majs[ch]) * P.dt), w2g, ts[ch]);
+          if (st == S_STEP) ts[ch] = mode1_flight(P, ts[ch], rnd, majs[ch], w2g);
         }
       }
     }
@@ -933,7 +947,7 @@ __device__ __forceinline__ void sample(const TrackParams &P, Slots &S, const Cha
   const int ch = (int)((m0 >> 4) & 15u);
   const float lim = S.lim[s];
   uint32_t rng = S.rng[s];
-  const float t = flight(S.t[s], last_draw(rng), S.maj[s], S.rmaj[s], P.dt, S.w2g[s]);
+  const float t = any_flight(P, S.t[s], last_draw(rng), S.maj[s], S.rmaj[s], S.w2g[s]);
   S.t[s] = t;
   float exitAt = lim;
   const bool n0 = ndda<MODE>(P);

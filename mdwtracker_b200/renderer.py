@@ -227,6 +227,18 @@ class Renderer:
         thread block, the reference's threadIdx under such a launch (deviceCode.cu:297)."""
         self._call("set_seed_block", C.c_int(edge))
 
+    def setArithmetic(self, fast: bool):
+        """Free-flight arithmetic: exact (the default, bit-identical to the CPU oracle) or
+        fast (hardware log2 flight lengths; per-pixel events match the oracle on at least
+        99.9 % of pixels).  After Init the majorant table is rebuilt."""
+        self._call("set_arithmetic", C.c_int(int(fast)))
+
+    def arithmetic(self) -> int:
+        """0 = exact, 1 = fast."""
+        v = C.c_int()
+        self._call("get_arithmetic", C.byref(v))
+        return v.value
+
     # ---------------------------------------------------------------- frames
     def Render(self, stream: Optional[int] = None):
         """Renderer::Render (renderer.cpp:944-973); asynchronous on ``stream``."""

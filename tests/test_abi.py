@@ -132,3 +132,17 @@ def test_tuning_knobs_read_back():
         r.setTuning(5, 9)
     with pytest.raises(MdwtError):
         r.getTuning(9)
+
+
+def test_arithmetic_is_exact_until_set():
+    r = Renderer(MDWT_HOST_ONLY)
+    assert r.arithmetic() == 0
+    r.setArithmetic(True)
+    assert r.arithmetic() == 1
+    r.setArithmetic(False)
+    assert r.arithmetic() == 0
+    for bad in (-1, 2):
+        with pytest.raises(MdwtError) as e:
+            r.setArithmetic(bad)
+        assert e.value.status == 1
+    assert r.arithmetic() == 0
