@@ -771,6 +771,17 @@ __device__ __forceinline__ int enter(const TrackParams &P, const DDA &d, uint32_
   cmask = cell_mask(P, cellID);
   return cellID;
 }
+// The index of the DDA cell's first majorant entry in the cell table (its mask entry + 1);
+// regroup_fits keeps every table index below 2^32.
+__device__ __forceinline__ uint32_t cell_tab(const TrackParams &P, const DDA &d) {
+  return ((uint32_t)d.cx + (uint32_t)d.cy * P.mc[0] + (uint32_t)d.cz * P.mc[0] * P.mc[1]) * (uint32_t)P.tabStride + 1u;
+}
+// enter with the table index: the cell's channel mask, and its first majorant entry
+__device__ __forceinline__ uint32_t enter_tab(const TrackParams &P, const DDA &d, uint32_t &cmask) {
+  const uint32_t tab = cell_tab(P, d);
+  cmask = __float_as_uint(__ldg(reinterpret_cast<const float *>(P.cellTab + (tab - 1u))));
+  return tab;
+}
 // End of a path: its record and, for features and gradient shading, the world distance
 // of its hit (0 for a miss); `lim` holds the grid distance of the recorded hit.
 __device__ __forceinline__ void finish(const TrackParams &P, Slots &S, unsigned s, uint32_t record, bool capped,
@@ -842,7 +853,12 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
   bool drawing = (m0 & kDraw) != 0u, advance = (m0 & kAdvance) != 0u, newdda = (m0 & kNewDda) != 0u;
   int ch = (int)((m0 >> 4) & 15u);
   uint32_t cmask = (m0 >> 9) & 0xfffu, visits = m0 >> 21;
-  uint32_t record = S.record[s], steps = S.steps[s], rng = S.rng[s];
+  uint32_t record = S.record[s], rng = S.rng[s];
+  // the path's draws so far: a draw that would make them kMaxStepsPerSample ends it as
+  // capped, so this walk has kLeft draws before that one; it stops after kStop
+  const uint32_t steps0 = S.steps[s];
+  const uint32_t kLeft = kMaxStepsPerSample - 1u - steps0;
+  const uint32_t kStop = min((uint32_t)P.trips, kLeft);
   float maj = S.maj[s], rmaj = S.rmaj[s], t = S.t[s], lim = S.lim[s];
   const float w2g = S.w2g[s];
   const float kd = P.dt * w2g * kLn2;   // the exit filter's scale, times the majorant's reciprocal
@@ -850,9 +866,11 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
   DDA d;
   load_dda(S, s, d);
   d.visits = visits;
+  uint32_t tab = cell_tab(P, d);   // the current cell's first majorant entry
   bool moved = false;
   uint32_t stage = WALK;
-  for (int k = 0;;) {
+  uint32_t k = 0;   // draws of this walk
+  for (;;) {
     if (!drawing) {
       bool ended = false;
       while (true) {
@@ -862,7 +880,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
             float gx, gy, gz, a, b;
             grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
             if (!dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) { ch++; continue; }
-            enter(P, d, cmask);
+            tab = enter_tab(P, d, cmask);
             d.visits = 1u;
             tot[2]++;
             moved = true;
@@ -872,14 +890,13 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
           } else if (advance) {
             advance = false;
             if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; newdda = true; continue; }
-            enter(P, d, cmask);
+            tab = enter_tab(P, d, cmask);
             d.visits++;
             tot[2]++;
             moved = true;
           }
           if ((cmask >> ch) & 1u) {   // zero-majorant cells are skipped (deviceCode.cu:893-894)
-            const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-            const float2 mr = cell_maj(P, cellID, ch);
+            const float2 mr = __ldg(P.cellTab + (tab + (uint32_t)ch));
             maj = mr.x;
             rmaj = mr.y;
             t = d.rt0 + d.ncb;   // the cell's entry distance
@@ -889,7 +906,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
         } else {
           if (advance) {
             if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ended = true; break; }
-            enter(P, d, cmask);
+            tab = enter_tab(P, d, cmask);
             d.visits++;
             tot[2]++;
             moved = true;
@@ -897,15 +914,14 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
             ch = 0;
             advance = false;
           }
-          const uint32_t rem = ch < 16 ? (cmask >> ch) : 0u;
+          const uint32_t rem = cmask >> ch;   // ch <= C <= 12
           if (rem == 0u) {   // end of the cell: a hit ends the traversal (deviceCode.cu:851-854)
             if (record) { ended = true; break; }
             advance = true;
             continue;
           }
           ch += __ffs(rem) - 1;
-          const int cellID = d.cx + d.cy * (int)P.mc[0] + d.cz * (int)P.mc[0] * (int)P.mc[1];
-          const float2 mr = cell_maj(P, cellID, ch);
+          const float2 mr = __ldg(P.cellTab + (tab + (uint32_t)ch));
           maj = mr.x;
           rmaj = mr.y;
           t = d.rt0 + d.ncb;   // the cell's entry distance
@@ -919,21 +935,22 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
     // the cell needs no exact length: the next channel or cell starts again from its
     // entry distance.  The others -- the few that end inside the cell -- go to the sample
     // stage, which computes the exact flight, its tests and the density sample together.
-    if (++steps >= kMaxStepsPerSample) { finish(P, S, s, record, true, lim, tot); return; }
+    if (k >= kLeft) { finish(P, S, s, record, true, lim, tot); return; }
     const float u = rng_next(rng);
     const float exitAt = ndda<MODE>(P) ? cell_exit(d) : lim;
     if (!flight_surely_exits(t, u, rmaj * kd, exitAt)) {
       stage = SAMPLE;   // the state left at this draw (S.rng) gives it back to the sample stage
+      k++;
       break;
     }
     if (ndda<MODE>(P)) advance = true;
     else ch++;
     drawing = false;
-    if (++k >= P.trips) break;
+    if (++k >= kStop) break;
   }
   S.meta[s] = pack_meta(stage, (drawing ? kDraw : 0u) | (advance ? kAdvance : 0u) | (newdda ? kNewDda : 0u), ch,
                         cmask, d.visits);
-  S.steps[s] = steps; S.rng[s] = rng; S.maj[s] = maj; S.rmaj[s] = rmaj; S.t[s] = t; S.lim[s] = lim;
+  S.steps[s] = steps0 + k; S.rng[s] = rng; S.maj[s] = maj; S.rmaj[s] = rmaj; S.t[s] = t; S.lim[s] = lim;
   if (moved) store_dda(S, s, d);
 }
 
@@ -1660,7 +1677,8 @@ int launch_track_batch_fused(const TrackParams *reqs, int nReq, unsigned *dispen
 bool regroup_fits(const TrackParams &p) {
   const size_t nrect = (size_t)(p.cullX1 - p.cullX0 + 1) * (size_t)(p.cullY1 - p.cullY0 + 1);
   return (p.mode == 2 || p.mode == 0) && p.regroup && p.mc[0] <= 1024u && p.mc[1] <= 1024u && p.mc[2] <= 1024u &&
-         p.mc[0] + p.mc[1] + p.mc[2] + 3u <= 2047u && nrect * (size_t)p.sCount < ((size_t)1 << 32);
+         p.mc[0] + p.mc[1] + p.mc[2] + 3u <= 2047u && nrect * (size_t)p.sCount < ((size_t)1 << 32) &&
+         (size_t)p.mc[0] * p.mc[1] * p.mc[2] * (size_t)p.tabStride < ((size_t)1 << 32);
 }
 
 int batch_trace_occupancy(int mode, int storeKind, bool stats, bool ext) {
