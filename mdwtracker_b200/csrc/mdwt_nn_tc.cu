@@ -112,6 +112,14 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
+// load 16 columns of this warp's 32 TMEM lanes (complete after tcgen05.wait::ld)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
 // store 16 zero columns of this warp's 32 TMEM lanes
 __device__ __forceinline__ void tmem_zero16(uint32_t taddr) {
   const uint32_t z = 0;
@@ -198,6 +206,8 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
   __shared__ __align__(8) uint64_t wRes, accFull[2], accEmpty[2], mmaDone;
   __shared__ uint32_t tmemBase;
   __shared__ volatile int abortFlag;
+  __shared__ float sBias[256];   // the epilogue's bias (Cout <= 256), loaded once
+  const bool hasBias = a.bias != nullptr;
   uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int R = a.R, Cout = a.Cout, G = a.KC / 8, chunks = a.Cin / a.KC, Gtot = a.Cin / 8;
@@ -226,6 +236,8 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     abortFlag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
+  if (hasBias)   // weights and biases are not written by the kernel this one may overlap
+    for (int i = threadIdx.x; i < a.Cout; i += blockDim.x) sBias[i] = a.bias[i];
   if (warp == kWarpW) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmemBase)),
                  "r"(a.tmemCols));
@@ -430,25 +442,22 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
           const bool validP = validX && y < a.H;
           for (int c0 = 0; c0 < Cout; c0 += 16) {
             float v[2][16];
+            uint32_t vb[2][16];   // the pair's two rows, loaded together
+#pragma unroll
+            for (int h2 = 0; h2 < 2; h2++) tmem_ld16(tBase + (uint32_t)((R - 1 - (2 * pr + h2)) * Cout + c0), vb[h2]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int h2 = 0; h2 < 2; h2++)   // ready for the next tile
+              tmem_zero16(tBase + (uint32_t)((R - 1 - (2 * pr + h2)) * Cout + c0));
 #pragma unroll
             for (int h2 = 0; h2 < 2; h2++) {
-              const uint32_t col = tBase + (uint32_t)((R - 1 - (2 * pr + h2)) * Cout + c0);
-              uint32_t v32[16];
-              asm volatile(
-                  "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                  "[%16];\n"
-                  : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
-                    "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]),
-                    "=r"(v32[13]), "=r"(v32[14]), "=r"(v32[15])
-                  : "r"(col));
-              asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-              tmem_zero16(col);   // ready for the next tile
+              const uint32_t *v32 = vb[h2];
               uint4 w[2];
               uint32_t *wp = reinterpret_cast<uint32_t *>(w);
 #pragma unroll
               for (int j = 0; j < 8; j++) {
                 float f0 = __uint_as_float(v32[2 * j]), f1 = __uint_as_float(v32[2 * j + 1]);
-                if (a.bias) { f0 += a.bias[c0 + 2 * j]; f1 += a.bias[c0 + 2 * j + 1]; }
+                if (hasBias) { f0 += sBias[c0 + 2 * j]; f1 += sBias[c0 + 2 * j + 1]; }
                 if (a.relu) { f0 = fmaxf(f0, 0.f); f1 = fmaxf(f1, 0.f); }
                 __nv_bfloat162 b2 = __floats2bfloat162_rn(f0, f1);
                 wp[j] = *reinterpret_cast<uint32_t *>(&b2);
@@ -491,16 +500,21 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
         const int y = ty * R + r;
         const bool valid = validX && y < a.H;
         const size_t pix = (((size_t)n * a.H + (y < a.H ? y : 0)) * a.W + (validX ? px : 0));
-        for (int c0 = 0; c0 < Cout; c0 += 16) {
-          uint32_t v32[16];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-              : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
-                "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]),
-                "=r"(v32[14]), "=r"(v32[15])
-              : "r"(tBase + (uint32_t)((R - 1 - r) * Cout + c0)));
-          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-          tmem_zero16(tBase + (uint32_t)((R - 1 - r) * Cout + c0));   // ready for the next tile
+        // up to 64 columns per tensor-memory wait: the loads of a batch are in flight together
+        for (int cb = 0; cb < Cout; cb += 64) {
+        uint32_t vb[4][16];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (cb + 16 * q < Cout) tmem_ld16(tBase + (uint32_t)((R - 1 - r) * Cout + cb + 16 * q), vb[q]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (cb + 16 * q < Cout) tmem_zero16(tBase + (uint32_t)((R - 1 - r) * Cout + cb + 16 * q));   // for the next tile
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c0 = cb + 16 * q;
+          if (c0 >= Cout) break;
+          const uint32_t *v32 = vb[q];
           if (a.resOut) {   // fused residual output: channels 0..2 of the real image only
             if (c0 == 0 && y < a.resH && px < a.resW) {
               const size_t q = ((size_t)n * a.resH + y) * a.resW + px;
@@ -508,7 +522,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 #pragma unroll
               for (int j = 0; j < 3; j++) {
                 float f = __uint_as_float(v32[j]);
-                if (a.bias) f += a.bias[j];
+                if (hasBias) f += sBias[j];
                 if (a.relu) f = fmaxf(f, 0.f);
                 o[j] = a.resF[q * 16 + j] + f;
               }
@@ -521,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 #pragma unroll
           for (int j = 0; j < 16; j++) {
             float f = __uint_as_float(v32[j]);
-            if (a.bias) f += a.bias[c0 + j];
+            if (hasBias) f += sBias[c0 + j];
             if (a.relu) f = fmaxf(f, 0.f);
             v[j] = f;
           }
@@ -541,6 +555,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
             o[0] = w[0];
             o[1] = w[1];
           }
+        }
         }
       }
       asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
