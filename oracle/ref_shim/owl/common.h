@@ -7,11 +7,13 @@
 namespace owl {
 namespace common {
 
+// the reference names the bounds both lo / hi (deviceCode.cu) and lower / upper (renderer.cu)
 template <typename T>
 struct interval {
-  T lo{}, hi{};
-  interval() = default;
-  interval(T a, T b) : lo(a), hi(b) {}
+  union { T lo; T lower; };
+  union { T hi; T upper; };
+  SHIM_HD interval() : lo(), hi() {}
+  SHIM_HD interval(T a, T b) : lo(a), hi(b) {}
 };
 
 }  // namespace common

@@ -15,10 +15,10 @@ static const OneTy one = OneTy();
 struct linear3f {
   vec3f vx, vy, vz;
   linear3f() = default;
-  linear3f(OneTy) : vx(1.f, 0.f, 0.f), vy(0.f, 1.f, 0.f), vz(0.f, 0.f, 1.f) {}
-  linear3f(const vec3f &a, const vec3f &b, const vec3f &c) : vx(a), vy(b), vz(c) {}
-  static linear3f rotate(const vec3f &axis, float radians);
-  float det() const { return dot(vx, cross(vy, vz)); }
+  SHIM_HD linear3f(OneTy) : vx(1.f, 0.f, 0.f), vy(0.f, 1.f, 0.f), vz(0.f, 0.f, 1.f) {}
+  SHIM_HD linear3f(const vec3f &a, const vec3f &b, const vec3f &c) : vx(a), vy(b), vz(c) {}
+  SHIM_HD static linear3f rotate(const vec3f &axis, float radians);
+  SHIM_HD float det() const { return dot(vx, cross(vy, vz)); }
 };
 typedef linear3f LinearSpace3f;
 linear3f operator*(const linear3f &a, const linear3f &b);

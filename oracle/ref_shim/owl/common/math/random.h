@@ -16,8 +16,8 @@ template <int N>
 struct LCG {
   uint32_t state = 0;
   LCG() = default;
-  LCG(uint32_t v0, uint32_t v1) { init(v0, v1); }
-  void init(uint32_t v0, uint32_t v1) {
+  SHIM_HD LCG(uint32_t v0, uint32_t v1) { init(v0, v1); }
+  SHIM_HD void init(uint32_t v0, uint32_t v1) {
     const uint32_t k0 = 0x6a09e667u, k1 = 0xbb67ae85u, k2 = 0x3c6ef372u, k3 = 0xa54ff53au;
     uint32_t sum = 0;
     for (int n = 0; n < N; n++) {
@@ -27,7 +27,7 @@ struct LCG {
     }
     state = v0;
   }
-  float operator()() {
+  SHIM_HD float operator()() {
     state = 1664525u * state + 1013904223u;
     return (float)(state >> 8) * (1.0f / 16777216.0f);
   }
