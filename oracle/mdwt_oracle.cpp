@@ -1579,6 +1579,32 @@ int orc_dda_trace(const float org[3], const float dir[3], float tMax, const uint
 
 // Test hooks: the primitives of the arithmetic specification.
 float orc_log(float x) { return mlog(x); }
+// The project's statement of the texture unit's linear filter, exposed for the tests that
+// hold it against the hardware: tex3D<float> on an X x Y x Z float volume (x fastest) and
+// tex2D<float4> on an N x 1 float4 array, at n normalized coordinates each.
+int orc_sample_tex3d(const float *vol, const int dims[3], const float *xyz, int n, float *out) {
+  const int X = dims[0], Y = dims[1], Z = dims[2];
+  auto at = [&](int x, int y, int z) { return vol[((size_t)z * Y + y) * X + x]; };
+  for (int i = 0; i < n; i++) {
+    const Axis ax = axis(xyz[3 * i], X), ay = axis(xyz[3 * i + 1], Y), az = axis(xyz[3 * i + 2], Z);
+    const float c00 = lerpf(ax.a, at(ax.i0, ay.i0, az.i0), at(ax.i1, ay.i0, az.i0));
+    const float c10 = lerpf(ax.a, at(ax.i0, ay.i1, az.i0), at(ax.i1, ay.i1, az.i0));
+    const float c01 = lerpf(ax.a, at(ax.i0, ay.i0, az.i1), at(ax.i1, ay.i0, az.i1));
+    const float c11 = lerpf(ax.a, at(ax.i0, ay.i1, az.i1), at(ax.i1, ay.i1, az.i1));
+    out[i] = lerpf(az.a, lerpf(ay.a, c00, c10), lerpf(ay.a, c01, c11));
+  }
+  return ORC_OK;
+}
+int orc_sample_tex2d(const float *rgba, int N, const float *uv, int n, float *out) {
+  for (int i = 0; i < n; i++) {
+    const Axis ax = axis(uv[2 * i], N), ay = axis(uv[2 * i + 1], 1);
+    for (int k = 0; k < 4; k++) {
+      const float r = lerpf(ax.a, rgba[4 * ax.i0 + k], rgba[4 * ax.i1 + k]);
+      out[4 * i + k] = lerpf(ay.a, r, r);
+    }
+  }
+  return ORC_OK;
+}
 // The trackers' quotient from a stored reciprocal (Markstein 1990: q = RN(a y), then
 // RN(q + y (a - q b)) with y = RN(1/b); the IEEE division outside the safe range), restated
 // on the host, against the IEEE quotient: the number of mismatches over `n` seeded pairs

@@ -1,7 +1,7 @@
 // TEST INFRASTRUCTURE ONLY.  The reference's own majorant pass and range raster, run on
 // the GPU.  The reference's renderer.cu is included unchanged, where it lies, with the
 // OWL/umesh stand-ins of ref_shim/ (made host-and-device for nvcc), and compiled by
-// oracle/Makefile (`make ref-gpu`) with nvcc's default flags, as the reference's CMake
+// oracle/Makefile (`make ref`) with nvcc's default flags, as the reference's CMake
 // build compiles it (FMA contraction on).  The entry points below set up the inputs the
 // reference's Renderer would hand its kernels and launch them with its launch shapes:
 //   refgpu_majorants: RecalculateDensityRanges (renderer.cu:206-274) -- the per-channel
@@ -135,5 +135,107 @@ extern "C" int refgpu_ranges(const float *scalars, const int *dims, int C, const
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, dMc, sizeof(float2) * M * C, cudaMemcpyDeviceToHost);
   cudaFree(dMc);
+  return status(e);
+}
+
+// ---------------------------------------------------------------- the texture unit
+// The reference samples its volumes with tex3D<float> on float 3-D arrays (normalized
+// coordinates, linear filtering, clamp addressing, element-type reads; renderer.cpp:
+// 251-311) and its transfer functions with tex2D<float4> on a float4 N x 1 array
+// (renderer.cpp:1094-1165).  These entry points sample such textures at given
+// coordinates on the GPU, so that the tests can hold the project's statement of the
+// linear filter (8 fractional weight bits, clamp, lerp(a, p, q) = fmaf(a, q, (1 - a) p),
+// x then y then z) against the hardware.
+namespace {
+__global__ void tex3d_probe(cudaTextureObject_t t, const float *xyz, int n, float *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = tex3D<float>(t, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+}
+__global__ void tex2d_probe(cudaTextureObject_t t, const float *uv, int n, float4 *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = tex2D<float4>(t, uv[2 * i], uv[2 * i + 1]);
+}
+}  // namespace
+
+// vol: X * Y * Z floats, x fastest; xyz: n normalized coordinates
+extern "C" int refgpu_tex3d(const float *vol, int X, int Y, int Z, const float *xyz, int n, float *out) {
+  cudaArray_t arr = nullptr;
+  cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+  cudaError_t e = cudaMalloc3DArray(&arr, &cd, make_cudaExtent(X, Y, Z));
+  if (e == cudaSuccess) {
+    cudaMemcpy3DParms p = {};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(vol), (size_t)X * sizeof(float), X, Y);
+    p.dstArray = arr;
+    p.extent = make_cudaExtent(X, Y, Z);
+    p.kind = cudaMemcpyHostToDevice;
+    e = cudaMemcpy3D(&p);
+  }
+  cudaTextureObject_t t = 0;
+  if (e == cudaSuccess) {
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.normalizedCoords = true;
+    td.filterMode = cudaFilterModeLinear;
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.addressMode[2] = cudaAddressModeClamp;
+    td.readMode = cudaReadModeElementType;
+    e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
+  }
+  float *dIn = nullptr, *dOut = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&dIn, sizeof(float) * 3 * (size_t)n);
+  if (e == cudaSuccess) e = cudaMemcpy(dIn, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&dOut, sizeof(float) * (size_t)n);
+  if (e == cudaSuccess) {
+    tex3d_probe<<<(n + 255) / 256, 256>>>(t, dIn, n, dOut);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dOut, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost);
+  if (t) cudaDestroyTextureObject(t);
+  if (arr) cudaFreeArray(arr);
+  cudaFree(dIn);
+  cudaFree(dOut);
+  return status(e);
+}
+
+// rgba: N texels (as uploaded: alpha already cubed); uv: n coordinates; out: n float4
+extern "C" int refgpu_tex2d(const float *rgba, int N, const float *uv, int n, float *out) {
+  cudaArray_t arr = nullptr;
+  cudaChannelFormatDesc cd = cudaCreateChannelDesc<float4>();
+  cudaError_t e = cudaMallocArray(&arr, &cd, N, 1);
+  const size_t pitch = (size_t)N * sizeof(float4);
+  if (e == cudaSuccess) e = cudaMemcpy2DToArray(arr, 0, 0, rgba, pitch, pitch, 1, cudaMemcpyHostToDevice);
+  cudaTextureObject_t t = 0;
+  if (e == cudaSuccess) {
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.normalizedCoords = 1;
+    td.maxAnisotropy = 1;
+    td.maxMipmapLevelClamp = 99;
+    td.mipmapFilterMode = cudaFilterModePoint;
+    e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
+  }
+  float *dIn = nullptr;
+  float4 *dOut = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&dIn, sizeof(float) * 2 * (size_t)n);
+  if (e == cudaSuccess) e = cudaMemcpy(dIn, uv, sizeof(float) * 2 * (size_t)n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&dOut, sizeof(float4) * (size_t)n);
+  if (e == cudaSuccess) {
+    tex2d_probe<<<(n + 255) / 256, 256>>>(t, dIn, n, dOut);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dOut, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost);
+  if (t) cudaDestroyTextureObject(t);
+  if (arr) cudaFreeArray(arr);
+  cudaFree(dIn);
+  cudaFree(dOut);
   return status(e);
 }
