@@ -715,7 +715,9 @@ __global__ void __launch_bounds__(kTPB, kMinBlocks) trace_kernel(const __grid_co
 // per traversal.
 //   -m 2: one traversal; `lim` is min(the cell's exit, the closest hit so far).
 //   -m 0: one traversal per channel (deviceCode.cu:965-969); `lim` is the closest hit so
-//   far (1e20 before the first), the cell's exit comes from the walk's DDA state.
+//   far (1e20 before the first), the cell's exit comes from the walk's DDA state.  A
+//   channel's traversal is set up by a fourth operation, restart, which the stage count
+//   treats as a stage of its own.
 namespace rg {
 constexpr int kTPB = 256;
 constexpr int kSPT = 2;                  // path slots per thread
@@ -724,8 +726,9 @@ constexpr int kMinBlocks = 4;            // 64 registers, 32 warps per SM
 enum : uint32_t { NEED = 0, WALK = 1, SAMPLE = 2, DONE = 3 };
 // meta word: bits 0-1 stage, bit 2 a channel is selected (free flights pending), bit 3
 // the cell's channels are exhausted (advance the walk), bits 4-7 channel, bit 8 (-m 0)
-// start the next channel's traversal, bits 9-20 the cell's non-zero-majorant channels,
-// bits 21-31 cells entered by the current traversal
+// start the next channel's traversal (a WALK slot with it set waits for the restart
+// operation), bits 9-20 the cell's non-zero-majorant channels, bits 21-31 cells entered
+// by the current traversal
 constexpr uint32_t kDraw = 4u, kAdvance = 8u, kNewDda = 256u;
 struct Slots {
   uint32_t meta[kSlots], recIdx[kSlots], rng[kSlots], steps[kSlots], record[kSlots], cell[kSlots];
@@ -872,21 +875,12 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
   uint32_t k = 0;   // draws of this walk
   for (;;) {
     if (!drawing) {
-      bool ended = false;
+      bool ended = false, restartNext = false;
       while (true) {
         if (ndda<MODE>(P)) {
-          if (newdda) {   // the next channel's traversal (deviceCode.cu:965-969)
-            if (ch >= P.C) { ended = true; break; }
-            float gx, gy, gz, a, b;
-            grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
-            if (!dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) { ch++; continue; }
-            tab = enter_tab(P, d, cmask);
-            d.visits = 1u;
-            tot[2]++;
-            moved = true;
-            newdda = false;
-            S.rt0[s] = d.rt0;   // the same for every channel's traversal of the ray
-            S.tsx[s] = d.tsx; S.tsy[s] = d.tsy; S.tsz[s] = d.tsz;
+          if (newdda) {   // the next channel's traversal: an operation of its own (restart)
+            restartNext = true;
+            break;
           } else if (advance) {
             advance = false;
             if (!dda_advance(P, d, wdx, wdy, wdz, maxCells)) { ch++; newdda = true; continue; }
@@ -929,6 +923,7 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
         }
       }
       if (ended) { finish(P, S, s, record, false, lim, tot); return; }
+      if (restartNext) break;
       drawing = true;
     }
     // free-flight draw (deviceCode.cu:800-820, 908-930).  A flight that certainly leaves
@@ -952,6 +947,32 @@ __device__ __forceinline__ void walk(const TrackParams &P, Slots &S, unsigned s,
                         cmask, d.visits);
   S.steps[s] = steps0 + k; S.rng[s] = rng; S.maj[s] = maj; S.rmaj[s] = rmaj; S.t[s] = t; S.lim[s] = lim;
   if (moved) store_dda(S, s, d);
+}
+
+// -m 0: the next channel's traversal (deviceCode.cu:965-969) as an operation of its own,
+// run together by the lanes that need one, so that no walk sets a traversal up while its
+// other lanes draw.  Every channel's traversal starts from the same grid origin and
+// direction, so when the ray misses the grid for one channel it misses it for all and the
+// path ends.
+template <int MODE>
+__device__ __forceinline__ void restart(const TrackParams &P, Slots &S, unsigned s, uint32_t (&tot)[5]) {
+  const uint32_t m0 = S.meta[s];
+  int ch = (int)((m0 >> 4) & 15u);
+  const float wdx = S.wdx[s], wdy = S.wdy[s], wdz = S.wdz[s];
+  DDA d;
+  for (;; ch++) {
+    if (ch >= P.C) { finish(P, S, s, S.record[s], false, S.lim[s], tot); return; }
+    float gx, gy, gz, a, b;
+    grid_dir(P, wdx, wdy, wdz, gx, gy, gz, a, b);
+    if (dda_init(P, P.gOrg.x, P.gOrg.y, P.gOrg.z, gx, gy, gz, d)) break;
+  }
+  uint32_t cmask;
+  enter_tab(P, d, cmask);
+  tot[2]++;
+  store_dda(S, s, d);
+  S.rt0[s] = d.rt0;   // the same for every channel's traversal of the ray
+  S.tsx[s] = d.tsx; S.tsy[s] = d.tsy; S.tsz[s] = d.tsz;
+  S.meta[s] = pack_meta(WALK, 0u, ch, cmask, 1u);
 }
 
 // The pending flight of slot s, then its density sample (phase 2 of trace_items, -m 2
@@ -1030,21 +1051,28 @@ __device__ __forceinline__ void run_warp(const TrackParams &P, Slots &S, uint16_
   while (true) {
     // the warp's slots by stage (two stage bits per slot); the most populated stage runs,
     // lane i on the i-th slot of that stage in slot order
-    unsigned ms[kSPT][3];
-    int n[3] = {0, 0, 0};
+    // (-m 0: walks waiting for their next channel's traversal form a fourth group, kRestart)
+    constexpr int kRestart = 3;
+    constexpr bool maybeRestart = MODE != 2;   // syncDDA never restarts a traversal
+    const bool n0 = maybeRestart && ndda<MODE>(P);
+    unsigned ms[kSPT][4];
+    int n[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int g = 0; g < kSPT; g++) {
       const uint32_t st = S.meta[wbase + 32u * g + lane];
       const unsigned b0 = __ballot_sync(kFull, st & 1u), b1 = __ballot_sync(kFull, st & 2u);
+      const unsigned bR = n0 ? __ballot_sync(kFull, st & kNewDda) : 0u;
       ms[g][NEED] = ~b0 & ~b1;
-      ms[g][WALK] = b0 & ~b1;
+      ms[g][WALK] = b0 & ~b1 & ~bR;
       ms[g][SAMPLE] = ~b0 & b1;
+      ms[g][kRestart] = b0 & ~b1 & bR;
 #pragma unroll
-      for (int X = 0; X < 3; X++) n[X] += __popc(ms[g][X]);
+      for (int X = 0; X < 4; X++) n[X] += __popc(ms[g][X]);
     }
-    if (n[0] + n[1] + n[2] == 0) break;   // every slot is out of work items
+    if (n[0] + n[1] + n[2] + (maybeRestart ? n[3] : 0) == 0) break;   // every slot is out of work items
     int X = SAMPLE, nX = n[SAMPLE];
     if (n[WALK] > nX) { X = WALK; nX = n[WALK]; }
+    if (maybeRestart && n[kRestart] > nX) { X = kRestart; nX = n[kRestart]; }
     if (n[NEED] > nX) { X = NEED; nX = n[NEED]; }
     const int nx = nX < 32 ? nX : 32;
     const bool mine = (int)lane < nx;
@@ -1053,7 +1081,8 @@ __device__ __forceinline__ void run_warp(const TrackParams &P, Slots &S, uint16_
     int below = 0;
 #pragma unroll
     for (int g = 0; g < kSPT; g++) {
-      const unsigned m = X == SAMPLE ? ms[g][SAMPLE] : (X == WALK ? ms[g][WALK] : ms[g][NEED]);
+      const unsigned m = X == SAMPLE ? ms[g][SAMPLE]
+                         : (X == WALK ? ms[g][WALK] : ((maybeRestart && X == kRestart) ? ms[g][kRestart] : ms[g][NEED]));
       const int r = below + __popc(m & lt);
       if (((m >> lane) & 1u) && r < 32) sel[r] = (uint16_t)(wbase + 32u * g + lane);
       below += __popc(m);
@@ -1064,6 +1093,8 @@ __device__ __forceinline__ void run_warp(const TrackParams &P, Slots &S, uint16_
       if (mine) sample<MODE, SK>(P, S, sch, s, tot);
     } else if (X == WALK) {
       if (mine) walk<MODE>(P, S, s, maxCells, tot);
+    } else if (maybeRestart && X == kRestart) {
+      if (mine) restart<MODE>(P, S, s, tot);
     } else {
       unsigned base = 0;
       if (lane == 0) base = atomicAdd(dispenser, (unsigned)nx);
