@@ -252,7 +252,8 @@ mdwt_status mdwt_get_pixel_stats(mdwt_ctx *ctx, uint32_t *host_out);
  * operation most of them need next (path start, walk, density sample), one path per
  * lane; a walk takes at most TRIPS free-flight draws.  0 = the warp-local tracker (32
  * paths per warp; POOL and QUORUM apply to it only).  Until set: 1 for -m 2, 0 for -m 0
- * (the warp-local tracker is the faster N-DDA tracker on the scenes measured); the
+ * (on the 1080p 6 x 512^3 float32 scene the warp-local tracker is the faster N-DDA
+ * tracker with macrocells of 16 voxels or fewer, the regrouped one with 32); the
  * schedule autotuner tries both.
  * MDWT_TUNE_RG_BLOCKS: blocks of 256 threads per SM the regrouped tracker runs (0, the
  * default: as many as its path slots' shared memory allows, 4); fewer blocks leave more of

@@ -1003,9 +1003,9 @@ static float feature_scale(const mdwt_ctx *c) {
 
 // Scene, camera, transfer functions and shading of the next frame.
 // Whether frames run the regrouped tracker (MDWT_TUNE_REGROUP): as set, or by default for
-// syncDDA only -- for N-DDA the warp-local tracker measured faster (2.20 vs 1.56 Gpath/s
-// on the 1080p 6 x 512^3 float32 scene): the per-channel traversal restarts diverge inside
-// the regrouped walks.
+// syncDDA only -- for N-DDA on the 1080p 6 x 512^3 float32 scene the warp-local tracker
+// measured faster with 16-voxel macrocells (2.22 vs 2.07 Gpath/s) and the regrouped one
+// with 32-voxel macrocells; the schedule autotuner picks per scene.
 static int regroup_on(const mdwt_ctx *c) { return c->regroup >= 0 ? c->regroup : (c->mode == 2 ? 1 : 0); }
 
 static void fill_scene(const mdwt_ctx *c, TrackParams &p) {
