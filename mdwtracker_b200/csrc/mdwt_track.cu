@@ -1419,10 +1419,22 @@ __device__ __forceinline__ uint32_t resolve_pixel(const TrackParams &P, int px, 
       f = reinterpret_cast<const float4 *>(P.partial)[q];
       if (STATS) sv = reinterpret_cast<const uint4 *>(P.partialStats)[q];
     }
-    for (int k = 0; k < P.sCount; k++) {
+    // the records of the next samples are loaded ahead (kAhead in flight per thread), so the
+    // pass streams them instead of waiting on one load per sample; the sums stay in sample
+    // order
+    constexpr int kAhead = 4;
+    const uint32_t *rec = P.records + q;
+    const int nS = P.sCount;
+    uint32_t ra[kAhead];
+#pragma unroll
+    for (int j = 0; j < kAhead; j++) ra[j] = j < nS ? __ldcs(rec + (size_t)j * nrect) : 0u;
+    for (int k = 0; k < nS; k++) {
       int s;   // this record's frame and sample
       const uint32_t fr = sample_frame(P, P.sBase + k, s);
-      const uint32_t r = P.records[(size_t)k * nrect + q];
+      const uint32_t r = ra[0];
+#pragma unroll
+      for (int j = 0; j + 1 < kAhead; j++) ra[j] = ra[j + 1];
+      ra[kAhead - 1] = k + kAhead < nS ? __ldcs(rec + (size_t)(k + kAhead) * nrect) : 0u;
       float cr = 0.f, cg = 0.f, cb = 0.f, ca = 0.f;
       if (r) {
         const int ch = (int)((r >> 27) & 15u);
