@@ -46,6 +46,13 @@ def test_defaults(monkeypatch):
     a = bench.parse_args()
     assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1 and a.config == "c3" and a.edge == 16 and a.impl == "mdwt"
     assert not a.no_autotune and a.regroup is None and a.split == "rows"
+    # the headline line runs the exact arithmetic; the fast one is an extra key
+    assert a.arith == "exact" and not a.no_fast
+
+
+def test_headline_traffic_is_the_committed_full_frame_capture():
+    t = bench.profiled_traffic("trace_regroup_kernel", "c3_syncdda_6x512f32_e16_mc32_1920x1080_256spp")
+    assert t is not None and 1e9 < t < 1e10
 
 
 def test_schedule_report_reads_the_knobs():
