@@ -1,5 +1,5 @@
 """The fast free-flight arithmetic (mdwt_set_arithmetic(ctx, MDWT_ARITH_FAST)) against
-the exact CPU oracle, judged by the per-pixel event bar: at equal spp, the per-pixel
+the exact CPU oracle, held to the per-pixel event bar: at equal spp, the per-pixel
 collision events -- density samples, rejections, hits and the hit channels over the
 frame's samples -- equal the oracle's on at least 99.9 % of the pixels, and the
 converged image stays within noise of the exact one.
